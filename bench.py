@@ -1,0 +1,415 @@
+#!/usr/bin/env python
+"""Benchmark of the dyGRASS update path on B200.
+
+Workload (default "mesh"): the plain incremental + decremental configuration
+at scale -- 3-D 7-point mesh 100x100x100 (1,000,000 vertices, 2,970,000
+edges) with FP32 log-uniform weights over [1e-2, 1e2], sparsifier =
+spanning tree + 5% off-tree edges, 200,000 insertions at hop distance
+2..10 (10 batches, threshold 100, 512 walkers, max_steps 100), then deletion
+of 10% of the dense graph's edges (317,000, 10 batches) recovered through
+walks on the updated dense graph.  Synthetic, seeded (dygrass_b200/workloads.py).
+
+One step = the whole update stream (insertions then deletions) from the
+initial graphs, which are restored (untimed) before every step together
+with an L2 flush (a 256 MB write).  value = edge updates (insertions +
+deletions) per second over all ranks; the device-resident run keeps inputs
+and outputs in HBM, e2e passes host (pinned) buffers through the C ABI.
+
+N > 1 (torchrun): every rank runs an independent replica of the workload
+(weak scaling, no data-path collective); times are the max over ranks.
+
+--impl reference: the reference has no CPU implementation of this path, so
+the reference arm times the CPU port of its update loop (oracle/, all host
+threads) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_PER_MOVE = 64   # two 32-byte sectors: row descriptor + chosen slot
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["mesh", "grid"], default="mesh")
+    ap.add_argument("--mesh-k", type=int, default=100)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--profile-only", action="store_true",
+                    help="one short device-resident step (for profilers)")
+    return ap.parse_args()
+
+
+def make_workload(args, rank):
+    import dygrass_b200.workloads as wl
+    seed = wl.MASTER_SEED + 1000 * rank
+    if args.workload == "grid":
+        return wl.grid_2d(seed=seed)
+    return wl.mesh_3d(k=args.mesh_k, seed=seed)
+
+
+def workload_config(W, args):
+    if args.workload == "grid":
+        return {"workload": "grid_2d 100x100, 1,000 insertions, threshold 10, 512 walkers, max_steps 64",
+                "vertices": W.n, "edges": int(len(W.g_src)), "insertions": int(len(W.ins_src)),
+                "deletions": 0}
+    return {"workload": f"mesh_3d {args.mesh_k}^3 incremental+decremental, threshold 100, 512 walkers, max_steps 100",
+            "vertices": W.n, "edges": int(len(W.g_src)), "sparsifier_edges": int(len(W.h_src)),
+            "insertions": int(len(W.ins_src)), "deletions": int(len(W.del_src)),
+            "batches": "10 insertion + 10 deletion (ceil(N/10) each)"}
+
+
+# --------------------------------------------------------------- clocks
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device_index}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
+                 "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1].split()[0]))
+                smax = float(parts[2].split()[0])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------- our arm
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import dygrass_b200 as dyg
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    W = make_workload(args, rank)
+    nin, ndel = len(W.ins_src), len(W.del_src)
+
+    H0 = dyg.Graph.from_edges(W.n, W.h_src, W.h_dst, W.h_w, device=local_rank)
+    G0 = dyg.Graph.from_edges(W.n, W.g_src, W.g_dst, W.g_w, device=local_rank)
+    H, G = H0.clone(), G0.clone()
+
+    def t(a, dt=None):
+        return torch.from_numpy(np.ascontiguousarray(a)).to(dev) if dt is None else \
+            torch.from_numpy(np.ascontiguousarray(a).view(dt)).to(dev)
+
+    d_is, d_id, d_iw = t(W.ins_src, np.int32), t(W.ins_dst, np.int32), t(W.ins_w)
+    d_ds, d_dd = t(W.del_src, np.int32), t(W.del_dst, np.int32)
+    rec_cap = max(ndel, 1) * (W.dparams.max_steps + 4 * W.dparams.heuristic_walkers) // 8 + 1024
+    o_inc = dyg.IncrementalResult(torch.empty(nin, dtype=torch.int32, device=dev),
+                                  torch.empty(nin, dtype=torch.float32, device=dev),
+                                  torch.empty(nin, dtype=torch.uint8, device=dev))
+    o_st = torch.empty(max(ndel, 1), dtype=torch.int32, device=dev)
+    o_cd = torch.empty(max(ndel, 1), dtype=torch.float32, device=dev)
+    o_rx = torch.empty(rec_cap, dtype=torch.int32, device=dev)
+    o_ry = torch.empty(rec_cap, dtype=torch.int32, device=dev)
+    o_rk = torch.empty(rec_cap, dtype=torch.uint8, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+
+    def reset():
+        H.copy_from(H0, sp)
+        G.copy_from(G0, sp)
+        flush.fill_(rank + 1)
+
+    def step_device():
+        dyg.incremental_stream(H, d_is, d_id, d_iw, W.params, G=G, stream=sp, out=o_inc)
+        nrec = 0
+        if ndel:
+            nrec = dyg.decremental_stream_into(G, H, d_ds, d_dd, W.dparams, o_st, o_cd, o_rx, o_ry,
+                                               o_rk, rec_cap, stream=sp)
+        return nrec
+
+    if args.profile_only:
+        reset()
+        step_device()
+        torch.cuda.synchronize()
+        return None
+
+    for _ in range(args.warmup):
+        reset()
+        step_device()
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    # ---- device-resident timed region
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    m0 = (H.counters()[0], G.counters()[0])
+    launches0 = dyg.kernel_launches()
+    dyg.profile_reset()
+    dyg.profile_enable(True)
+    times = []
+    nrec = 0
+    for _ in range(args.steps):
+        reset()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        nrec = step_device()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    dyg.profile_enable(False)
+    prof = dyg.profile_read()
+    launches = dyg.kernel_launches() - launches0
+    m1 = (H.counters()[0], G.counters()[0])
+    clk = clocks.stop()
+    barrier()
+    ms = float(np.mean(times))
+    ms_max = ms
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms_max = float(tt.item())
+    incr_moves = (m1[0] - m0[0]) / args.steps
+    decr_moves = (m1[1] - m0[1]) / args.steps
+    accepted = int(o_inc.accepted.sum().item())
+
+    # ---- end-to-end through host buffers (pinned), copies inside the region
+    e2e = None
+    if not args.no_e2e:
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+        h_is, h_id, h_iw = pin(W.ins_src), pin(W.ins_dst), pin(W.ins_w)
+        h_ds, h_dd = pin(W.del_src), pin(W.del_dst)
+        h_out = dyg.IncrementalResult(pin(np.empty(nin, np.int32)), pin(np.empty(nin, np.float32)),
+                                      pin(np.empty(nin, np.uint8)))
+        h_st, h_cd = pin(np.empty(max(ndel, 1), np.int32)), pin(np.empty(max(ndel, 1), np.float32))
+        h_rx, h_ry = pin(np.empty(rec_cap, np.uint32)), pin(np.empty(rec_cap, np.uint32))
+        h_rk = pin(np.empty(rec_cap, np.uint8))
+        barrier()
+        torch.cuda.synchronize()
+        et = []
+        nrec_h = 0
+        for _ in range(max(1, args.steps)):
+            reset()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            dyg.incremental_stream(H, h_is, h_id, h_iw, W.params, G=G, stream=sp, out=h_out)
+            if ndel:
+                nrec_h = dyg.decremental_stream_into(G, H, h_ds, h_dd, W.dparams, h_st, h_cd, h_rx,
+                                                     h_ry, h_rk, rec_cap, stream=sp)
+            e1.record(stream)
+            e1.synchronize()
+            et.append(e0.elapsed_time(e1))
+        barrier()
+        ems = float(np.mean(et))
+        if world > 1:
+            import torch.distributed as dist
+            tt = torch.tensor([ems], dtype=torch.float64, device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ems = float(tt.item())
+        assert np.array_equal(h_out.accepted, o_inc.accepted.cpu().numpy())
+        e2e = {"value": world * (nin + ndel) / (ems / 1e3), "unit": "edge_updates/s",
+               "ms_per_step": ems,
+               "h2d_bytes_per_step": int(nin * 12 + ndel * 8),
+               "d2h_bytes_per_step": int(nin * 9 + ndel * 8 + nrec_h * 9)}
+
+    walk_ms = prof["incr_walk_ms"] + prof["decr_walk_ms"]
+    walk_launches = prof["incr_walk_launches"] + prof["decr_walk_launches"]
+    moves_total = (incr_moves + decr_moves) * args.steps
+    res = {
+        "ms_per_step": ms_max, "steps_ms": times, "nin": nin, "ndel": ndel, "accepted": accepted,
+        "recovered": nrec, "incr_moves": incr_moves, "decr_moves": decr_moves,
+        "walk_ms_per_step": walk_ms / args.steps, "walk_launches": walk_launches,
+        "prof": prof, "launches_per_step": launches / args.steps, "clocks": clk, "e2e": e2e,
+        "walk_bytes_per_launch": moves_total * BYTES_PER_MOVE / max(walk_launches, 1),
+        "walk_ms_per_launch": walk_ms / max(walk_launches, 1),
+        "W": W,
+    }
+    for g in (H, G, H0, G0):
+        g.close()
+    return res
+
+
+# --------------------------------------------------------- CPU baseline
+
+def cpu_baseline(W, threads=None, max_incr=None):
+    """The oracle (CPU port of the reference update loop) on a bounded sample:
+    the full insertion stream (or its first max_incr edges), then the first
+    deletion batch; per-edge costs are extrapolated to the workload's mix."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    th = threads or pyoracle.max_threads()
+    nin, ndel = len(W.ins_src), len(W.del_src)
+    ni = nin if max_incr is None else min(nin, max_incr)
+    Ho = pyoracle.OGraph(W.n, W.h_src, W.h_dst, W.h_w)
+    Go = pyoracle.OGraph(W.n, W.g_src, W.g_dst, W.g_w) if ndel else None
+    from dygrass_b200 import reference_batch_size
+    B = reference_batch_size(nin)
+    t0 = time.perf_counter()
+    pyoracle.incremental(Ho, W.ins_src[:ni], W.ins_dst[:ni], W.ins_w[:ni], W.params,
+                         batch_size=B, G=Go, threads=th)
+    t_in = time.perf_counter() - t0
+    t_de, nd = 0.0, 0
+    if ndel:
+        Bd = reference_batch_size(ndel)
+        nd = Bd
+        t0 = time.perf_counter()
+        pyoracle.decremental(Go, Ho, W.del_src[:nd], W.del_dst[:nd], W.dparams, batch_size=Bd,
+                             threads=th)
+        t_de = time.perf_counter() - t0
+    est = t_in / ni * nin + (t_de / nd * ndel if nd else 0.0)
+    return {"value": (nin + ndel) / est, "unit": "edge_updates/s", "cores": th,
+            "kind": "port", "seconds": t_in + t_de,
+            "sample": f"oracle (C/OpenMP, {th} threads): {ni} insertions in batches of {B}"
+                      + (f" + first deletion batch ({nd} deletions) on the updated graphs" if nd else "")
+                      + "; per-edge costs extrapolated to the full stream"}
+
+
+# ---------------------------------------------------------------- main
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        W = make_workload(args, 0)
+        vals = []
+        for i in range(args.warmup + args.steps):
+            r = cpu_baseline(W)
+            if i >= args.warmup:
+                vals.append(r)
+        v = float(np.mean([r["value"] for r in vals]))
+        out = {"metric": "edge updates/sec (incr+decr)", "value": v, "unit": "edge_updates/s",
+               "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+               "ms_per_step": (len(W.ins_src) + len(W.del_src)) / v * 1e3,
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+               "data": "synthetic (seeded)", "config": workload_config(W, args),
+               "cpu_baseline": {k: vals[-1][k] for k in ("value", "unit", "cores", "kind", "sample")},
+               "e2e": {"value": v, "unit": "edge_updates/s", "h2d_bytes_per_step": 0,
+                       "d2h_bytes_per_step": 0}}
+        out["cpu_baseline"]["value"] = v
+        print(json.dumps(out))
+        return 0
+
+    import torch
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    res = run_ours(args, rank, world, local_rank)
+    if res is None:
+        return 0
+    W = res.pop("W")
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return 0
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = peaks.get("hbm_gbs")
+    peak_note = "measured" if hbm else "fallback"
+    hbm = hbm or 6650.0
+    achieved = res["walk_bytes_per_launch"] / (res["walk_ms_per_launch"] / 1e3) / 1e9
+    nin, ndel = res["nin"], res["ndel"]
+    ms = res["ms_per_step"]
+    value = world * (nin + ndel) / (ms / 1e3)
+    moves = res["incr_moves"] + res["decr_moves"]
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        cpu = cpu_baseline(W)
+    out = {
+        "metric": "edge updates/sec (incr+decr)",
+        "value": value, "unit": "edge_updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators, dygrass_b200/workloads.py)",
+        "config": dict(workload_config(W, args), l2="flushed between steps (256 MB write)",
+                       parallelism=f"replicas x{world}"),
+        "walker_steps_per_s": world * moves / (ms / 1e3),
+        "breakdown": {"insertions_added": res["accepted"], "edges_recovered": res["recovered"],
+                      "incr_walker_moves": res["incr_moves"], "decr_walker_moves": res["decr_moves"],
+                      "walk_kernel_ms_per_step": res["walk_ms_per_step"],
+                      "walk_launches_per_step": res["walk_launches"] / args.steps,
+                      "steps_ms": res["steps_ms"]},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": None,
+                     "peak_source": f"{peak_note} hbm_gbs (MEASURED_PEAKS.json)",
+                     "kernel": "k_walk (incremental + decremental launches)",
+                     "bytes_model": f"{BYTES_PER_MOVE} B per walker move (row descriptor sector + slot sector)"},
+        "clocks": res["clocks"],
+        "e2e": res["e2e"],
+        "gpu_launches": int(round(res["launches_per_step"] * args.steps)),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(out))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

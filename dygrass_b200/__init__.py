@@ -1,0 +1,331 @@
+"""dygrass_b200 -- B200 (sm_100a) implementation of the dyGRASS update path.
+
+The product is the C ABI in include/dyg.h, implemented by the in-tree
+libdygrass.so (CUDA kernels + host runtime).  This module is a thin ctypes
+mirror of that ABI for Python callers, tests and the benchmark: numpy arrays
+are passed as host pointers, torch CUDA tensors as device pointers.  There is
+no CPU fallback: if the library is missing, importing fails.
+
+The reference's interface is two executables (incremental_update,
+decremental_update); dygrass_b200/bin holds drop-ins built on this ABI.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libdygrass.so")
+
+DYG_OK = 0
+STATUS_NAMES = {0: "DYG_OK", 1: "DYG_EINVAL", 2: "DYG_ENOMEM", 3: "DYG_ECUDA", 4: "DYG_ERANGE",
+                5: "DYG_ESTATE", 6: "DYG_ENOTSUP", 7: "DYG_EIO"}
+TRANSITION_UNIFORM = 0
+TRANSITION_WEIGHTED = 1
+DEL_NOT_IN_G = -3
+DEL_NOT_IN_H = -2
+DEL_NO_PATH = -1
+REC_PATH = 0
+REC_FALLBACK = 1
+
+
+class DygError(RuntimeError):
+    def __init__(self, status: int, what: str, msg: str):
+        super().__init__(f"{what}: {STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class WalkParams(C.Structure):
+    """Mirror of dyg_walk_params (include/dyg.h)."""
+    _fields_ = [("threshold", C.c_float), ("walkers", C.c_uint32), ("max_steps", C.c_uint32),
+                ("transition", C.c_uint32), ("heuristic_walkers", C.c_uint32),
+                ("flags", C.c_uint32), ("seed", C.c_uint64)]
+
+    @classmethod
+    def make(cls, threshold=100.0, walkers=512, max_steps=100, transition=TRANSITION_UNIFORM,
+             heuristic_walkers=16, seed=20251203):
+        return cls(float(threshold), int(walkers), int(max_steps), int(transition),
+                   int(heuristic_walkers), 0, int(seed))
+
+
+class Profile(C.Structure):
+    """Mirror of dyg_profile (include/dyg.h)."""
+    _fields_ = [("incr_walk_ms", C.c_double), ("decr_walk_ms", C.c_double),
+                ("other_walk_ms", C.c_double), ("incr_walk_launches", C.c_uint64),
+                ("decr_walk_launches", C.c_uint64), ("other_walk_launches", C.c_uint64)]
+
+
+class GraphOpts(C.Structure):
+    _fields_ = [("slack_per_row", C.c_uint32), ("reserved", C.c_uint32),
+                ("arena_headroom", C.c_double), ("device", C.c_int32), ("pad", C.c_int32)]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libdygrass.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: run `python -m dygrass_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    vp, u32, u64, i32 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int32
+    sig = {
+        "dyg_version": ([], C.c_char_p),
+        "dyg_last_error_string": ([], C.c_char_p),
+        "dyg_walk_params_default": ([C.POINTER(WalkParams)], None),
+        "dyg_graph_opts_default": ([C.POINTER(GraphOpts)], None),
+        "dyg_reference_batch_size": ([u32], u32),
+        "dyg_graph_create_from_edges": ([u32, u64, vp, vp, vp, C.POINTER(GraphOpts), C.POINTER(vp)], C.c_int),
+        "dyg_graph_clone": ([vp, C.POINTER(vp)], C.c_int),
+        "dyg_graph_copy_from": ([vp, vp, vp], C.c_int),
+        "dyg_graph_destroy": ([vp], C.c_int),
+        "dyg_graph_info": ([vp, C.POINTER(u32), C.POINTER(u64), C.POINTER(u64), C.POINTER(u64)], C.c_int),
+        "dyg_graph_export": ([vp, vp, vp, vp, u64], C.c_int),
+        "dyg_graph_compact": ([vp, vp], C.c_int),
+        "dyg_graph_counters": ([vp, C.POINTER(u64), C.POINTER(u64)], C.c_int),
+        "dyg_incremental_batch": ([vp, vp, vp, vp, vp, u32, u64, C.POINTER(WalkParams), vp, vp, vp, vp], C.c_int),
+        "dyg_incremental_stream": ([vp, vp, vp, vp, vp, u32, u32, C.POINTER(WalkParams), vp, vp, vp, vp], C.c_int),
+        "dyg_decremental_batch": ([vp, vp, vp, vp, u32, u64, C.POINTER(WalkParams), vp, vp, vp, vp, vp, u64,
+                                   C.POINTER(u64), vp], C.c_int),
+        "dyg_decremental_stream": ([vp, vp, vp, vp, u32, u32, C.POINTER(WalkParams), vp, vp, vp, vp, vp, u64,
+                                    C.POINTER(u64), vp], C.c_int),
+        "dyg_mtx_read": ([C.c_char_p, u32, C.c_int, C.POINTER(u64), C.POINTER(vp), C.POINTER(vp),
+                          C.POINTER(vp), C.POINTER(u32)], C.c_int),
+        "dyg_mtx_free": ([vp], None),
+        "dyg_mtx_write": ([C.c_char_p, C.c_int, u64, vp, vp, vp, u32], C.c_int),
+        "dyg_synth_lattice_edges": ([u32, u32, u32], u64),
+        "dyg_synth_lattice": ([u32, u32, u32, u32, C.c_float, C.c_float, u64, vp, vp, vp], None),
+        "dyg_synth_sparsifier": ([u32, u64, vp, vp, vp, C.c_double, u64, vp], u64),
+        "dyg_synth_lattice_inserts": ([u32, u32, u32, u64, vp, vp, u64, u32, u32, u32, C.c_float, C.c_float,
+                                       u64, vp, vp, vp], u64),
+        "dyg_synth_sample": ([u64, u64, u64, vp], None),
+        "dyg_profile_enable": ([C.c_int], C.c_int),
+        "dyg_profile_reset": ([], C.c_int),
+        "dyg_profile_read": ([C.POINTER(Profile)], C.c_int),
+        "dyg_kernel_launches": ([], u64),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def _check(status: int, what: str) -> None:
+    if status != DYG_OK:
+        raise DygError(status, what, lib().dyg_last_error_string().decode())
+
+
+def _ptr(a):
+    """Pointer of a numpy array (host) or a torch tensor (host or device)."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        assert a.flags.c_contiguous
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        assert a.is_contiguous()
+        return a.data_ptr()
+    raise TypeError(type(a))
+
+
+def _as(a, dtype):
+    if a is None or hasattr(a, "data_ptr"):
+        return a
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def profile_enable(on: bool = True) -> None:
+    _check(lib().dyg_profile_enable(1 if on else 0), "dyg_profile_enable")
+
+
+def profile_reset() -> None:
+    _check(lib().dyg_profile_reset(), "dyg_profile_reset")
+
+
+def profile_read() -> dict:
+    p = Profile()
+    _check(lib().dyg_profile_read(C.byref(p)), "dyg_profile_read")
+    return {f: getattr(p, f) for f, _ in Profile._fields_}
+
+
+def kernel_launches() -> int:
+    return int(lib().dyg_kernel_launches())
+
+
+def version() -> str:
+    return lib().dyg_version().decode()
+
+
+def reference_batch_size(n: int) -> int:
+    return int(lib().dyg_reference_batch_size(int(n)))
+
+
+class Graph:
+    """A device-resident dynamic CSR (dyg_graph handle)."""
+
+    def __init__(self, handle: int):
+        self._h = C.c_void_p(handle)
+
+    @classmethod
+    def from_edges(cls, n_vertices: int, src, dst, w, slack_per_row: int = 2,
+                   arena_headroom: float = 0.5, device: int = -1) -> "Graph":
+        src = _as(src, np.uint32)
+        dst = _as(dst, np.uint32)
+        w = _as(w, np.float32)
+        opts = GraphOpts(int(slack_per_row), 0, float(arena_headroom), int(device), 0)
+        h = C.c_void_p()
+        _check(lib().dyg_graph_create_from_edges(int(n_vertices), len(src), _ptr(src), _ptr(dst),
+                                                 _ptr(w), C.byref(opts), C.byref(h)),
+               "dyg_graph_create_from_edges")
+        return cls(h.value)
+
+    def clone(self) -> "Graph":
+        h = C.c_void_p()
+        _check(lib().dyg_graph_clone(self._h, C.byref(h)), "dyg_graph_clone")
+        return Graph(h.value)
+
+    def copy_from(self, other: "Graph", stream: int | None = None) -> None:
+        _check(lib().dyg_graph_copy_from(self._h, other._h, stream), "dyg_graph_copy_from")
+
+    def close(self) -> None:
+        if self._h is not None and self._h.value:
+            lib().dyg_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    def info(self) -> dict:
+        n = C.c_uint32()
+        s, u, c = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        _check(lib().dyg_graph_info(self._h, C.byref(n), C.byref(s), C.byref(u), C.byref(c)),
+               "dyg_graph_info")
+        return {"n_vertices": n.value, "n_slots": s.value, "arena_used": u.value,
+                "arena_cap": c.value}
+
+    def export(self):
+        """(row_ptr[n+1] u64, col u32, w f32) in row order."""
+        inf = self.info()
+        n, s = inf["n_vertices"], inf["n_slots"]
+        rp = np.zeros(n + 1, np.uint64)
+        col = np.zeros(max(s, 1), np.uint32)
+        w = np.zeros(max(s, 1), np.float32)
+        _check(lib().dyg_graph_export(self._h, _ptr(rp), _ptr(col), _ptr(w), s), "dyg_graph_export")
+        return rp, col[:s], w[:s]
+
+    def compact(self, stream: int | None = None) -> None:
+        _check(lib().dyg_graph_compact(self._h, stream), "dyg_graph_compact")
+
+    def counters(self) -> tuple[int, int]:
+        m, k = C.c_uint64(), C.c_uint64()
+        _check(lib().dyg_graph_counters(self._h, C.byref(m), C.byref(k)), "dyg_graph_counters")
+        return m.value, k.value
+
+
+@dataclass
+class IncrementalResult:
+    found_at: np.ndarray   # i32: winner's step count or -1
+    conductance: np.ndarray  # f32: winner's 1/R (0 if none)
+    accepted: np.ndarray   # u8: 1 iff the edge was added to H
+
+
+def incremental_batch(H: Graph, src, dst, w, params: WalkParams, first_update_id: int = 0,
+                      G: Graph | None = None, stream: int | None = None) -> IncrementalResult:
+    src, dst, w = _as(src, np.uint32), _as(dst, np.uint32), _as(w, np.float32)
+    n = len(src)
+    out = IncrementalResult(np.empty(n, np.int32), np.empty(n, np.float32), np.empty(n, np.uint8))
+    _check(lib().dyg_incremental_batch(H.handle, G.handle if G else None, _ptr(src), _ptr(dst),
+                                       _ptr(w), n, int(first_update_id), C.byref(params),
+                                       _ptr(out.found_at), _ptr(out.conductance),
+                                       _ptr(out.accepted), stream), "dyg_incremental_batch")
+    return out
+
+
+def incremental_stream(H: Graph, src, dst, w, params: WalkParams, batch_size: int = 0,
+                       G: Graph | None = None, stream: int | None = None,
+                       out: IncrementalResult | None = None) -> IncrementalResult:
+    """The reference's update loop: batches of ceil(n/10) unless batch_size."""
+    src, dst, w = _as(src, np.uint32), _as(dst, np.uint32), _as(w, np.float32)
+    n = len(src)
+    if out is None:
+        out = IncrementalResult(np.empty(n, np.int32), np.empty(n, np.float32),
+                                np.empty(n, np.uint8))
+    _check(lib().dyg_incremental_stream(H.handle, G.handle if G else None, _ptr(src), _ptr(dst),
+                                        _ptr(w), n, int(batch_size), C.byref(params),
+                                        _ptr(out.found_at), _ptr(out.conductance),
+                                        _ptr(out.accepted), stream), "dyg_incremental_stream")
+    return out
+
+
+@dataclass
+class DecrementalResult:
+    status: np.ndarray      # i32: path length or DEL_* code
+    conductance: np.ndarray  # f32
+    rec_src: np.ndarray     # u32 recovered edges, commit order
+    rec_dst: np.ndarray
+    rec_kind: np.ndarray    # u8: REC_PATH / REC_FALLBACK
+
+
+def _decremental(fn, G, H, src, dst, params, arg, stream, rec_cap):
+    src, dst = _as(src, np.uint32), _as(dst, np.uint32)
+    n = len(src)
+    if rec_cap is None:
+        rec_cap = n * (params.max_steps + 4 * params.heuristic_walkers) + 16
+    st = np.empty(n, np.int32)
+    cd = np.empty(n, np.float32)
+    rx = np.empty(max(rec_cap, 1), np.uint32)
+    ry = np.empty(max(rec_cap, 1), np.uint32)
+    rk = np.empty(max(rec_cap, 1), np.uint8)
+    nrec = C.c_uint64()
+    _check(fn(G.handle, H.handle, _ptr(src), _ptr(dst), n, int(arg), C.byref(params), _ptr(st),
+              _ptr(cd), _ptr(rx), _ptr(ry), _ptr(rk), rec_cap, C.byref(nrec), stream),
+           fn.__name__)
+    k = nrec.value
+    return DecrementalResult(st, cd, rx[:k].copy(), ry[:k].copy(), rk[:k].copy())
+
+
+def decremental_stream_into(G: Graph, H: Graph, src, dst, params: WalkParams, status, conductance,
+                            rec_src, rec_dst, rec_kind, rec_cap: int, batch_size: int = 0,
+                            stream: int | None = None) -> int:
+    """decremental_stream writing into caller buffers (numpy or torch, host or
+    device); returns the number of recovered edges."""
+    src, dst = _as(src, np.uint32), _as(dst, np.uint32)
+    nrec = C.c_uint64()
+    _check(lib().dyg_decremental_stream(G.handle, H.handle, _ptr(src), _ptr(dst), len(src),
+                                        int(batch_size), C.byref(params), _ptr(status),
+                                        _ptr(conductance), _ptr(rec_src), _ptr(rec_dst),
+                                        _ptr(rec_kind), int(rec_cap), C.byref(nrec), stream),
+           "dyg_decremental_stream")
+    return nrec.value
+
+
+def decremental_batch(G: Graph, H: Graph, src, dst, params: WalkParams, first_update_id: int = 0,
+                      stream: int | None = None, rec_cap: int | None = None) -> DecrementalResult:
+    return _decremental(lib().dyg_decremental_batch, G, H, src, dst, params, first_update_id,
+                        stream, rec_cap)
+
+
+def decremental_stream(G: Graph, H: Graph, src, dst, params: WalkParams, batch_size: int = 0,
+                       stream: int | None = None, rec_cap: int | None = None) -> DecrementalResult:
+    return _decremental(lib().dyg_decremental_stream, G, H, src, dst, params, batch_size, stream,
+                        rec_cap)
+
+
+__all__ = ["Graph", "WalkParams", "GraphOpts", "DygError", "incremental_batch",
+           "incremental_stream", "decremental_batch", "decremental_stream", "lib", "version",
+           "reference_batch_size", "IncrementalResult", "DecrementalResult"]

@@ -1,0 +1,230 @@
+// dyg_internal.cuh -- device data layout, Philox stream and shared helpers of
+// the B200 dyGRASS update path.
+//
+// HBM layout of one graph (a dynamic CSR with per-row slack):
+//   desc[v]   uint2 {offset, degree}: one 8-byte load gives a walker both the
+//             row start and its live length.
+//   cap[v]    u32 row capacity (slots reserved at `offset`), touched only by
+//             commits and compaction, never by walkers.
+//   slots[i]  uint2 {column, weight bits}: the neighbour id and its weight
+//             arrive in one 8-byte load (the reference stores them degree
+//             floats apart through a pointer table, gpu_graph.cuh:205-235).
+//   top       arena bump pointer; rows that outgrow their capacity move to
+//             [top, top + new_cap) and leave a hole reclaimed by compaction.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/dyg.h"
+
+namespace dyg {
+
+constexpr uint32_t kFull = 0xFFFFFFFFu;
+constexpr uint32_t kDomainIncr = 0u;   // incremental walks
+constexpr uint32_t kDomainDecr = 1u;   // decremental walks
+constexpr uint32_t kDomainHeur = 2u;   // 2-step fallback walks
+
+// Device error bits (sticky per workspace until read).
+constexpr uint32_t kErrVertex = 1u;    // vertex id >= n in a batch
+constexpr uint32_t kErrPath = 2u;      // winner re-walk disagreed with its key
+constexpr uint32_t kErrArena = 4u;     // arena overflow in a commit
+
+struct DevGraph {
+    uint2 *desc;
+    uint32_t *cap;
+    uint2 *slots;
+    unsigned long long *top;   // device scalar
+    uint64_t arena_cap;        // slots
+    uint32_t n;
+};
+
+// ------------------------------------------------------------------ Philox
+// Philox4x32-10 (Salmon et al., SC'11).  Counter = {draw block, walker,
+// update id low, update id high | domain << 24}, key = seed.
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+        k.x += 0x9E3779B9u;
+        k.y += 0xBB67AE85u;
+    }
+    return c;
+}
+
+__device__ __forceinline__ uint32_t pick4(uint4 v, uint32_t i) {
+    return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w));
+}
+
+__host__ __device__ __forceinline__ uint32_t ctr3_of(uint64_t uid, uint32_t domain) {
+    return ((uint32_t)(uid >> 32) & 0x00FFFFFFu) | (domain << 24);
+}
+
+// Winner key: max conductance 1/R, then lowest walker id; the low bits carry
+// the winner's step count.  0 means no walker reached the target.
+__device__ __forceinline__ unsigned long long pack_key(float cond, uint32_t walker,
+                                                       uint32_t found) {
+    return ((unsigned long long)__float_as_uint(cond) << 32) |
+           ((unsigned long long)(1023u - walker) << 22) |
+           (unsigned long long)(found & 0x3FFFFFu);
+}
+__host__ __device__ __forceinline__ uint32_t key_walker(unsigned long long k) {
+    return 1023u - (uint32_t)((k >> 22) & 0x3FFu);
+}
+__host__ __device__ __forceinline__ int32_t key_found(unsigned long long k) {
+    return k ? (int32_t)(k & 0x3FFFFFu) : -1;
+}
+
+// Fixed-point weight of the weight-proportional mode (exact w * 2^32,
+// truncated) so that prefix sums are associative and match the host.
+__device__ __forceinline__ unsigned long long wq(float w) {
+    const double v = (double)w * 4294967296.0;
+    if (!(v > 0.0)) return 0ull;
+    if (v >= 18446744073709551615.0) return 0xFFFFFFFFFFFFFFFFull;
+    return (unsigned long long)v;
+}
+__device__ __forceinline__ unsigned long long mul_hi32(uint32_t r, unsigned long long total) {
+    // floor(r * total / 2^32) for a 96-bit product
+    const unsigned long long lo = (unsigned long long)r * (total & 0xFFFFFFFFull);
+    const unsigned long long hi = (unsigned long long)r * (total >> 32);
+    return hi + (lo >> 32);
+}
+
+// ------------------------------------------------------------- workspace
+// Device scratch owned by a graph handle, grown on demand.
+struct Buf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+struct Workspace {
+    Buf in_src, in_dst, in_w;                 // staged batch inputs
+    Buf keys;                                 // u64 per edge
+    Buf work;                                 // u64 counters: [0] work chunks
+    Buf flags, pos;                           // u32 per edge
+    Buf f_src, f_dst, f_idx;                  // filtered deletions
+    Buf f_uid;                                // u64 per filtered edge
+    Buf found;                                // u8 per half-edge
+    Buf hx, hy, hw, hseq;                     // half-edge lists (u32/f32)
+    Buf skeys, svals;                         // sorted keys / values
+    Buf need;                                 // u32 per half-edge
+    Buf path_v, path_w;                       // winner paths
+    Buf path_len;                             // i32 per filtered edge
+    Buf cand_x, cand_y, cand_w;               // recovery candidates
+    Buf keep;                                 // u32 per candidate
+    Buf htab_k, htab_v;                       // dedup hash table
+    Buf nop;                                  // u32 no-path filtered indices
+    Buf rec_x, rec_y, rec_k;                  // recovered edges (device)
+    Buf out_found, out_cond, out_acc, out_status;
+    Buf cub_tmp;
+    Buf s_src, s_dst, s_w, s_o1, s_o2, s_o3;  // whole-stream staging
+    Buf rx2, ry2;                             // recovered edges of a whole stream
+    Buf rk2;
+    Buf scalars;                              // u64 scalars (see Scalar)
+    Buf counts;                               // u32 counts (see Count)
+    unsigned long long *host_scalars = nullptr;   // pinned mirror
+    uint32_t *host_counts = nullptr;              // pinned mirror
+};
+
+// Indices into Workspace::scalars (u64, device) and Workspace::counts (u32).
+enum Scalar : int {
+    S_NEED = 0,       // relocation slots needed by a commit
+    S_ERR = 1,        // device error bits (kErr*)
+    S_MOVES = 2,      // walker moves (accumulating)
+    S_WALKS = 3,      // walks finished (accumulating)
+    S_TOP = 4,        // arena bump pointer of the owning graph
+    S_WORK = 5,       // work-chunk counter of the persistent walk kernel
+    S_NSCALARS = 8
+};
+enum Count : int {
+    C_FILTERED = 0,   // decremental: edges to walk
+    C_CANDS = 1,      // recovery candidates
+    C_KEPT = 2,       // recovery candidates kept
+    C_NOPATH = 3,     // decremental: edges without a path
+    C_ACCEPTED = 4,   // incremental: accepted edges
+    C_NCOUNTS = 8
+};
+
+}  // namespace dyg
+
+struct dyg_graph {
+    int device = 0;
+    dyg::DevGraph g{};
+    uint32_t slack = 2;
+    double headroom = 0.5;
+    dyg::Workspace ws;
+    uint64_t moves_total = 0, walks_total = 0;
+};
+
+namespace dyg {
+
+void set_error(const std::string &msg);
+dyg_status cuda_fail(cudaError_t e, const char *what, const char *file, int line);
+
+#define DYG_CUDA(call)                                                          \
+    do {                                                                        \
+        cudaError_t _e = (call);                                                \
+        if (_e != cudaSuccess) return ::dyg::cuda_fail(_e, #call, __FILE__, __LINE__); \
+    } while (0)
+
+#define DYG_TRY(call)                      \
+    do {                                   \
+        dyg_status _s = (call);            \
+        if (_s != DYG_OK) return _s;       \
+    } while (0)
+
+dyg_status ensure(Buf &b, size_t bytes);
+template <typename T>
+inline T *ptr(const Buf &b) { return static_cast<T *>(b.p); }
+
+int num_sms();
+// Counts launches of this library's own kernels (not cub's).
+void count_launch();
+
+// --- walk.cu
+struct WalkJob {
+    const uint32_t *src, *dst;
+    const float *w;              // incremental: per-edge weight; else null
+    const unsigned long long *uid;   // per-edge update id, or null -> uid0 + e
+    unsigned long long uid0;
+    const uint32_t *n_dev;       // device edge count, or null -> n_host
+    uint32_t n_host;
+    uint32_t domain;
+};
+dyg_status launch_walk(dyg_graph *G, const WalkJob &job, const dyg_walk_params &p, bool incremental,
+                       unsigned long long *keys, cudaStream_t st);
+dyg_status launch_winner_paths(dyg_graph *G, const WalkJob &job, const dyg_walk_params &p,
+                               const unsigned long long *keys, uint32_t n_max, uint32_t path_stride,
+                               uint32_t *path_v, float *path_w, int32_t *path_len, cudaStream_t st);
+dyg_status launch_fallback_walks(dyg_graph *G, const uint32_t *f_src, const uint32_t *f_dst,
+                                 const unsigned long long *f_uid, const uint32_t *nop,
+                                 uint32_t n_nop, const dyg_walk_params &p, uint32_t *cx,
+                                 uint32_t *cy, float *cw, cudaStream_t st);
+
+// --- graph.cu
+dyg_status upload_graph(dyg_graph *G, uint32_t n, const uint64_t *row_ptr, const uint32_t *col,
+                        const float *w);
+// Appends half-edge i (row hx[i], column hy[i], weight hw[i]) for i < m, in
+// list order per row.  Uses G's own workspace; may synchronize `st`.
+dyg_status commit_append(dyg_graph *G, const uint32_t *hx, const uint32_t *hy,
+                         const float *hw, uint32_t m, cudaStream_t st);
+dyg_status delete_half_edges(dyg_graph *G, const uint32_t *sorted_row,
+                             const uint32_t *sorted_idx, const uint32_t *hy, uint32_t m,
+                             const uint8_t *mask_found, uint8_t *found, cudaStream_t st);
+dyg_status sort_pairs_u32(Workspace &ws, const uint32_t *keys_in, uint32_t *keys_out,
+                          const uint32_t *vals_in, uint32_t *vals_out, uint32_t m,
+                          uint32_t key_bits, cudaStream_t st);
+dyg_status exclusive_scan_u32(Workspace &ws, const uint32_t *in, uint32_t *out, uint32_t m,
+                              cudaStream_t st);
+dyg_status compact_graph(dyg_graph *G, cudaStream_t st);
+dyg_status grow_arena(dyg_graph *G, uint64_t min_cap, cudaStream_t st);
+dyg_status read_scalars(dyg_graph *G, cudaStream_t st);
+dyg_status dedup_keep(dyg_graph *H, const uint32_t *cx, const uint32_t *cy,
+                      uint32_t m, uint32_t *keep, cudaStream_t st);
+uint32_t bits_for(uint32_t n);
+__global__ void k_iota(uint32_t *v, uint32_t m);
+
+}  // namespace dyg

@@ -1,0 +1,183 @@
+// synth.cpp -- seeded synthetic workloads (include/dyg_synth.h).
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+
+#include <algorithm>
+#include <numeric>
+#include <unordered_set>
+#include <vector>
+
+#include "../../include/dyg_synth.h"
+
+namespace {
+
+struct SplitMix {
+    uint64_t s;
+    explicit SplitMix(uint64_t seed) : s(seed) {}
+    uint64_t next() {
+        uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    }
+    double unit() { return (double)(next() >> 11) * (1.0 / 9007199254740992.0); }
+    uint64_t below(uint64_t n) { return n ? next() % n : 0; }
+};
+
+float draw_weight(SplitMix &r, uint32_t dist, float lo, float hi) {
+    const double u = r.unit();
+    if (dist == DYG_W_LOGUNIFORM) {
+        const double a = log10((double)lo), b = log10((double)hi);
+        return (float)pow(10.0, a + (b - a) * u);
+    }
+    return (float)((double)lo + ((double)hi - (double)lo) * u);
+}
+
+struct DSU {
+    std::vector<uint32_t> p;
+    explicit DSU(uint32_t n) : p(n) { std::iota(p.begin(), p.end(), 0u); }
+    uint32_t find(uint32_t x) {
+        while (p[x] != x) {
+            p[x] = p[p[x]];
+            x = p[x];
+        }
+        return x;
+    }
+    bool unite(uint32_t a, uint32_t b) {
+        a = find(a);
+        b = find(b);
+        if (a == b) return false;
+        p[a] = b;
+        return true;
+    }
+};
+
+inline uint64_t pair_key(uint32_t a, uint32_t b) {
+    if (a > b) std::swap(a, b);
+    return ((uint64_t)a << 32) | b;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint64_t dyg_synth_lattice_edges(uint32_t nx, uint32_t ny, uint32_t nz) {
+    const uint64_t X = nx, Y = ny, Z = nz ? nz : 1;
+    return (X - 1) * Y * Z + X * (Y - 1) * Z + X * Y * (Z - 1);
+}
+
+void dyg_synth_lattice(uint32_t nx, uint32_t ny, uint32_t nz, uint32_t wdist, float lo, float hi,
+                       uint64_t seed, uint32_t *src, uint32_t *dst, float *w) {
+    if (nz == 0) nz = 1;
+    SplitMix r(seed);
+    uint64_t k = 0;
+    for (uint32_t z = 0; z < nz; ++z)
+        for (uint32_t y = 0; y < ny; ++y)
+            for (uint32_t x = 0; x < nx; ++x) {
+                const uint32_t v = x + nx * (y + ny * z);
+                if (x + 1 < nx) {
+                    src[k] = v; dst[k] = v + 1; w[k] = draw_weight(r, wdist, lo, hi); ++k;
+                }
+                if (y + 1 < ny) {
+                    src[k] = v; dst[k] = v + nx; w[k] = draw_weight(r, wdist, lo, hi); ++k;
+                }
+                if (z + 1 < nz) {
+                    src[k] = v; dst[k] = v + nx * ny; w[k] = draw_weight(r, wdist, lo, hi); ++k;
+                }
+            }
+}
+
+uint64_t dyg_synth_sparsifier(uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst,
+                              const float *w, double frac, uint64_t seed, uint64_t *out_idx) {
+    std::vector<uint64_t> order(m);
+    std::iota(order.begin(), order.end(), 0ull);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint64_t a, uint64_t b) { return w[a] > w[b]; });
+    DSU dsu(n);
+    std::vector<uint8_t> in_tree(m, 0);
+    std::vector<uint64_t> off;
+    off.reserve(m);
+    for (uint64_t i : order) {
+        if (src[i] != dst[i] && dsu.unite(src[i], dst[i])) in_tree[i] = 1;
+    }
+    for (uint64_t i = 0; i < m; ++i)
+        if (!in_tree[i]) off.push_back(i);
+    const uint64_t k = (uint64_t)floor(frac * (double)off.size());
+    SplitMix r(seed);
+    for (uint64_t i = 0; i < k; ++i) {  // partial Fisher-Yates
+        const uint64_t j = i + r.below(off.size() - i);
+        std::swap(off[i], off[j]);
+    }
+    for (uint64_t i = 0; i < k; ++i) in_tree[off[i]] = 1;
+    uint64_t c = 0;
+    for (uint64_t i = 0; i < m; ++i)
+        if (in_tree[i]) out_idx[c++] = i;
+    return c;
+}
+
+uint64_t dyg_synth_lattice_inserts(uint32_t nx, uint32_t ny, uint32_t nz, uint64_t m,
+                                   const uint32_t *src, const uint32_t *dst, uint64_t count,
+                                   uint32_t hop_lo, uint32_t hop_hi, uint32_t wdist, float lo,
+                                   float hi, uint64_t seed, uint32_t *out_src, uint32_t *out_dst,
+                                   float *out_w) {
+    if (nz == 0) nz = 1;
+    const bool three = nz > 1;
+    std::unordered_set<uint64_t> seen;
+    seen.reserve((size_t)(m + count) * 2);
+    for (uint64_t i = 0; i < m; ++i) seen.insert(pair_key(src[i], dst[i]));
+    SplitMix r(seed);
+    const uint64_t nv = (uint64_t)nx * ny * nz;
+    uint64_t k = 0, tries = 0;
+    const uint64_t max_tries = count * 1000 + 1000000;
+    while (k < count && tries < max_tries) {
+        ++tries;
+        const uint32_t u = (uint32_t)r.below(nv);
+        const int64_t d = (int64_t)hop_lo + (int64_t)r.below((uint64_t)(hop_hi - hop_lo + 1));
+        const int64_t ux = u % nx, uy = (u / nx) % ny, uz = u / ((uint64_t)nx * ny);
+        int64_t dx = (int64_t)r.below((uint64_t)(2 * d + 1)) - d;
+        int64_t rem = d - (dx < 0 ? -dx : dx);
+        int64_t dy, dz = 0;
+        if (three) {
+            dy = (int64_t)r.below((uint64_t)(2 * rem + 1)) - rem;
+            const int64_t rz = rem - (dy < 0 ? -dy : dy);
+            dz = (r.next() & 1) ? rz : -rz;
+        } else {
+            dy = (r.next() & 1) ? rem : -rem;
+        }
+        const int64_t vx = ux + dx, vy = uy + dy, vz = uz + dz;
+        if (vx < 0 || vy < 0 || vz < 0 || vx >= nx || vy >= ny || vz >= nz) continue;
+        const uint32_t v = (uint32_t)(vx + (int64_t)nx * (vy + (int64_t)ny * vz));
+        if (v == u) continue;
+        if (!seen.insert(pair_key(u, v)).second) continue;
+        out_src[k] = u;
+        out_dst[k] = v;
+        out_w[k] = draw_weight(r, wdist, lo, hi);
+        ++k;
+    }
+    return k;
+}
+
+void dyg_synth_sample(uint64_t m, uint64_t k, uint64_t seed, uint64_t *out_idx) {
+    if (k > m) k = m;
+    SplitMix r(seed);
+    if (k * 4 >= m) {
+        std::vector<uint64_t> a(m);
+        std::iota(a.begin(), a.end(), 0ull);
+        for (uint64_t i = 0; i < k; ++i) {
+            const uint64_t j = i + r.below(m - i);
+            std::swap(a[i], a[j]);
+            out_idx[i] = a[i];
+        }
+        return;
+    }
+    std::unordered_set<uint64_t> used;
+    used.reserve((size_t)k * 2);
+    uint64_t c = 0;
+    while (c < k) {
+        const uint64_t j = r.below(m);
+        if (used.insert(j).second) out_idx[c++] = j;
+    }
+}
+
+}  // extern "C"

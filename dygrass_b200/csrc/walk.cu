@@ -1,0 +1,450 @@
+// walk.cu -- sm_100a random-walk kernels of the dyGRASS update path.
+//
+// One walker = one non-backtracking random walk from an edge's source towards
+// its target (random_walk_incremental/main.cu:70-211 and
+// random_walk_decremental/main.cu:77-220 restated).  Walk lengths differ by
+// two orders of magnitude between walkers (dead ends after one step, full
+// max_steps walks), so instead of the reference's one-block-per-edge with a
+// 512-thread barrier tree, each warp of a persistent grid keeps its 32 lanes
+// busy: a lane whose walker ends takes the next walker of the warp's current
+// edge, and the warp pulls a new edge from a global counter when the current
+// one is handed out.  The per-edge winner (max 1/R, lowest walker id) is a
+// 64-bit key reduced with atomicMax, so no barrier and no global scratch
+// arrays are needed.
+//
+// Draw d of walker k of update u is word d&3 of
+// Philox4x32-10({d>>2, k, u_lo, u_hi | domain<<24}, seed): any walker can be
+// replayed, which is how the decremental winner's path is recovered without
+// the reference's per-thread path[100] arrays.
+#include <mutex>
+#include <vector>
+
+#include "dyg_internal.cuh"
+
+namespace dyg {
+
+// ------------------------------------------------------------- profiling
+namespace {
+struct ProfEvent {
+    cudaEvent_t a, b;
+    int kind;  // 0 incremental walk, 1 decremental walk, 2 replay/fallback
+};
+std::mutex g_prof_mu;
+bool g_prof_on = false;
+std::vector<ProfEvent> g_prof_events;
+dyg_profile g_prof_acc{};
+
+void prof_flush_locked() {
+    for (ProfEvent &e : g_prof_events) {
+        float ms = 0.f;
+        if (cudaEventSynchronize(e.b) == cudaSuccess && cudaEventElapsedTime(&ms, e.a, e.b) == cudaSuccess) {
+            if (e.kind == 0) { g_prof_acc.incr_walk_ms += ms; g_prof_acc.incr_walk_launches++; }
+            else if (e.kind == 1) { g_prof_acc.decr_walk_ms += ms; g_prof_acc.decr_walk_launches++; }
+            else { g_prof_acc.other_walk_ms += ms; g_prof_acc.other_walk_launches++; }
+        }
+        cudaGetLastError();
+        cudaEventDestroy(e.a);
+        cudaEventDestroy(e.b);
+    }
+    g_prof_events.clear();
+}
+
+struct ProfScope {
+    bool on = false;
+    ProfEvent ev{};
+    cudaStream_t st;
+    ProfScope(int kind, cudaStream_t s) : st(s) {
+        std::lock_guard<std::mutex> lk(g_prof_mu);
+        if (!g_prof_on) return;
+        ev.kind = kind;
+        if (cudaEventCreate(&ev.a) != cudaSuccess || cudaEventCreate(&ev.b) != cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
+        cudaEventRecord(ev.a, st);
+        on = true;
+    }
+    ~ProfScope() {
+        if (!on) return;
+        cudaEventRecord(ev.b, st);
+        std::lock_guard<std::mutex> lk(g_prof_mu);
+        g_prof_events.push_back(ev);
+        if (g_prof_events.size() > 4096) prof_flush_locked();
+    }
+};
+}  // namespace
+
+constexpr int kWalkThreads = 256;
+
+struct WalkArgs {
+    DevGraph g;
+    WalkJob job;
+    uint32_t walkers, max_steps;
+    float threshold;
+    uint2 key;
+    unsigned long long *keys;
+    unsigned long long *scalars;
+};
+
+struct Walker {
+    uint32_t cur, prev, step, tgt, walker, c2, c3, rblk;
+    uint4 rbuf;
+    float R, we;
+};
+
+enum : int { kContinue = 0, kFail = 1, kFound = 2 };
+
+// One move of one walker, mirroring the reference loop body:
+//   step 1:  any neighbour, r % deg                    (main.cu:99-106)
+//   step >1: dead end if deg == 1; r % (deg - 1) and the last slot when the
+//            draw lands on the previous vertex          (main.cu:118-137)
+//   R += 1/w; distortion test (incremental only, from step 2 on), then the
+//   target test; walk ends when the step counter reaches max_steps
+//                                                       (main.cu:116, 139-157)
+// *moved is set when a neighbour was drawn; *taken receives its slot.
+template <bool INCR, bool WEIGHTED>
+__device__ __forceinline__ int step_once(Walker &s, const uint2 *__restrict__ desc,
+                                         const uint2 *__restrict__ slots, uint32_t max_steps,
+                                         float thr, uint2 key, bool *moved, uint2 *taken) {
+    *moved = false;
+    const uint2 d = __ldg(desc + s.cur);
+    const uint32_t deg = d.y;
+    const bool first = (s.step == 1u);
+    if (first ? (deg == 0u) : (deg <= 1u)) return kFail;
+    const uint32_t di = s.step - 1u, b = di >> 2;
+    if (b != s.rblk) {
+        s.rbuf = philox4x32_10(make_uint4(b, s.walker, s.c2, s.c3), key);
+        s.rblk = b;
+    }
+    const uint32_t r = pick4(s.rbuf, di & 3u);
+    uint2 sl;
+    if (!WEIGHTED) {
+        const uint32_t idx = first ? (r % deg) : (r % (deg - 1u));
+        sl = __ldg(slots + d.x + idx);
+        if (!first && sl.x == s.prev) sl = __ldg(slots + d.x + deg - 1u);
+    } else {
+        unsigned long long total = 0ull;
+        for (uint32_t j = 0; j < deg; ++j) {
+            const uint2 t = __ldg(slots + d.x + j);
+            if (!first && t.x == s.prev) continue;
+            total += wq(__uint_as_float(t.y));
+        }
+        if (total == 0ull) return kFail;
+        const unsigned long long target = mul_hi32(r, total);
+        unsigned long long acc = 0ull;
+        uint32_t last = deg;
+        for (uint32_t j = 0; j < deg; ++j) {
+            const uint2 t = __ldg(slots + d.x + j);
+            if (!first && t.x == s.prev) continue;
+            acc += wq(__uint_as_float(t.y));
+            last = j;
+            if (acc > target) break;
+        }
+        sl = __ldg(slots + d.x + last);
+    }
+    *moved = true;
+    *taken = sl;
+    s.R = __fadd_rn(s.R, __frcp_rn(__uint_as_float(sl.y)));
+    if (INCR && !first && __fmul_rn(s.R, s.we) >= thr) return kFail;
+    if (sl.x == s.tgt) return kFound;
+    s.prev = s.cur;
+    s.cur = sl.x;
+    s.step += 1u;
+    if (s.step >= max_steps) return kFail;
+    return kContinue;
+}
+
+template <bool INCR, bool WEIGHTED>
+__global__ void __launch_bounds__(kWalkThreads) k_walk(WalkArgs a) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    const uint32_t n = a.job.n_dev ? *a.job.n_dev : a.job.n_host;
+    const uint32_t W = a.walkers;
+    unsigned long long *work = a.scalars + S_WORK;
+
+    uint32_t ce = 0, c_next = 0, c_end = 0;  // warp-uniform: current edge chunk
+    bool exhausted = false;
+
+    bool active = false;
+    Walker s;
+    s.cur = s.prev = s.step = s.tgt = s.walker = s.c2 = s.c3 = 0u;
+    s.rblk = 0xFFFFFFFFu;
+    s.rbuf = make_uint4(0u, 0u, 0u, 0u);
+    s.R = 0.f;
+    s.we = 0.f;
+    unsigned long long best = 0ull;
+    uint32_t best_e = 0xFFFFFFFFu;
+    uint32_t moves = 0u, walks = 0u;
+
+    while (true) {
+        uint32_t free_mask = __ballot_sync(kFull, !active);
+        while (free_mask != 0u && !exhausted) {
+            if (c_next >= c_end) {
+                unsigned long long c = 0ull;
+                if (lane == 0u) c = atomicAdd(work, 1ull);
+                c = __shfl_sync(kFull, c, 0);
+                if (c >= (unsigned long long)n) {
+                    exhausted = true;
+                    break;
+                }
+                ce = (uint32_t)c;
+                c_next = 0u;
+                c_end = W;
+            }
+            const uint32_t take = min((uint32_t)__popc(free_mask), c_end - c_next);
+            const uint32_t rank = __popc(free_mask & lt_mask);
+            if (((free_mask >> lane) & 1u) && rank < take) {
+                const uint32_t e = ce;
+                if (best_e != e) {
+                    if (best) atomicMax(a.keys + best_e, best);
+                    best = 0ull;
+                    best_e = e;
+                }
+                s.walker = c_next + rank;
+                s.cur = a.job.src[e];
+                s.tgt = a.job.dst[e];
+                s.we = INCR ? a.job.w[e] : 0.f;
+                const unsigned long long uid = a.job.uid ? a.job.uid[e] : a.job.uid0 + e;
+                s.c2 = (uint32_t)uid;
+                s.c3 = ctr3_of(uid, a.job.domain);
+                s.rblk = 0xFFFFFFFFu;
+                s.step = 1u;
+                s.R = 0.f;
+                s.prev = 0u;
+                if (s.cur >= a.g.n || s.tgt >= a.g.n) {
+                    atomicOr(a.scalars + S_ERR, (unsigned long long)kErrVertex);
+                    ++walks;
+                } else {
+                    active = true;
+                }
+            }
+            for (uint32_t i = 0; i < take; ++i) free_mask &= free_mask - 1u;
+            c_next += take;
+        }
+        if (!__any_sync(kFull, active)) break;
+        if (active) {
+            bool moved;
+            uint2 taken;
+            const int r = step_once<INCR, WEIGHTED>(s, a.g.desc, a.g.slots, a.max_steps,
+                                                   a.threshold, a.key, &moved, &taken);
+            moves += moved ? 1u : 0u;
+            if (r != kContinue) {
+                if (r == kFound) {
+                    const unsigned long long k = pack_key(__frcp_rn(s.R), s.walker, s.step);
+                    if (k > best) best = k;
+                }
+                active = false;
+                ++walks;
+            }
+        }
+    }
+    if (best) atomicMax(a.keys + best_e, best);
+    const uint32_t wm = __reduce_add_sync(kFull, moves);
+    const uint32_t ww = __reduce_add_sync(kFull, walks);
+    if (lane == 0u) {
+        if (wm) atomicAdd(a.scalars + S_MOVES, (unsigned long long)wm);
+        if (ww) atomicAdd(a.scalars + S_WALKS, (unsigned long long)ww);
+    }
+}
+
+// Replays the winner of each decremental edge and writes its path
+// (random_walk_decremental/main.cu:206-217 writes the same vertices from a
+// per-thread local array).
+template <bool WEIGHTED>
+__global__ void k_winner_paths(DevGraph g, WalkJob job, uint32_t max_steps, uint2 key,
+                               const unsigned long long *keys, uint32_t stride, uint32_t *pv,
+                               float *pw, int32_t *plen, unsigned long long *scalars) {
+    const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t n = job.n_dev ? *job.n_dev : job.n_host;
+    if (f >= n) return;
+    const unsigned long long k = keys[f];
+    if (!k) {
+        plen[f] = -1;
+        return;
+    }
+    Walker s;
+    s.walker = key_walker(k);
+    s.cur = job.src[f];
+    s.tgt = job.dst[f];
+    s.we = 0.f;
+    const unsigned long long uid = job.uid ? job.uid[f] : job.uid0 + f;
+    s.c2 = (uint32_t)uid;
+    s.c3 = ctr3_of(uid, job.domain);
+    s.rblk = 0xFFFFFFFFu;
+    s.rbuf = make_uint4(0u, 0u, 0u, 0u);
+    s.step = 1u;
+    s.R = 0.f;
+    s.prev = 0u;
+    uint32_t *row_v = pv + (size_t)f * stride;
+    float *row_w = pw + (size_t)f * stride;
+    row_v[0] = s.cur;
+    row_w[0] = 0.f;
+    int r;
+    do {
+        const uint32_t at = s.step;
+        bool moved;
+        uint2 taken;
+        r = step_once<false, WEIGHTED>(s, g.desc, g.slots, max_steps, 0.f, key, &moved, &taken);
+        if (moved && at < stride) {
+            row_v[at] = taken.x;
+            row_w[at] = __uint_as_float(taken.y);
+        }
+    } while (r == kContinue);
+    const int32_t found = (r == kFound) ? (int32_t)s.step : -1;
+    plen[f] = found;
+    if (found != key_found(k)) atomicOr(scalars + S_ERR, (unsigned long long)kErrPath);
+}
+
+// 2-step fallback walks from both endpoints of each edge that found no path
+// (random_walk_decremental/main.cu:243-290, with the second step reading the
+// row of the vertex the walker stands on).  Candidate pair 2i, 2i+1 of item
+// i = (q * 2 + side) * hw + j is (s0, x1), (x1, x2); x = ~0u marks none.
+__global__ void k_fallback(DevGraph g, const uint32_t *f_src, const uint32_t *f_dst,
+                           const unsigned long long *f_uid, const uint32_t *nop, uint32_t n_nop,
+                           uint32_t hw, uint2 key, uint32_t *cx, uint32_t *cy, float *cw) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t per = 2u * hw;
+    if (i >= n_nop * per) return;
+    const uint32_t q = i / per, rem = i - q * per, side = rem / hw, j = rem - side * hw;
+    const uint32_t f = nop[q];
+    const uint32_t s0 = side ? f_dst[f] : f_src[f];
+    const unsigned long long uid = f_uid[f];
+    const uint4 rb = philox4x32_10(make_uint4(0u, side * hw + j, (uint32_t)uid,
+                                              ctr3_of(uid, kDomainHeur)), key);
+    uint32_t x1 = ~0u, x2 = ~0u;
+    float w1 = 0.f, w2 = 0.f;
+    const uint2 d0 = __ldg(g.desc + s0);
+    if (d0.y != 0u) {
+        const uint2 a = __ldg(g.slots + d0.x + rb.x % d0.y);
+        x1 = a.x;
+        w1 = __uint_as_float(a.y);
+        const uint2 d1 = __ldg(g.desc + x1);
+        if (d1.y != 0u) {
+            uint2 b = __ldg(g.slots + d1.x + rb.y % d1.y);
+            if (b.x == s0) b = __ldg(g.slots + d1.x + d1.y - 1u);
+            x2 = b.x;
+            w2 = __uint_as_float(b.y);
+        }
+    }
+    cx[2 * i] = (x1 == ~0u) ? ~0u : s0;
+    cy[2 * i] = x1;
+    cw[2 * i] = w1;
+    cx[2 * i + 1] = (x2 == ~0u) ? ~0u : x1;
+    cy[2 * i + 1] = x2;
+    cw[2 * i + 1] = w2;
+}
+
+template <typename K>
+static int persistent_blocks(K kernel) {
+    static int cached = 0;
+    if (!cached) {
+        int nb = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, kWalkThreads, 0);
+        if (nb < 1) nb = 1;
+        cached = nb * num_sms();
+    }
+    return cached;
+}
+
+dyg_status launch_walk(dyg_graph *G, const WalkJob &job, const dyg_walk_params &p, bool incremental,
+                       unsigned long long *keys, cudaStream_t st) {
+    WalkArgs a;
+    a.g = G->g;
+    a.job = job;
+    a.walkers = p.walkers;
+    a.max_steps = p.max_steps;
+    a.threshold = p.threshold;
+    a.key = make_uint2((uint32_t)p.seed, (uint32_t)(p.seed >> 32));
+    a.keys = keys;
+    a.scalars = ptr<unsigned long long>(G->ws.scalars);
+    DYG_CUDA(cudaMemsetAsync(a.scalars + S_WORK, 0, sizeof(unsigned long long), st));
+    const bool wtd = p.transition == DYG_TRANSITION_WEIGHTED;
+    int grid;
+    ProfScope prof(incremental ? 0 : 1, st);
+    if (incremental) {
+        if (wtd) {
+            grid = persistent_blocks(k_walk<true, true>);
+            k_walk<true, true><<<grid, kWalkThreads, 0, st>>>(a);
+            count_launch();
+        } else {
+            grid = persistent_blocks(k_walk<true, false>);
+            k_walk<true, false><<<grid, kWalkThreads, 0, st>>>(a);
+            count_launch();
+        }
+    } else {
+        if (wtd) {
+            grid = persistent_blocks(k_walk<false, true>);
+            k_walk<false, true><<<grid, kWalkThreads, 0, st>>>(a);
+            count_launch();
+        } else {
+            grid = persistent_blocks(k_walk<false, false>);
+            k_walk<false, false><<<grid, kWalkThreads, 0, st>>>(a);
+            count_launch();
+        }
+    }
+    DYG_CUDA(cudaGetLastError());
+    return DYG_OK;
+}
+
+dyg_status launch_winner_paths(dyg_graph *G, const WalkJob &job, const dyg_walk_params &p,
+                               const unsigned long long *keys, uint32_t n_max, uint32_t stride,
+                               uint32_t *path_v, float *path_w, int32_t *path_len, cudaStream_t st) {
+    if (n_max == 0) return DYG_OK;
+    const uint2 key = make_uint2((uint32_t)p.seed, (uint32_t)(p.seed >> 32));
+    const int threads = 128;
+    const int grid = (int)((n_max + threads - 1) / threads);
+    unsigned long long *sc = ptr<unsigned long long>(G->ws.scalars);
+    ProfScope prof(2, st);
+    if (p.transition == DYG_TRANSITION_WEIGHTED)
+        k_winner_paths<true><<<grid, threads, 0, st>>>(G->g, job, p.max_steps, key, keys, stride,
+                                                       path_v, path_w, path_len, sc);
+    else
+        k_winner_paths<false><<<grid, threads, 0, st>>>(G->g, job, p.max_steps, key, keys, stride,
+                                                        path_v, path_w, path_len, sc);
+    count_launch();
+    DYG_CUDA(cudaGetLastError());
+    return DYG_OK;
+}
+
+dyg_status launch_fallback_walks(dyg_graph *G, const uint32_t *f_src, const uint32_t *f_dst,
+                                 const unsigned long long *f_uid, const uint32_t *nop,
+                                 uint32_t n_nop, const dyg_walk_params &p, uint32_t *cx,
+                                 uint32_t *cy, float *cw, cudaStream_t st) {
+    const uint32_t items = n_nop * 2u * p.heuristic_walkers;
+    if (items == 0) return DYG_OK;
+    const uint2 key = make_uint2((uint32_t)p.seed, (uint32_t)(p.seed >> 32));
+    const int threads = 128;
+    ProfScope prof(2, st);
+    k_fallback<<<(items + threads - 1) / threads, threads, 0, st>>>(
+        G->g, f_src, f_dst, f_uid, nop, n_nop, p.heuristic_walkers, key, cx, cy, cw);
+    count_launch();
+    DYG_CUDA(cudaGetLastError());
+    return DYG_OK;
+}
+
+}  // namespace dyg
+
+extern "C" {
+
+dyg_status dyg_profile_enable(int on) {
+    std::lock_guard<std::mutex> lk(dyg::g_prof_mu);
+    dyg::g_prof_on = on != 0;
+    return DYG_OK;
+}
+
+dyg_status dyg_profile_reset(void) {
+    std::lock_guard<std::mutex> lk(dyg::g_prof_mu);
+    dyg::prof_flush_locked();
+    dyg::g_prof_acc = dyg_profile{};
+    return DYG_OK;
+}
+
+dyg_status dyg_profile_read(dyg_profile *out) {
+    if (!out) return DYG_EINVAL;
+    std::lock_guard<std::mutex> lk(dyg::g_prof_mu);
+    dyg::prof_flush_locked();
+    *out = dyg::g_prof_acc;
+    return DYG_OK;
+}
+
+}  // extern "C"

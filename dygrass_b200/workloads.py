@@ -1,0 +1,109 @@
+"""Seeded synthetic workloads with the shapes of the benchmark configurations.
+
+The reference's datasets are not available (they are downloaded from a
+private drive by datasetdownload.py), so every workload here is generated:
+
+  grid_2d   -- 2-D grid, FP32 weights U[0.5, 2.0], sparsifier = maximum-weight
+               spanning tree + 10% of the off-tree edges, insertions at grid
+               hop distance 2..8 with weights U[0.5, 2.0]; threshold 10,
+               512 walkers, max_steps 64.  At 100x100: 10,000 vertices,
+               19,800 edges, 1,000 insertions.
+  mesh_3d   -- 3-D 7-point mesh, FP32 weights log-uniform [1e-2, 1e2],
+               sparsifier = spanning tree + 5% off-tree, insertions at hop
+               distance 2..10 with the same weight law, then deletion of 10%
+               of the dense graph's edges (after insertions), uniform;
+               threshold 100, 512 walkers, max_steps 100.  At 100^3:
+               1,000,000 vertices, 2,970,000 edges, 200,000 insertions,
+               317,000 deletions.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import WalkParams, _ptr, lib
+
+MASTER_SEED = 20251203
+W_UNIFORM = 0
+W_LOGUNIFORM = 1
+
+
+def lattice(nx: int, ny: int, nz: int, wdist: int, lo: float, hi: float, seed: int):
+    m = int(lib().dyg_synth_lattice_edges(nx, ny, nz))
+    src = np.empty(m, np.uint32)
+    dst = np.empty(m, np.uint32)
+    w = np.empty(m, np.float32)
+    lib().dyg_synth_lattice(nx, ny, nz, wdist, lo, hi, seed, _ptr(src), _ptr(dst), _ptr(w))
+    return src, dst, w
+
+
+def sparsifier(n: int, src, dst, w, frac: float, seed: int) -> np.ndarray:
+    idx = np.empty(len(src), np.uint64)
+    k = lib().dyg_synth_sparsifier(n, len(src), _ptr(src), _ptr(dst), _ptr(w), frac, seed, _ptr(idx))
+    return idx[:k]
+
+
+def lattice_inserts(nx, ny, nz, src, dst, count, hop_lo, hop_hi, wdist, lo, hi, seed):
+    os_ = np.empty(count, np.uint32)
+    od = np.empty(count, np.uint32)
+    ow = np.empty(count, np.float32)
+    k = lib().dyg_synth_lattice_inserts(nx, ny, nz, len(src), _ptr(src), _ptr(dst), count, hop_lo,
+                                        hop_hi, wdist, lo, hi, seed, _ptr(os_), _ptr(od), _ptr(ow))
+    return os_[:k], od[:k], ow[:k]
+
+
+def sample(m: int, k: int, seed: int) -> np.ndarray:
+    out = np.empty(k, np.uint64)
+    lib().dyg_synth_sample(m, k, seed, _ptr(out))
+    return out
+
+
+@dataclass
+class Workload:
+    name: str
+    n: int
+    g_src: np.ndarray          # dense graph G0 (file order)
+    g_dst: np.ndarray
+    g_w: np.ndarray
+    h_src: np.ndarray          # sparsifier H0 (file order)
+    h_dst: np.ndarray
+    h_w: np.ndarray
+    ins_src: np.ndarray        # insertion stream
+    ins_dst: np.ndarray
+    ins_w: np.ndarray
+    del_src: np.ndarray = field(default_factory=lambda: np.empty(0, np.uint32))
+    del_dst: np.ndarray = field(default_factory=lambda: np.empty(0, np.uint32))
+    params: WalkParams = None   # incremental
+    dparams: WalkParams = None  # decremental
+    meta: dict = field(default_factory=dict)
+
+
+def grid_2d(nx: int = 100, ny: int = 100, inserts: int = 1000, seed: int = MASTER_SEED,
+            walkers: int = 512, max_steps: int = 64, threshold: float = 10.0) -> Workload:
+    src, dst, w = lattice(nx, ny, 1, W_UNIFORM, 0.5, 2.0, seed + 1)
+    n = nx * ny
+    idx = sparsifier(n, src, dst, w, 0.10, seed + 2)
+    isrc, idst, iw = lattice_inserts(nx, ny, 1, src, dst, inserts, 2, 8, W_UNIFORM, 0.5, 2.0, seed + 3)
+    p = WalkParams.make(threshold=threshold, walkers=walkers, max_steps=max_steps, seed=seed)
+    return Workload(f"grid_{nx}x{ny}", n, src, dst, w, src[idx], dst[idx], w[idx], isrc, idst, iw,
+                    params=p, dparams=WalkParams.make(walkers=walkers, max_steps=100, seed=seed),
+                    meta={"nx": nx, "ny": ny, "seed": seed})
+
+
+def mesh_3d(k: int = 100, inserts: int = 200_000, del_frac: float = 0.10,
+            seed: int = MASTER_SEED, walkers: int = 512, max_steps: int = 100,
+            threshold: float = 100.0) -> Workload:
+    src, dst, w = lattice(k, k, k, W_LOGUNIFORM, 1e-2, 1e2, seed + 1)
+    n = k * k * k
+    idx = sparsifier(n, src, dst, w, 0.05, seed + 2)
+    isrc, idst, iw = lattice_inserts(k, k, k, src, dst, inserts, 2, 10, W_LOGUNIFORM, 1e-2, 1e2,
+                                     seed + 3)
+    gs = np.concatenate([src, isrc])
+    gd = np.concatenate([dst, idst])
+    nd = int(np.floor(del_frac * len(gs)))
+    di = sample(len(gs), nd, seed + 4)
+    p = WalkParams.make(threshold=threshold, walkers=walkers, max_steps=max_steps, seed=seed)
+    dp = WalkParams.make(walkers=walkers, max_steps=max_steps, seed=seed)
+    return Workload(f"mesh_{k}^3", n, src, dst, w, src[idx], dst[idx], w[idx], isrc, idst, iw,
+                    gs[di], gd[di], params=p, dparams=dp, meta={"k": k, "seed": seed})

@@ -1,0 +1,189 @@
+/*
+ * dyg.h -- C ABI of the B200 dyGRASS update path.
+ *
+ * The reference has no library API: its boundary is two executables and a
+ * file contract.  Each entry point below replaces one piece of what those
+ * executables do between reading the .mtx files and writing the result:
+ *
+ *   dyg_graph_create_from_edges  <- read_graph + gpu_graph ctor + copyToDevice
+ *                                   (random_walk_incremental/functions.cpp:58-239,
+ *                                    random_walk_incremental/gpu_graph.cuh:123-162, 205-275;
+ *                                    random_walk_decremental/functions.cpp:69-281,
+ *                                    random_walk_decremental/gpu_graph.cuh:179-268, 479-489)
+ *   dyg_incremental_batch        <- one iteration of the batch loop:
+ *                                   random_walk<<<>>> + get_result + updateGraphFromResult
+ *                                   (random_walk_incremental/main.cu:301-328,
+ *                                    random_walk_incremental/gpu_graph.cuh:292-336, 551-554)
+ *   dyg_incremental_stream       <- the whole loop with the reference batching
+ *                                   (random_walk_incremental/main.cu:297-340,
+ *                                    random_walk_incremental/gpu_graph.cuh:135, 395-413)
+ *   dyg_decremental_batch        <- removeAndUpdateDelEdges + random_walk_decremental<<<>>>
+ *                                   + incrementalUpdateSparse + random_walk_small<<<>>>
+ *                                   + heuristicRecovery
+ *                                   (random_walk_decremental/gpu_graph.cuh:328-615,
+ *                                    random_walk_decremental/main.cu:77-290, 392-408)
+ *   dyg_decremental_stream       <- the decremental batch loop (random_walk_decremental/main.cu:388-444)
+ *   dyg_graph_export             <- saveCurrentMtx / save_added_edges data source
+ *                                   (random_walk_incremental/gpu_graph.cuh:427-454,
+ *                                    random_walk_decremental/gpu_graph.cuh:633-646)
+ *   dyg_last_error_string        <- HandleError / HRR printing (random_walk_incremental/gpu_graph.cuh:38-50,
+ *                                   random_walk_incremental/herror.h:1-11); errors are
+ *                                   returned, never exit().
+ *
+ * Conventions: the caller owns every host buffer; the library owns device
+ * graph state.  Array arguments may be host or device pointers (detected per
+ * call); with host outputs the call returns after the results are on the
+ * host.  A handle is not thread-safe; distinct handles are.  Calls are
+ * ordered on the given CUDA stream (NULL = legacy default stream).
+ * No torch types cross this boundary.
+ */
+#ifndef DYG_H
+#define DYG_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DYG_ABI_VERSION 1
+
+typedef enum dyg_status {
+    DYG_OK = 0,
+    DYG_EINVAL = 1,    /* bad argument (walkers not a multiple of 32, vertex id out of range, ...) */
+    DYG_ENOMEM = 2,    /* device or host allocation failed                                         */
+    DYG_ECUDA = 3,     /* a CUDA runtime call failed; see dyg_last_error_string()                  */
+    DYG_ERANGE = 4,    /* a result did not fit the caller's buffer                                 */
+    DYG_ESTATE = 5,    /* handle in an unusable state (previous device error)                      */
+    DYG_ENOTSUP = 6,   /* feature not supported on this device                                     */
+    DYG_EIO = 7        /* file I/O error (MTX reader/writer)                                       */
+} dyg_status;
+
+typedef struct dyg_graph dyg_graph;
+/* Same object as cudaStream_t. */
+typedef struct CUstream_st *dyg_stream_t;
+
+/* Transition rules for the walk. */
+#define DYG_TRANSITION_UNIFORM 0u   /* the reference's non-backtracking uniform choice */
+#define DYG_TRANSITION_WEIGHTED 1u  /* opt-in: weight-proportional, not reference parity */
+
+typedef struct dyg_walk_params {
+    float threshold;            /* distortion threshold (incremental)           */
+    uint32_t walkers;           /* walkers per edge: multiple of 32, <= 1024    */
+    uint32_t max_steps;         /* the reference's max_steps (default 100)      */
+    uint32_t transition;        /* DYG_TRANSITION_*                             */
+    uint32_t heuristic_walkers; /* decremental fallback walkers per endpoint (16) */
+    uint32_t flags;             /* reserved, 0                                  */
+    uint64_t seed;              /* Philox key                                   */
+} dyg_walk_params;
+
+typedef struct dyg_graph_opts {
+    uint32_t slack_per_row;     /* free slots reserved after each row (default 2)       */
+    uint32_t reserved;
+    double arena_headroom;      /* extra arena capacity as a fraction of slots (0.5)    */
+    int32_t device;             /* CUDA device ordinal, -1 = current device             */
+    int32_t pad;
+} dyg_graph_opts;
+
+/* Decremental status codes, per deletion (otherwise: path length >= 1). */
+#define DYG_DEL_NOT_IN_G (-3)  /* edge absent from G: skipped (gpu_graph.cuh:345-347)   */
+#define DYG_DEL_NOT_IN_H (-2)  /* removed from G only; H unchanged, no walk             */
+#define DYG_DEL_NO_PATH (-1)   /* no walker reached the other end: fallback recovery    */
+
+/* Kinds of recovered edges. */
+#define DYG_REC_PATH 0u
+#define DYG_REC_FALLBACK 1u
+
+const char *dyg_version(void);
+/* Message of the last failing call on this host thread ("" if none). */
+const char *dyg_last_error_string(void);
+void dyg_walk_params_default(dyg_walk_params *p);
+void dyg_graph_opts_default(dyg_graph_opts *o);
+/* Batch size the reference uses for a stream of n updates: ceil(n / 10)
+ * (random_walk_incremental/gpu_graph.cuh:135). */
+uint32_t dyg_reference_batch_size(uint32_t n);
+
+/* Build a device graph from an edge list in file order.  Rows keep the
+ * reference's order: line (s, d, w) appends d to row s, then s to row d
+ * (random_walk_incremental/functions.cpp:168-232).  Weights must be finite
+ * and > 0.  Host pointers only. */
+dyg_status dyg_graph_create_from_edges(uint32_t n_vertices, uint64_t n_edges,
+                                       const uint32_t *src, const uint32_t *dst,
+                                       const float *w, const dyg_graph_opts *opts,
+                                       dyg_graph **out);
+/* Deep copy on the same device (used to restore a snapshot). */
+dyg_status dyg_graph_clone(const dyg_graph *g, dyg_graph **out);
+/* Overwrite dst's rows with src's (same vertex count); stream-ordered. */
+dyg_status dyg_graph_copy_from(dyg_graph *dst, const dyg_graph *src, dyg_stream_t stream);
+dyg_status dyg_graph_destroy(dyg_graph *g);
+/* Vertex count, live directed slots, arena slots used / allocated. */
+dyg_status dyg_graph_info(const dyg_graph *g, uint32_t *n_vertices, uint64_t *n_slots,
+                          uint64_t *arena_used, uint64_t *arena_cap);
+/* Copy the rows to host CSR arrays: row_ptr[n+1], col/w[slot_cap]. */
+dyg_status dyg_graph_export(dyg_graph *g, uint64_t *row_ptr, uint32_t *col, float *w,
+                            uint64_t slot_cap);
+/* Repack rows into a fresh arena with the configured slack (stream-ordered). */
+dyg_status dyg_graph_compact(dyg_graph *g, dyg_stream_t stream);
+/* Walker moves (neighbour draws) executed on this handle since creation. */
+dyg_status dyg_graph_counters(const dyg_graph *g, uint64_t *walker_moves, uint64_t *walks);
+
+/* One incremental batch on the snapshot H: every edge is tested by
+ * p->walkers walks on the same H, then edges that no walker connected are
+ * appended to H in input order.  If G is not NULL every edge of the batch is
+ * appended to G too (G = dense graph after insertions).  Update ids
+ * first_update_id + e key the random streams.  Outputs (any may be NULL):
+ * found_at[e] = winner's step count or -1, conductance[e] = winner's 1/R,
+ * accepted[e] = 1 iff the edge was added to H. */
+dyg_status dyg_incremental_batch(dyg_graph *H, dyg_graph *G, const uint32_t *src,
+                                 const uint32_t *dst, const float *w, uint32_t n,
+                                 uint64_t first_update_id, const dyg_walk_params *p,
+                                 int32_t *found_at, float *conductance, uint8_t *accepted,
+                                 dyg_stream_t stream);
+/* The whole insertion stream in batches of batch_size (0 = the reference's
+ * ceil(n/10)); update ids are stream positions. */
+dyg_status dyg_incremental_stream(dyg_graph *H, dyg_graph *G, const uint32_t *src,
+                                  const uint32_t *dst, const float *w, uint32_t n,
+                                  uint32_t batch_size, const dyg_walk_params *p,
+                                  int32_t *found_at, float *conductance, uint8_t *accepted,
+                                  dyg_stream_t stream);
+
+/* One decremental batch: delete each edge from G (swap with the row's last
+ * slot, in input order), erase the ones also in H, walk G from min(u,v) to
+ * max(u,v), append the winning path's edges absent from H to H (in order),
+ * and run the 2-step fallback walks for edges without a path.
+ * status[e] = path length or DYG_DEL_*; conductance[e] = winner's 1/R.
+ * Recovered edges (x, y, kind) go to rec_src/rec_dst/rec_kind in commit
+ * order, at most rec_cap of them; *n_rec gets the total (DYG_ERANGE if it
+ * exceeds rec_cap; the graph update itself is complete). */
+dyg_status dyg_decremental_batch(dyg_graph *G, dyg_graph *H, const uint32_t *src,
+                                 const uint32_t *dst, uint32_t n, uint64_t first_update_id,
+                                 const dyg_walk_params *p, int32_t *status, float *conductance,
+                                 uint32_t *rec_src, uint32_t *rec_dst, uint8_t *rec_kind,
+                                 uint64_t rec_cap, uint64_t *n_rec, dyg_stream_t stream);
+dyg_status dyg_decremental_stream(dyg_graph *G, dyg_graph *H, const uint32_t *src,
+                                  const uint32_t *dst, uint32_t n, uint32_t batch_size,
+                                  const dyg_walk_params *p, int32_t *status, float *conductance,
+                                  uint32_t *rec_src, uint32_t *rec_dst, uint8_t *rec_kind,
+                                  uint64_t rec_cap, uint64_t *n_rec, dyg_stream_t stream);
+
+/* Kernel timing for benchmarks: while enabled, CUDA events are recorded on
+ * the launching stream around every walk-kernel launch of this process.
+ * dyg_profile_read synchronizes those events and returns the totals since
+ * the last reset (milliseconds, launches, walker moves are not split). */
+typedef struct dyg_profile {
+    double incr_walk_ms;
+    double decr_walk_ms;
+    double other_walk_ms;      /* winner replays and fallback walks */
+    uint64_t incr_walk_launches;
+    uint64_t decr_walk_launches;
+    uint64_t other_walk_launches;
+} dyg_profile;
+dyg_status dyg_profile_enable(int on);
+dyg_status dyg_profile_reset(void);
+dyg_status dyg_profile_read(dyg_profile *out);
+/* Number of this library's own kernel launches so far in this process. */
+uint64_t dyg_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

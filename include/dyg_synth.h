@@ -1,0 +1,52 @@
+/*
+ * dyg_synth.h -- seeded synthetic workloads for the update path.
+ *
+ * The reference's datasets (G2, fe_*, del*, ...) are downloaded from a
+ * private drive (datasetdownload.py) and are not available; these generators
+ * produce graphs with the shapes, sizes and weight distributions of the
+ * benchmark configurations instead.  Host-only; no device needed.
+ * Every generator is deterministic in its seed.
+ */
+#ifndef DYG_SYNTH_H
+#define DYG_SYNTH_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Weight distributions. */
+#define DYG_W_UNIFORM 0u     /* U[lo, hi)             */
+#define DYG_W_LOGUNIFORM 1u  /* 10^U[log10 lo, log10 hi) */
+
+/* Number of edges of an nx*ny*nz lattice with axis neighbours (nz = 1: 2-D). */
+uint64_t dyg_synth_lattice_edges(uint32_t nx, uint32_t ny, uint32_t nz);
+/* Lattice edges in vertex order, each vertex's +x, +y, +z edge in turn;
+ * v = x + nx*(y + ny*z). */
+void dyg_synth_lattice(uint32_t nx, uint32_t ny, uint32_t nz, uint32_t wdist, float lo, float hi,
+                       uint64_t seed, uint32_t *src, uint32_t *dst, float *w);
+
+/* Maximum-weight spanning forest (Kruskal, ties by edge index) plus
+ * floor(frac * #off-tree) off-tree edges chosen uniformly without
+ * replacement.  Selected edge indices are written in increasing order to
+ * out_idx (capacity m); returns their count. */
+uint64_t dyg_synth_sparsifier(uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst,
+                              const float *w, double frac, uint64_t seed, uint64_t *out_idx);
+
+/* `count` new edges on the lattice: u uniform, hop distance d uniform in
+ * [hop_lo, hop_hi], a lattice point at L1 distance d from u, rejecting pairs
+ * outside the lattice, already in the edge list (src, dst, m) or already
+ * drawn.  Returns the number produced (== count unless the lattice is too
+ * small). */
+uint64_t dyg_synth_lattice_inserts(uint32_t nx, uint32_t ny, uint32_t nz, uint64_t m,
+                                   const uint32_t *src, const uint32_t *dst, uint64_t count,
+                                   uint32_t hop_lo, uint32_t hop_hi, uint32_t wdist, float lo,
+                                   float hi, uint64_t seed, uint32_t *out_src, uint32_t *out_dst,
+                                   float *out_w);
+
+/* k distinct indices of [0, m) in uniformly random order. */
+void dyg_synth_sample(uint64_t m, uint64_t k, uint64_t seed, uint64_t *out_idx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,160 @@
+"""ctypes wrapper of the CPU oracle (oracle/_build/liboracle.so).
+
+TEST INFRASTRUCTURE: imported only by tests/, __graft_entry__.smoke() and
+the CPU-baseline leg of bench.py, as the checker or the timed host baseline.
+Its API mirrors dygrass_b200's so that parity tests read alike.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "liboracle.so")
+
+
+class Params(C.Structure):
+    _fields_ = [("threshold", C.c_float), ("walkers", C.c_uint32), ("max_steps", C.c_uint32),
+                ("transition", C.c_uint32), ("heuristic_walkers", C.c_uint32),
+                ("pad", C.c_uint32), ("seed", C.c_uint64)]
+
+    @classmethod
+    def from_walk_params(cls, p):
+        return cls(p.threshold, p.walkers, p.max_steps, p.transition, p.heuristic_walkers, 0,
+                   p.seed)
+
+
+_lib = None
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", HERE, "ORACLE_CC=gcc"], check=True)
+    return LIB
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = C.CDLL(LIB)
+        vp, u32, u64 = C.c_void_p, C.c_uint32, C.c_uint64
+        P = C.POINTER(Params)
+        sig = {
+            "orc_philox4x32_10": ([vp, vp, vp], None),
+            "orc_draw": ([u64, u64, u32, u32, u32], u32),
+            "orc_graph_from_edges": ([u32, u64, vp, vp, vp], vp),
+            "orc_graph_free": ([vp], None),
+            "orc_graph_num_vertices": ([vp], u32),
+            "orc_graph_num_slots": ([vp], u64),
+            "orc_graph_export": ([vp, vp, vp, vp], u64),
+            "orc_graph_has_edge": ([vp, u32, u32], C.c_int),
+            "orc_incremental_batch": ([vp, vp, vp, vp, vp, u32, u64, P, C.c_int, vp, vp, vp], u64),
+            "orc_incremental_stream": ([vp, vp, vp, vp, vp, u32, u32, P, C.c_int, vp, vp, vp], u64),
+            "orc_decremental_batch": ([vp, vp, vp, vp, u32, u64, P, C.c_int, vp, vp, vp, vp, vp, u64,
+                                       C.POINTER(u64)], u64),
+            "orc_decremental_stream": ([vp, vp, vp, vp, u32, u32, P, C.c_int, vp, vp, vp, vp, vp, u64,
+                                        C.POINTER(u64)], u64),
+            "orc_decremental_walk_path": ([vp, u32, u32, u64, u32, P, vp, C.POINTER(C.c_float)], C.c_int32),
+            "orc_max_threads": ([], C.c_int),
+        }
+        for name, (a, r) in sig.items():
+            f = getattr(L, name)
+            f.argtypes = a
+            f.restype = r
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+def philox(ctr, key):
+    c = np.ascontiguousarray(ctr, np.uint32)
+    k = np.ascontiguousarray(key, np.uint32)
+    out = np.zeros(4, np.uint32)
+    lib().orc_philox4x32_10(_p(c), _p(k), _p(out))
+    return out
+
+
+def draw(seed, uid, domain, walker, d) -> int:
+    return int(lib().orc_draw(seed, uid, domain, walker, d))
+
+
+def max_threads() -> int:
+    return int(lib().orc_max_threads())
+
+
+class OGraph:
+    def __init__(self, n, src, dst, w):
+        src = np.ascontiguousarray(src, np.uint32)
+        dst = np.ascontiguousarray(dst, np.uint32)
+        w = np.ascontiguousarray(w, np.float32)
+        self.h = lib().orc_graph_from_edges(int(n), len(src), _p(src), _p(dst), _p(w))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_graph_free(self.h)
+            self.h = None
+
+    def export(self):
+        n = lib().orc_graph_num_vertices(self.h)
+        s = lib().orc_graph_num_slots(self.h)
+        rp = np.zeros(n + 1, np.uint64)
+        col = np.zeros(max(s, 1), np.uint32)
+        w = np.zeros(max(s, 1), np.float32)
+        lib().orc_graph_export(self.h, _p(rp), _p(col), _p(w))
+        return rp, col[:s], w[:s]
+
+    def has_edge(self, a, b) -> bool:
+        return bool(lib().orc_graph_has_edge(self.h, a, b))
+
+
+def incremental(H: OGraph, src, dst, w, params, batch_size=0, G: OGraph | None = None,
+                threads=None, first_uid=0, single_batch=False):
+    """Returns (found_at, cond, accepted, walker_moves)."""
+    src = np.ascontiguousarray(src, np.uint32)
+    dst = np.ascontiguousarray(dst, np.uint32)
+    w = np.ascontiguousarray(w, np.float32)
+    n = len(src)
+    fa = np.empty(n, np.int32)
+    cd = np.empty(n, np.float32)
+    ac = np.empty(n, np.uint8)
+    P = Params.from_walk_params(params)
+    th = threads or max_threads()
+    if single_batch:
+        mv = lib().orc_incremental_batch(H.h, G.h if G else None, _p(src), _p(dst), _p(w), n,
+                                         first_uid, C.byref(P), th, _p(fa), _p(cd), _p(ac))
+    else:
+        mv = lib().orc_incremental_stream(H.h, G.h if G else None, _p(src), _p(dst), _p(w), n,
+                                          batch_size, C.byref(P), th, _p(fa), _p(cd), _p(ac))
+    return fa, cd, ac, int(mv)
+
+
+def decremental(G: OGraph, H: OGraph, src, dst, params, batch_size=0, threads=None,
+                first_uid=0, single_batch=False):
+    """Returns (status, cond, rec_src, rec_dst, rec_kind, walker_moves)."""
+    src = np.ascontiguousarray(src, np.uint32)
+    dst = np.ascontiguousarray(dst, np.uint32)
+    n = len(src)
+    cap = n * (params.max_steps + 4 * params.heuristic_walkers) + 16
+    st = np.empty(n, np.int32)
+    cd = np.empty(n, np.float32)
+    rx = np.empty(cap, np.uint32)
+    ry = np.empty(cap, np.uint32)
+    rk = np.empty(cap, np.uint8)
+    nr = C.c_uint64()
+    P = Params.from_walk_params(params)
+    th = threads or max_threads()
+    if single_batch:
+        mv = lib().orc_decremental_batch(G.h, H.h, _p(src), _p(dst), n, first_uid, C.byref(P), th,
+                                         _p(st), _p(cd), _p(rx), _p(ry), _p(rk), cap, C.byref(nr))
+    else:
+        mv = lib().orc_decremental_stream(G.h, H.h, _p(src), _p(dst), n, batch_size, C.byref(P), th,
+                                          _p(st), _p(cd), _p(rx), _p(ry), _p(rk), cap, C.byref(nr))
+    k = nr.value
+    return st, cd, rx[:k].copy(), ry[:k].copy(), rk[:k].copy(), int(mv)
