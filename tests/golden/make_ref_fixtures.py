@@ -42,20 +42,24 @@ def main(out_path):
         out = open(os.path.join(d, "updated_adj_sparse.mtx")).read() if cp.returncode == 0 else None
         lines = [ln for ln in cp.stdout.splitlines() if ln.startswith(("No path", "Edges added"))]
         result["incremental"][name] = {"returncode": cp.returncode, "updated_adj_sparse": out,
-                                       "summary": lines}
+                                       "summary": lines, "stderr_tail": cp.stderr[-400:]}
         print(name, cp.returncode, lines, flush=True)
     for name, case in kat_cases.DECREMENTAL.items():
         d = os.path.join(ds, name)
         kat_cases.write_decremental(case, d)
         cp = subprocess.run([os.path.join(REF, "decremental_update"), name], cwd=run,
                             capture_output=True, text=True, timeout=120)
+        # The reference writes added_edges.mtx and prints "Added edges saved
+        # to" before its teardown; its teardown can abort (heap damage from the
+        # out-of-range degree[v_max] write, random_walk_decremental/
+        # functions.cpp:123, 169), so the file is kept when it was completed.
         edges = None
-        if cp.returncode == 0:
-            edges = sorted([int(x) for x in ln.split()[:2]]
-                           for ln in open(os.path.join(d, "added_edges.mtx")) if ln.strip())
+        path = os.path.join(d, "added_edges.mtx")
+        if "Added edges saved to" in cp.stdout and os.path.exists(path):
+            edges = sorted([int(x) for x in ln.split()[:2]] for ln in open(path) if ln.strip())
         lines = [ln for ln in cp.stdout.splitlines() if ln.startswith(("Increased", "Density", "No path count"))]
         result["decremental"][name] = {"returncode": cp.returncode, "added_edges": edges,
-                                       "summary": lines}
+                                       "summary": lines, "stderr_tail": cp.stderr[-400:]}
         print(name, cp.returncode, edges, lines, flush=True)
     shutil.rmtree(scratch, ignore_errors=True)
     with open(out_path, "w") as f:

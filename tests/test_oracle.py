@@ -87,7 +87,11 @@ def test_decremental_known_answers(oracle, name):
 @pytest.mark.skipif(not os.path.exists(REF_KAT), reason="no reference outputs recorded")
 def test_oracle_matches_reference_outputs(oracle):
     ref = json.load(open(REF_KAT))
+    n_checked = 0
     for name, rec in ref["incremental"].items():
+        if rec.get("updated_adj_sparse") is None:
+            continue
+        n_checked += 1
         case = kat_cases.INCREMENTAL[name]
         n, hs, hd, hw, es, ed, ew = incr_inputs(case)
         H = oracle.OGraph(n, hs, hd, hw)
@@ -95,6 +99,9 @@ def test_oracle_matches_reference_outputs(oracle):
                                                            walkers=case["walkers"]))
         assert updated_sparse_text(hs, hd, hw, es, ed, ew, ac) == rec["updated_adj_sparse"], name
     for name, rec in ref["decremental"].items():
+        if rec.get("added_edges") is None:
+            continue
+        n_checked += 1
         case = kat_cases.DECREMENTAL[name]
         n, gs, gd, gw, hs, hd, hw, ds, dd = decr_inputs(case)
         G = oracle.OGraph(n, gs, gd, gw)
@@ -102,6 +109,7 @@ def test_oracle_matches_reference_outputs(oracle):
         _, _, rx, ry, rk, _ = oracle.decremental(G, H, ds, dd, P())
         got = sorted((int(min(a, b)) + 1, int(max(a, b)) + 1) for a, b, k in zip(rx, ry, rk) if k == 0)
         assert got == sorted(tuple(e) for e in rec["added_edges"]), name
+    assert n_checked >= len(kat_cases.INCREMENTAL)
 
 
 def test_snapshot_vs_sequential(oracle):
