@@ -109,6 +109,8 @@ def lib() -> C.CDLL:
         "dyg_profile_reset": ([], C.c_int),
         "dyg_profile_read": ([C.POINTER(Profile)], C.c_int),
         "dyg_kernel_launches": ([], u64),
+        "dyg_incremental_walk_noalloc": ([vp, vp, vp, vp, u32, u64, C.POINTER(WalkParams), vp, vp, vp, vp],
+                                         C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

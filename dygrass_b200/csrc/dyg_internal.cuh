@@ -196,6 +196,9 @@ struct WalkJob {
 };
 dyg_status launch_walk(dyg_graph *G, const WalkJob &job, const dyg_walk_params &p, bool incremental,
                        unsigned long long *keys, cudaStream_t st);
+dyg_status launch_walk_scalars(const DevGraph &g, const WalkJob &job, const dyg_walk_params &p,
+                               bool incremental, unsigned long long *keys,
+                               unsigned long long *scalars, cudaStream_t st);
 dyg_status launch_winner_paths(dyg_graph *G, const WalkJob &job, const dyg_walk_params &p,
                                const unsigned long long *keys, uint32_t n_max, uint32_t path_stride,
                                uint32_t *path_v, float *path_w, int32_t *path_len, cudaStream_t st);

@@ -386,6 +386,45 @@ dyg_status launch_walk(dyg_graph *G, const WalkJob &job, const dyg_walk_params &
     return DYG_OK;
 }
 
+// Same launch as launch_walk, with the kernel's counters (work chunks,
+// error bits, move counts) at `scalars` instead of the handle's workspace, and
+// without profiling events.
+dyg_status launch_walk_scalars(const DevGraph &g, const WalkJob &job, const dyg_walk_params &p,
+                               bool incremental, unsigned long long *keys,
+                               unsigned long long *scalars, cudaStream_t st) {
+    WalkArgs a;
+    a.g = g;
+    a.job = job;
+    a.walkers = p.walkers;
+    a.max_steps = p.max_steps;
+    a.threshold = p.threshold;
+    a.key = make_uint2((uint32_t)p.seed, (uint32_t)(p.seed >> 32));
+    a.keys = keys;
+    a.scalars = scalars;
+    const bool wtd = p.transition == DYG_TRANSITION_WEIGHTED;
+    int grid;
+    if (incremental) {
+        if (wtd) {
+            grid = persistent_blocks(k_walk<true, true>);
+            k_walk<true, true><<<grid, kWalkThreads, 0, st>>>(a);
+        } else {
+            grid = persistent_blocks(k_walk<true, false>);
+            k_walk<true, false><<<grid, kWalkThreads, 0, st>>>(a);
+        }
+    } else {
+        if (wtd) {
+            grid = persistent_blocks(k_walk<false, true>);
+            k_walk<false, true><<<grid, kWalkThreads, 0, st>>>(a);
+        } else {
+            grid = persistent_blocks(k_walk<false, false>);
+            k_walk<false, false><<<grid, kWalkThreads, 0, st>>>(a);
+        }
+    }
+    count_launch();
+    DYG_CUDA(cudaGetLastError());
+    return DYG_OK;
+}
+
 dyg_status launch_winner_paths(dyg_graph *G, const WalkJob &job, const dyg_walk_params &p,
                                const unsigned long long *keys, uint32_t n_max, uint32_t stride,
                                uint32_t *path_v, float *path_w, int32_t *path_len, cudaStream_t st) {

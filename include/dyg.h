@@ -165,6 +165,28 @@ dyg_status dyg_decremental_stream(dyg_graph *G, dyg_graph *H, const uint32_t *sr
                                   uint32_t *rec_src, uint32_t *rec_dst, uint8_t *rec_kind,
                                   uint64_t rec_cap, uint64_t *n_rec, dyg_stream_t stream);
 
+/* No counterpart in the reference.  Incremental walk decision for one batch
+ * (found_at / conductance / accepted exactly as dyg_incremental_batch reports
+ * them for the same H and update ids) without any device allocation, for
+ * callers that cannot call cudaMalloc: a serving loop that reserves its device
+ * memory at start-up and allows no allocation afterwards, or a plugin inside a
+ * host framework that owns all device allocations.  Accepted edges are NOT
+ * appended to H.  All array arguments must be device pointers; found_at is -2
+ * for an edge whose endpoint is not a vertex of H.  Scratch lives in a static
+ * device array of DYG_NOALLOC_MAX_EDGES 64-bit keys (512 KiB) plus counters,
+ * held by every device that loads the library until exit; batches larger than
+ * DYG_NOALLOC_MAX_EDGES are rejected with DYG_EINVAL.  Calls share that array:
+ * calls that overlap on the GPU race and must be serialized by the caller.
+ * The first call on a device looks up the array's address (set-up); make it
+ * before any stream capture.  Stream-ordered; returns before the results are
+ * ready. */
+#define DYG_NOALLOC_MAX_EDGES 65536u
+dyg_status dyg_incremental_walk_noalloc(const dyg_graph *H, const uint32_t *src,
+                                        const uint32_t *dst, const float *w, uint32_t n,
+                                        uint64_t first_update_id, const dyg_walk_params *p,
+                                        int32_t *found_at, float *conductance,
+                                        uint8_t *accepted, dyg_stream_t stream);
+
 /* Kernel timing for benchmarks: while enabled, CUDA events are recorded on
  * the launching stream around every walk-kernel launch of this process.
  * dyg_profile_read synchronizes those events and returns the totals since
