@@ -25,6 +25,7 @@ STATUS_NAMES = {0: "DYG_OK", 1: "DYG_EINVAL", 2: "DYG_ENOMEM", 3: "DYG_ECUDA", 4
                 5: "DYG_ESTATE", 6: "DYG_ENOTSUP", 7: "DYG_EIO"}
 TRANSITION_UNIFORM = 0
 TRANSITION_WEIGHTED = 1
+FLAG_EXHAUSTIVE = 1
 DEL_NOT_IN_G = -3
 DEL_NOT_IN_H = -2
 DEL_NO_PATH = -1
@@ -46,9 +47,9 @@ class WalkParams(C.Structure):
 
     @classmethod
     def make(cls, threshold=100.0, walkers=512, max_steps=100, transition=TRANSITION_UNIFORM,
-             heuristic_walkers=16, seed=20251203):
+             heuristic_walkers=16, seed=20251203, flags=0):
         return cls(float(threshold), int(walkers), int(max_steps), int(transition),
-                   int(heuristic_walkers), 0, int(seed))
+                   int(heuristic_walkers), int(flags), int(seed))
 
 
 class Profile(C.Structure):

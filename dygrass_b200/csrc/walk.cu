@@ -80,6 +80,7 @@ struct WalkArgs {
     DevGraph g;
     WalkJob job;
     uint32_t walkers, max_steps;
+    uint32_t prune;
     float threshold;
     uint2 key;
     unsigned long long *keys;
@@ -164,6 +165,10 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(WalkArgs a) {
 
     uint32_t ce = 0, c_next = 0, c_end = 0;  // warp-uniform: current edge chunk
     bool exhausted = false;
+    // Best conductance bits found so far for the current chunk's edge and the
+    // previous one (warp-uniform).  Every walker of an edge runs in this warp.
+    uint32_t ce_best = 0u, pe = 0xFFFFFFFFu, pe_best = 0u;
+    uint32_t my_e = 0xFFFFFFFFu;
 
     bool active = false;
     Walker s;
@@ -187,7 +192,10 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(WalkArgs a) {
                     exhausted = true;
                     break;
                 }
+                pe = ce;
+                pe_best = ce_best;
                 ce = (uint32_t)c;
+                ce_best = 0u;
                 c_next = 0u;
                 c_end = W;
             }
@@ -201,6 +209,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(WalkArgs a) {
                     best_e = e;
                 }
                 s.walker = c_next + rank;
+                my_e = e;
                 s.cur = a.job.src[e];
                 s.tgt = a.job.dst[e];
                 s.we = INCR ? a.job.w[e] : 0.f;
@@ -222,6 +231,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(WalkArgs a) {
             c_next += take;
         }
         if (!__any_sync(kFull, active)) break;
+        uint32_t fc = 0u;  // conductance bits of a walker that found its target now
         if (active) {
             bool moved;
             uint2 taken;
@@ -230,11 +240,28 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(WalkArgs a) {
             moves += moved ? 1u : 0u;
             if (r != kContinue) {
                 if (r == kFound) {
-                    const unsigned long long k = pack_key(__frcp_rn(s.R), s.walker, s.step);
+                    const float cond = __frcp_rn(s.R);
+                    fc = __float_as_uint(cond);
+                    const unsigned long long k = pack_key(cond, s.walker, s.step);
                     if (k > best) best = k;
                 }
                 active = false;
                 ++walks;
+            }
+        }
+        if (a.prune) {
+            // R only grows along a walk and 1/R is monotone, so a walker whose
+            // 1/R is already below its edge's best success can neither win
+            // nor tie: stopping it leaves every result unchanged.
+            ce_best = max(ce_best, __reduce_max_sync(kFull, (fc && my_e == ce) ? fc : 0u));
+            pe_best = max(pe_best, __reduce_max_sync(kFull, (fc && my_e == pe) ? fc : 0u));
+            if (active) {
+                const uint32_t known = (my_e == ce) ? ce_best
+                                     : (my_e == pe ? pe_best : (uint32_t)(best >> 32));
+                if (known && __frcp_rn(s.R) < __uint_as_float(known)) {
+                    active = false;
+                    ++walks;
+                }
             }
         }
     }
@@ -353,6 +380,7 @@ dyg_status launch_walk(dyg_graph *G, const WalkJob &job, const dyg_walk_params &
     a.job = job;
     a.walkers = p.walkers;
     a.max_steps = p.max_steps;
+    a.prune = (p.flags & DYG_FLAG_EXHAUSTIVE) ? 0u : 1u;
     a.threshold = p.threshold;
     a.key = make_uint2((uint32_t)p.seed, (uint32_t)(p.seed >> 32));
     a.keys = keys;
@@ -397,6 +425,7 @@ dyg_status launch_walk_scalars(const DevGraph &g, const WalkJob &job, const dyg_
     a.job = job;
     a.walkers = p.walkers;
     a.max_steps = p.max_steps;
+    a.prune = (p.flags & DYG_FLAG_EXHAUSTIVE) ? 0u : 1u;
     a.threshold = p.threshold;
     a.key = make_uint2((uint32_t)p.seed, (uint32_t)(p.seed >> 32));
     a.keys = keys;

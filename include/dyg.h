@@ -66,13 +66,20 @@ typedef struct CUstream_st *dyg_stream_t;
 #define DYG_TRANSITION_UNIFORM 0u   /* the reference's non-backtracking uniform choice */
 #define DYG_TRANSITION_WEIGHTED 1u  /* opt-in: weight-proportional, not reference parity */
 
+/* dyg_walk_params.flags bits.  By default a walker stops as soon as its 1/R
+ * falls below the best success of its edge: it can then neither win nor tie,
+ * so every result is unchanged and only the walker-move count drops.
+ * DYG_FLAG_EXHAUSTIVE runs every walker to its natural end, as the
+ * reference does. */
+#define DYG_FLAG_EXHAUSTIVE 1u
+
 typedef struct dyg_walk_params {
     float threshold;            /* distortion threshold (incremental)           */
     uint32_t walkers;           /* walkers per edge: multiple of 32, <= 1024    */
     uint32_t max_steps;         /* the reference's max_steps (default 100)      */
     uint32_t transition;        /* DYG_TRANSITION_*                             */
     uint32_t heuristic_walkers; /* decremental fallback walkers per endpoint (16) */
-    uint32_t flags;             /* reserved, 0                                  */
+    uint32_t flags;             /* DYG_FLAG_* bits (0 = default)                */
     uint64_t seed;              /* Philox key                                   */
 } dyg_walk_params;
 

@@ -86,9 +86,17 @@ def test_grid_100x100_full(dyg, oracle):
     H, Ho, r, mv = run_incr_both(dyg, oracle, W.n, W.h_src, W.h_dst, W.h_w, W.ins_src, W.ins_dst,
                                  W.ins_w, W.params, with_g=(W.g_src, W.g_dst, W.g_w))
     moves, walks = H.counters()
-    assert moves == mv
     assert walks == len(W.ins_src) * W.params.walkers
+    assert 0 < moves < mv          # pruned walkers stop early; results are unchanged
     assert 0 < r.accepted.sum() < len(r.accepted)
+    # exhaustive mode executes exactly the oracle's walker moves
+    pe = dyg.WalkParams.make(threshold=W.params.threshold, walkers=W.params.walkers,
+                             max_steps=W.params.max_steps, seed=W.params.seed,
+                             flags=dyg.FLAG_EXHAUSTIVE)
+    H2, _, r2, mv2 = run_incr_both(dyg, oracle, W.n, W.h_src, W.h_dst, W.h_w, W.ins_src, W.ins_dst,
+                                   W.ins_w, pe)
+    assert H2.counters()[0] == mv2 == mv
+    assert np.array_equal(r2.accepted, r.accepted)
 
 
 @pytest.mark.parametrize("walkers", [32, 96, 160, 1024])
@@ -175,6 +183,27 @@ def test_mesh_incremental_then_decremental(dyg, oracle):
     same_graph(G, Go)
     same_graph(H, Ho)
     assert (st > 0).sum() > 0 and (st == -2).sum() > 0
+
+
+def test_mesh_exhaustive_and_pruned_agree(dyg, oracle):
+    """Pruning changes only how many moves run, never a result."""
+    W = small_mesh(k=10, inserts=300)
+    outs = []
+    for flags in (0, dyg.FLAG_EXHAUSTIVE):
+        p = dyg.WalkParams.make(threshold=W.params.threshold, walkers=W.params.walkers,
+                                max_steps=W.params.max_steps, seed=W.params.seed, flags=flags)
+        dp = dyg.WalkParams.make(walkers=W.dparams.walkers, max_steps=W.dparams.max_steps,
+                                 seed=W.dparams.seed, flags=flags)
+        H = dyg.Graph.from_edges(W.n, W.h_src, W.h_dst, W.h_w)
+        G = dyg.Graph.from_edges(W.n, W.g_src, W.g_dst, W.g_w)
+        r = dyg.incremental_stream(H, W.ins_src, W.ins_dst, W.ins_w, p, G=G)
+        d = dyg.decremental_stream(G, H, W.del_src, W.del_dst, dp)
+        outs.append((r.found_at.tobytes(), r.conductance.tobytes(), d.status.tobytes(),
+                     d.conductance.tobytes(), d.rec_src.tobytes(), d.rec_dst.tobytes(),
+                     H.export()[1].tobytes(), G.export()[1].tobytes(),
+                     H.counters()[0] + G.counters()[0]))
+    assert outs[0][:-1] == outs[1][:-1]
+    assert outs[0][-1] < outs[1][-1]
 
 
 def test_decremental_fallback_path(dyg, oracle):
