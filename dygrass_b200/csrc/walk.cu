@@ -16,6 +16,8 @@
 // Philox4x32-10({d>>2, k, u_lo, u_hi | domain<<24}, seed): any walker can be
 // replayed, which is how the decremental winner's path is recovered without
 // the reference's per-thread path[100] arrays.
+#include <stdlib.h>
+
 #include <mutex>
 #include <vector>
 
@@ -81,6 +83,7 @@ struct WalkArgs {
     WalkJob job;
     uint32_t walkers, max_steps;
     uint32_t prune;
+    uint32_t chunk;   // walkers handed to a warp at a time
     float threshold;
     uint2 key;
     unsigned long long *keys;
@@ -160,25 +163,27 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(WalkArgs a) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
     const uint32_t n = a.job.n_dev ? *a.job.n_dev : a.job.n_host;
-    const uint32_t W = a.walkers;
+    const uint32_t CW = a.chunk;                // walkers per chunk (divides walkers)
+    const uint32_t cpe = a.walkers / CW;        // chunks per edge
+    const unsigned long long n_chunks = (unsigned long long)n * cpe;
     unsigned long long *work = a.scalars + S_WORK;
 
-    uint32_t ce = 0, c_next = 0, c_end = 0;  // warp-uniform: current edge chunk
+    // warp-uniform: the edge and walker range of the current chunk
+    uint32_t ce = 0xFFFFFFFFu, c_next = 0u, c_end = 0u;
     bool exhausted = false;
-    // Best conductance bits found so far for the current chunk's edge and the
-    // previous one (warp-uniform).  Every walker of an edge runs in this warp.
+    // best conductance bits seen in this warp for the current chunk's edge and
+    // the previous one (warp-uniform)
     uint32_t ce_best = 0u, pe = 0xFFFFFFFFu, pe_best = 0u;
-    uint32_t my_e = 0xFFFFFFFFu;
 
     bool active = false;
+    uint32_t my_e = 0xFFFFFFFFu;
+    uint32_t gbest = 0u;  // lane: last read of the edge's global best (cond bits)
     Walker s;
     s.cur = s.prev = s.step = s.tgt = s.walker = s.c2 = s.c3 = 0u;
     s.rblk = 0xFFFFFFFFu;
     s.rbuf = make_uint4(0u, 0u, 0u, 0u);
     s.R = 0.f;
     s.we = 0.f;
-    unsigned long long best = 0ull;
-    uint32_t best_e = 0xFFFFFFFFu;
     uint32_t moves = 0u, walks = 0u;
 
     while (true) {
@@ -188,28 +193,26 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(WalkArgs a) {
                 unsigned long long c = 0ull;
                 if (lane == 0u) c = atomicAdd(work, 1ull);
                 c = __shfl_sync(kFull, c, 0);
-                if (c >= (unsigned long long)n) {
+                if (c >= n_chunks) {
                     exhausted = true;
                     break;
                 }
-                pe = ce;
-                pe_best = ce_best;
-                ce = (uint32_t)c;
-                ce_best = 0u;
-                c_next = 0u;
-                c_end = W;
+                const uint32_t e = (uint32_t)(c / cpe);
+                if (e != ce) {
+                    pe = ce;
+                    pe_best = ce_best;
+                    ce = e;
+                    ce_best = 0u;
+                }
+                c_next = (uint32_t)(c - (unsigned long long)e * cpe) * CW;
+                c_end = c_next + CW;
             }
             const uint32_t take = min((uint32_t)__popc(free_mask), c_end - c_next);
             const uint32_t rank = __popc(free_mask & lt_mask);
             if (((free_mask >> lane) & 1u) && rank < take) {
                 const uint32_t e = ce;
-                if (best_e != e) {
-                    if (best) atomicMax(a.keys + best_e, best);
-                    best = 0ull;
-                    best_e = e;
-                }
-                s.walker = c_next + rank;
                 my_e = e;
+                s.walker = c_next + rank;
                 s.cur = a.job.src[e];
                 s.tgt = a.job.dst[e];
                 s.we = INCR ? a.job.w[e] : 0.f;
@@ -220,6 +223,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(WalkArgs a) {
                 s.step = 1u;
                 s.R = 0.f;
                 s.prev = 0u;
+                gbest = a.prune ? (uint32_t)(*(volatile unsigned long long *)(a.keys + e) >> 32) : 0u;
                 if (s.cur >= a.g.n || s.tgt >= a.g.n) {
                     atomicOr(a.scalars + S_ERR, (unsigned long long)kErrVertex);
                     ++walks;
@@ -242,8 +246,9 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(WalkArgs a) {
                 if (r == kFound) {
                     const float cond = __frcp_rn(s.R);
                     fc = __float_as_uint(cond);
-                    const unsigned long long k = pack_key(cond, s.walker, s.step);
-                    if (k > best) best = k;
+                    // published at once, so walkers of this edge in other warps
+                    // can stop early
+                    atomicMax(a.keys + my_e, pack_key(cond, s.walker, s.step));
                 }
                 active = false;
                 ++walks;
@@ -256,8 +261,10 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(WalkArgs a) {
             ce_best = max(ce_best, __reduce_max_sync(kFull, (fc && my_e == ce) ? fc : 0u));
             pe_best = max(pe_best, __reduce_max_sync(kFull, (fc && my_e == pe) ? fc : 0u));
             if (active) {
-                const uint32_t known = (my_e == ce) ? ce_best
-                                     : (my_e == pe ? pe_best : (uint32_t)(best >> 32));
+                if ((s.step & 3u) == 0u)
+                    gbest = max(gbest, (uint32_t)(*(volatile unsigned long long *)(a.keys + my_e) >> 32));
+                const uint32_t known = max(gbest, (my_e == ce) ? ce_best
+                                                  : (my_e == pe ? pe_best : 0u));
                 if (known && __frcp_rn(s.R) < __uint_as_float(known)) {
                     active = false;
                     ++walks;
@@ -265,7 +272,6 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(WalkArgs a) {
             }
         }
     }
-    if (best) atomicMax(a.keys + best_e, best);
     const uint32_t wm = __reduce_add_sync(kFull, moves);
     const uint32_t ww = __reduce_add_sync(kFull, walks);
     if (lane == 0u) {
@@ -361,6 +367,21 @@ __global__ void k_fallback(DevGraph g, const uint32_t *f_src, const uint32_t *f_
     cw[2 * i + 1] = w2;
 }
 
+// Walkers handed to a warp at a time: 32 by default, so that the 512 walks
+// of an edge nobody connects spread over 16 warps instead of running as 16
+// waves on one.  DYG_WALK_CHUNK (a multiple of 32 dividing the walker count)
+// overrides it for tuning sweeps.
+static uint32_t chunk_for(uint32_t walkers) {
+    static int env = -1;
+    if (env < 0) {
+        const char *v = getenv("DYG_WALK_CHUNK");
+        env = v ? atoi(v) : 0;
+    }
+    uint32_t c = 32u;
+    if (env > 0 && env % 32 == 0 && walkers % (uint32_t)env == 0) c = (uint32_t)env;
+    return c;
+}
+
 template <typename K>
 static int persistent_blocks(K kernel) {
     static int cached = 0;
@@ -381,6 +402,7 @@ dyg_status launch_walk(dyg_graph *G, const WalkJob &job, const dyg_walk_params &
     a.walkers = p.walkers;
     a.max_steps = p.max_steps;
     a.prune = (p.flags & DYG_FLAG_EXHAUSTIVE) ? 0u : 1u;
+    a.chunk = chunk_for(p.walkers);
     a.threshold = p.threshold;
     a.key = make_uint2((uint32_t)p.seed, (uint32_t)(p.seed >> 32));
     a.keys = keys;
@@ -426,6 +448,7 @@ dyg_status launch_walk_scalars(const DevGraph &g, const WalkJob &job, const dyg_
     a.walkers = p.walkers;
     a.max_steps = p.max_steps;
     a.prune = (p.flags & DYG_FLAG_EXHAUSTIVE) ? 0u : 1u;
+    a.chunk = chunk_for(p.walkers);
     a.threshold = p.threshold;
     a.key = make_uint2((uint32_t)p.seed, (uint32_t)(p.seed >> 32));
     a.keys = keys;
