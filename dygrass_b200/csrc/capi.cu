@@ -359,6 +359,7 @@ void free_graph(dyg_graph *G) {
     if (G->g.desc) cudaFree(G->g.desc);
     if (G->g.cap) cudaFree(G->g.cap);
     if (G->g.slots) cudaFree(G->g.slots);
+    if (G->g.wts) cudaFree(G->g.wts);
     cudaGetLastError();
     delete G;
 }
@@ -380,6 +381,8 @@ dyg_status incremental_batch_dev(dyg_graph *H, dyg_graph *G, const uint32_t *src
     DYG_TRY(ensure(ws.hw, sizeof(float) * (size_t)n * 2));
     unsigned long long *keys = ptr<unsigned long long>(ws.keys);
     DYG_CUDA(cudaMemsetAsync(keys, 0, sizeof(unsigned long long) * n, st));
+    // unused entries of the accepted half-edge list stay 0xFFFFFFFF (ignored)
+    DYG_CUDA(cudaMemsetAsync(ws.hx.p, 0xFF, sizeof(uint32_t) * (size_t)n * 2, st));
     WalkJob job{src, dst, w, nullptr, (unsigned long long)uid0, nullptr, n, kDomainIncr};
     DYG_TRY(launch_walk(H, job, p, true, keys, st));
     k_incr_decode<<<blocks(n, 256), 256, 0, st>>>(keys, n, ptr<int32_t>(ws.out_found),
@@ -393,19 +396,26 @@ dyg_status incremental_batch_dev(dyg_graph *H, dyg_graph *G, const uint32_t *src
                                                   ptr<uint32_t>(ws.counts) + C_ACCEPTED);
     count_launch();
     DYG_CUDA(cudaGetLastError());
-    DYG_TRY(check_device_errors(H, st));
-    const uint32_t acc = ws.host_counts[C_ACCEPTED];
-    DYG_TRY(commit_append(H, ptr<uint32_t>(ws.hx), ptr<uint32_t>(ws.hy), ptr<float>(ws.hw),
-                          2u * acc, st));
+    // both commits are sized by the upper bound 2n, so one synchronize serves
+    // the error check and both arena checks
+    DYG_TRY(commit_prepare(H, ptr<uint32_t>(ws.hx), 2u * n, st));
     if (G) {
+        Workspace &wg = G->ws;
+        DYG_TRY(ensure(wg.hx, sizeof(uint32_t) * (size_t)n * 2));
+        DYG_TRY(ensure(wg.hy, sizeof(uint32_t) * (size_t)n * 2));
+        DYG_TRY(ensure(wg.hw, sizeof(float) * (size_t)n * 2));
         k_half_edges<<<blocks(n, 256), 256, 0, st>>>(src, dst, w, n, nullptr, nullptr,
-                                                      ptr<uint32_t>(ws.hx), ptr<uint32_t>(ws.hy),
-                                                      ptr<float>(ws.hw), nullptr);
+                                                      ptr<uint32_t>(wg.hx), ptr<uint32_t>(wg.hy),
+                                                      ptr<float>(wg.hw), nullptr);
         count_launch();
         DYG_CUDA(cudaGetLastError());
-        DYG_TRY(commit_append(G, ptr<uint32_t>(ws.hx), ptr<uint32_t>(ws.hy), ptr<float>(ws.hw),
-                              2u * n, st));
+        DYG_TRY(commit_prepare(G, ptr<uint32_t>(wg.hx), 2u * n, st));
     }
+    DYG_TRY(read_scalars2(H, G, st));
+    const unsigned long long err = ws.host_scalars[S_ERR];
+    if (err) DYG_TRY(check_device_errors(H, st));
+    DYG_TRY(commit_finish(H, ptr<uint32_t>(ws.hy), ptr<float>(ws.hw), 2u * n, st));
+    if (G) DYG_TRY(commit_finish(G, ptr<uint32_t>(G->ws.hy), ptr<float>(G->ws.hw), 2u * n, st));
     return DYG_OK;
 }
 
@@ -658,19 +668,26 @@ dyg_status dyg_graph_copy_from(dyg_graph *dst, const dyg_graph *src, dyg_stream_
     const unsigned long long top = s->ws.host_scalars[S_TOP];
     if (dst->g.arena_cap < top) {
         uint2 *ns = nullptr;
-        if (cudaMalloc(&ns, sizeof(uint2) * (size_t)src->g.arena_cap) != cudaSuccess) {
+        float *nw = nullptr;
+        if (cudaMalloc(&ns, sizeof(uint2) * (size_t)src->g.arena_cap) != cudaSuccess ||
+            cudaMalloc(&nw, sizeof(float) * (size_t)src->g.arena_cap) != cudaSuccess) {
             cudaGetLastError();
+            if (ns) cudaFree(ns);
             set_error("cudaMalloc in copy_from failed");
             return DYG_ENOMEM;
         }
         DYG_CUDA(cudaFree(dst->g.slots));
+        DYG_CUDA(cudaFree(dst->g.wts));
         dst->g.slots = ns;
+        dst->g.wts = nw;
         dst->g.arena_cap = src->g.arena_cap;
     }
     const uint32_t n = src->g.n;
     DYG_CUDA(cudaMemcpyAsync(dst->g.desc, src->g.desc, sizeof(uint2) * n, cudaMemcpyDeviceToDevice, st));
     DYG_CUDA(cudaMemcpyAsync(dst->g.cap, src->g.cap, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st));
     DYG_CUDA(cudaMemcpyAsync(dst->g.slots, src->g.slots, sizeof(uint2) * (size_t)top,
+                             cudaMemcpyDeviceToDevice, st));
+    DYG_CUDA(cudaMemcpyAsync(dst->g.wts, src->g.wts, sizeof(float) * (size_t)top,
                              cudaMemcpyDeviceToDevice, st));
     DYG_CUDA(cudaMemcpyAsync(dst->g.top, src->g.top, sizeof(unsigned long long),
                              cudaMemcpyDeviceToDevice, st));
@@ -696,7 +713,8 @@ dyg_status dyg_graph_clone(const dyg_graph *g, dyg_graph **out) {
     if (rc == DYG_OK &&
         (cudaMalloc(&G->g.desc, sizeof(uint2) * (size_t)(g->g.n ? g->g.n : 1)) != cudaSuccess ||
          cudaMalloc(&G->g.cap, sizeof(uint32_t) * (size_t)(g->g.n ? g->g.n : 1)) != cudaSuccess ||
-         cudaMalloc(&G->g.slots, sizeof(uint2) * (size_t)g->g.arena_cap) != cudaSuccess)) {
+         cudaMalloc(&G->g.slots, sizeof(uint2) * (size_t)g->g.arena_cap) != cudaSuccess ||
+         cudaMalloc(&G->g.wts, sizeof(float) * (size_t)g->g.arena_cap) != cudaSuccess)) {
         cudaGetLastError();
         set_error("cudaMalloc in clone failed");
         rc = DYG_ENOMEM;
@@ -767,15 +785,17 @@ dyg_status dyg_graph_export(dyg_graph *g, uint64_t *row_ptr, uint32_t *col, floa
     const uint32_t n = g->g.n;
     uint2 *hd = (uint2 *)malloc(sizeof(uint2) * (size_t)(n ? n : 1));
     uint2 *hs = (uint2 *)malloc(sizeof(uint2) * (size_t)(top ? top : 1));
-    if (!hd || !hs) {
-        free(hd); free(hs);
+    float *hw = (float *)malloc(sizeof(float) * (size_t)(top ? top : 1));
+    if (!hd || !hs || !hw) {
+        free(hd); free(hs); free(hw);
         set_error("host allocation failed");
         return DYG_ENOMEM;
     }
     cudaError_t e = cudaMemcpy(hd, g->g.desc, sizeof(uint2) * n, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(hs, g->g.slots, sizeof(uint2) * (size_t)top, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(hw, g->g.wts, sizeof(float) * (size_t)top, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) {
-        free(hd); free(hs);
+        free(hd); free(hs); free(hw);
         return cuda_fail(e, "export", __FILE__, __LINE__);
     }
     uint64_t o = 0;
@@ -784,9 +804,8 @@ dyg_status dyg_graph_export(dyg_graph *g, uint64_t *row_ptr, uint32_t *col, floa
         row_ptr[v] = o;
         for (uint32_t j = 0; j < hd[v].y; ++j) {
             if (o + j < slot_cap) {
-                const uint2 s = hs[hd[v].x + j];
-                if (col) col[o + j] = s.x;
-                if (w) memcpy(&w[o + j], &s.y, 4);
+                if (col) col[o + j] = hs[hd[v].x + j].x;
+                if (w) w[o + j] = hw[hd[v].x + j];
             } else {
                 rc = DYG_ERANGE;
             }
@@ -796,6 +815,7 @@ dyg_status dyg_graph_export(dyg_graph *g, uint64_t *row_ptr, uint32_t *col, floa
     row_ptr[n] = o;
     free(hd);
     free(hs);
+    free(hw);
     if (rc != DYG_OK) set_error("slot_cap smaller than the number of slots");
     return rc;
 }

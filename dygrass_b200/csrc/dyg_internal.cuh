@@ -6,9 +6,15 @@
 //             row start and its live length.
 //   cap[v]    u32 row capacity (slots reserved at `offset`), touched only by
 //             commits and compaction, never by walkers.
-//   slots[i]  uint2 {column, weight bits}: the neighbour id and its weight
-//             arrive in one 8-byte load (the reference stores them degree
-//             floats apart through a pointer table, gpu_graph.cuh:205-235).
+//   slots[i]  uint2 {column, bits of 1/weight}: the neighbour id and the
+//             resistance a walker adds arrive in one 8-byte load (the
+//             reference stores them degree floats apart through a pointer
+//             table, gpu_graph.cuh:205-235).  1/w is the correctly rounded
+//             float reciprocal, so R += 1/w is bit-identical to dividing on
+//             every move.
+//   wts[i]    f32 weight of slot i (same offsets as slots); read by exports,
+//             recovered edges and the weight-proportional mode, never by the
+//             uniform walk.
 //   top       arena bump pointer; rows that outgrow their capacity move to
 //             [top, top + new_cap) and leave a hole reclaimed by compaction.
 #pragma once
@@ -35,6 +41,7 @@ struct DevGraph {
     uint2 *desc;
     uint32_t *cap;
     uint2 *slots;
+    float *wts;
     unsigned long long *top;   // device scalar
     uint64_t arena_cap;        // slots
     uint32_t n;
@@ -214,6 +221,11 @@ dyg_status upload_graph(dyg_graph *G, uint32_t n, const uint64_t *row_ptr, const
 // list order per row.  Uses G's own workspace; may synchronize `st`.
 dyg_status commit_append(dyg_graph *G, const uint32_t *hx, const uint32_t *hy,
                          const float *hw, uint32_t m, cudaStream_t st);
+dyg_status commit_prepare(dyg_graph *G, const uint32_t *hx, uint32_t m, cudaStream_t st);
+dyg_status commit_finish(dyg_graph *G, const uint32_t *hy, const float *hw, uint32_t m,
+                         cudaStream_t st);
+// Copies both graphs' scalars and counts to the host with one synchronize.
+dyg_status read_scalars2(dyg_graph *A, dyg_graph *B, cudaStream_t st);
 dyg_status delete_half_edges(dyg_graph *G, const uint32_t *sorted_row,
                              const uint32_t *sorted_idx, const uint32_t *hy, uint32_t m,
                              const uint8_t *mask_found, uint8_t *found, cudaStream_t st);

@@ -64,6 +64,19 @@ dyg_status read_scalars(dyg_graph *G, cudaStream_t st) {
     return DYG_OK;
 }
 
+dyg_status read_scalars2(dyg_graph *A, dyg_graph *B, cudaStream_t st) {
+    if (!B || B == A) return read_scalars(A, st);
+    for (dyg_graph *G : {A, B}) {
+        Workspace &ws = G->ws;
+        DYG_CUDA(cudaMemcpyAsync(ws.host_scalars, ws.scalars.p,
+                                 S_NSCALARS * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+        DYG_CUDA(cudaMemcpyAsync(ws.host_counts, ws.counts.p, C_NCOUNTS * sizeof(uint32_t),
+                                 cudaMemcpyDeviceToHost, st));
+    }
+    DYG_CUDA(cudaStreamSynchronize(st));
+    return DYG_OK;
+}
+
 // ------------------------------------------------------------------ upload
 
 dyg_status upload_graph(dyg_graph *G, uint32_t n, const uint64_t *row_ptr, const uint32_t *col,
@@ -95,18 +108,23 @@ dyg_status upload_graph(dyg_graph *G, uint32_t n, const uint64_t *row_ptr, const
         return DYG_EINVAL;
     }
     uint2 *h_slots = (uint2 *)calloc((size_t)(used ? used : 1), sizeof(uint2));
-    if (!h_slots) {
+    float *h_w = (float *)calloc((size_t)(used ? used : 1), sizeof(float));
+    if (!h_slots || !h_w) {
         free(h_desc);
         free(h_cap);
+        free(h_slots);
+        free(h_w);
         set_error("host allocation failed");
         return DYG_ENOMEM;
     }
     for (uint32_t v = 0; v < n; ++v) {
         const uint64_t o = h_desc[v].x;
         for (uint64_t j = row_ptr[v]; j < row_ptr[v + 1]; ++j) {
-            uint32_t wb;
-            memcpy(&wb, &w[j], 4);
-            h_slots[o + (j - row_ptr[v])] = make_uint2(col[j], wb);
+            const float rw = 1.0f / w[j];   // IEEE division: equals __frcp_rn(w)
+            uint32_t rb;
+            memcpy(&rb, &rw, 4);
+            h_slots[o + (j - row_ptr[v])] = make_uint2(col[j], rb);
+            h_w[o + (j - row_ptr[v])] = w[j];
         }
     }
     dyg_status rc = DYG_OK;
@@ -114,7 +132,8 @@ dyg_status upload_graph(dyg_graph *G, uint32_t n, const uint64_t *row_ptr, const
     G->g.arena_cap = arena;
     if (cudaMalloc(&G->g.desc, sizeof(uint2) * (size_t)(n ? n : 1)) != cudaSuccess ||
         cudaMalloc(&G->g.cap, sizeof(uint32_t) * (size_t)(n ? n : 1)) != cudaSuccess ||
-        cudaMalloc(&G->g.slots, sizeof(uint2) * (size_t)arena) != cudaSuccess) {
+        cudaMalloc(&G->g.slots, sizeof(uint2) * (size_t)arena) != cudaSuccess ||
+        cudaMalloc(&G->g.wts, sizeof(float) * (size_t)arena) != cudaSuccess) {
         cudaGetLastError();
         set_error("cudaMalloc of the graph arena failed");
         rc = DYG_ENOMEM;
@@ -123,6 +142,7 @@ dyg_status upload_graph(dyg_graph *G, uint32_t n, const uint64_t *row_ptr, const
         cudaError_t e = cudaMemcpy(G->g.desc, h_desc, sizeof(uint2) * n, cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(G->g.cap, h_cap, sizeof(uint32_t) * n, cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(G->g.slots, h_slots, sizeof(uint2) * used, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(G->g.wts, h_w, sizeof(float) * used, cudaMemcpyHostToDevice);
         unsigned long long top = used;
         if (e == cudaSuccess) e = cudaMemcpy(G->g.top, &top, sizeof(top), cudaMemcpyHostToDevice);
         if (e != cudaSuccess) rc = cuda_fail(e, "graph upload", __FILE__, __LINE__);
@@ -130,6 +150,7 @@ dyg_status upload_graph(dyg_graph *G, uint32_t n, const uint64_t *row_ptr, const
     free(h_desc);
     free(h_cap);
     free(h_slots);
+    free(h_w);
     return rc;
 }
 
@@ -142,18 +163,24 @@ dyg_status grow_arena(dyg_graph *G, uint64_t min_cap, cudaStream_t st) {
         return DYG_ENOMEM;
     }
     uint2 *ns = nullptr;
+    float *nw = nullptr;
     cudaError_t e = cudaMalloc(&ns, sizeof(uint2) * (size_t)cap);
+    if (e == cudaSuccess) e = cudaMalloc(&nw, sizeof(float) * (size_t)cap);
     if (e != cudaSuccess) {
         cudaGetLastError();
+        if (ns) cudaFree(ns);
         set_error("cudaMalloc while growing the arena failed");
         return DYG_ENOMEM;
     }
     DYG_TRY(read_scalars(G, st));
     const unsigned long long top = G->ws.host_scalars[S_TOP];
     DYG_CUDA(cudaMemcpyAsync(ns, G->g.slots, sizeof(uint2) * (size_t)top, cudaMemcpyDeviceToDevice, st));
+    DYG_CUDA(cudaMemcpyAsync(nw, G->g.wts, sizeof(float) * (size_t)top, cudaMemcpyDeviceToDevice, st));
     DYG_CUDA(cudaStreamSynchronize(st));
     DYG_CUDA(cudaFree(G->g.slots));
+    DYG_CUDA(cudaFree(G->g.wts));
     G->g.slots = ns;
+    G->g.wts = nw;
     G->g.arena_cap = cap;
     return DYG_OK;
 }
@@ -212,6 +239,7 @@ __global__ void k_append_prepare(DevGraph g, const uint32_t *rows, uint32_t m, u
     need[p] = 0;
     if (!run_head(rows, p)) return;
     const uint32_t x = rows[p];
+    if (x >= g.n) return;
     const uint32_t k = run_len(rows, p, m);
     const uint2 d = g.desc[x];
     const uint32_t newdeg = d.y + k;
@@ -228,25 +256,35 @@ __global__ void k_append_apply(DevGraph g, const uint32_t *rows, const uint32_t 
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= m || !run_head(rows, p)) return;
     const uint32_t x = rows[p];
+    if (x >= g.n) return;
     const uint32_t k = run_len(rows, p, m);
     const uint2 d = g.desc[x];
     uint32_t off = d.x;
     if (need[p]) {
         off = (uint32_t)atomicAdd(g.top, (unsigned long long)need[p]);
-        for (uint32_t j = 0; j < d.y; ++j) g.slots[off + j] = g.slots[d.x + j];
+        for (uint32_t j = 0; j < d.y; ++j) {
+            g.slots[off + j] = g.slots[d.x + j];
+            g.wts[off + j] = g.wts[d.x + j];
+        }
         g.cap[x] = need[p];
     }
     for (uint32_t q = 0; q < k; ++q) {
         const uint32_t i = idx[p + q];
-        g.slots[off + d.y + q] = make_uint2(hy[i], __float_as_uint(hw[i]));
+        g.slots[off + d.y + q] = make_uint2(hy[i], __float_as_uint(__frcp_rn(hw[i])));
+        g.wts[off + d.y + q] = hw[i];
     }
     g.desc[x] = make_uint2(off, d.y + k);
 }
 
-dyg_status commit_append(dyg_graph *G, const uint32_t *hx, const uint32_t *hy,
-                         const float *hw, uint32_t m, cudaStream_t st) {
-    if (m == 0) return DYG_OK;
+// Phase 1 of an append: sort the half-edge list by row (stable, so list order
+// is kept within a row) and compute each overflowing row's new capacity.
+// Entries whose row is >= n (0xFFFFFFFF) sort last and are ignored, so a list
+// may be sized by an upper bound.  The relocation total lands in S_NEED.
+dyg_status commit_prepare(dyg_graph *G, const uint32_t *hx, uint32_t m, cudaStream_t st) {
     Workspace &ws = G->ws;
+    unsigned long long *sc = ptr<unsigned long long>(ws.scalars);
+    DYG_CUDA(cudaMemsetAsync(sc + S_NEED, 0, sizeof(unsigned long long), st));
+    if (m == 0) return DYG_OK;
     DYG_TRY(ensure(ws.skeys, sizeof(uint32_t) * m));
     DYG_TRY(ensure(ws.svals, sizeof(uint32_t) * m));
     DYG_TRY(ensure(ws.need, sizeof(uint32_t) * m * 2));
@@ -256,22 +294,38 @@ dyg_status commit_append(dyg_graph *G, const uint32_t *hx, const uint32_t *hy,
     k_iota<<<gr, th, 0, st>>>(iota, m);
     count_launch();
     DYG_TRY(sort_pairs_u32(ws, hx, ptr<uint32_t>(ws.skeys), iota, ptr<uint32_t>(ws.svals), m,
-                           bits_for(G->g.n), st));
-    unsigned long long *sc = ptr<unsigned long long>(ws.scalars);
-    DYG_CUDA(cudaMemsetAsync(sc + S_NEED, 0, sizeof(unsigned long long), st));
+                           bits_for(G->g.n + 1u), st));
     k_append_prepare<<<gr, th, 0, st>>>(G->g, ptr<uint32_t>(ws.skeys), m, G->slack,
                                         ptr<uint32_t>(ws.need), sc);
     count_launch();
     DYG_CUDA(cudaGetLastError());
-    DYG_TRY(read_scalars(G, st));
+    return DYG_OK;
+}
+
+// Phase 2: after the caller has read the scalars (read_scalars), grow the
+// arena if the relocations do not fit, then write the rows.
+dyg_status commit_finish(dyg_graph *G, const uint32_t *hy, const float *hw, uint32_t m,
+                         cudaStream_t st) {
+    if (m == 0) return DYG_OK;
+    Workspace &ws = G->ws;
     const unsigned long long need = ws.host_scalars[S_NEED];
     const unsigned long long top = ws.host_scalars[S_TOP];
     if (top + need > G->g.arena_cap) DYG_TRY(grow_arena(G, top + need, st));
+    const int th = 256;
+    const int gr = (int)((m + th - 1) / th);
     k_append_apply<<<gr, th, 0, st>>>(G->g, ptr<uint32_t>(ws.skeys), ptr<uint32_t>(ws.svals), m,
                                       hy, hw, ptr<uint32_t>(ws.need));
     count_launch();
     DYG_CUDA(cudaGetLastError());
     return DYG_OK;
+}
+
+dyg_status commit_append(dyg_graph *G, const uint32_t *hx, const uint32_t *hy,
+                         const float *hw, uint32_t m, cudaStream_t st) {
+    if (m == 0) return DYG_OK;
+    DYG_TRY(commit_prepare(G, hx, m, st));
+    DYG_TRY(read_scalars(G, st));
+    return commit_finish(G, hy, hw, m, st);
 }
 
 // ------------------------------------------------------------------ delete
@@ -294,6 +348,7 @@ __global__ void k_delete(DevGraph g, const uint32_t *rows, const uint32_t *idx, 
         for (uint32_t j = 0; j < deg; ++j) {
             if (g.slots[d.x + j].x == y) {
                 g.slots[d.x + j] = g.slots[d.x + deg - 1u];
+                g.wts[d.x + j] = g.wts[d.x + deg - 1u];
                 --deg;
                 found[i] = 1;
                 break;
@@ -322,11 +377,15 @@ __global__ void k_new_caps(DevGraph g, uint32_t slack, uint32_t *caps) {
     if (v < g.n) caps[v] = g.desc[v].y + slack;
 }
 
-__global__ void k_move_rows(DevGraph g, uint2 *ns, const uint32_t *off, const uint32_t *caps) {
+__global__ void k_move_rows(DevGraph g, uint2 *ns, float *nw, const uint32_t *off,
+                            const uint32_t *caps) {
     const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= g.n) return;
     const uint2 d = g.desc[v];
-    for (uint32_t j = 0; j < d.y; ++j) ns[off[v] + j] = g.slots[d.x + j];
+    for (uint32_t j = 0; j < d.y; ++j) {
+        ns[off[v] + j] = g.slots[d.x + j];
+        nw[off[v] + j] = g.wts[d.x + j];
+    }
     g.desc[v] = make_uint2(off[v], d.y);
     g.cap[v] = caps[v];
 }
@@ -351,20 +410,25 @@ dyg_status compact_graph(dyg_graph *G, cudaStream_t st) {
     if (cap < G->g.arena_cap / 2) cap = G->g.arena_cap / 2 > used ? G->g.arena_cap / 2 : cap;
     if (cap >= 0xFFFFFFFFull) cap = 0xFFFFFFFEull;
     uint2 *ns = nullptr;
+    float *nw = nullptr;
     cudaError_t e = cudaMalloc(&ns, sizeof(uint2) * (size_t)cap);
+    if (e == cudaSuccess) e = cudaMalloc(&nw, sizeof(float) * (size_t)cap);
     if (e != cudaSuccess) {
         cudaGetLastError();
+        if (ns) cudaFree(ns);
         set_error("cudaMalloc during compaction failed");
         return DYG_ENOMEM;
     }
-    k_move_rows<<<gr, th, 0, st>>>(G->g, ns, ptr<uint32_t>(ws.pos), ptr<uint32_t>(ws.flags));
+    k_move_rows<<<gr, th, 0, st>>>(G->g, ns, nw, ptr<uint32_t>(ws.pos), ptr<uint32_t>(ws.flags));
     count_launch();
     DYG_CUDA(cudaGetLastError());
     unsigned long long top = used;
     DYG_CUDA(cudaMemcpyAsync(G->g.top, &top, sizeof(top), cudaMemcpyHostToDevice, st));
     DYG_CUDA(cudaStreamSynchronize(st));
     DYG_CUDA(cudaFree(G->g.slots));
+    DYG_CUDA(cudaFree(G->g.wts));
     G->g.slots = ns;
+    G->g.wts = nw;
     G->g.arena_cap = cap;
     return DYG_OK;
 }

@@ -108,8 +108,10 @@ enum : int { kContinue = 0, kFail = 1, kFound = 2 };
 // *moved is set when a neighbour was drawn; *taken receives its slot.
 template <bool INCR, bool WEIGHTED>
 __device__ __forceinline__ int step_once(Walker &s, const uint2 *__restrict__ desc,
-                                         const uint2 *__restrict__ slots, uint32_t max_steps,
-                                         float thr, uint2 key, bool *moved, uint2 *taken) {
+                                         const uint2 *__restrict__ slots,
+                                         const float *__restrict__ wts, uint32_t max_steps,
+                                         float thr, uint2 key, bool *moved, uint2 *taken,
+                                         uint32_t *taken_at) {
     *moved = false;
     const uint2 d = __ldg(desc + s.cur);
     const uint32_t deg = d.y;
@@ -122,33 +124,39 @@ __device__ __forceinline__ int step_once(Walker &s, const uint2 *__restrict__ de
     }
     const uint32_t r = pick4(s.rbuf, di & 3u);
     uint2 sl;
+    uint32_t at;
     if (!WEIGHTED) {
         const uint32_t idx = first ? (r % deg) : (r % (deg - 1u));
-        sl = __ldg(slots + d.x + idx);
-        if (!first && sl.x == s.prev) sl = __ldg(slots + d.x + deg - 1u);
+        at = d.x + idx;
+        sl = __ldg(slots + at);
+        if (!first && sl.x == s.prev) {
+            at = d.x + deg - 1u;
+            sl = __ldg(slots + at);
+        }
     } else {
         unsigned long long total = 0ull;
         for (uint32_t j = 0; j < deg; ++j) {
-            const uint2 t = __ldg(slots + d.x + j);
-            if (!first && t.x == s.prev) continue;
-            total += wq(__uint_as_float(t.y));
+            if (!first && __ldg(&slots[d.x + j].x) == s.prev) continue;
+            total += wq(__ldg(wts + d.x + j));
         }
         if (total == 0ull) return kFail;
         const unsigned long long target = mul_hi32(r, total);
         unsigned long long acc = 0ull;
         uint32_t last = deg;
         for (uint32_t j = 0; j < deg; ++j) {
-            const uint2 t = __ldg(slots + d.x + j);
-            if (!first && t.x == s.prev) continue;
-            acc += wq(__uint_as_float(t.y));
+            if (!first && __ldg(&slots[d.x + j].x) == s.prev) continue;
+            acc += wq(__ldg(wts + d.x + j));
             last = j;
             if (acc > target) break;
         }
-        sl = __ldg(slots + d.x + last);
+        at = d.x + last;
+        sl = __ldg(slots + at);
     }
     *moved = true;
     *taken = sl;
-    s.R = __fadd_rn(s.R, __frcp_rn(__uint_as_float(sl.y)));
+    *taken_at = at;
+    // the slot holds the correctly rounded 1/w: one add per move, as R += 1/w
+    s.R = __fadd_rn(s.R, __uint_as_float(sl.y));
     if (INCR && !first && __fmul_rn(s.R, s.we) >= thr) return kFail;
     if (sl.x == s.tgt) return kFound;
     s.prev = s.cur;
@@ -239,8 +247,9 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(WalkArgs a) {
         if (active) {
             bool moved;
             uint2 taken;
-            const int r = step_once<INCR, WEIGHTED>(s, a.g.desc, a.g.slots, a.max_steps,
-                                                   a.threshold, a.key, &moved, &taken);
+            uint32_t taken_at;
+            const int r = step_once<INCR, WEIGHTED>(s, a.g.desc, a.g.slots, a.g.wts, a.max_steps,
+                                                   a.threshold, a.key, &moved, &taken, &taken_at);
             moves += moved ? 1u : 0u;
             if (r != kContinue) {
                 if (r == kFound) {
@@ -317,10 +326,12 @@ __global__ void k_winner_paths(DevGraph g, WalkJob job, uint32_t max_steps, uint
         const uint32_t at = s.step;
         bool moved;
         uint2 taken;
-        r = step_once<false, WEIGHTED>(s, g.desc, g.slots, max_steps, 0.f, key, &moved, &taken);
+        uint32_t taken_at;
+        r = step_once<false, WEIGHTED>(s, g.desc, g.slots, g.wts, max_steps, 0.f, key, &moved,
+                                       &taken, &taken_at);
         if (moved && at < stride) {
             row_v[at] = taken.x;
-            row_w[at] = __uint_as_float(taken.y);
+            row_w[at] = g.wts[taken_at];
         }
     } while (r == kContinue);
     const int32_t found = (r == kFound) ? (int32_t)s.step : -1;
@@ -348,15 +359,15 @@ __global__ void k_fallback(DevGraph g, const uint32_t *f_src, const uint32_t *f_
     float w1 = 0.f, w2 = 0.f;
     const uint2 d0 = __ldg(g.desc + s0);
     if (d0.y != 0u) {
-        const uint2 a = __ldg(g.slots + d0.x + rb.x % d0.y);
-        x1 = a.x;
-        w1 = __uint_as_float(a.y);
+        const uint32_t i0 = d0.x + rb.x % d0.y;
+        x1 = __ldg(&g.slots[i0].x);
+        w1 = __ldg(g.wts + i0);
         const uint2 d1 = __ldg(g.desc + x1);
         if (d1.y != 0u) {
-            uint2 b = __ldg(g.slots + d1.x + rb.y % d1.y);
-            if (b.x == s0) b = __ldg(g.slots + d1.x + d1.y - 1u);
-            x2 = b.x;
-            w2 = __uint_as_float(b.y);
+            uint32_t i1 = d1.x + rb.y % d1.y;
+            if (__ldg(&g.slots[i1].x) == s0) i1 = d1.x + d1.y - 1u;
+            x2 = __ldg(&g.slots[i1].x);
+            w2 = __ldg(g.wts + i1);
         }
     }
     cx[2 * i] = (x1 == ~0u) ? ~0u : s0;
