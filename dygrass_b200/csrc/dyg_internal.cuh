@@ -130,6 +130,10 @@ struct Workspace {
     Buf s_src, s_dst, s_w, s_o1, s_o2, s_o3;  // whole-stream staging
     Buf rx2, ry2;                             // recovered edges of a whole stream
     Buf rk2;
+    Buf rank, lneed, dtmp;                    // row operations: per-entry rank / need / run
+    Buf rowcnt, rowtmp;                       // row operations: per-row counter / run base
+    Buf tmask;                                // dedup table size (device)
+    Buf del_hx, del_hy;                       // deletion half-edges
     Buf scalars;                              // u64 scalars (see Scalar)
     Buf counts;                               // u32 counts (see Count)
     unsigned long long *host_scalars = nullptr;   // pinned mirror
@@ -138,21 +142,43 @@ struct Workspace {
 
 // Indices into Workspace::scalars (u64, device) and Workspace::counts (u32).
 enum Scalar : int {
-    S_NEED = 0,       // relocation slots needed by a commit
-    S_ERR = 1,        // device error bits (kErr*)
-    S_MOVES = 2,      // walker moves (accumulating)
-    S_WALKS = 3,      // walks finished (accumulating)
-    S_TOP = 4,        // arena bump pointer of the owning graph
-    S_WORK = 5,       // work-chunk counter of the persistent walk kernel
-    S_NSCALARS = 8
+    S_NEED = 0,       // arena slots a pending append needs (row moves)
+    S_CURSOR = 1,     // arena cursor of the moves of that append (follows S_NEED)
+    S_ERR = 2,        // device error bits (kErr*)
+    S_MOVES = 3,      // walker moves (accumulating)
+    S_WALKS = 4,      // walks finished (accumulating)
+    S_TOP = 5,        // arena bump pointer of the owning graph
+    S_WORK = 6,       // work-chunk counter of the persistent walk kernel
+    S_OPRAN = 7,      // set when an append took its row ranks
+    S_TMPCUR = 8,     // scratch cursor of a delete
+    S_HALT = 9,       // halt code of a stream this handle drives (0 = running)
+    S_RECCNT = 10,    // recovered edges recorded so far in a decremental stream
+    S_RECCAP = 11,    // capacity of the record buffers
+    S_NSCALARS = 16
 };
 enum Count : int {
     C_FILTERED = 0,   // decremental: edges to walk
     C_CANDS = 1,      // recovery candidates
-    C_KEPT = 2,       // recovery candidates kept
+    C_KEPT = 2,       // half-edges of the kept recovery candidates
     C_NOPATH = 3,     // decremental: edges without a path
     C_ACCEPTED = 4,   // incremental: accepted edges
+    C_CANDS2 = 5,     // fallback candidates
     C_NCOUNTS = 8
+};
+
+// Halt codes: (batch + 1) << 8 | kind << 4 | phase.
+constexpr unsigned long long kHaltArena = 1;    // an arena reservation did not fit
+constexpr unsigned long long kHaltRecords = 2;  // the recovered-edge buffers are full
+__host__ __device__ __forceinline__ unsigned long long halt_code(uint32_t batch, uint32_t kind,
+                                                                 uint32_t phase) {
+    return ((unsigned long long)(batch + 1) << 8) | (kind << 4) | phase;
+}
+
+struct AppendList {
+    const uint32_t *hx, *hy;
+    const float *hw;
+    const uint32_t *m_dev;   // device length, or null
+    uint32_t m_host;         // host length or upper bound
 };
 
 }  // namespace dyg
@@ -193,6 +219,7 @@ void count_launch();
 
 // --- walk.cu
 struct WalkJob {
+    const unsigned long long *halt;  // kernels return at once when *halt != 0 (may be null)
     const uint32_t *src, *dst;
     const float *w;              // incremental: per-edge weight; else null
     const unsigned long long *uid;   // per-edge update id, or null -> uid0 + e
@@ -209,37 +236,36 @@ dyg_status launch_walk_scalars(const DevGraph &g, const WalkJob &job, const dyg_
 dyg_status launch_winner_paths(dyg_graph *G, const WalkJob &job, const dyg_walk_params &p,
                                const unsigned long long *keys, uint32_t n_max, uint32_t path_stride,
                                uint32_t *path_v, float *path_w, int32_t *path_len, cudaStream_t st);
-dyg_status launch_fallback_walks(dyg_graph *G, const uint32_t *f_src, const uint32_t *f_dst,
+dyg_status launch_fallback_walks(dyg_graph *G, const unsigned long long *halt,
+                                 const uint32_t *f_src, const uint32_t *f_dst,
                                  const unsigned long long *f_uid, const uint32_t *nop,
-                                 uint32_t n_nop, const dyg_walk_params &p, uint32_t *cx,
-                                 uint32_t *cy, float *cw, cudaStream_t st);
+                                 const uint32_t *n_nop_dev, uint32_t n_nop_max,
+                                 const dyg_walk_params &p, uint32_t *cx, uint32_t *cy, float *cw,
+                                 cudaStream_t st);
+
+// --- pipeline.cu
+dyg_status incremental_run(dyg_graph *H, dyg_graph *G, const uint32_t *src, const uint32_t *dst,
+                           const float *w, uint32_t n, uint32_t B, uint64_t uid_base,
+                           const dyg_walk_params &p, int32_t *found, float *cond, uint8_t *acc,
+                           cudaStream_t st);
+dyg_status decremental_run(dyg_graph *G, dyg_graph *H, const uint32_t *src, const uint32_t *dst,
+                           uint32_t n, uint32_t B, uint64_t uid_base, const dyg_walk_params &p,
+                           int32_t *status, float *cond, uint64_t *n_rec, cudaStream_t st);
 
 // --- graph.cu
 dyg_status upload_graph(dyg_graph *G, uint32_t n, const uint64_t *row_ptr, const uint32_t *col,
                         const float *w);
-// Appends half-edge i (row hx[i], column hy[i], weight hw[i]) for i < m, in
-// list order per row.  Uses G's own workspace; may synchronize `st`.
-dyg_status commit_append(dyg_graph *G, const uint32_t *hx, const uint32_t *hy,
-                         const float *hw, uint32_t m, cudaStream_t st);
-dyg_status commit_prepare(dyg_graph *G, const uint32_t *hx, uint32_t m, cudaStream_t st);
-dyg_status commit_finish(dyg_graph *G, const uint32_t *hy, const float *hw, uint32_t m,
-                         cudaStream_t st);
+dyg_status append_enqueue(dyg_graph *GA, const AppendList &A, dyg_graph *GB, const AppendList *B,
+                          unsigned long long *halt, unsigned long long code, cudaStream_t st);
+dyg_status delete_enqueue(dyg_graph *G, const uint32_t *hx, const uint32_t *hy, uint32_t m,
+                          const uint8_t *mask, uint8_t *found, unsigned long long *halt,
+                          cudaStream_t st);
 // Copies both graphs' scalars and counts to the host with one synchronize.
 dyg_status read_scalars2(dyg_graph *A, dyg_graph *B, cudaStream_t st);
-dyg_status delete_half_edges(dyg_graph *G, const uint32_t *sorted_row,
-                             const uint32_t *sorted_idx, const uint32_t *hy, uint32_t m,
-                             const uint8_t *mask_found, uint8_t *found, cudaStream_t st);
-dyg_status sort_pairs_u32(Workspace &ws, const uint32_t *keys_in, uint32_t *keys_out,
-                          const uint32_t *vals_in, uint32_t *vals_out, uint32_t m,
-                          uint32_t key_bits, cudaStream_t st);
 dyg_status exclusive_scan_u32(Workspace &ws, const uint32_t *in, uint32_t *out, uint32_t m,
                               cudaStream_t st);
 dyg_status compact_graph(dyg_graph *G, cudaStream_t st);
 dyg_status grow_arena(dyg_graph *G, uint64_t min_cap, cudaStream_t st);
 dyg_status read_scalars(dyg_graph *G, cudaStream_t st);
-dyg_status dedup_keep(dyg_graph *H, const uint32_t *cx, const uint32_t *cy,
-                      uint32_t m, uint32_t *keep, cudaStream_t st);
-uint32_t bits_for(uint32_t n);
-__global__ void k_iota(uint32_t *v, uint32_t m);
 
 }  // namespace dyg

@@ -147,7 +147,7 @@ extern "C" dyg_status dyg_incremental_walk_noalloc(const dyg_graph *H, const uin
             e = cudaMemsetAsync(scalars, 0, sizeof(unsigned long long) * kNoallocScalars, st);
         if (e != cudaSuccess) rc = cuda_fail(e, "cudaMemsetAsync", __FILE__, __LINE__);
         if (rc == DYG_OK) {
-            WalkJob job{src, dst, w, nullptr, (unsigned long long)first_update_id, nullptr, n,
+            WalkJob job{nullptr, src, dst, w, nullptr, (unsigned long long)first_update_id, nullptr, n,
                         kDomainIncr};
             rc = launch_walk_scalars(H->g, job, *p, true, keys, scalars, st);
         }

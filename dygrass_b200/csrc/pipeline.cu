@@ -1,0 +1,631 @@
+// pipeline.cu -- the incremental and decremental update pipelines.
+//
+// A whole update stream is enqueued on one CUDA stream with no host
+// round-trip: counts stay on the device (grid-stride loops bounded by device
+// counts), row updates go through rowops.cu, and the only host check is a
+// single synchronize at the end.  A reservation that does not fit (arena or
+// record buffers) halts every later kernel; the host then grows the buffer and
+// resumes at the halted batch and phase, which reproduces the same results
+// because no kernel changed anything after the halt.
+//
+// Incremental batch (one iteration of random_walk_incremental/main.cu:314-340):
+//   walk H -> decode winner keys -> exclusive scan of accept flags (input
+//   order) -> accepted half-edges to H [and every half-edge to G], reserved
+//   together.  Resumes at the batch start (nothing of the batch changed).
+// Decremental batch (random_walk_decremental/main.cu:413-444), phases:
+//   0: delete from G and H in input order, compact the edges found in both,
+//      walk G, replay winners, path candidates in (edge, step) order;
+//   1: dedup the path edges, drop those in H, append the rest in order;
+//   2: 2-step fallback walks for the edges without a path, same dedup/append.
+#include "dyg_internal.cuh"
+
+namespace dyg {
+
+namespace {
+
+inline int blocks(uint64_t n, int th) { return (int)((n + th - 1) / th); }
+
+int grid_for(uint64_t m) {
+    const uint64_t b = (m + 255) / 256;
+    const uint64_t cap = (uint64_t)num_sms() * 8;
+    return (int)(b < 1 ? 1 : (b > cap ? cap : b));
+}
+
+__device__ __forceinline__ uint32_t dcount(const uint32_t *dev, uint32_t host) {
+    return dev ? min(*dev, host) : host;
+}
+
+#define HALTED(h) ((h) && *(h))
+#define GSTRIDE(i, m) \
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < (m); i += gridDim.x * blockDim.x)
+
+// --------------------------------------------------------- incremental
+
+__global__ void k_incr_decode(const unsigned long long *halt, const unsigned long long *keys,
+                              uint32_t n, int32_t *found, float *cond, uint8_t *acc,
+                              uint32_t *flags) {
+    if (HALTED(halt)) return;
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const unsigned long long k = keys[e];
+    if (found) found[e] = key_found(k);
+    if (cond) cond[e] = k ? __uint_as_float((uint32_t)(k >> 32)) : 0.f;
+    if (acc) acc[e] = k ? 0 : 1;
+    flags[e] = k ? 0u : 1u;
+}
+
+// Half-edges in input order (u gets v, then v gets u:
+// random_walk_incremental/gpu_graph.cuh:320-325); with flags only the
+// accepted edges, at their scanned positions; entries not written keep the
+// 0xFFFFFFFF row that append ignores.
+__global__ void k_half_edges(const unsigned long long *halt, const uint32_t *src,
+                             const uint32_t *dst, const float *w, uint32_t n,
+                             const uint32_t *flags, const uint32_t *pos, uint32_t *hx,
+                             uint32_t *hy, float *hw) {
+    if (HALTED(halt)) return;
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    if (flags && !flags[e]) return;
+    const uint32_t q = flags ? pos[e] : e;
+    const uint32_t u = src[e], v = dst[e];
+    const float ww = w[e];
+    hx[2 * q] = u;
+    hy[2 * q] = v;
+    hw[2 * q] = ww;
+    hx[2 * q + 1] = v;
+    hy[2 * q + 1] = u;
+    hw[2 * q + 1] = ww;
+}
+
+// ---------------------------------------------------------- decremental
+
+// Deletion half-edges with endpoints ordered min -> max
+// (random_walk_decremental/gpu_graph.cuh:340-343).
+__global__ void k_del_half_edges(const unsigned long long *halt, const uint32_t *src,
+                                 const uint32_t *dst, uint32_t n, uint32_t nv, uint32_t *hx,
+                                 uint32_t *hy, unsigned long long *err) {
+    if (HALTED(halt)) return;
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    uint32_t a = src[e], b = dst[e];
+    if (a > b) {
+        const uint32_t t = a;
+        a = b;
+        b = t;
+    }
+    if (b >= nv) {
+        atomicOr(err, (unsigned long long)kErrVertex);
+        a = b = 0xFFFFFFFFu;   // ignored by the row operations: never found
+    }
+    hx[2 * e] = a;
+    hy[2 * e] = b;
+    hx[2 * e + 1] = b;
+    hy[2 * e + 1] = a;
+}
+
+__global__ void k_del_filter(const unsigned long long *halt, const uint8_t *fG, const uint8_t *fH,
+                             uint32_t n, uint32_t *flags, int32_t *status, float *cond) {
+    if (HALTED(halt)) return;
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const bool inG = fG[2 * e] && fG[2 * e + 1];
+    const bool inH = inG && fH[2 * e] && fH[2 * e + 1];
+    flags[e] = inH ? 1u : 0u;
+    status[e] = !inG ? DYG_DEL_NOT_IN_G : (!inH ? DYG_DEL_NOT_IN_H : DYG_DEL_NO_PATH);
+    cond[e] = 0.f;
+}
+
+__global__ void k_del_compact(const unsigned long long *halt, const uint32_t *hx,
+                              const uint32_t *hy, uint32_t n, const uint32_t *flags,
+                              const uint32_t *pos, unsigned long long uid0, uint32_t *f_src,
+                              uint32_t *f_dst, unsigned long long *f_uid, uint32_t *f_idx,
+                              uint32_t *count) {
+    if (HALTED(halt)) return;
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    if (e == n - 1) *count = pos[e] + flags[e];
+    if (!flags[e]) return;
+    const uint32_t f = pos[e];
+    f_src[f] = hx[2 * e];   // min
+    f_dst[f] = hy[2 * e];   // max
+    f_uid[f] = uid0 + e;
+    f_idx[f] = e;
+}
+
+// Per filtered edge: status / conductance, path-candidate counts and the
+// no-path flags (zero for f >= F).
+__global__ void k_decr_results(const unsigned long long *halt, const unsigned long long *keys,
+                               const int32_t *plen, const uint32_t *f_idx, const uint32_t *F_dev,
+                               uint32_t n, int32_t *status, float *cond, uint32_t *clen,
+                               uint32_t *noflag) {
+    if (HALTED(halt)) return;
+    const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= n) return;
+    const uint32_t F = *F_dev;
+    if (f >= F) {
+        clen[f] = 0;
+        noflag[f] = 0;
+        return;
+    }
+    const uint32_t e = f_idx[f];
+    const int32_t L = plen[f];
+    const unsigned long long k = keys[f];
+    status[e] = L > 0 ? L : DYG_DEL_NO_PATH;
+    cond[e] = k ? __uint_as_float((uint32_t)(k >> 32)) : 0.f;
+    clen[f] = L > 0 ? (uint32_t)L : 0u;
+    noflag[f] = L > 0 ? 0u : 1u;
+}
+
+__global__ void k_path_cands(const unsigned long long *halt, const uint32_t *pv, const float *pw,
+                             uint32_t stride, const uint32_t *clen, const uint32_t *coff,
+                             uint32_t n, const uint32_t *noflag, const uint32_t *nopos,
+                             uint32_t *cx, uint32_t *cy, float *cw, uint32_t *nop,
+                             uint32_t *counts, uint32_t hw) {
+    if (HALTED(halt)) return;
+    const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= n) return;
+    if (f == n - 1) {
+        counts[C_CANDS] = coff[f] + clen[f];
+        counts[C_NOPATH] = nopos[f] + noflag[f];
+        counts[C_CANDS2] = (nopos[f] + noflag[f]) * 4u * hw;
+    }
+    if (noflag[f]) nop[nopos[f]] = f;
+    const uint32_t L = clen[f];
+    const uint32_t base = coff[f];
+    const uint32_t *v = pv + (size_t)f * stride;
+    const float *w = pw + (size_t)f * stride;
+    for (uint32_t j = 0; j < L; ++j) {
+        cx[base + j] = v[j];
+        cy[base + j] = v[j + 1];
+        cw[base + j] = w[j + 1];
+    }
+}
+
+// ------------------------------------------------------------- recovery
+
+__device__ __forceinline__ unsigned long long ekey(uint32_t x, uint32_t y) {
+    const uint32_t a = min(x, y), b = max(x, y);
+    return ((unsigned long long)a << 32) | b;
+}
+__device__ __forceinline__ uint32_t hslot(unsigned long long k, uint32_t mask) {
+    k ^= k >> 33;
+    k *= 0xff51afd7ed558ccdull;
+    k ^= k >> 33;
+    k *= 0xc4ceb9fe1a85ec53ull;
+    k ^= k >> 33;
+    return (uint32_t)k & mask;
+}
+
+__global__ void k_rec_setup(const unsigned long long *halt, const uint32_t *M_dev, uint32_t M_host,
+                            uint32_t *tmask, uint32_t *counts) {
+    if (HALTED(halt)) return;
+    const uint32_t M = dcount(M_dev, M_host);
+    uint32_t T = 1024u;
+    while (T < 2u * M) T <<= 1;
+    *tmask = T - 1u;
+    counts[C_KEPT] = 0u;
+}
+
+__global__ void k_hash_clear(const unsigned long long *halt, unsigned long long *tk, uint32_t *tv,
+                             const uint32_t *tmask) {
+    if (HALTED(halt)) return;
+    const uint32_t T = *tmask + 1u;
+    GSTRIDE(i, T) {
+        tk[i] = ~0ull;
+        tv[i] = ~0u;
+    }
+}
+
+__global__ void k_hash_insert(const unsigned long long *halt, const uint32_t *cx,
+                              const uint32_t *cy, const uint32_t *M_dev, uint32_t M_host,
+                              unsigned long long *tk, uint32_t *tv, const uint32_t *tmask) {
+    if (HALTED(halt)) return;
+    const uint32_t M = dcount(M_dev, M_host), mask = *tmask;
+    GSTRIDE(i, M) {
+        const uint32_t x = cx[i], y = cy[i];
+        if (x == ~0u || y == ~0u || x == y) continue;
+        const unsigned long long k = ekey(x, y);
+        uint32_t h = hslot(k, mask);
+        while (true) {
+            const unsigned long long prev = atomicCAS(tk + h, ~0ull, k);
+            if (prev == ~0ull || prev == k) {
+                atomicMin(tv + h, i);
+                break;
+            }
+            h = (h + 1u) & mask;
+        }
+    }
+}
+
+// keep[i] = candidate i is the first occurrence of its edge and the edge is
+// not in H (gpu_graph.cuh:534-538 and 599-601 test sparse_map the same way);
+// zero for M <= i < M_host.
+__global__ void k_hash_keep(const unsigned long long *halt, DevGraph h, const uint32_t *cx,
+                            const uint32_t *cy, const uint32_t *M_dev, uint32_t M_host,
+                            const unsigned long long *tk, const uint32_t *tv,
+                            const uint32_t *tmask, uint32_t *keep) {
+    if (HALTED(halt)) return;
+    const uint32_t M = dcount(M_dev, M_host), mask = *tmask;
+    GSTRIDE(i, M_host) {
+        uint32_t kp = 0;
+        if (i < M) {
+            const uint32_t x = cx[i], y = cy[i];
+            if (x != ~0u && y != ~0u && x != y) {
+                const unsigned long long k = ekey(x, y);
+                uint32_t s = hslot(k, mask);
+                while (tk[s] != k) s = (s + 1u) & mask;
+                if (tv[s] == i) {
+                    kp = 1;
+                    if (x < h.n) {
+                        const uint2 d = h.desc[x];
+                        for (uint32_t j = 0; j < d.y; ++j)
+                            if (h.slots[d.x + j].x == y) {
+                                kp = 0;
+                                break;
+                            }
+                    }
+                }
+            }
+        }
+        keep[i] = kp;
+    }
+}
+
+// One thread: the kept edges must fit the record buffers, or halt.
+__global__ void k_rec_check(unsigned long long *halt, const uint32_t *keep, const uint32_t *kpos,
+                            const uint32_t *M_dev, uint32_t M_host, const unsigned long long *sc,
+                            unsigned long long code) {
+    if (*halt) return;
+    const uint32_t M = dcount(M_dev, M_host);
+    const unsigned long long K = M ? (unsigned long long)kpos[M - 1] + keep[M - 1] : 0ull;
+    if (sc[S_RECCNT] + K > sc[S_RECCAP]) *halt = code;
+}
+
+// Kept candidates -> half-edges (x gets y, then y gets x), in candidate order,
+// and the recovered-edge records after the ones recorded so far.
+__global__ void k_emit_kept(const unsigned long long *halt, const uint32_t *cx, const uint32_t *cy,
+                            const float *cw, const uint32_t *M_dev, uint32_t M_host,
+                            const uint32_t *keep, const uint32_t *kpos, uint8_t kind,
+                            const unsigned long long *sc, uint32_t *hx, uint32_t *hy, float *hw,
+                            uint32_t *rx, uint32_t *ry, uint8_t *rk, uint32_t *counts) {
+    if (HALTED(halt)) return;
+    const uint32_t M = dcount(M_dev, M_host);
+    const unsigned long long base = sc[S_RECCNT];
+    GSTRIDE(i, M) {
+        if (i == M - 1) counts[C_KEPT] = 2u * (kpos[i] + keep[i]);
+        if (!keep[i]) continue;
+        const uint32_t q = kpos[i];
+        const uint32_t x = cx[i], y = cy[i];
+        const float w = cw[i];
+        hx[2 * q] = x;
+        hy[2 * q] = y;
+        hw[2 * q] = w;
+        hx[2 * q + 1] = y;
+        hy[2 * q + 1] = x;
+        hw[2 * q + 1] = w;
+        rx[base + q] = x;
+        ry[base + q] = y;
+        rk[base + q] = kind;
+    }
+}
+
+__global__ void k_rec_advance(const unsigned long long *halt, const uint32_t *counts,
+                              unsigned long long *sc) {
+    if (HALTED(halt)) return;
+    sc[S_RECCNT] += counts[C_KEPT] / 2u;
+}
+
+dyg_status grow_keep(Buf &b, size_t bytes, size_t used, cudaStream_t st) {
+    if (b.bytes >= bytes) return DYG_OK;
+    Buf nb;
+    DYG_TRY(ensure(nb, bytes));
+    if (used && b.p) {
+        DYG_CUDA(cudaMemcpyAsync(nb.p, b.p, used, cudaMemcpyDeviceToDevice, st));
+        DYG_CUDA(cudaStreamSynchronize(st));
+    }
+    if (b.p) cudaFree(b.p);
+    b = nb;
+    return DYG_OK;
+}
+
+// Dedup + membership + ordered append of one candidate list (phase 1 or 2).
+dyg_status recover_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *cx, const uint32_t *cy,
+                           const float *cw, const uint32_t *M_dev, uint32_t M_host, uint8_t kind,
+                           unsigned long long *halt, uint32_t batch, uint32_t phase,
+                           cudaStream_t st) {
+    if (M_host == 0) return DYG_OK;
+    Workspace &ws = G->ws;
+    uint32_t T = 1024;
+    while (T < 2u * M_host) T <<= 1;
+    DYG_TRY(ensure(ws.htab_k, sizeof(unsigned long long) * T));
+    DYG_TRY(ensure(ws.htab_v, sizeof(uint32_t) * T));
+    DYG_TRY(ensure(ws.tmask, sizeof(uint32_t)));
+    DYG_TRY(ensure(ws.keep, sizeof(uint32_t) * (size_t)M_host * 2));
+    DYG_TRY(ensure(ws.hx, sizeof(uint32_t) * (size_t)M_host * 2));
+    DYG_TRY(ensure(ws.hy, sizeof(uint32_t) * (size_t)M_host * 2));
+    DYG_TRY(ensure(ws.hw, sizeof(float) * (size_t)M_host * 2));
+    uint32_t *keep = ptr<uint32_t>(ws.keep), *kpos = keep + M_host;
+    uint32_t *counts = ptr<uint32_t>(ws.counts);
+    unsigned long long *sc = ptr<unsigned long long>(ws.scalars);
+    const int gr = grid_for(M_host);
+    k_rec_setup<<<1, 1, 0, st>>>(halt, M_dev, M_host, ptr<uint32_t>(ws.tmask), counts);
+    count_launch();
+    k_hash_clear<<<grid_for((uint64_t)T), 256, 0, st>>>(halt, ptr<unsigned long long>(ws.htab_k),
+                                                        ptr<uint32_t>(ws.htab_v),
+                                                        ptr<uint32_t>(ws.tmask));
+    count_launch();
+    k_hash_insert<<<gr, 256, 0, st>>>(halt, cx, cy, M_dev, M_host, ptr<unsigned long long>(ws.htab_k),
+                                      ptr<uint32_t>(ws.htab_v), ptr<uint32_t>(ws.tmask));
+    count_launch();
+    k_hash_keep<<<gr, 256, 0, st>>>(halt, H->g, cx, cy, M_dev, M_host,
+                                    ptr<unsigned long long>(ws.htab_k), ptr<uint32_t>(ws.htab_v),
+                                    ptr<uint32_t>(ws.tmask), keep);
+    count_launch();
+    DYG_TRY(exclusive_scan_u32(ws, keep, kpos, M_host, st));
+    k_rec_check<<<1, 1, 0, st>>>(halt, keep, kpos, M_dev, M_host, sc,
+                                 halt_code(batch, (uint32_t)kHaltRecords, phase));
+    count_launch();
+    k_emit_kept<<<gr, 256, 0, st>>>(halt, cx, cy, cw, M_dev, M_host, keep, kpos, kind, sc,
+                                    ptr<uint32_t>(ws.hx), ptr<uint32_t>(ws.hy), ptr<float>(ws.hw),
+                                    ptr<uint32_t>(ws.rx2), ptr<uint32_t>(ws.ry2),
+                                    ptr<uint8_t>(ws.rk2), counts);
+    count_launch();
+    DYG_CUDA(cudaGetLastError());
+    AppendList L{ptr<uint32_t>(ws.hx), ptr<uint32_t>(ws.hy), ptr<float>(ws.hw), counts + C_KEPT,
+                 2u * M_host};
+    DYG_TRY(append_enqueue(H, L, nullptr, nullptr, halt,
+                           halt_code(batch, (uint32_t)kHaltArena, phase), st));
+    k_rec_advance<<<1, 1, 0, st>>>(halt, counts, sc);
+    count_launch();
+    DYG_CUDA(cudaGetLastError());
+    return DYG_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ batches
+
+// Enqueues incremental batch `batch` (edges src/dst/w[0, n), update ids
+// uid0 + e).  Outputs go to found/cond/acc (device, may be null).
+dyg_status incr_enqueue(dyg_graph *H, dyg_graph *G, const uint32_t *src, const uint32_t *dst,
+                        const float *w, uint32_t n, uint64_t uid0, const dyg_walk_params &p,
+                        unsigned long long *halt, uint32_t batch, int32_t *found, float *cond,
+                        uint8_t *acc, cudaStream_t st) {
+    Workspace &ws = H->ws;
+    DYG_TRY(ensure(ws.keys, sizeof(unsigned long long) * n));
+    DYG_TRY(ensure(ws.flags, sizeof(uint32_t) * n));
+    DYG_TRY(ensure(ws.pos, sizeof(uint32_t) * n));
+    DYG_TRY(ensure(ws.hx, sizeof(uint32_t) * (size_t)n * 2));
+    DYG_TRY(ensure(ws.hy, sizeof(uint32_t) * (size_t)n * 2));
+    DYG_TRY(ensure(ws.hw, sizeof(float) * (size_t)n * 2));
+    unsigned long long *keys = ptr<unsigned long long>(ws.keys);
+    DYG_CUDA(cudaMemsetAsync(keys, 0, sizeof(unsigned long long) * n, st));
+    DYG_CUDA(cudaMemsetAsync(ws.hx.p, 0xFF, sizeof(uint32_t) * (size_t)n * 2, st));
+    WalkJob job{halt, src, dst, w, nullptr, (unsigned long long)uid0, nullptr, n, kDomainIncr};
+    DYG_TRY(launch_walk(H, job, p, true, keys, st));
+    k_incr_decode<<<blocks(n, 256), 256, 0, st>>>(halt, keys, n, found, cond, acc,
+                                                   ptr<uint32_t>(ws.flags));
+    count_launch();
+    DYG_TRY(exclusive_scan_u32(ws, ptr<uint32_t>(ws.flags), ptr<uint32_t>(ws.pos), n, st));
+    k_half_edges<<<blocks(n, 256), 256, 0, st>>>(halt, src, dst, w, n, ptr<uint32_t>(ws.flags),
+                                                  ptr<uint32_t>(ws.pos), ptr<uint32_t>(ws.hx),
+                                                  ptr<uint32_t>(ws.hy), ptr<float>(ws.hw));
+    count_launch();
+    AppendList LH{ptr<uint32_t>(ws.hx), ptr<uint32_t>(ws.hy), ptr<float>(ws.hw), nullptr, 2u * n};
+    AppendList LG{};
+    if (G) {
+        Workspace &wg = G->ws;
+        DYG_TRY(ensure(wg.hx, sizeof(uint32_t) * (size_t)n * 2));
+        DYG_TRY(ensure(wg.hy, sizeof(uint32_t) * (size_t)n * 2));
+        DYG_TRY(ensure(wg.hw, sizeof(float) * (size_t)n * 2));
+        k_half_edges<<<blocks(n, 256), 256, 0, st>>>(halt, src, dst, w, n, nullptr, nullptr,
+                                                      ptr<uint32_t>(wg.hx), ptr<uint32_t>(wg.hy),
+                                                      ptr<float>(wg.hw));
+        count_launch();
+        LG = AppendList{ptr<uint32_t>(wg.hx), ptr<uint32_t>(wg.hy), ptr<float>(wg.hw), nullptr,
+                        2u * n};
+    }
+    DYG_CUDA(cudaGetLastError());
+    return append_enqueue(H, LH, G, G ? &LG : nullptr, halt,
+                          halt_code(batch, (uint32_t)kHaltArena, 0), st);
+}
+
+// Enqueues decremental batch `batch` from phase `phase0`.  status/cond
+// (device, length n) receive the per-deletion results.
+dyg_status decr_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src, const uint32_t *dst,
+                        uint32_t n, uint64_t uid0, const dyg_walk_params &p,
+                        unsigned long long *halt, uint32_t batch, uint32_t phase0,
+                        int32_t *status, float *cond, cudaStream_t st) {
+    Workspace &ws = G->ws;
+    const uint32_t m = 2u * n;
+    const uint32_t stride = p.max_steps > 2 ? p.max_steps : 2;
+    const uint32_t hwk = p.heuristic_walkers;
+    DYG_TRY(ensure(ws.del_hx, sizeof(uint32_t) * (size_t)m));
+    DYG_TRY(ensure(ws.del_hy, sizeof(uint32_t) * (size_t)m));
+    DYG_TRY(ensure(ws.found, (size_t)m * 2));
+    DYG_TRY(ensure(ws.flags, sizeof(uint32_t) * n));
+    DYG_TRY(ensure(ws.pos, sizeof(uint32_t) * n));
+    DYG_TRY(ensure(ws.f_src, sizeof(uint32_t) * n));
+    DYG_TRY(ensure(ws.f_dst, sizeof(uint32_t) * n));
+    DYG_TRY(ensure(ws.f_idx, sizeof(uint32_t) * n));
+    DYG_TRY(ensure(ws.f_uid, sizeof(unsigned long long) * n));
+    DYG_TRY(ensure(ws.keys, sizeof(unsigned long long) * n));
+    DYG_TRY(ensure(ws.path_v, sizeof(uint32_t) * (size_t)n * stride));
+    DYG_TRY(ensure(ws.path_w, sizeof(float) * (size_t)n * stride));
+    DYG_TRY(ensure(ws.path_len, sizeof(int32_t) * n));
+    DYG_TRY(ensure(ws.nop, sizeof(uint32_t) * (size_t)n * 4));
+    DYG_TRY(ensure(ws.cand_x, sizeof(uint32_t) * (size_t)n * stride));
+    DYG_TRY(ensure(ws.cand_y, sizeof(uint32_t) * (size_t)n * stride));
+    DYG_TRY(ensure(ws.cand_w, sizeof(float) * (size_t)n * stride));
+    uint32_t *hx = ptr<uint32_t>(ws.del_hx), *hy = ptr<uint32_t>(ws.del_hy);
+    uint8_t *fG = ptr<uint8_t>(ws.found), *fH = fG + m;
+    uint32_t *counts = ptr<uint32_t>(ws.counts);
+    unsigned long long *sc = ptr<unsigned long long>(ws.scalars);
+    uint32_t *clen = ptr<uint32_t>(ws.nop) + n, *coff = clen + n, *noflag = coff + n;
+    uint32_t *nopos = ptr<uint32_t>(ws.flags);
+    WalkJob job{halt, ptr<uint32_t>(ws.f_src), ptr<uint32_t>(ws.f_dst), nullptr,
+                ptr<unsigned long long>(ws.f_uid), 0ull, counts + C_FILTERED, n, kDomainDecr};
+
+    if (phase0 <= 0) {
+        // deletions (gpu_graph.cuh:338-458): G first, then H for edges found in G
+        k_del_half_edges<<<blocks(n, 256), 256, 0, st>>>(halt, src, dst, n, G->g.n, hx, hy,
+                                                          sc + S_ERR);
+        count_launch();
+        DYG_TRY(delete_enqueue(G, hx, hy, m, nullptr, fG, halt, st));
+        DYG_TRY(delete_enqueue(H, hx, hy, m, fG, fH, halt, st));
+        k_del_filter<<<blocks(n, 256), 256, 0, st>>>(halt, fG, fH, n, ptr<uint32_t>(ws.flags),
+                                                      status, cond);
+        count_launch();
+        DYG_TRY(exclusive_scan_u32(ws, ptr<uint32_t>(ws.flags), ptr<uint32_t>(ws.pos), n, st));
+        k_del_compact<<<blocks(n, 256), 256, 0, st>>>(
+            halt, hx, hy, n, ptr<uint32_t>(ws.flags), ptr<uint32_t>(ws.pos), uid0,
+            ptr<uint32_t>(ws.f_src), ptr<uint32_t>(ws.f_dst), ptr<unsigned long long>(ws.f_uid),
+            ptr<uint32_t>(ws.f_idx), counts + C_FILTERED);
+        count_launch();
+        // walks on the updated G (main.cu:392, 420); F stays on the device
+        unsigned long long *keys = ptr<unsigned long long>(ws.keys);
+        DYG_CUDA(cudaMemsetAsync(keys, 0, sizeof(unsigned long long) * n, st));
+        DYG_TRY(launch_walk(G, job, p, false, keys, st));
+        DYG_TRY(launch_winner_paths(G, job, p, keys, n, stride, ptr<uint32_t>(ws.path_v),
+                                    ptr<float>(ws.path_w), ptr<int32_t>(ws.path_len), st));
+        k_decr_results<<<blocks(n, 256), 256, 0, st>>>(halt, keys, ptr<int32_t>(ws.path_len),
+                                                        ptr<uint32_t>(ws.f_idx), counts + C_FILTERED,
+                                                        n, status, cond, clen, noflag);
+        count_launch();
+        DYG_TRY(exclusive_scan_u32(ws, clen, coff, n, st));
+        DYG_TRY(exclusive_scan_u32(ws, noflag, nopos, n, st));
+        k_path_cands<<<blocks(n, 256), 256, 0, st>>>(halt, ptr<uint32_t>(ws.path_v),
+                                                      ptr<float>(ws.path_w), stride, clen, coff, n,
+                                                      noflag, nopos, ptr<uint32_t>(ws.cand_x),
+                                                      ptr<uint32_t>(ws.cand_y), ptr<float>(ws.cand_w),
+                                                      ptr<uint32_t>(ws.nop), counts, hwk);
+        count_launch();
+        DYG_CUDA(cudaGetLastError());
+    }
+    if (phase0 <= 1) {
+        // path recovery (gpu_graph.cuh:514-552)
+        DYG_TRY(recover_enqueue(G, H, ptr<uint32_t>(ws.cand_x), ptr<uint32_t>(ws.cand_y),
+                                ptr<float>(ws.cand_w), counts + C_CANDS, n * (stride - 1u),
+                                DYG_REC_PATH, halt, batch, 1, st));
+    }
+    if (hwk > 0) {
+        // fallback walks for the edges without a path (main.cu:400-408, 428-436)
+        const uint32_t hm = n * 4u * hwk;
+        DYG_TRY(ensure(ws.cand_x, sizeof(uint32_t) * (size_t)hm));
+        DYG_TRY(ensure(ws.cand_y, sizeof(uint32_t) * (size_t)hm));
+        DYG_TRY(ensure(ws.cand_w, sizeof(float) * (size_t)hm));
+        DYG_TRY(launch_fallback_walks(G, halt, ptr<uint32_t>(ws.f_src), ptr<uint32_t>(ws.f_dst),
+                                      ptr<unsigned long long>(ws.f_uid), ptr<uint32_t>(ws.nop),
+                                      counts + C_NOPATH, n, p, ptr<uint32_t>(ws.cand_x),
+                                      ptr<uint32_t>(ws.cand_y), ptr<float>(ws.cand_w), st));
+        DYG_TRY(recover_enqueue(G, H, ptr<uint32_t>(ws.cand_x), ptr<uint32_t>(ws.cand_y),
+                                ptr<float>(ws.cand_w), counts + C_CANDS2, hm, DYG_REC_FALLBACK,
+                                halt, batch, 2, st));
+    }
+    return DYG_OK;
+}
+
+// --------------------------------------------------------- stream drivers
+
+namespace {
+
+struct HaltInfo {
+    uint32_t batch, kind, phase;
+};
+
+HaltInfo decode_halt(unsigned long long h) {
+    return HaltInfo{(uint32_t)(h >> 8) - 1u, (uint32_t)((h >> 4) & 0xF), (uint32_t)(h & 0xF)};
+}
+
+dyg_status clear_halt(dyg_graph *D, cudaStream_t st) {
+    DYG_CUDA(cudaMemsetAsync(ptr<unsigned long long>(D->ws.scalars) + S_HALT, 0,
+                             sizeof(unsigned long long), st));
+    return DYG_OK;
+}
+
+dyg_status grow_for_halt(dyg_graph *A, dyg_graph *B, cudaStream_t st) {
+    DYG_TRY(grow_arena(A, A->g.arena_cap * 2, st));
+    if (B) DYG_TRY(grow_arena(B, B->g.arena_cap * 2, st));
+    return DYG_OK;
+}
+
+}  // namespace
+
+dyg_status incremental_run(dyg_graph *H, dyg_graph *G, const uint32_t *src, const uint32_t *dst,
+                           const float *w, uint32_t n, uint32_t B, uint64_t uid_base,
+                           const dyg_walk_params &p, int32_t *found, float *cond, uint8_t *acc,
+                           cudaStream_t st) {
+    unsigned long long *halt = ptr<unsigned long long>(H->ws.scalars) + S_HALT;
+    DYG_TRY(clear_halt(H, st));
+    uint32_t b_start = 0;
+    for (int round = 0; round < 64; ++round) {
+        for (uint32_t b = b_start; (uint64_t)b * B < n; ++b) {
+            const uint32_t b0 = b * B, nb = (n - b0 < B) ? n - b0 : B;
+            DYG_TRY(incr_enqueue(H, G, src + b0, dst + b0, w + b0, nb, uid_base + b0, p, halt, b,
+                                 found ? found + b0 : nullptr, cond ? cond + b0 : nullptr,
+                                 acc ? acc + b0 : nullptr, st));
+        }
+        DYG_TRY(read_scalars2(H, G, st));
+        const unsigned long long h = H->ws.host_scalars[S_HALT];
+        if (!h) return DYG_OK;
+        const HaltInfo hi = decode_halt(h);
+        DYG_TRY(grow_for_halt(H, G, st));
+        DYG_TRY(clear_halt(H, st));
+        b_start = hi.batch;   // nothing of the halted batch changed: redo it whole
+    }
+    set_error("incremental stream: too many arena regrowths");
+    return DYG_ENOMEM;
+}
+
+dyg_status decremental_run(dyg_graph *G, dyg_graph *H, const uint32_t *src, const uint32_t *dst,
+                           uint32_t n, uint32_t B, uint64_t uid_base, const dyg_walk_params &p,
+                           int32_t *status, float *cond, uint64_t *n_rec, cudaStream_t st) {
+    Workspace &ws = G->ws;
+    unsigned long long *sc = ptr<unsigned long long>(ws.scalars);
+    unsigned long long *halt = sc + S_HALT;
+    // record buffers: start at 4 per deletion, grown on demand (halt + resume)
+    const uint64_t want = (uint64_t)n * 4 + 1024;
+    DYG_TRY(ensure(ws.rx2, sizeof(uint32_t) * want));
+    DYG_TRY(ensure(ws.ry2, sizeof(uint32_t) * want));
+    DYG_TRY(ensure(ws.rk2, want));
+    uint64_t cap = ws.rx2.bytes / 4;
+    if (ws.ry2.bytes / 4 < cap) cap = ws.ry2.bytes / 4;
+    if (ws.rk2.bytes < cap) cap = ws.rk2.bytes;
+    unsigned long long init[2] = {0ull, cap};   // S_RECCNT, S_RECCAP
+    DYG_CUDA(cudaMemcpyAsync(sc + S_RECCNT, init, sizeof(init), cudaMemcpyHostToDevice, st));
+    DYG_TRY(clear_halt(G, st));
+    uint32_t b_start = 0, ph_start = 0;
+    for (int round = 0; round < 64; ++round) {
+        for (uint32_t b = b_start; (uint64_t)b * B < n; ++b) {
+            const uint32_t b0 = b * B, nb = (n - b0 < B) ? n - b0 : B;
+            DYG_TRY(decr_enqueue(G, H, src + b0, dst + b0, nb, uid_base + b0, p, halt, b,
+                                 b == b_start ? ph_start : 0, status + b0, cond + b0, st));
+        }
+        DYG_TRY(read_scalars2(G, H, st));
+        const unsigned long long h = ws.host_scalars[S_HALT];
+        if (!h) {
+            *n_rec = ws.host_scalars[S_RECCNT];
+            return DYG_OK;
+        }
+        const HaltInfo hi = decode_halt(h);
+        if (hi.kind == kHaltRecords) {
+            const uint64_t used = ws.host_scalars[S_RECCNT];
+            const uint64_t ncap = cap * 2;
+            DYG_TRY(grow_keep(ws.rx2, sizeof(uint32_t) * ncap, sizeof(uint32_t) * used, st));
+            DYG_TRY(grow_keep(ws.ry2, sizeof(uint32_t) * ncap, sizeof(uint32_t) * used, st));
+            DYG_TRY(grow_keep(ws.rk2, ncap, used, st));
+            cap = ncap;
+            DYG_CUDA(cudaMemcpyAsync(sc + S_RECCAP, &cap, sizeof(cap), cudaMemcpyHostToDevice, st));
+            DYG_CUDA(cudaStreamSynchronize(st));
+        } else {
+            DYG_TRY(grow_arena(H, H->g.arena_cap * 2, st));
+        }
+        DYG_TRY(clear_halt(G, st));
+        b_start = hi.batch;
+        ph_start = hi.phase;   // deletions and walks of this batch are done: resume there
+    }
+    set_error("decremental stream: too many buffer regrowths");
+    return DYG_ENOMEM;
+}
+
+}  // namespace dyg

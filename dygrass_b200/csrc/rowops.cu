@@ -1,0 +1,322 @@
+// rowops.cu -- device-driven row updates of the dynamic CSR.
+//
+// Both operations take a half-edge list (row hx[i], column hy[i], weight
+// hw[i], i < m) whose length may live on the device, and apply it in list
+// order per row without sorting the list:
+//   append: each entry takes a rank in its row with an atomic counter; the
+//           row's leader (rank 0) sizes the row, moves it when it overflows,
+//           and after the entries have written themselves into the row's tail
+//           restores list order in that tail (the list index rides in the
+//           slot's second word until then).  Row order is therefore exactly
+//           the order the reference's host loop produces
+//           (random_walk_incremental/gpu_graph.cuh:297-329).
+//   delete: entries of a row are gathered into a scratch run, sorted by list
+//           index, and removed one by one with swap-with-last
+//           (random_walk_decremental/gpu_graph.cuh:359-399).
+// Arena space for the moves of one or two graphs is reserved by one thread,
+// all or nothing.  When it does not fit, that thread writes a halt code; every
+// kernel that changes a graph (and every kernel of the batch pipelines) then
+// returns at once, and the host grows the arena and resumes the stream at the
+// halted phase.  Nothing here needs a host-visible count, so a whole update
+// stream is enqueued with a single synchronize at its end.
+#include "dyg_internal.cuh"
+
+namespace dyg {
+
+namespace {
+
+__device__ __forceinline__ uint32_t dcount(const uint32_t *dev, uint32_t host) {
+    return dev ? min(*dev, host) : host;
+}
+
+__global__ void k_rank(DevGraph g, const uint32_t *hx, const uint32_t *m_dev, uint32_t m_host,
+                       uint32_t *rank, uint32_t *rowcnt, const unsigned long long *halt,
+                       unsigned long long *ran) {
+    if (*halt) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && ran) *ran = 1ull;
+    const uint32_t m = dcount(m_dev, m_host);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        const uint32_t x = hx[i];
+        rank[i] = (x < g.n) ? atomicAdd(rowcnt + x, 1u) : 0xFFFFFFFFu;
+    }
+}
+
+// ------------------------------------------------------------------ append
+
+__global__ void k_app_need(DevGraph g, const uint32_t *hx, const uint32_t *m_dev, uint32_t m_host,
+                           const uint32_t *rank, const uint32_t *rowcnt, uint32_t slack,
+                           uint32_t *lneed, unsigned long long *need_total,
+                           const unsigned long long *halt) {
+    if (*halt) return;
+    const uint32_t m = dcount(m_dev, m_host);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        if (rank[i] != 0u) continue;
+        const uint32_t x = hx[i];
+        const uint2 d = g.desc[x];
+        const uint32_t nd = d.y + rowcnt[x];
+        uint32_t need = 0u;
+        if (nd > g.cap[x]) {
+            need = max(2u * nd, nd + slack);
+            need = (need + 1u) & ~1u;
+            atomicAdd(need_total, (unsigned long long)need);
+        }
+        lneed[i] = need;
+    }
+}
+
+// One thread: reserve both graphs' moves or halt.
+__global__ void k_reserve(unsigned long long *top1, uint64_t cap1, const unsigned long long *need1,
+                          unsigned long long *cursor1, unsigned long long *top2, uint64_t cap2,
+                          const unsigned long long *need2, unsigned long long *cursor2,
+                          unsigned long long *halt, unsigned long long code) {
+    if (*halt) return;
+    const bool ok1 = *top1 + *need1 <= cap1;
+    const bool ok2 = !top2 || *top2 + *need2 <= cap2;
+    if (!(ok1 && ok2)) {
+        *halt = code;
+        return;
+    }
+    *cursor1 = *top1;
+    *top1 += *need1;
+    if (top2) {
+        *cursor2 = *top2;
+        *top2 += *need2;
+    }
+}
+
+__global__ void k_app_move(DevGraph g, const uint32_t *hx, const uint32_t *m_dev, uint32_t m_host,
+                           const uint32_t *rank, const uint32_t *lneed, unsigned long long *cursor,
+                           const unsigned long long *halt) {
+    if (*halt) return;
+    const uint32_t m = dcount(m_dev, m_host);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        if (rank[i] != 0u || lneed[i] == 0u) continue;
+        const uint32_t x = hx[i];
+        const uint2 d = g.desc[x];
+        const uint32_t off = (uint32_t)atomicAdd(cursor, (unsigned long long)lneed[i]);
+        for (uint32_t j = 0; j < d.y; ++j) {
+            g.slots[off + j] = g.slots[d.x + j];
+            g.wts[off + j] = g.wts[d.x + j];
+        }
+        g.cap[x] = lneed[i];
+        g.desc[x] = make_uint2(off, d.y);
+    }
+}
+
+__global__ void k_app_write(DevGraph g, const uint32_t *hx, const uint32_t *hy, const float *hw,
+                            const uint32_t *m_dev, uint32_t m_host, const uint32_t *rank,
+                            const unsigned long long *halt) {
+    if (*halt) return;
+    const uint32_t m = dcount(m_dev, m_host);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        const uint32_t x = hx[i];
+        if (x >= g.n) continue;
+        const uint2 d = g.desc[x];
+        const uint32_t pos = d.x + d.y + rank[i];
+        g.slots[pos] = make_uint2(hy[i], i);   // list index until the tail is ordered
+        g.wts[pos] = hw[i];
+    }
+}
+
+// Leaders order their row's new tail by list index, store 1/w in place of the
+// index, publish the degree and clear the row counter (also after a halt, if
+// this operation's ranks were taken).
+__global__ void k_app_finish(DevGraph g, const uint32_t *hx, const uint32_t *m_dev,
+                             uint32_t m_host, const uint32_t *rank, uint32_t *rowcnt,
+                             const unsigned long long *halt, const unsigned long long *ran) {
+    const bool halted = *halt != 0ull;
+    if (halted && !*ran) return;
+    const uint32_t m = dcount(m_dev, m_host);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        if (rank[i] != 0u) continue;
+        const uint32_t x = hx[i];
+        const uint32_t cnt = rowcnt[x];
+        rowcnt[x] = 0u;
+        if (halted) continue;
+        const uint2 d = g.desc[x];
+        const uint32_t base = d.x + d.y;
+        for (uint32_t a = 1; a < cnt; ++a) {   // insertion sort by list index
+            const uint2 s = g.slots[base + a];
+            const float w = g.wts[base + a];
+            uint32_t b = a;
+            while (b > 0 && g.slots[base + b - 1].y > s.y) {
+                g.slots[base + b] = g.slots[base + b - 1];
+                g.wts[base + b] = g.wts[base + b - 1];
+                --b;
+            }
+            g.slots[base + b] = s;
+            g.wts[base + b] = w;
+        }
+        for (uint32_t a = 0; a < cnt; ++a)
+            g.slots[base + a].y = __float_as_uint(__frcp_rn(g.wts[base + a]));
+        g.desc[x] = make_uint2(d.x, d.y + cnt);
+    }
+}
+
+// ------------------------------------------------------------------ delete
+
+__global__ void k_del_base(DevGraph g, const uint32_t *hx, uint32_t m, const uint32_t *rank,
+                           const uint32_t *rowcnt, uint32_t *rowtmp, unsigned long long *cursor,
+                           const unsigned long long *halt) {
+    if (*halt) return;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        if (rank[i] != 0u) continue;
+        const uint32_t x = hx[i];
+        rowtmp[x] = (uint32_t)atomicAdd(cursor, (unsigned long long)rowcnt[x]);
+    }
+}
+
+__global__ void k_del_scatter(DevGraph g, const uint32_t *hx, uint32_t m, const uint32_t *rank,
+                              const uint32_t *rowtmp, uint32_t *tmp,
+                              const unsigned long long *halt) {
+    if (*halt) return;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        const uint32_t x = hx[i];
+        if (x < g.n) tmp[rowtmp[x] + rank[i]] = i;
+    }
+}
+
+// Leaders remove their row's entries in list order.  With `mask`, entry
+// i = 2e + side is applied only if edge e was found on both sides of `mask`.
+__global__ void k_del_apply(DevGraph g, const uint32_t *hx, const uint32_t *hy, uint32_t m,
+                            const uint32_t *rank, uint32_t *rowcnt, const uint32_t *rowtmp,
+                            uint32_t *tmp, const uint8_t *mask, uint8_t *found,
+                            const unsigned long long *halt) {
+    if (*halt) return;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        if (rank[i] != 0u) continue;
+        const uint32_t x = hx[i];
+        const uint32_t cnt = rowcnt[x];
+        rowcnt[x] = 0u;
+        uint32_t *run = tmp + rowtmp[x];
+        for (uint32_t a = 1; a < cnt; ++a) {
+            const uint32_t v = run[a];
+            uint32_t b = a;
+            while (b > 0 && run[b - 1] > v) {
+                run[b] = run[b - 1];
+                --b;
+            }
+            run[b] = v;
+        }
+        const uint2 d = g.desc[x];
+        uint32_t deg = d.y;
+        for (uint32_t a = 0; a < cnt; ++a) {
+            const uint32_t k = run[a];
+            if (mask && !(mask[k & ~1u] && mask[k | 1u])) continue;
+            const uint32_t y = hy[k];
+            for (uint32_t j = 0; j < deg; ++j) {
+                if (g.slots[d.x + j].x == y) {
+                    g.slots[d.x + j] = g.slots[d.x + deg - 1u];
+                    g.wts[d.x + j] = g.wts[d.x + deg - 1u];
+                    --deg;
+                    found[k] = 1;
+                    break;
+                }
+            }
+        }
+        g.desc[x] = make_uint2(d.x, deg);
+    }
+}
+
+int grid_for(uint64_t m) {
+    const uint64_t b = (m + 255) / 256;
+    const uint64_t cap = (uint64_t)num_sms() * 8;
+    return (int)(b < 1 ? 1 : (b > cap ? cap : b));
+}
+
+}  // namespace
+
+dyg_status rowops_ensure(dyg_graph *G, uint32_t m_host) {
+    Workspace &ws = G->ws;
+    DYG_TRY(ensure(ws.rank, sizeof(uint32_t) * (size_t)(m_host ? m_host : 1)));
+    DYG_TRY(ensure(ws.lneed, sizeof(uint32_t) * (size_t)(m_host ? m_host : 1)));
+    DYG_TRY(ensure(ws.dtmp, sizeof(uint32_t) * (size_t)(m_host ? m_host : 1)));
+    if (!ws.rowcnt.p) {
+        DYG_TRY(ensure(ws.rowcnt, sizeof(uint32_t) * (size_t)(G->g.n ? G->g.n : 1)));
+        DYG_TRY(ensure(ws.rowtmp, sizeof(uint32_t) * (size_t)(G->g.n ? G->g.n : 1)));
+        DYG_CUDA(cudaMemset(ws.rowcnt.p, 0, ws.rowcnt.bytes));
+    }
+    return DYG_OK;
+}
+
+// Appends list A to graph GA and (optionally) list B to GB; the arena space
+// of both is reserved together, so either both appends happen or neither
+// (halt = code).
+dyg_status append_enqueue(dyg_graph *GA, const AppendList &A, dyg_graph *GB, const AppendList *B,
+                          unsigned long long *halt, unsigned long long code, cudaStream_t st) {
+    dyg_graph *gs[2] = {GA, B ? GB : nullptr};
+    const AppendList *ls[2] = {&A, B};
+    for (int k = 0; k < 2; ++k) {
+        dyg_graph *G = gs[k];
+        if (!G) continue;
+        DYG_TRY(rowops_ensure(G, ls[k]->m_host));
+        unsigned long long *sc = ptr<unsigned long long>(G->ws.scalars);
+        DYG_CUDA(cudaMemsetAsync(sc + S_NEED, 0, sizeof(unsigned long long) * 2, st));  // need, cursor
+        DYG_CUDA(cudaMemsetAsync(sc + S_OPRAN, 0, sizeof(unsigned long long), st));
+        if (ls[k]->m_host == 0) continue;
+        const int gr = grid_for(ls[k]->m_host);
+        k_rank<<<gr, 256, 0, st>>>(G->g, ls[k]->hx, ls[k]->m_dev, ls[k]->m_host,
+                                   ptr<uint32_t>(G->ws.rank), ptr<uint32_t>(G->ws.rowcnt), halt,
+                                   sc + S_OPRAN);
+        count_launch();
+        k_app_need<<<gr, 256, 0, st>>>(G->g, ls[k]->hx, ls[k]->m_dev, ls[k]->m_host,
+                                       ptr<uint32_t>(G->ws.rank), ptr<uint32_t>(G->ws.rowcnt),
+                                       G->slack, ptr<uint32_t>(G->ws.lneed), sc + S_NEED, halt);
+        count_launch();
+    }
+    unsigned long long *s1 = ptr<unsigned long long>(GA->ws.scalars);
+    unsigned long long *s2 = gs[1] ? ptr<unsigned long long>(gs[1]->ws.scalars) : nullptr;
+    k_reserve<<<1, 1, 0, st>>>(GA->g.top, GA->g.arena_cap, s1 + S_NEED, s1 + S_CURSOR,
+                               s2 ? gs[1]->g.top : nullptr, s2 ? gs[1]->g.arena_cap : 0,
+                               s2 ? s2 + S_NEED : nullptr, s2 ? s2 + S_CURSOR : nullptr, halt, code);
+    count_launch();
+    for (int k = 0; k < 2; ++k) {
+        dyg_graph *G = gs[k];
+        if (!G || ls[k]->m_host == 0) continue;
+        unsigned long long *sc = ptr<unsigned long long>(G->ws.scalars);
+        const int gr = grid_for(ls[k]->m_host);
+        k_app_move<<<gr, 256, 0, st>>>(G->g, ls[k]->hx, ls[k]->m_dev, ls[k]->m_host,
+                                       ptr<uint32_t>(G->ws.rank), ptr<uint32_t>(G->ws.lneed),
+                                       sc + S_CURSOR, halt);
+        count_launch();
+        k_app_write<<<gr, 256, 0, st>>>(G->g, ls[k]->hx, ls[k]->hy, ls[k]->hw, ls[k]->m_dev,
+                                        ls[k]->m_host, ptr<uint32_t>(G->ws.rank), halt);
+        count_launch();
+        k_app_finish<<<gr, 256, 0, st>>>(G->g, ls[k]->hx, ls[k]->m_dev, ls[k]->m_host,
+                                         ptr<uint32_t>(G->ws.rank), ptr<uint32_t>(G->ws.rowcnt),
+                                         halt, sc + S_OPRAN);
+        count_launch();
+    }
+    DYG_CUDA(cudaGetLastError());
+    return DYG_OK;
+}
+
+// Deletes the half-edges of a list whose length m is known on the host.
+dyg_status delete_enqueue(dyg_graph *G, const uint32_t *hx, const uint32_t *hy, uint32_t m,
+                          const uint8_t *mask, uint8_t *found, unsigned long long *halt,
+                          cudaStream_t st) {
+    if (m == 0) return DYG_OK;
+    DYG_TRY(rowops_ensure(G, m));
+    unsigned long long *sc = ptr<unsigned long long>(G->ws.scalars);
+    DYG_CUDA(cudaMemsetAsync(sc + S_TMPCUR, 0, sizeof(unsigned long long), st));
+    DYG_CUDA(cudaMemsetAsync(found, 0, m, st));
+    const int gr = grid_for(m);
+    k_rank<<<gr, 256, 0, st>>>(G->g, hx, nullptr, m, ptr<uint32_t>(G->ws.rank),
+                               ptr<uint32_t>(G->ws.rowcnt), halt, nullptr);
+    count_launch();
+    k_del_base<<<gr, 256, 0, st>>>(G->g, hx, m, ptr<uint32_t>(G->ws.rank),
+                                   ptr<uint32_t>(G->ws.rowcnt), ptr<uint32_t>(G->ws.rowtmp),
+                                   sc + S_TMPCUR, halt);
+    count_launch();
+    k_del_scatter<<<gr, 256, 0, st>>>(G->g, hx, m, ptr<uint32_t>(G->ws.rank),
+                                      ptr<uint32_t>(G->ws.rowtmp), ptr<uint32_t>(G->ws.dtmp), halt);
+    count_launch();
+    k_del_apply<<<gr, 256, 0, st>>>(G->g, hx, hy, m, ptr<uint32_t>(G->ws.rank),
+                                    ptr<uint32_t>(G->ws.rowcnt), ptr<uint32_t>(G->ws.rowtmp),
+                                    ptr<uint32_t>(G->ws.dtmp), mask, found, halt);
+    count_launch();
+    DYG_CUDA(cudaGetLastError());
+    return DYG_OK;
+}
+
+}  // namespace dyg

@@ -168,6 +168,7 @@ __device__ __forceinline__ int step_once(Walker &s, const uint2 *__restrict__ de
 
 template <bool INCR, bool WEIGHTED>
 __global__ void __launch_bounds__(kWalkThreads) k_walk(WalkArgs a) {
+    if (a.job.halt && *a.job.halt) return;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
     const uint32_t n = a.job.n_dev ? *a.job.n_dev : a.job.n_host;
@@ -296,6 +297,7 @@ template <bool WEIGHTED>
 __global__ void k_winner_paths(DevGraph g, WalkJob job, uint32_t max_steps, uint2 key,
                                const unsigned long long *keys, uint32_t stride, uint32_t *pv,
                                float *pw, int32_t *plen, unsigned long long *scalars) {
+    if (job.halt && *job.halt) return;
     const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t n = job.n_dev ? *job.n_dev : job.n_host;
     if (f >= n) return;
@@ -343,12 +345,14 @@ __global__ void k_winner_paths(DevGraph g, WalkJob job, uint32_t max_steps, uint
 // (random_walk_decremental/main.cu:243-290, with the second step reading the
 // row of the vertex the walker stands on).  Candidate pair 2i, 2i+1 of item
 // i = (q * 2 + side) * hw + j is (s0, x1), (x1, x2); x = ~0u marks none.
-__global__ void k_fallback(DevGraph g, const uint32_t *f_src, const uint32_t *f_dst,
-                           const unsigned long long *f_uid, const uint32_t *nop, uint32_t n_nop,
-                           uint32_t hw, uint2 key, uint32_t *cx, uint32_t *cy, float *cw) {
+__global__ void k_fallback(DevGraph g, const unsigned long long *halt, const uint32_t *f_src,
+                           const uint32_t *f_dst, const unsigned long long *f_uid,
+                           const uint32_t *nop, const uint32_t *n_nop_dev, uint32_t hw, uint2 key,
+                           uint32_t *cx, uint32_t *cy, float *cw) {
+    if (halt && *halt) return;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t per = 2u * hw;
-    if (i >= n_nop * per) return;
+    if (i >= *n_nop_dev * per) return;
     const uint32_t q = i / per, rem = i - q * per, side = rem / hw, j = rem - side * hw;
     const uint32_t f = nop[q];
     const uint32_t s0 = side ? f_dst[f] : f_src[f];
@@ -508,17 +512,19 @@ dyg_status launch_winner_paths(dyg_graph *G, const WalkJob &job, const dyg_walk_
     return DYG_OK;
 }
 
-dyg_status launch_fallback_walks(dyg_graph *G, const uint32_t *f_src, const uint32_t *f_dst,
+dyg_status launch_fallback_walks(dyg_graph *G, const unsigned long long *halt,
+                                 const uint32_t *f_src, const uint32_t *f_dst,
                                  const unsigned long long *f_uid, const uint32_t *nop,
-                                 uint32_t n_nop, const dyg_walk_params &p, uint32_t *cx,
-                                 uint32_t *cy, float *cw, cudaStream_t st) {
-    const uint32_t items = n_nop * 2u * p.heuristic_walkers;
+                                 const uint32_t *n_nop_dev, uint32_t n_nop_max,
+                                 const dyg_walk_params &p, uint32_t *cx, uint32_t *cy, float *cw,
+                                 cudaStream_t st) {
+    const uint64_t items = (uint64_t)n_nop_max * 2u * p.heuristic_walkers;
     if (items == 0) return DYG_OK;
     const uint2 key = make_uint2((uint32_t)p.seed, (uint32_t)(p.seed >> 32));
     const int threads = 128;
     ProfScope prof(2, st);
-    k_fallback<<<(items + threads - 1) / threads, threads, 0, st>>>(
-        G->g, f_src, f_dst, f_uid, nop, n_nop, p.heuristic_walkers, key, cx, cy, cw);
+    k_fallback<<<(unsigned)((items + threads - 1) / threads), threads, 0, st>>>(
+        G->g, halt, f_src, f_dst, f_uid, nop, n_nop_dev, p.heuristic_walkers, key, cx, cy, cw);
     count_launch();
     DYG_CUDA(cudaGetLastError());
     return DYG_OK;

@@ -185,6 +185,36 @@ def test_mesh_incremental_then_decremental(dyg, oracle):
     assert (st > 0).sum() > 0 and (st == -2).sum() > 0
 
 
+@pytest.mark.parametrize("slack,headroom", [(0, 0.0), (1, 0.05)])
+def test_tight_arenas_resume(dyg, oracle, slack, headroom):
+    """Arenas with no room: appends halt the stream, the host grows the arena
+    and resumes; recovered-edge records overflow their first buffer the same
+    way.  Results must not change."""
+    W = small_mesh(k=10, inserts=300)
+    gs = np.concatenate([W.g_src, W.ins_src])
+    gd = np.concatenate([W.g_dst, W.ins_dst])
+    gw = np.concatenate([W.g_w, W.ins_w])
+    H = dyg.Graph.from_edges(W.n, W.h_src, W.h_dst, W.h_w, slack_per_row=slack,
+                             arena_headroom=headroom)
+    G = dyg.Graph.from_edges(W.n, W.g_src, W.g_dst, W.g_w, slack_per_row=slack,
+                             arena_headroom=headroom)
+    Ho = oracle.OGraph(W.n, W.h_src, W.h_dst, W.h_w)
+    Go = oracle.OGraph(W.n, W.g_src, W.g_dst, W.g_w)
+    r = dyg.incremental_stream(H, W.ins_src, W.ins_dst, W.ins_w, W.params, G=G)
+    fa, cd, ac, _ = oracle.incremental(Ho, W.ins_src, W.ins_dst, W.ins_w, W.params, G=Go)
+    assert np.array_equal(r.accepted, ac) and np.array_equal(r.found_at, fa)
+    same_graph(H, Ho)
+    same_graph(G, Go)
+    d = dyg.decremental_stream(G, H, W.del_src, W.del_dst, W.dparams)
+    st, cd2, rx, ry, rk, _ = oracle.decremental(Go, Ho, W.del_src, W.del_dst, W.dparams)
+    assert np.array_equal(d.status, st)
+    assert np.array_equal(d.rec_src, rx) and np.array_equal(d.rec_dst, ry)
+    assert np.array_equal(d.rec_kind, rk)
+    assert len(rx) > 4 * len(W.del_src) // 10    # more than one record buffer's worth per batch
+    same_graph(G, Go)
+    same_graph(H, Ho)
+
+
 def test_mesh_exhaustive_and_pruned_agree(dyg, oracle):
     """Pruning changes only how many moves run, never a result."""
     W = small_mesh(k=10, inserts=300)
