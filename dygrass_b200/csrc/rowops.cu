@@ -155,14 +155,33 @@ __global__ void k_app_finish(DevGraph g, const uint32_t *hx, const uint32_t *m_d
 
 // ------------------------------------------------------------------ delete
 
+// Leaders take a run of `rowcnt[x]` scratch entries.  One atomic per warp:
+// the warp's requests are prefix-summed with shuffles, lane 31 takes the sum.
 __global__ void k_del_base(DevGraph g, const uint32_t *hx, uint32_t m, const uint32_t *rank,
                            const uint32_t *rowcnt, uint32_t *rowtmp, unsigned long long *cursor,
                            const unsigned long long *halt) {
     if (*halt) return;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
-        if (rank[i] != 0u) continue;
-        const uint32_t x = hx[i];
-        rowtmp[x] = (uint32_t)atomicAdd(cursor, (unsigned long long)rowcnt[x]);
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    // every lane of a warp runs the same number of iterations
+    const uint32_t first = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t warp0 = first - lane;
+    for (uint32_t base = warp0; base < m; base += stride) {
+        const uint32_t i = base + lane;
+        const bool lead = i < m && rank[i] == 0u;
+        const uint32_t x = lead ? hx[i] : 0u;
+        const uint32_t want = lead ? rowcnt[x] : 0u;
+        uint32_t incl = want;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t v = __shfl_up_sync(kFull, incl, d);
+            if (lane >= (uint32_t)d) incl += v;
+        }
+        const uint32_t total = __shfl_sync(kFull, incl, 31);
+        unsigned long long start = 0ull;
+        if (lane == 31u && total) start = atomicAdd(cursor, (unsigned long long)total);
+        start = __shfl_sync(kFull, start, 31);
+        if (lead) rowtmp[x] = (uint32_t)start + incl - want;
     }
 }
 
