@@ -172,7 +172,7 @@ void free_graph(dyg_graph *G) {
                    &ws.out_cond, &ws.out_acc, &ws.out_status, &ws.cub_tmp, &ws.s_src, &ws.s_dst,
                    &ws.s_w, &ws.s_o1, &ws.s_o2, &ws.s_o3, &ws.rx2, &ws.ry2, &ws.rk2,
                    &ws.rank, &ws.lneed, &ws.dtmp, &ws.rowcnt, &ws.rowtmp, &ws.tmask,
-                   &ws.del_hx, &ws.del_hy, &ws.scalars, &ws.counts};
+                   &ws.del_hx, &ws.del_hy, &ws.nopos, &ws.scalars, &ws.counts};
     for (Buf *b : bufs) free_buf(*b);
     if (ws.host_scalars) cudaFreeHost(ws.host_scalars);
     if (ws.host_counts) cudaFreeHost(ws.host_counts);

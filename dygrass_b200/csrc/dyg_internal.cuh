@@ -134,6 +134,7 @@ struct Workspace {
     Buf rowcnt, rowtmp;                       // row operations: per-row counter / run base
     Buf tmask;                                // dedup table size (device)
     Buf del_hx, del_hy;                       // deletion half-edges
+    Buf nopos;                                // no-path positions
     Buf scalars;                              // u64 scalars (see Scalar)
     Buf counts;                               // u32 counts (see Count)
     unsigned long long *host_scalars = nullptr;   // pinned mirror
@@ -163,6 +164,8 @@ enum Count : int {
     C_NOPATH = 3,     // decremental: edges without a path
     C_ACCEPTED = 4,   // incremental: accepted edges
     C_CANDS2 = 5,     // fallback candidates
+    C_RANGE = 6,      // walk-list entries of the current range
+    C_WALKLIST = 7,   // stream insertions left to walk
     C_NCOUNTS = 8
 };
 

@@ -132,6 +132,13 @@ __global__ void k_del_compact(const unsigned long long *halt, const uint32_t *hx
     f_idx[f] = e;
 }
 
+__global__ void k_range_count(const unsigned long long *halt, const uint32_t *F_dev, uint32_t f0,
+                              uint32_t nf, uint32_t *out) {
+    if (HALTED(halt)) return;
+    const uint32_t F = *F_dev;
+    *out = F > f0 ? min(F - f0, nf) : 0u;
+}
+
 // Per filtered edge: status / conductance, path-candidate counts and the
 // no-path flags (zero for f >= F).
 __global__ void k_decr_results(const unsigned long long *halt, const unsigned long long *keys,
@@ -141,7 +148,7 @@ __global__ void k_decr_results(const unsigned long long *halt, const unsigned lo
     if (HALTED(halt)) return;
     const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= n) return;
-    const uint32_t F = *F_dev;
+    const uint32_t F = F_dev ? *F_dev : n;
     if (f >= F) {
         clen[f] = 0;
         noflag[f] = 0;
@@ -430,16 +437,16 @@ dyg_status incr_enqueue(dyg_graph *H, dyg_graph *G, const uint32_t *src, const u
                           halt_code(batch, (uint32_t)kHaltArena, 0), st);
 }
 
-// Enqueues decremental batch `batch` from phase `phase0`.  status/cond
-// (device, length n) receive the per-deletion results.
-dyg_status decr_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src, const uint32_t *dst,
-                        uint32_t n, uint64_t uid0, const dyg_walk_params &p,
-                        unsigned long long *halt, uint32_t batch, uint32_t phase0,
-                        int32_t *status, float *cond, cudaStream_t st) {
+// Deletion stage of a decremental batch: delete every edge from G (swap with
+// the row's last slot, in input order), erase the ones also in H, and compact
+// the edges found in both into the walk list f_* (gpu_graph.cuh:338-458).
+// status/cond (device, length n) get the per-deletion codes.
+dyg_status decr_delete_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src,
+                               const uint32_t *dst, uint32_t n, uint64_t uid0,
+                               unsigned long long *halt, int32_t *status, float *cond,
+                               cudaStream_t st) {
     Workspace &ws = G->ws;
     const uint32_t m = 2u * n;
-    const uint32_t stride = p.max_steps > 2 ? p.max_steps : 2;
-    const uint32_t hwk = p.heuristic_walkers;
     DYG_TRY(ensure(ws.del_hx, sizeof(uint32_t) * (size_t)m));
     DYG_TRY(ensure(ws.del_hy, sizeof(uint32_t) * (size_t)m));
     DYG_TRY(ensure(ws.found, (size_t)m * 2));
@@ -449,48 +456,74 @@ dyg_status decr_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src, const u
     DYG_TRY(ensure(ws.f_dst, sizeof(uint32_t) * n));
     DYG_TRY(ensure(ws.f_idx, sizeof(uint32_t) * n));
     DYG_TRY(ensure(ws.f_uid, sizeof(unsigned long long) * n));
+    uint32_t *hx = ptr<uint32_t>(ws.del_hx), *hy = ptr<uint32_t>(ws.del_hy);
+    uint8_t *fG = ptr<uint8_t>(ws.found), *fH = fG + m;
+    uint32_t *counts = ptr<uint32_t>(ws.counts);
+    unsigned long long *sc = ptr<unsigned long long>(ws.scalars);
+    k_del_half_edges<<<blocks(n, 256), 256, 0, st>>>(halt, src, dst, n, G->g.n, hx, hy,
+                                                      sc + S_ERR);
+    count_launch();
+    DYG_TRY(delete_enqueue(G, hx, hy, m, nullptr, fG, halt, st));
+    DYG_TRY(delete_enqueue(H, hx, hy, m, fG, fH, halt, st));
+    k_del_filter<<<blocks(n, 256), 256, 0, st>>>(halt, fG, fH, n, ptr<uint32_t>(ws.flags), status,
+                                                  cond);
+    count_launch();
+    DYG_TRY(exclusive_scan_u32(ws, ptr<uint32_t>(ws.flags), ptr<uint32_t>(ws.pos), n, st));
+    k_del_compact<<<blocks(n, 256), 256, 0, st>>>(
+        halt, hx, hy, n, ptr<uint32_t>(ws.flags), ptr<uint32_t>(ws.pos), uid0,
+        ptr<uint32_t>(ws.f_src), ptr<uint32_t>(ws.f_dst), ptr<unsigned long long>(ws.f_uid),
+        ptr<uint32_t>(ws.f_idx), counts + C_FILTERED);
+    count_launch();
+    DYG_CUDA(cudaGetLastError());
+    return DYG_OK;
+}
+
+// Walk-and-recover stage over walk-list entries [f0, f0 + nf) (nf a host
+// bound; F_dev, if given, is the device count of the whole list), from phase
+// `phase0` (0 = walks, 1 = path recovery, 2 = fallback).
+dyg_status decr_walk_enqueue(dyg_graph *G, dyg_graph *H, uint32_t f0, uint32_t nf,
+                             const uint32_t *F_dev, const dyg_walk_params &p,
+                             unsigned long long *halt, uint32_t batch, uint32_t phase0,
+                             int32_t *status, float *cond, cudaStream_t st) {
+    if (nf == 0) return DYG_OK;
+    Workspace &ws = G->ws;
+    const uint32_t n = nf;
+    const uint32_t stride = p.max_steps > 2 ? p.max_steps : 2;
+    const uint32_t hwk = p.heuristic_walkers;
     DYG_TRY(ensure(ws.keys, sizeof(unsigned long long) * n));
     DYG_TRY(ensure(ws.path_v, sizeof(uint32_t) * (size_t)n * stride));
     DYG_TRY(ensure(ws.path_w, sizeof(float) * (size_t)n * stride));
     DYG_TRY(ensure(ws.path_len, sizeof(int32_t) * n));
     DYG_TRY(ensure(ws.nop, sizeof(uint32_t) * (size_t)n * 4));
+    DYG_TRY(ensure(ws.nopos, sizeof(uint32_t) * (size_t)n));
     DYG_TRY(ensure(ws.cand_x, sizeof(uint32_t) * (size_t)n * stride));
     DYG_TRY(ensure(ws.cand_y, sizeof(uint32_t) * (size_t)n * stride));
     DYG_TRY(ensure(ws.cand_w, sizeof(float) * (size_t)n * stride));
-    uint32_t *hx = ptr<uint32_t>(ws.del_hx), *hy = ptr<uint32_t>(ws.del_hy);
-    uint8_t *fG = ptr<uint8_t>(ws.found), *fH = fG + m;
     uint32_t *counts = ptr<uint32_t>(ws.counts);
-    unsigned long long *sc = ptr<unsigned long long>(ws.scalars);
     uint32_t *clen = ptr<uint32_t>(ws.nop) + n, *coff = clen + n, *noflag = coff + n;
-    uint32_t *nopos = ptr<uint32_t>(ws.flags);
-    WalkJob job{halt, ptr<uint32_t>(ws.f_src), ptr<uint32_t>(ws.f_dst), nullptr,
-                ptr<unsigned long long>(ws.f_uid), 0ull, counts + C_FILTERED, n, kDomainDecr};
+    uint32_t *nopos = ptr<uint32_t>(ws.nopos);
+    const uint32_t *fsrc = ptr<uint32_t>(ws.f_src) + f0, *fdst = ptr<uint32_t>(ws.f_dst) + f0;
+    const unsigned long long *fuid = ptr<unsigned long long>(ws.f_uid) + f0;
+    const uint32_t *fidx = ptr<uint32_t>(ws.f_idx) + f0;
+    // device count of this range: min(F - f0, nf) when F lives on the device
+    const uint32_t *cnt_dev = nullptr;
+    if (F_dev) {
+        k_range_count<<<1, 1, 0, st>>>(halt, F_dev, f0, nf, counts + C_RANGE);
+        count_launch();
+        cnt_dev = counts + C_RANGE;
+    }
+    WalkJob job{halt, fsrc, fdst, nullptr, fuid, 0ull, cnt_dev, n, kDomainDecr};
 
     if (phase0 <= 0) {
-        // deletions (gpu_graph.cuh:338-458): G first, then H for edges found in G
-        k_del_half_edges<<<blocks(n, 256), 256, 0, st>>>(halt, src, dst, n, G->g.n, hx, hy,
-                                                          sc + S_ERR);
-        count_launch();
-        DYG_TRY(delete_enqueue(G, hx, hy, m, nullptr, fG, halt, st));
-        DYG_TRY(delete_enqueue(H, hx, hy, m, fG, fH, halt, st));
-        k_del_filter<<<blocks(n, 256), 256, 0, st>>>(halt, fG, fH, n, ptr<uint32_t>(ws.flags),
-                                                      status, cond);
-        count_launch();
-        DYG_TRY(exclusive_scan_u32(ws, ptr<uint32_t>(ws.flags), ptr<uint32_t>(ws.pos), n, st));
-        k_del_compact<<<blocks(n, 256), 256, 0, st>>>(
-            halt, hx, hy, n, ptr<uint32_t>(ws.flags), ptr<uint32_t>(ws.pos), uid0,
-            ptr<uint32_t>(ws.f_src), ptr<uint32_t>(ws.f_dst), ptr<unsigned long long>(ws.f_uid),
-            ptr<uint32_t>(ws.f_idx), counts + C_FILTERED);
-        count_launch();
-        // walks on the updated G (main.cu:392, 420); F stays on the device
+        // walks on the updated G (main.cu:392, 420)
         unsigned long long *keys = ptr<unsigned long long>(ws.keys);
         DYG_CUDA(cudaMemsetAsync(keys, 0, sizeof(unsigned long long) * n, st));
         DYG_TRY(launch_walk(G, job, p, false, keys, st));
         DYG_TRY(launch_winner_paths(G, job, p, keys, n, stride, ptr<uint32_t>(ws.path_v),
                                     ptr<float>(ws.path_w), ptr<int32_t>(ws.path_len), st));
         k_decr_results<<<blocks(n, 256), 256, 0, st>>>(halt, keys, ptr<int32_t>(ws.path_len),
-                                                        ptr<uint32_t>(ws.f_idx), counts + C_FILTERED,
-                                                        n, status, cond, clen, noflag);
+                                                        fidx, cnt_dev, n, status, cond, clen,
+                                                        noflag);
         count_launch();
         DYG_TRY(exclusive_scan_u32(ws, clen, coff, n, st));
         DYG_TRY(exclusive_scan_u32(ws, noflag, nopos, n, st));
@@ -514,8 +547,7 @@ dyg_status decr_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src, const u
         DYG_TRY(ensure(ws.cand_x, sizeof(uint32_t) * (size_t)hm));
         DYG_TRY(ensure(ws.cand_y, sizeof(uint32_t) * (size_t)hm));
         DYG_TRY(ensure(ws.cand_w, sizeof(float) * (size_t)hm));
-        DYG_TRY(launch_fallback_walks(G, halt, ptr<uint32_t>(ws.f_src), ptr<uint32_t>(ws.f_dst),
-                                      ptr<unsigned long long>(ws.f_uid), ptr<uint32_t>(ws.nop),
+        DYG_TRY(launch_fallback_walks(G, halt, fsrc, fdst, fuid, ptr<uint32_t>(ws.nop),
                                       counts + C_NOPATH, n, p, ptr<uint32_t>(ws.cand_x),
                                       ptr<uint32_t>(ws.cand_y), ptr<float>(ws.cand_w), st));
         DYG_TRY(recover_enqueue(G, H, ptr<uint32_t>(ws.cand_x), ptr<uint32_t>(ws.cand_y),
@@ -523,6 +555,17 @@ dyg_status decr_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src, const u
                                 halt, batch, 2, st));
     }
     return DYG_OK;
+}
+
+// Decremental batch `batch` of the standalone updater: deletion stage, then
+// walks over the batch's whole walk list.
+dyg_status decr_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src, const uint32_t *dst,
+                        uint32_t n, uint64_t uid0, const dyg_walk_params &p,
+                        unsigned long long *halt, uint32_t batch, uint32_t phase0,
+                        int32_t *status, float *cond, cudaStream_t st) {
+    if (phase0 <= 0) DYG_TRY(decr_delete_enqueue(G, H, src, dst, n, uid0, halt, status, cond, st));
+    return decr_walk_enqueue(G, H, 0, n, ptr<uint32_t>(G->ws.counts) + C_FILTERED, p, halt, batch,
+                             phase0, status, cond, st);
 }
 
 // --------------------------------------------------------- stream drivers

@@ -158,6 +158,88 @@ uint64_t dyg_synth_lattice_inserts(uint32_t nx, uint32_t ny, uint32_t nz, uint64
     return k;
 }
 
+static inline void rmat_pair(SplitMix &r, uint32_t scale, double a, double b, double c,
+                             uint32_t *u, uint32_t *v) {
+    uint32_t x = 0, y = 0;
+    for (uint32_t l = 0; l < scale; ++l) {
+        const double p = r.unit();
+        uint32_t bx = 0, by = 0;
+        if (p < a) {
+        } else if (p < a + b) {
+            by = 1;
+        } else if (p < a + b + c) {
+            bx = 1;
+        } else {
+            bx = by = 1;
+        }
+        x = (x << 1) | bx;
+        y = (y << 1) | by;
+    }
+    *u = x;
+    *v = y;
+}
+
+void dyg_synth_rmat_pairs(uint32_t scale, uint64_t count, double a, double b, double c,
+                          uint64_t seed, uint32_t *src, uint32_t *dst) {
+    SplitMix r(seed);
+    for (uint64_t i = 0; i < count; ++i) rmat_pair(r, scale, a, b, c, &src[i], &dst[i]);
+}
+
+uint64_t dyg_synth_rmat(uint32_t scale, uint32_t edge_factor, double a, double b, double c,
+                        float wlo, float whi, uint64_t seed, uint32_t *n_out, uint32_t **src,
+                        uint32_t **dst, float **w, uint32_t **id_map) {
+    const uint64_t nv = 1ull << scale;
+    const uint64_t m0 = (uint64_t)edge_factor * nv;
+    SplitMix r(seed);
+    std::vector<uint64_t> keys;
+    keys.reserve(m0);
+    for (uint64_t i = 0; i < m0; ++i) {
+        uint32_t u, v;
+        rmat_pair(r, scale, a, b, c, &u, &v);
+        if (u == v) continue;
+        if (u > v) std::swap(u, v);
+        keys.push_back(((uint64_t)u << 32) | v);
+    }
+    std::sort(keys.begin(), keys.end());
+    keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+    DSU dsu((uint32_t)nv);
+    for (uint64_t k : keys) dsu.unite((uint32_t)(k >> 32), (uint32_t)k);
+    std::vector<uint32_t> size(nv, 0);
+    std::vector<uint8_t> touched(nv, 0);
+    for (uint64_t k : keys) {
+        touched[k >> 32] = 1;
+        touched[(uint32_t)k] = 1;
+    }
+    for (uint64_t v = 0; v < nv; ++v)
+        if (touched[v]) size[dsu.find((uint32_t)v)]++;
+    uint32_t best = 0;
+    for (uint64_t v = 0; v < nv; ++v)
+        if (size[v] > size[best]) best = (uint32_t)v;
+    uint32_t *map = (uint32_t *)malloc(sizeof(uint32_t) * nv);
+    uint32_t n = 0;
+    for (uint64_t v = 0; v < nv; ++v)
+        map[v] = (touched[v] && dsu.find((uint32_t)v) == best) ? n++ : 0xFFFFFFFFu;
+    uint64_t m = 0;
+    for (uint64_t k : keys)
+        if (map[k >> 32] != 0xFFFFFFFFu) ++m;
+    *src = (uint32_t *)malloc(sizeof(uint32_t) * (m ? m : 1));
+    *dst = (uint32_t *)malloc(sizeof(uint32_t) * (m ? m : 1));
+    *w = (float *)malloc(sizeof(float) * (m ? m : 1));
+    SplitMix rw(seed ^ 0x5bd1e995ull);
+    uint64_t j = 0;
+    for (uint64_t k : keys) {
+        const uint32_t u = map[k >> 32], v = map[(uint32_t)k];
+        if (u == 0xFFFFFFFFu) continue;
+        (*src)[j] = u;
+        (*dst)[j] = v;
+        (*w)[j] = draw_weight(rw, DYG_W_UNIFORM, wlo, whi);
+        ++j;
+    }
+    *n_out = n;
+    *id_map = map;
+    return m;
+}
+
 void dyg_synth_sample(uint64_t m, uint64_t k, uint64_t seed, uint64_t *out_idx) {
     if (k > m) k = m;
     SplitMix r(seed);

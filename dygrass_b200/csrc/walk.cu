@@ -268,8 +268,10 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(WalkArgs a) {
             // R only grows along a walk and 1/R is monotone, so a walker whose
             // 1/R is already below its edge's best success can neither win
             // nor tie: stopping it leaves every result unchanged.
-            ce_best = max(ce_best, __reduce_max_sync(kFull, (fc && my_e == ce) ? fc : 0u));
-            pe_best = max(pe_best, __reduce_max_sync(kFull, (fc && my_e == pe) ? fc : 0u));
+            if (__any_sync(kFull, fc != 0u)) {
+                ce_best = max(ce_best, __reduce_max_sync(kFull, (fc && my_e == ce) ? fc : 0u));
+                pe_best = max(pe_best, __reduce_max_sync(kFull, (fc && my_e == pe) ? fc : 0u));
+            }
             if (active) {
                 if ((s.step & 3u) == 0u)
                     gbest = max(gbest, (uint32_t)(*(volatile unsigned long long *)(a.keys + my_e) >> 32));

@@ -43,6 +43,20 @@ uint64_t dyg_synth_lattice_inserts(uint32_t nx, uint32_t ny, uint32_t nz, uint64
                                    float hi, uint64_t seed, uint32_t *out_src, uint32_t *out_dst,
                                    float *out_w);
 
+/* R-MAT graph (Chakrabarti, Zhan, Faloutsos, SDM'04): 2^scale ids,
+ * edge_factor * 2^scale generated pairs, quadrant probabilities a, b, c
+ * (d = 1 - a - b - c), symmetrised (u < v), deduplicated, self-loops dropped,
+ * restricted to the largest connected component and relabelled 0..n-1 in id
+ * order; weights U[wlo, whi).  Edges are sorted by (u, v).  *src, *dst, *w and
+ * *id_map (2^scale entries: new id or 0xFFFFFFFF) are malloc'ed (free with
+ * dyg_mtx_free).  Returns the edge count; *n_out = vertex count. */
+uint64_t dyg_synth_rmat(uint32_t scale, uint32_t edge_factor, double a, double b, double c,
+                        float wlo, float whi, uint64_t seed, uint32_t *n_out, uint32_t **src,
+                        uint32_t **dst, float **w, uint32_t **id_map);
+/* `count` further R-MAT pairs in the original id space (no filtering). */
+void dyg_synth_rmat_pairs(uint32_t scale, uint64_t count, double a, double b, double c,
+                          uint64_t seed, uint32_t *src, uint32_t *dst);
+
 /* k distinct indices of [0, m) in uniformly random order. */
 void dyg_synth_sample(uint64_t m, uint64_t k, uint64_t seed, uint64_t *out_idx);
 
