@@ -31,6 +31,10 @@ DEL_NOT_IN_H = -2
 DEL_NO_PATH = -1
 REC_PATH = 0
 REC_FALLBACK = 1
+STREAM_INSERT = 0
+STREAM_DELETE = 1
+INS_MERGED = -4
+INS_SELF_LOOP = -5
 
 
 class DygError(RuntimeError):
@@ -96,6 +100,15 @@ def lib() -> C.CDLL:
                                    C.POINTER(u64), vp], C.c_int),
         "dyg_decremental_stream": ([vp, vp, vp, vp, u32, u32, C.POINTER(WalkParams), vp, vp, vp, vp, vp, u64,
                                     C.POINTER(u64), vp], C.c_int),
+        "dyg_stream_default_chunk": ([u32], u32),
+        "dyg_stream_file": ([vp, vp, u32, vp, vp, vp, u32, u64, u32, C.POINTER(WalkParams), vp, vp, vp,
+                             vp, vp, u64, C.POINTER(u64), vp], C.c_int),
+        "dyg_synth_rmat": ([u32, u32, C.c_double, C.c_double, C.c_double, C.c_float, C.c_float, u64,
+                            C.POINTER(u32), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
+                            C.POINTER(vp)], u64),
+        "dyg_synth_rmat_pairs": ([u32, u64, C.c_double, C.c_double, C.c_double, u64, vp, vp], None),
+        "dyg_synth_rmat_stream": ([u32, C.c_double, C.c_double, C.c_double, vp, u64, vp, vp, u64, u32,
+                                   C.c_double, C.c_float, C.c_float, u64, vp, vp, vp, vp], u64),
         "dyg_mtx_read": ([C.c_char_p, u32, C.c_int, C.POINTER(u64), C.POINTER(vp), C.POINTER(vp),
                           C.POINTER(vp), C.POINTER(u32)], C.c_int),
         "dyg_mtx_free": ([vp], None),
@@ -329,6 +342,39 @@ def decremental_stream(G: Graph, H: Graph, src, dst, params: WalkParams, batch_s
                         rec_cap)
 
 
+def stream_default_chunk(n_vertices: int) -> int:
+    """Walk-list chunk of the mixed updater: 5% of |V|, at least 10000."""
+    return int(lib().dyg_stream_default_chunk(int(n_vertices)))
+
+
+def stream_file(G: Graph, H: Graph, op: int, src, dst, w, params: WalkParams,
+                first_update_id: int = 0, chunk: int = 0, stream: int | None = None,
+                rec_cap: int | None = None) -> DecrementalResult:
+    """One file of the mixed insert/delete stream (dyg_stream_file).
+
+    op STREAM_INSERT: status = found_at / -1 (accepted) / INS_MERGED /
+    INS_SELF_LOOP; op STREAM_DELETE: status = path length / DEL_* codes, plus
+    the recovered edges.  w may be None for delete files."""
+    src, dst = _as(src, np.uint32), _as(dst, np.uint32)
+    w = None if w is None else _as(w, np.float32)
+    n = len(src)
+    if rec_cap is None:
+        rec_cap = 0 if op == STREAM_INSERT else n * (params.max_steps + 4 * params.heuristic_walkers) + 16
+    st = np.empty(n, np.int32)
+    cd = np.empty(n, np.float32)
+    rx = np.empty(max(rec_cap, 1), np.uint32)
+    ry = np.empty(max(rec_cap, 1), np.uint32)
+    rk = np.empty(max(rec_cap, 1), np.uint8)
+    nrec = C.c_uint64()
+    _check(lib().dyg_stream_file(G.handle, H.handle, int(op), _ptr(src), _ptr(dst), _ptr(w), n,
+                                 int(first_update_id), int(chunk), C.byref(params), _ptr(st),
+                                 _ptr(cd), _ptr(rx), _ptr(ry), _ptr(rk), int(rec_cap),
+                                 C.byref(nrec), stream), "dyg_stream_file")
+    k = nrec.value
+    return DecrementalResult(st, cd, rx[:k].copy(), ry[:k].copy(), rk[:k].copy())
+
+
 __all__ = ["Graph", "WalkParams", "GraphOpts", "DygError", "incremental_batch",
            "incremental_stream", "decremental_batch", "decremental_stream", "lib", "version",
-           "reference_batch_size", "IncrementalResult", "DecrementalResult"]
+           "reference_batch_size", "IncrementalResult", "DecrementalResult", "stream_file",
+           "stream_default_chunk"]

@@ -19,7 +19,7 @@ LIB = os.path.join(PKG, "libdygrass.so")
 BIN_INCR = os.path.join(PKG, "bin", "incremental_update")
 BIN_DECR = os.path.join(PKG, "bin", "decremental_update")
 
-CUDA_SOURCES = ["walk.cu", "graph.cu", "rowops.cu", "pipeline.cu", "capi.cu", "noalloc.cu"]
+CUDA_SOURCES = ["walk.cu", "graph.cu", "rowops.cu", "pipeline.cu", "capi.cu", "noalloc.cu", "stream.cu"]
 HOST_SOURCES = ["synth.cpp", "mtx_io.cpp"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

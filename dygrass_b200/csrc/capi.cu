@@ -164,15 +164,13 @@ void free_graph(dyg_graph *G) {
     if (!G) return;
     DeviceGuard dg(G->device);
     Workspace &ws = G->ws;
-    Buf *bufs[] = {&ws.in_src, &ws.in_dst, &ws.in_w, &ws.keys, &ws.work, &ws.flags, &ws.pos,
-                   &ws.f_src, &ws.f_dst, &ws.f_idx, &ws.f_uid, &ws.found, &ws.hx, &ws.hy,
-                   &ws.hw, &ws.hseq, &ws.skeys, &ws.svals, &ws.need, &ws.path_v, &ws.path_w,
+    Buf *bufs[] = {&ws.keys, &ws.flags, &ws.pos, &ws.f_src, &ws.f_dst, &ws.f_idx, &ws.f_uid,
+                   &ws.f_w, &ws.found, &ws.hx, &ws.hy, &ws.hw, &ws.path_v, &ws.path_w,
                    &ws.path_len, &ws.cand_x, &ws.cand_y, &ws.cand_w, &ws.keep, &ws.htab_k,
-                   &ws.htab_v, &ws.nop, &ws.rec_x, &ws.rec_y, &ws.rec_k, &ws.out_found,
-                   &ws.out_cond, &ws.out_acc, &ws.out_status, &ws.cub_tmp, &ws.s_src, &ws.s_dst,
-                   &ws.s_w, &ws.s_o1, &ws.s_o2, &ws.s_o3, &ws.rx2, &ws.ry2, &ws.rk2,
-                   &ws.rank, &ws.lneed, &ws.dtmp, &ws.rowcnt, &ws.rowtmp, &ws.tmask,
-                   &ws.del_hx, &ws.del_hy, &ws.nopos, &ws.scalars, &ws.counts};
+                   &ws.htab_v, &ws.nop, &ws.cub_tmp, &ws.s_src, &ws.s_dst, &ws.s_w, &ws.s_o1,
+                   &ws.s_o2, &ws.s_o3, &ws.rx2, &ws.ry2, &ws.rk2, &ws.rank, &ws.lneed, &ws.dtmp,
+                   &ws.rowcnt, &ws.rowtmp, &ws.tmask, &ws.del_hx, &ws.del_hy, &ws.nopos,
+                   &ws.st_key, &ws.st_val, &ws.st_pos, &ws.st_wapp, &ws.scalars, &ws.counts};
     for (Buf *b : bufs) free_buf(*b);
     if (ws.host_scalars) cudaFreeHost(ws.host_scalars);
     if (ws.host_counts) cudaFreeHost(ws.host_counts);
@@ -618,6 +616,77 @@ dyg_status dyg_decremental_stream(dyg_graph *G, dyg_graph *H, const uint32_t *sr
                                   uint64_t rec_cap, uint64_t *n_rec, dyg_stream_t stream) {
     return decremental_common(G, H, src, dst, n, batch_size, 0, p, status, conductance, rec_src,
                               rec_dst, rec_kind, rec_cap, n_rec, stream);
+}
+
+uint32_t dyg_stream_default_chunk(uint32_t n_vertices) {
+    return stream_default_chunk(n_vertices);
+}
+
+dyg_status dyg_stream_file(dyg_graph *G, dyg_graph *H, uint32_t op, const uint32_t *src,
+                           const uint32_t *dst, const float *w, uint32_t n,
+                           uint64_t first_update_id, uint32_t chunk, const dyg_walk_params *p,
+                           int32_t *status, float *conductance, uint32_t *rec_src,
+                           uint32_t *rec_dst, uint8_t *rec_kind, uint64_t rec_cap,
+                           uint64_t *n_rec, dyg_stream_t stream) {
+    set_error("");
+    const bool ins = op == DYG_STREAM_INSERT;
+    if (!G || !H || (n && (!src || !dst || (ins && !w)))) {
+        set_error("NULL argument");
+        return DYG_EINVAL;
+    }
+    if (op != DYG_STREAM_INSERT && op != DYG_STREAM_DELETE) {
+        set_error("op must be DYG_STREAM_INSERT or DYG_STREAM_DELETE");
+        return DYG_EINVAL;
+    }
+    DYG_TRY(check_params(p));
+    if (G->g.n != H->g.n || G->device != H->device) {
+        set_error("G and H must have the same vertex count and device");
+        return DYG_EINVAL;
+    }
+    if (n_rec) *n_rec = 0;
+    if (n == 0) return DYG_OK;
+    DeviceGuard dg(G->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    DYG_TRY(check_host_ids(src, n, G->g.n, "src"));
+    DYG_TRY(check_host_ids(dst, n, G->g.n, "dst"));
+    if (ins) DYG_TRY(check_host_weights(w, n));
+    Workspace &ws = G->ws;
+    const uint32_t *d_src, *d_dst;
+    const float *d_w = nullptr;
+    DYG_TRY(stage_in(ws.s_src, src, n, st, &d_src));
+    DYG_TRY(stage_in(ws.s_dst, dst, n, st, &d_dst));
+    if (ins) DYG_TRY(stage_in(ws.s_w, w, n, st, &d_w));
+    int32_t *o_st = status && on_device(status) ? status : nullptr;
+    float *o_cd = conductance && on_device(conductance) ? conductance : nullptr;
+    if (!o_st) {
+        DYG_TRY(ensure(ws.s_o1, sizeof(int32_t) * n));
+        o_st = ptr<int32_t>(ws.s_o1);
+    }
+    if (!o_cd) {
+        DYG_TRY(ensure(ws.s_o2, sizeof(float) * n));
+        o_cd = ptr<float>(ws.s_o2);
+    }
+    uint64_t total = 0;
+    DYG_TRY(stream_file_run(G, H, op, d_src, d_dst, d_w, n, first_update_id, chunk, *p, o_st, o_cd,
+                            &total, st));
+    if (G->ws.host_scalars[S_ERR]) DYG_TRY(check_device_errors(G, st));
+    bool host_out = false;
+    if (status && o_st != status) DYG_TRY(copy_out(status, (const int32_t *)o_st, n, st, &host_out));
+    if (conductance && o_cd != conductance)
+        DYG_TRY(copy_out(conductance, (const float *)o_cd, n, st, &host_out));
+    const uint64_t nout = total < rec_cap ? total : rec_cap;
+    if (!ins) {
+        DYG_TRY(copy_out(rec_src, (const uint32_t *)ptr<uint32_t>(ws.rx2), nout, st, &host_out));
+        DYG_TRY(copy_out(rec_dst, (const uint32_t *)ptr<uint32_t>(ws.ry2), nout, st, &host_out));
+        DYG_TRY(copy_out(rec_kind, (const uint8_t *)ptr<uint8_t>(ws.rk2), nout, st, &host_out));
+    }
+    if (host_out) DYG_CUDA(cudaStreamSynchronize(st));
+    if (n_rec) *n_rec = total;
+    if (total > rec_cap && (rec_src || rec_dst || rec_kind)) {
+        set_error("more recovered edges than rec_cap");
+        return DYG_ERANGE;
+    }
+    return DYG_OK;
 }
 
 }  // extern "C"

@@ -108,24 +108,19 @@ struct Buf {
 };
 
 struct Workspace {
-    Buf in_src, in_dst, in_w;                 // staged batch inputs
     Buf keys;                                 // u64 per edge
-    Buf work;                                 // u64 counters: [0] work chunks
     Buf flags, pos;                           // u32 per edge
-    Buf f_src, f_dst, f_idx;                  // filtered deletions
-    Buf f_uid;                                // u64 per filtered edge
+    Buf f_src, f_dst, f_idx;                  // walk list (filtered deletions / new insertions)
+    Buf f_uid;                                // u64 per walk-list entry
+    Buf f_w;                                  // f32 per walk-list entry (insertions)
     Buf found;                                // u8 per half-edge
-    Buf hx, hy, hw, hseq;                     // half-edge lists (u32/f32)
-    Buf skeys, svals;                         // sorted keys / values
-    Buf need;                                 // u32 per half-edge
+    Buf hx, hy, hw;                           // half-edge lists (u32/f32)
     Buf path_v, path_w;                       // winner paths
     Buf path_len;                             // i32 per filtered edge
     Buf cand_x, cand_y, cand_w;               // recovery candidates
     Buf keep;                                 // u32 per candidate
     Buf htab_k, htab_v;                       // dedup hash table
     Buf nop;                                  // u32 no-path filtered indices
-    Buf rec_x, rec_y, rec_k;                  // recovered edges (device)
-    Buf out_found, out_cond, out_acc, out_status;
     Buf cub_tmp;
     Buf s_src, s_dst, s_w, s_o1, s_o2, s_o3;  // whole-stream staging
     Buf rx2, ry2;                             // recovered edges of a whole stream
@@ -135,6 +130,9 @@ struct Workspace {
     Buf tmask;                                // dedup table size (device)
     Buf del_hx, del_hy;                       // deletion half-edges
     Buf nopos;                                // no-path positions
+    Buf st_key, st_val;                       // stream file: (min, max) keys and indices, sorted
+    Buf st_pos;                               // stream file: uint4 slot positions in G and H
+    Buf st_wapp;                              // stream file: G weight of each new edge
     Buf scalars;                              // u64 scalars (see Scalar)
     Buf counts;                               // u32 counts (see Count)
     unsigned long long *host_scalars = nullptr;   // pinned mirror
@@ -165,8 +163,9 @@ enum Count : int {
     C_ACCEPTED = 4,   // incremental: accepted edges
     C_CANDS2 = 5,     // fallback candidates
     C_RANGE = 6,      // walk-list entries of the current range
-    C_WALKLIST = 7,   // stream insertions left to walk
-    C_NCOUNTS = 8
+    C_WALKLIST = 7,   // stream file: new insertions to walk
+    C_GHALF = 8,      // stream file: half-edges of the new insertions (G append)
+    C_NCOUNTS = 12
 };
 
 // Halt codes: (batch + 1) << 8 | kind << 4 | phase.
@@ -254,6 +253,24 @@ dyg_status incremental_run(dyg_graph *H, dyg_graph *G, const uint32_t *src, cons
 dyg_status decremental_run(dyg_graph *G, dyg_graph *H, const uint32_t *src, const uint32_t *dst,
                            uint32_t n, uint32_t B, uint64_t uid_base, const dyg_walk_params &p,
                            int32_t *status, float *cond, uint64_t *n_rec, cudaStream_t st);
+
+dyg_status decr_delete_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src,
+                               const uint32_t *dst, uint32_t n, uint64_t uid0, bool file_orient,
+                               unsigned long long *halt, int32_t *status, float *cond,
+                               cudaStream_t st);
+dyg_status decr_walk_enqueue(dyg_graph *G, dyg_graph *H, uint32_t f0, uint32_t nf,
+                             const uint32_t *F_dev, const dyg_walk_params &p,
+                             unsigned long long *halt, uint32_t batch, uint32_t phase0,
+                             int32_t *status, float *cond, cudaStream_t st);
+// Grows b to `bytes`, keeping its first `used` bytes.
+dyg_status grow_keep(Buf &b, size_t bytes, size_t used, cudaStream_t st);
+
+// --- stream.cu
+uint32_t stream_default_chunk(uint32_t n_vertices);
+dyg_status stream_file_run(dyg_graph *G, dyg_graph *H, uint32_t op, const uint32_t *src,
+                           const uint32_t *dst, const float *w, uint32_t n, uint64_t uid0,
+                           uint32_t chunk, const dyg_walk_params &p, int32_t *status, float *cond,
+                           uint64_t *n_rec, cudaStream_t st);
 
 // --- graph.cu
 dyg_status upload_graph(dyg_graph *G, uint32_t n, const uint64_t *row_ptr, const uint32_t *col,

@@ -115,19 +115,21 @@ __global__ void k_del_filter(const unsigned long long *halt, const uint8_t *fG, 
     cond[e] = 0.f;
 }
 
+// Walk list entry f of deletion e: min -> max, or with osrc/odst the file
+// orientation.
 __global__ void k_del_compact(const unsigned long long *halt, const uint32_t *hx,
-                              const uint32_t *hy, uint32_t n, const uint32_t *flags,
-                              const uint32_t *pos, unsigned long long uid0, uint32_t *f_src,
-                              uint32_t *f_dst, unsigned long long *f_uid, uint32_t *f_idx,
-                              uint32_t *count) {
+                              const uint32_t *hy, const uint32_t *osrc, const uint32_t *odst,
+                              uint32_t n, const uint32_t *flags, const uint32_t *pos,
+                              unsigned long long uid0, uint32_t *f_src, uint32_t *f_dst,
+                              unsigned long long *f_uid, uint32_t *f_idx, uint32_t *count) {
     if (HALTED(halt)) return;
     const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n) return;
     if (e == n - 1) *count = pos[e] + flags[e];
     if (!flags[e]) return;
     const uint32_t f = pos[e];
-    f_src[f] = hx[2 * e];   // min
-    f_dst[f] = hy[2 * e];   // max
+    f_src[f] = osrc ? osrc[e] : hx[2 * e];
+    f_dst[f] = odst ? odst[e] : hy[2 * e];
     f_uid[f] = uid0 + e;
     f_idx[f] = e;
 }
@@ -322,19 +324,6 @@ __global__ void k_rec_advance(const unsigned long long *halt, const uint32_t *co
     sc[S_RECCNT] += counts[C_KEPT] / 2u;
 }
 
-dyg_status grow_keep(Buf &b, size_t bytes, size_t used, cudaStream_t st) {
-    if (b.bytes >= bytes) return DYG_OK;
-    Buf nb;
-    DYG_TRY(ensure(nb, bytes));
-    if (used && b.p) {
-        DYG_CUDA(cudaMemcpyAsync(nb.p, b.p, used, cudaMemcpyDeviceToDevice, st));
-        DYG_CUDA(cudaStreamSynchronize(st));
-    }
-    if (b.p) cudaFree(b.p);
-    b = nb;
-    return DYG_OK;
-}
-
 // Dedup + membership + ordered append of one candidate list (phase 1 or 2).
 dyg_status recover_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *cx, const uint32_t *cy,
                            const float *cw, const uint32_t *M_dev, uint32_t M_host, uint8_t kind,
@@ -390,6 +379,19 @@ dyg_status recover_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *cx, const
 
 }  // namespace
 
+dyg_status grow_keep(Buf &b, size_t bytes, size_t used, cudaStream_t st) {
+    if (b.bytes >= bytes) return DYG_OK;
+    Buf nb;
+    DYG_TRY(ensure(nb, bytes));
+    if (used && b.p) {
+        DYG_CUDA(cudaMemcpyAsync(nb.p, b.p, used, cudaMemcpyDeviceToDevice, st));
+        DYG_CUDA(cudaStreamSynchronize(st));
+    }
+    if (b.p) cudaFree(b.p);
+    b = nb;
+    return DYG_OK;
+}
+
 // ------------------------------------------------------------ batches
 
 // Enqueues incremental batch `batch` (edges src/dst/w[0, n), update ids
@@ -439,10 +441,12 @@ dyg_status incr_enqueue(dyg_graph *H, dyg_graph *G, const uint32_t *src, const u
 
 // Deletion stage of a decremental batch: delete every edge from G (swap with
 // the row's last slot, in input order), erase the ones also in H, and compact
-// the edges found in both into the walk list f_* (gpu_graph.cuh:338-458).
+// the edges found in both into the walk list f_* (gpu_graph.cuh:338-458), each
+// walked min -> max (random_walk_decremental/gpu_graph.cuh:342) or, with
+// file_orient, src -> dst (dynamic_update/gpu_graph.cuh:874-875).
 // status/cond (device, length n) get the per-deletion codes.
 dyg_status decr_delete_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src,
-                               const uint32_t *dst, uint32_t n, uint64_t uid0,
+                               const uint32_t *dst, uint32_t n, uint64_t uid0, bool file_orient,
                                unsigned long long *halt, int32_t *status, float *cond,
                                cudaStream_t st) {
     Workspace &ws = G->ws;
@@ -470,7 +474,8 @@ dyg_status decr_delete_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src,
     count_launch();
     DYG_TRY(exclusive_scan_u32(ws, ptr<uint32_t>(ws.flags), ptr<uint32_t>(ws.pos), n, st));
     k_del_compact<<<blocks(n, 256), 256, 0, st>>>(
-        halt, hx, hy, n, ptr<uint32_t>(ws.flags), ptr<uint32_t>(ws.pos), uid0,
+        halt, hx, hy, file_orient ? src : nullptr, file_orient ? dst : nullptr, n,
+        ptr<uint32_t>(ws.flags), ptr<uint32_t>(ws.pos), uid0,
         ptr<uint32_t>(ws.f_src), ptr<uint32_t>(ws.f_dst), ptr<unsigned long long>(ws.f_uid),
         ptr<uint32_t>(ws.f_idx), counts + C_FILTERED);
     count_launch();
@@ -563,7 +568,8 @@ dyg_status decr_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src, const u
                         uint32_t n, uint64_t uid0, const dyg_walk_params &p,
                         unsigned long long *halt, uint32_t batch, uint32_t phase0,
                         int32_t *status, float *cond, cudaStream_t st) {
-    if (phase0 <= 0) DYG_TRY(decr_delete_enqueue(G, H, src, dst, n, uid0, halt, status, cond, st));
+    if (phase0 <= 0)
+        DYG_TRY(decr_delete_enqueue(G, H, src, dst, n, uid0, false, halt, status, cond, st));
     return decr_walk_enqueue(G, H, 0, n, ptr<uint32_t>(G->ws.counts) + C_FILTERED, p, halt, batch,
                              phase0, status, cond, st);
 }

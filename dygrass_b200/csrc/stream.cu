@@ -1,0 +1,472 @@
+// stream.cu -- one file of the mixed insert/delete edge stream
+// (dynamic_update/main.cu:96-126: preprocessStreamEdges, then walks in
+// chunks with the sparsifier updated after each chunk).
+//
+// Insert file (gpu_graph.cuh:373-396, 620-643), all on the device:
+//   probe    every edge's slot positions in G and H (rows scanned by groups
+//            of 8 lanes, the shorter row first);
+//   sort     (min, max) keys with their file indices (stable radix sort), so
+//            the occurrences of one edge sit together in file order;
+//   merge    one thread per edge group: an edge already in G adds every
+//            occurrence's weight to G (and H) in file order; a new edge's
+//            first occurrence enters G with the later occurrences' weights
+//            folded in, and is listed for walking;
+//   append   the new edges to G in file order (row order as the reference's
+//            edgeInsertion produces);
+//   chunks   of the walk list: walk H, then append the accepted edges to H
+//            with their stream weight before the next chunk walks.
+// Delete file (gpu_graph.cuh:398-431, 645-700): the whole file is deleted
+// from G and H, then the walk list is walked on G and recovered in chunks.
+// One host synchronize per file; a reservation that does not fit halts every
+// later kernel and the file resumes at the halted stage after the arena or
+// record buffers grew (nothing changed after the halt; the weight merges
+// come before any reservation and are not repeated).
+#include <cub/cub.cuh>
+
+#include "dyg_internal.cuh"
+
+namespace dyg {
+
+namespace {
+
+constexpr uint32_t kProbeLanes = 8;
+
+inline int blocks(uint64_t n, int th) { return (int)((n + th - 1) / th); }
+
+#define HALTED(h) ((h) && *(h))
+
+// Arena index of the first slot of row x holding y, or ~0u.  Called by the
+// kProbeLanes lanes of one group together (`gmask` = the group's lanes).
+__device__ __forceinline__ uint32_t group_find(const DevGraph &g, uint32_t x, uint32_t y,
+                                               uint32_t lane, uint32_t gbase, uint32_t gmask) {
+    const uint2 d = g.desc[x];
+    for (uint32_t j0 = 0; j0 < d.y; j0 += kProbeLanes) {
+        const uint32_t j = j0 + lane;
+        const bool hit = j < d.y && g.slots[d.x + j].x == y;
+        const uint32_t bits = (__ballot_sync(gmask, hit) >> gbase) & ((1u << kProbeLanes) - 1u);
+        if (bits) return d.x + j0 + (uint32_t)(__ffs(bits) - 1);
+    }
+    return ~0u;
+}
+
+// Slots of edge {a, b} in g: .x in row a, .y in row b (~0u when absent).
+__device__ __forceinline__ uint2 group_edge(const DevGraph &g, uint32_t a, uint32_t b,
+                                            uint32_t lane, uint32_t gbase, uint32_t gmask) {
+    const bool a_short = g.desc[a].y <= g.desc[b].y;
+    const uint32_t s = a_short ? a : b, l = a_short ? b : a;
+    const uint32_t ps = group_find(g, s, l, lane, gbase, gmask);
+    if (ps == ~0u) return make_uint2(~0u, ~0u);
+    const uint32_t pl = group_find(g, l, s, lane, gbase, gmask);
+    return a_short ? make_uint2(ps, pl) : make_uint2(pl, ps);
+}
+
+// One group of kProbeLanes lanes per edge: slot positions in G and H, the
+// sort key (min << nb | max) and index; self-loops and invalid endpoints get
+// key ~0 (sorted last, never merged or walked).
+__global__ void k_st_probe(const unsigned long long *halt, DevGraph G, DevGraph H,
+                           const uint32_t *src, const uint32_t *dst, uint32_t n, uint32_t nb,
+                           unsigned long long *key, uint32_t *val, uint4 *pos, uint32_t *nflag,
+                           int32_t *status, float *cond, unsigned long long *err) {
+    if (HALTED(halt)) return;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t i = t / kProbeLanes;
+    const uint32_t lane = t % kProbeLanes;
+    const uint32_t gbase = (threadIdx.x & 31u) & ~(kProbeLanes - 1u);
+    const uint32_t gmask = ((1u << kProbeLanes) - 1u) << gbase;
+    if (i >= n) return;   // whole groups leave together (n is per group)
+    uint32_t a = src[i], b = dst[i];
+    if (a > b) {
+        const uint32_t x = a;
+        a = b;
+        b = x;
+    }
+    if (a == b || b >= G.n) {
+        if (lane == 0) {
+            if (b >= G.n) atomicOr(err, (unsigned long long)kErrVertex);
+            key[i] = ~0ull;
+            val[i] = i;
+            pos[i] = make_uint4(~0u, ~0u, ~0u, ~0u);
+            nflag[i] = 0;
+            status[i] = DYG_INS_SELF_LOOP;
+            cond[i] = 0.f;
+        }
+        return;
+    }
+    const uint2 pg = group_edge(G, a, b, lane, gbase, gmask);
+    const uint2 ph = group_edge(H, a, b, lane, gbase, gmask);
+    if (lane == 0) {
+        key[i] = ((unsigned long long)a << nb) | b;
+        val[i] = i;
+        pos[i] = make_uint4(pg.x, pg.y, ph.x, ph.y);
+        nflag[i] = 0;
+    }
+}
+
+__device__ __forceinline__ void set_weight(DevGraph &g, uint32_t slot, float w) {
+    g.wts[slot] = w;
+    g.slots[slot].y = __float_as_uint(__frcp_rn(w));
+}
+
+// One thread per group of equal keys (dynamic_update/gpu_graph.cuh:373-396,
+// 452-465): weights are folded in file order, one float add per occurrence.
+__global__ void k_st_merge(const unsigned long long *halt, DevGraph G, DevGraph H,
+                           const unsigned long long *skey, const uint32_t *sval, uint32_t n,
+                           const uint4 *pos, const float *w, uint32_t *nflag, float *wapp,
+                           int32_t *status, float *cond) {
+    if (HALTED(halt)) return;
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const unsigned long long k = skey[j];
+    if (k == ~0ull || (j > 0 && skey[j - 1] == k)) return;
+    uint32_t e = j + 1;
+    while (e < n && skey[e] == k) ++e;
+    const uint32_t i0 = sval[j];
+    const uint4 p = pos[i0];
+    const bool inH = p.z != ~0u;
+    float ha = inH ? H.wts[p.z] : 0.f, hb = (inH && p.w != ~0u) ? H.wts[p.w] : 0.f;
+    if (p.x != ~0u) {
+        // already in G: every occurrence adds its weight to G and (if there) H
+        float ga = G.wts[p.x], gb = p.y != ~0u ? G.wts[p.y] : 0.f;
+        for (uint32_t q = j; q < e; ++q) {
+            const uint32_t i = sval[q];
+            const float wi = w[i];
+            ga = __fadd_rn(ga, wi);
+            gb = __fadd_rn(gb, wi);
+            if (inH) {
+                ha = __fadd_rn(ha, wi);
+                hb = __fadd_rn(hb, wi);
+            }
+            status[i] = DYG_INS_MERGED;
+            cond[i] = 0.f;
+        }
+        set_weight(G, p.x, ga);
+        if (p.y != ~0u) set_weight(G, p.y, gb);
+    } else {
+        // new: the first occurrence enters G and is walked; the later ones
+        // add their weights to its G copy (and to H's, if H has the edge)
+        float wa = w[i0];
+        for (uint32_t q = j + 1; q < e; ++q) {
+            const uint32_t i = sval[q];
+            const float wi = w[i];
+            wa = __fadd_rn(wa, wi);
+            if (inH) {
+                ha = __fadd_rn(ha, wi);
+                hb = __fadd_rn(hb, wi);
+            }
+            status[i] = DYG_INS_MERGED;
+            cond[i] = 0.f;
+        }
+        nflag[i0] = 1u;
+        wapp[i0] = wa;
+    }
+    if (inH) {
+        set_weight(H, p.z, ha);
+        if (p.w != ~0u) set_weight(H, p.w, hb);
+    }
+}
+
+// New edges in file order: the walk list (file orientation, stream weight)
+// and G's half-edges (src gets dst, dst gets src; merged weight).
+__global__ void k_st_compact(const unsigned long long *halt, const uint32_t *src,
+                             const uint32_t *dst, const float *w, uint32_t n,
+                             const uint32_t *nflag, const uint32_t *npos, const float *wapp,
+                             unsigned long long uid0, uint32_t *f_src, uint32_t *f_dst,
+                             float *f_w, unsigned long long *f_uid, uint32_t *f_idx, uint32_t *hx,
+                             uint32_t *hy, float *hw, uint32_t *counts) {
+    if (HALTED(halt)) return;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (i == n - 1) {
+        const uint32_t tot = npos[i] + nflag[i];
+        counts[C_WALKLIST] = tot;
+        counts[C_GHALF] = 2u * tot;
+    }
+    if (!nflag[i]) return;
+    const uint32_t q = npos[i];
+    const uint32_t u = src[i], v = dst[i];
+    f_src[q] = u;
+    f_dst[q] = v;
+    f_w[q] = w[i];
+    f_uid[q] = uid0 + i;
+    f_idx[q] = i;
+    const float wa = wapp[i];
+    hx[2 * q] = u;
+    hy[2 * q] = v;
+    hw[2 * q] = wa;
+    hx[2 * q + 1] = v;
+    hy[2 * q + 1] = u;
+    hw[2 * q + 1] = wa;
+}
+
+__global__ void k_st_range(const unsigned long long *halt, const uint32_t *F_dev, uint32_t f0,
+                           uint32_t nf, uint32_t *out) {
+    if (HALTED(halt)) return;
+    const uint32_t F = *F_dev;
+    *out = F > f0 ? min(F - f0, nf) : 0u;
+}
+
+// Chunk results: found_at / conductance by file index, accept flags by
+// chunk position (zero past the chunk's device count).
+__global__ void k_st_decode(const unsigned long long *halt, const unsigned long long *keys,
+                            const uint32_t *f_idx, const uint32_t *cnt, uint32_t nc,
+                            int32_t *status, float *cond, uint32_t *flags) {
+    if (HALTED(halt)) return;
+    const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nc) return;
+    if (f >= *cnt) {
+        flags[f] = 0u;
+        return;
+    }
+    const unsigned long long k = keys[f];
+    const uint32_t i = f_idx[f];
+    status[i] = key_found(k);
+    cond[i] = k ? __uint_as_float((uint32_t)(k >> 32)) : 0.f;
+    flags[f] = k ? 0u : 1u;
+}
+
+__global__ void k_st_accept(const unsigned long long *halt, const uint32_t *f_src,
+                            const uint32_t *f_dst, const float *f_w, uint32_t nc,
+                            const uint32_t *flags, const uint32_t *pos, uint32_t *hx, uint32_t *hy,
+                            float *hw, uint32_t *counts) {
+    if (HALTED(halt)) return;
+    const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nc) return;
+    if (f == nc - 1) counts[C_ACCEPTED] = 2u * (pos[f] + flags[f]);
+    if (!flags[f]) return;
+    const uint32_t q = pos[f];
+    const uint32_t u = f_src[f], v = f_dst[f];
+    const float ww = f_w[f];
+    hx[2 * q] = u;
+    hy[2 * q] = v;
+    hw[2 * q] = ww;
+    hx[2 * q + 1] = v;
+    hy[2 * q + 1] = u;
+    hw[2 * q + 1] = ww;
+}
+
+uint32_t key_bits(uint32_t nv) {
+    uint32_t b = 1;
+    while (b < 32 && (nv - 1u) >> b) ++b;
+    return b;
+}
+
+// Probe, sort, merge and compact an insert file (no reservation: never halts).
+dyg_status insert_prep_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src,
+                               const uint32_t *dst, const float *w, uint32_t n, uint64_t uid0,
+                               unsigned long long *halt, int32_t *status, float *cond,
+                               cudaStream_t st) {
+    Workspace &ws = G->ws;
+    const uint32_t nb = key_bits(G->g.n);
+    unsigned long long *key = ptr<unsigned long long>(ws.st_key), *skey = key + n;
+    uint32_t *val = ptr<uint32_t>(ws.st_val), *sval = val + n;
+    uint32_t *nflag = ptr<uint32_t>(ws.flags), *npos = ptr<uint32_t>(ws.pos);
+    uint32_t *counts = ptr<uint32_t>(ws.counts);
+    unsigned long long *sc = ptr<unsigned long long>(ws.scalars);
+    k_st_probe<<<blocks((uint64_t)n * kProbeLanes, 256), 256, 0, st>>>(
+        halt, G->g, H->g, src, dst, n, nb, key, val, ptr<uint4>(ws.st_pos), nflag, status, cond,
+        sc + S_ERR);
+    count_launch();
+    size_t tmp = 0;
+    DYG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, key, skey, val, sval, (int)n, 0,
+                                             (int)(2 * nb), st));
+    DYG_TRY(ensure(ws.cub_tmp, tmp));
+    tmp = ws.cub_tmp.bytes;
+    // keys ~0 (self-loops) have all bits set: sorting on the low 2*nb bits
+    // still places them after every real key (each real key is < 2^(2nb) - 1)
+    DYG_CUDA(cub::DeviceRadixSort::SortPairs(ws.cub_tmp.p, tmp, key, skey, val, sval, (int)n, 0,
+                                             (int)(2 * nb), st));
+    k_st_merge<<<blocks(n, 256), 256, 0, st>>>(halt, G->g, H->g, skey, sval, n,
+                                                ptr<uint4>(ws.st_pos), w, nflag,
+                                                ptr<float>(ws.st_wapp), status, cond);
+    count_launch();
+    DYG_TRY(exclusive_scan_u32(ws, nflag, npos, n, st));
+    k_st_compact<<<blocks(n, 256), 256, 0, st>>>(
+        halt, src, dst, w, n, nflag, npos, ptr<float>(ws.st_wapp), (unsigned long long)uid0,
+        ptr<uint32_t>(ws.f_src), ptr<uint32_t>(ws.f_dst), ptr<float>(ws.f_w),
+        ptr<unsigned long long>(ws.f_uid), ptr<uint32_t>(ws.f_idx), ptr<uint32_t>(ws.hx),
+        ptr<uint32_t>(ws.hy), ptr<float>(ws.hw), counts);
+    count_launch();
+    DYG_CUDA(cudaGetLastError());
+    return DYG_OK;
+}
+
+dyg_status insert_gappend_enqueue(dyg_graph *G, uint32_t n, unsigned long long *halt,
+                                  cudaStream_t st) {
+    Workspace &ws = G->ws;
+    AppendList L{ptr<uint32_t>(ws.hx), ptr<uint32_t>(ws.hy), ptr<float>(ws.hw),
+                 ptr<uint32_t>(ws.counts) + C_GHALF, 2u * n};
+    return append_enqueue(G, L, nullptr, nullptr, halt, halt_code(0, (uint32_t)kHaltArena, 1), st);
+}
+
+// Walks chunk c (walk-list entries [c*chunk, c*chunk + nc)) on H and appends
+// its accepted edges to H.
+dyg_status insert_chunk_enqueue(dyg_graph *G, dyg_graph *H, uint32_t c, uint32_t chunk,
+                                uint32_t nc, const dyg_walk_params &p, unsigned long long *halt,
+                                int32_t *status, float *cond, cudaStream_t st) {
+    Workspace &wg = G->ws, &wh = H->ws;
+    const uint32_t f0 = c * chunk;
+    uint32_t *gcounts = ptr<uint32_t>(wg.counts), *hcounts = ptr<uint32_t>(wh.counts);
+    k_st_range<<<1, 1, 0, st>>>(halt, gcounts + C_WALKLIST, f0, nc, gcounts + C_RANGE);
+    count_launch();
+    const uint32_t *cnt = gcounts + C_RANGE;
+    const uint32_t *fsrc = ptr<uint32_t>(wg.f_src) + f0, *fdst = ptr<uint32_t>(wg.f_dst) + f0;
+    const float *fw = ptr<float>(wg.f_w) + f0;
+    unsigned long long *keys = ptr<unsigned long long>(wh.keys);
+    DYG_CUDA(cudaMemsetAsync(keys, 0, sizeof(unsigned long long) * nc, st));
+    WalkJob job{halt, fsrc, fdst, fw, ptr<unsigned long long>(wg.f_uid) + f0, 0ull, cnt, nc,
+                kDomainIncr};
+    DYG_TRY(launch_walk(H, job, p, true, keys, st));
+    k_st_decode<<<blocks(nc, 256), 256, 0, st>>>(halt, keys, ptr<uint32_t>(wg.f_idx) + f0, cnt,
+                                                  nc, status, cond, ptr<uint32_t>(wh.flags));
+    count_launch();
+    DYG_TRY(exclusive_scan_u32(wh, ptr<uint32_t>(wh.flags), ptr<uint32_t>(wh.pos), nc, st));
+    k_st_accept<<<blocks(nc, 256), 256, 0, st>>>(halt, fsrc, fdst, fw, nc, ptr<uint32_t>(wh.flags),
+                                                  ptr<uint32_t>(wh.pos), ptr<uint32_t>(wh.hx),
+                                                  ptr<uint32_t>(wh.hy), ptr<float>(wh.hw), hcounts);
+    count_launch();
+    DYG_CUDA(cudaGetLastError());
+    AppendList L{ptr<uint32_t>(wh.hx), ptr<uint32_t>(wh.hy), ptr<float>(wh.hw),
+                 hcounts + C_ACCEPTED, 2u * nc};
+    return append_enqueue(H, L, nullptr, nullptr, halt,
+                          halt_code(c + 1, (uint32_t)kHaltArena, 0), st);
+}
+
+struct HaltInfo {
+    uint32_t batch, kind, phase;
+};
+
+HaltInfo decode_halt(unsigned long long h) {
+    return HaltInfo{(uint32_t)(h >> 8) - 1u, (uint32_t)((h >> 4) & 0xF), (uint32_t)(h & 0xF)};
+}
+
+dyg_status clear_halt(dyg_graph *D, cudaStream_t st) {
+    DYG_CUDA(cudaMemsetAsync(ptr<unsigned long long>(D->ws.scalars) + S_HALT, 0,
+                             sizeof(unsigned long long), st));
+    return DYG_OK;
+}
+
+dyg_status insert_file_run(dyg_graph *G, dyg_graph *H, const uint32_t *src, const uint32_t *dst,
+                           const float *w, uint32_t n, uint64_t uid0, uint32_t chunk,
+                           const dyg_walk_params &p, int32_t *status, float *cond,
+                           cudaStream_t st) {
+    Workspace &wg = G->ws, &wh = H->ws;
+    const uint32_t nc_max = n < chunk ? n : chunk;
+    // every buffer at its final size before anything is enqueued: a resumed
+    // stage finds the earlier stages' lists where they were left
+    DYG_TRY(ensure(wg.st_key, sizeof(unsigned long long) * (size_t)n * 2));
+    DYG_TRY(ensure(wg.st_val, sizeof(uint32_t) * (size_t)n * 2));
+    DYG_TRY(ensure(wg.st_pos, sizeof(uint4) * (size_t)n));
+    DYG_TRY(ensure(wg.st_wapp, sizeof(float) * (size_t)n));
+    DYG_TRY(ensure(wg.flags, sizeof(uint32_t) * (size_t)n));
+    DYG_TRY(ensure(wg.pos, sizeof(uint32_t) * (size_t)n));
+    DYG_TRY(ensure(wg.f_src, sizeof(uint32_t) * (size_t)n));
+    DYG_TRY(ensure(wg.f_dst, sizeof(uint32_t) * (size_t)n));
+    DYG_TRY(ensure(wg.f_w, sizeof(float) * (size_t)n));
+    DYG_TRY(ensure(wg.f_uid, sizeof(unsigned long long) * (size_t)n));
+    DYG_TRY(ensure(wg.f_idx, sizeof(uint32_t) * (size_t)n));
+    DYG_TRY(ensure(wg.hx, sizeof(uint32_t) * (size_t)n * 2));
+    DYG_TRY(ensure(wg.hy, sizeof(uint32_t) * (size_t)n * 2));
+    DYG_TRY(ensure(wg.hw, sizeof(float) * (size_t)n * 2));
+    DYG_TRY(ensure(wh.keys, sizeof(unsigned long long) * (size_t)nc_max));
+    DYG_TRY(ensure(wh.flags, sizeof(uint32_t) * (size_t)nc_max));
+    DYG_TRY(ensure(wh.pos, sizeof(uint32_t) * (size_t)nc_max));
+    DYG_TRY(ensure(wh.hx, sizeof(uint32_t) * (size_t)nc_max * 2));
+    DYG_TRY(ensure(wh.hy, sizeof(uint32_t) * (size_t)nc_max * 2));
+    DYG_TRY(ensure(wh.hw, sizeof(float) * (size_t)nc_max * 2));
+    unsigned long long *halt = ptr<unsigned long long>(wg.scalars) + S_HALT;
+    DYG_TRY(clear_halt(G, st));
+    DYG_TRY(insert_prep_enqueue(G, H, src, dst, w, n, uid0, halt, status, cond, st));
+    const uint32_t nchunks = (uint32_t)(((uint64_t)n + chunk - 1) / chunk);
+    uint32_t start = 0;   // 0 = G append, c + 1 = chunk c
+    for (int round = 0; round < 64; ++round) {
+        if (start == 0) DYG_TRY(insert_gappend_enqueue(G, n, halt, st));
+        for (uint32_t c = start ? start - 1 : 0; c < nchunks; ++c) {
+            const uint32_t f0 = c * chunk;
+            const uint32_t nc = n - f0 < chunk ? n - f0 : chunk;
+            DYG_TRY(insert_chunk_enqueue(G, H, c, chunk, nc, p, halt, status, cond, st));
+        }
+        DYG_TRY(read_scalars2(G, H, st));
+        const unsigned long long h = wg.host_scalars[S_HALT];
+        if (!h) return DYG_OK;
+        const HaltInfo hi = decode_halt(h);
+        dyg_graph *grow = hi.batch == 0 ? G : H;
+        DYG_TRY(grow_arena(grow, grow->g.arena_cap * 2, st));
+        DYG_TRY(clear_halt(G, st));
+        start = hi.batch;
+    }
+    set_error("insert file: too many arena regrowths");
+    return DYG_ENOMEM;
+}
+
+dyg_status delete_file_run(dyg_graph *G, dyg_graph *H, const uint32_t *src, const uint32_t *dst,
+                           uint32_t n, uint64_t uid0, uint32_t chunk, const dyg_walk_params &p,
+                           int32_t *status, float *cond, uint64_t *n_rec, cudaStream_t st) {
+    Workspace &ws = G->ws;
+    unsigned long long *sc = ptr<unsigned long long>(ws.scalars);
+    unsigned long long *halt = sc + S_HALT;
+    const uint64_t want = (uint64_t)n * 4 + 1024;
+    DYG_TRY(ensure(ws.rx2, sizeof(uint32_t) * want));
+    DYG_TRY(ensure(ws.ry2, sizeof(uint32_t) * want));
+    DYG_TRY(ensure(ws.rk2, want));
+    uint64_t cap = ws.rx2.bytes / 4;
+    if (ws.ry2.bytes / 4 < cap) cap = ws.ry2.bytes / 4;
+    if (ws.rk2.bytes < cap) cap = ws.rk2.bytes;
+    unsigned long long init[2] = {0ull, cap};   // S_RECCNT, S_RECCAP
+    DYG_CUDA(cudaMemcpyAsync(sc + S_RECCNT, init, sizeof(init), cudaMemcpyHostToDevice, st));
+    DYG_TRY(clear_halt(G, st));
+    DYG_TRY(decr_delete_enqueue(G, H, src, dst, n, uid0, true, halt, status, cond, st));
+    const uint32_t nchunks = (uint32_t)(((uint64_t)n + chunk - 1) / chunk);
+    uint32_t c_start = 0, ph_start = 0;
+    for (int round = 0; round < 64; ++round) {
+        for (uint32_t c = c_start; c < nchunks; ++c) {
+            const uint32_t f0 = c * chunk;
+            const uint32_t nc = n - f0 < chunk ? n - f0 : chunk;
+            DYG_TRY(decr_walk_enqueue(G, H, f0, nc, ptr<uint32_t>(ws.counts) + C_FILTERED, p, halt,
+                                      c, c == c_start ? ph_start : 0, status, cond, st));
+        }
+        DYG_TRY(read_scalars2(G, H, st));
+        const unsigned long long h = ws.host_scalars[S_HALT];
+        if (!h) {
+            *n_rec = ws.host_scalars[S_RECCNT];
+            return DYG_OK;
+        }
+        const HaltInfo hi = decode_halt(h);
+        if (hi.kind == kHaltRecords) {
+            const uint64_t used = ws.host_scalars[S_RECCNT];
+            const uint64_t ncap = cap * 2;
+            DYG_TRY(grow_keep(ws.rx2, sizeof(uint32_t) * ncap, sizeof(uint32_t) * used, st));
+            DYG_TRY(grow_keep(ws.ry2, sizeof(uint32_t) * ncap, sizeof(uint32_t) * used, st));
+            DYG_TRY(grow_keep(ws.rk2, ncap, used, st));
+            cap = ncap;
+            DYG_CUDA(cudaMemcpyAsync(sc + S_RECCAP, &cap, sizeof(cap), cudaMemcpyHostToDevice, st));
+            DYG_CUDA(cudaStreamSynchronize(st));
+        } else {
+            DYG_TRY(grow_arena(H, H->g.arena_cap * 2, st));
+        }
+        DYG_TRY(clear_halt(G, st));
+        c_start = hi.batch;
+        ph_start = hi.phase;
+    }
+    set_error("delete file: too many buffer regrowths");
+    return DYG_ENOMEM;
+}
+
+}  // namespace
+
+uint32_t stream_default_chunk(uint32_t n_vertices) {
+    const uint32_t c = (uint32_t)((double)n_vertices * 0.05);
+    return c < 10000u ? 10000u : c;
+}
+
+dyg_status stream_file_run(dyg_graph *G, dyg_graph *H, uint32_t op, const uint32_t *src,
+                           const uint32_t *dst, const float *w, uint32_t n, uint64_t uid0,
+                           uint32_t chunk, const dyg_walk_params &p, int32_t *status, float *cond,
+                           uint64_t *n_rec, cudaStream_t st) {
+    *n_rec = 0;
+    if (chunk == 0) chunk = stream_default_chunk(G->g.n);
+    if (op == DYG_STREAM_INSERT)
+        return insert_file_run(G, H, src, dst, w, n, uid0, chunk, p, status, cond, st);
+    return delete_file_run(G, H, src, dst, n, uid0, chunk, p, status, cond, n_rec, st);
+}
+
+}  // namespace dyg

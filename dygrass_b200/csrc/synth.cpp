@@ -240,6 +240,59 @@ uint64_t dyg_synth_rmat(uint32_t scale, uint32_t edge_factor, double a, double b
     return m;
 }
 
+uint64_t dyg_synth_rmat_stream(uint32_t scale, double a, double b, double c,
+                               const uint32_t *id_map, uint64_t m, const uint32_t *src,
+                               const uint32_t *dst, uint64_t n_updates, uint32_t file_size,
+                               double del_frac, float wlo, float whi, uint64_t seed,
+                               uint8_t *file_op, uint32_t *out_src, uint32_t *out_dst,
+                               float *out_w) {
+    if (file_size == 0) return 0;
+    std::unordered_set<uint64_t> live;
+    live.reserve((size_t)(m + n_updates) * 2);
+    std::vector<uint64_t> alive;
+    alive.reserve((size_t)(m + n_updates));
+    for (uint64_t i = 0; i < m; ++i) {
+        const uint64_t k = pair_key(src[i], dst[i]);
+        if (live.insert(k).second) alive.push_back(k);
+    }
+    SplitMix r(seed);
+    const uint64_t nfiles = (n_updates + file_size - 1) / file_size;
+    uint64_t o = 0;
+    for (uint64_t f = 0; f < nfiles; ++f) {
+        const uint64_t cnt = std::min<uint64_t>(file_size, n_updates - o);
+        const bool del = (uint64_t)floor((double)(f + 1) * del_frac) > (uint64_t)floor((double)f * del_frac);
+        file_op[f] = del ? 1 : 0;
+        for (uint64_t k = 0; k < cnt; ++k, ++o) {
+            if (del && !alive.empty()) {
+                const uint64_t j = r.below(alive.size());
+                const uint64_t key = alive[j];
+                alive[j] = alive.back();
+                alive.pop_back();
+                live.erase(key);
+                out_src[o] = (uint32_t)(key >> 32);
+                out_dst[o] = (uint32_t)key;
+                out_w[o] = 1.0f;
+                continue;
+            }
+            uint32_t u = 0, v = 0;
+            for (int tries = 0; tries < 1000000; ++tries) {
+                uint32_t x, y;
+                rmat_pair(r, scale, a, b, c, &x, &y);
+                u = id_map[x];
+                v = id_map[y];
+                if (u != 0xFFFFFFFFu && v != 0xFFFFFFFFu && u != v) break;
+                u = v = 0xFFFFFFFFu;
+            }
+            out_src[o] = u;
+            out_dst[o] = v;
+            out_w[o] = draw_weight(r, DYG_W_UNIFORM, wlo, whi);
+            const uint64_t key = pair_key(u, v);
+            if (u != 0xFFFFFFFFu && live.insert(key).second) alive.push_back(key);
+        }
+    }
+    return nfiles;
+}
+
 void dyg_synth_sample(uint64_t m, uint64_t k, uint64_t seed, uint64_t *out_idx) {
     if (k > m) k = m;
     SplitMix r(seed);

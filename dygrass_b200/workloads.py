@@ -15,9 +15,18 @@ private drive by datasetdownload.py), so every workload here is generated:
                threshold 100, 512 walkers, max_steps 100.  At 100^3:
                1,000,000 vertices, 2,970,000 edges, 200,000 insertions,
                317,000 deletions.
+  rmat_mixed -- R-MAT (a, b, c) = (0.57, 0.19, 0.19), edge factor 16,
+               symmetrised, deduplicated, largest connected component,
+               FP32 weights U[0.1, 10]; sparsifier = spanning tree + 5%
+               off-tree; a mixed stream of insert / delete files of 4,096
+               updates, 70% insertions (further R-MAT pairs; existing edges
+               merge their weight) and 30% deletions (uniform over the edges
+               present); threshold 50, 256 walkers, max_steps 128.  At
+               scale 20: 2^20 ids, 500,000 updates in 123 files.
 """
 from __future__ import annotations
 
+import ctypes as C
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -57,6 +66,81 @@ def sample(m: int, k: int, seed: int) -> np.ndarray:
     out = np.empty(k, np.uint64)
     lib().dyg_synth_sample(m, k, seed, _ptr(out))
     return out
+
+
+def rmat(scale: int, edge_factor: int, a: float, b: float, c: float, wlo: float, whi: float,
+         seed: int):
+    """Returns (n, src, dst, w, id_map) of the R-MAT graph's largest component."""
+    n = C.c_uint32()
+    ps, pd, pw, pm = C.c_void_p(), C.c_void_p(), C.c_void_p(), C.c_void_p()
+    m = int(lib().dyg_synth_rmat(scale, edge_factor, a, b, c, wlo, whi, seed, C.byref(n),
+                                 C.byref(ps), C.byref(pd), C.byref(pw), C.byref(pm)))
+    try:
+        src = np.ctypeslib.as_array(C.cast(ps, C.POINTER(C.c_uint32)), (max(m, 1),))[:m].copy()
+        dst = np.ctypeslib.as_array(C.cast(pd, C.POINTER(C.c_uint32)), (max(m, 1),))[:m].copy()
+        w = np.ctypeslib.as_array(C.cast(pw, C.POINTER(C.c_float)), (max(m, 1),))[:m].copy()
+        idm = np.ctypeslib.as_array(C.cast(pm, C.POINTER(C.c_uint32)), (1 << scale,)).copy()
+    finally:
+        for p in (ps, pd, pw, pm):
+            lib().dyg_mtx_free(p)
+    return int(n.value), src, dst, w, idm
+
+
+def rmat_stream(scale, a, b, c, id_map, src, dst, n_updates, file_size, del_frac, wlo, whi,
+                seed):
+    """Returns a list of (op, src, dst, w) stream files (op 0 insert, 1 delete)."""
+    nf = (n_updates + file_size - 1) // file_size
+    ops = np.zeros(max(nf, 1), np.uint8)
+    os_ = np.empty(max(n_updates, 1), np.uint32)
+    od = np.empty(max(n_updates, 1), np.uint32)
+    ow = np.empty(max(n_updates, 1), np.float32)
+    src = np.ascontiguousarray(src, np.uint32)
+    dst = np.ascontiguousarray(dst, np.uint32)
+    nf = int(lib().dyg_synth_rmat_stream(scale, a, b, c, _ptr(id_map), len(src), _ptr(src),
+                                         _ptr(dst), n_updates, file_size, del_frac, wlo, whi,
+                                         seed, _ptr(ops), _ptr(os_), _ptr(od), _ptr(ow)))
+    files = []
+    for f in range(nf):
+        lo, hi = f * file_size, min((f + 1) * file_size, n_updates)
+        files.append((int(ops[f]), os_[lo:hi].copy(), od[lo:hi].copy(),
+                      None if ops[f] else ow[lo:hi].copy()))
+    return files
+
+
+@dataclass
+class MixedWorkload:
+    name: str
+    n: int
+    g_src: np.ndarray
+    g_dst: np.ndarray
+    g_w: np.ndarray
+    h_src: np.ndarray
+    h_dst: np.ndarray
+    h_w: np.ndarray
+    files: list                 # (op, src, dst, w or None) in stream order
+    iparams: WalkParams = None  # insert files
+    dparams: WalkParams = None  # delete files
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def n_updates(self) -> int:
+        return sum(len(f[1]) for f in self.files)
+
+
+def rmat_mixed(scale: int = 20, edge_factor: int = 16, n_updates: int = 500_000,
+               file_size: int = 4096, del_frac: float = 0.30, seed: int = MASTER_SEED,
+               walkers: int = 256, max_steps: int = 128, threshold: float = 50.0) -> MixedWorkload:
+    a, b, c = 0.57, 0.19, 0.19
+    n, src, dst, w, idm = rmat(scale, edge_factor, a, b, c, 0.1, 10.0, seed + 11)
+    idx = sparsifier(n, src, dst, w, 0.05, seed + 12)
+    files = rmat_stream(scale, a, b, c, idm, src, dst, n_updates, file_size, del_frac, 0.1, 10.0,
+                        seed + 13)
+    ip = WalkParams.make(threshold=threshold, walkers=walkers, max_steps=max_steps, seed=seed)
+    dp = WalkParams.make(walkers=walkers, max_steps=max_steps, seed=seed)
+    return MixedWorkload(f"rmat_{scale}", n, src, dst, w, src[idx], dst[idx], w[idx], files,
+                         iparams=ip, dparams=dp,
+                         meta={"scale": scale, "edge_factor": edge_factor, "seed": seed,
+                               "file_size": file_size, "del_frac": del_frac})
 
 
 @dataclass

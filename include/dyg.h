@@ -23,6 +23,12 @@
  *                                   (random_walk_decremental/gpu_graph.cuh:328-615,
  *                                    random_walk_decremental/main.cu:77-290, 392-408)
  *   dyg_decremental_stream       <- the decremental batch loop (random_walk_decremental/main.cu:388-444)
+ *   dyg_stream_file              <- one stream_*.mtx file of the mixed updater:
+ *                                   preprocessStreamEdges + the chunked
+ *                                   NBRW_incremental / NBRW_decremental loop +
+ *                                   updateSparsiferFromResult
+ *                                   (dynamic_update/main.cu:96-126,
+ *                                    dynamic_update/gpu_graph.cuh:361-465, 620-723)
  *   dyg_graph_export             <- saveCurrentMtx / save_added_edges data source
  *                                   (random_walk_incremental/gpu_graph.cuh:427-454,
  *                                    random_walk_decremental/gpu_graph.cuh:633-646)
@@ -95,6 +101,13 @@ typedef struct dyg_graph_opts {
 #define DYG_DEL_NOT_IN_G (-3)  /* edge absent from G: skipped (gpu_graph.cuh:345-347)   */
 #define DYG_DEL_NOT_IN_H (-2)  /* removed from G only; H unchanged, no walk             */
 #define DYG_DEL_NO_PATH (-1)   /* no walker reached the other end: fallback recovery    */
+
+/* Stream-file operations and insertion status codes (otherwise: found_at). */
+#define DYG_STREAM_INSERT 0u
+#define DYG_STREAM_DELETE 1u
+#define DYG_INS_MERGED (-4)     /* edge already in G (or repeated in the file): weight
+                                   added to G and H (dynamic_update/gpu_graph.cuh:374-382) */
+#define DYG_INS_SELF_LOOP (-5)  /* u == v: ignored                                        */
 
 /* Kinds of recovered edges. */
 #define DYG_REC_PATH 0u
@@ -171,6 +184,28 @@ dyg_status dyg_decremental_stream(dyg_graph *G, dyg_graph *H, const uint32_t *sr
                                   const dyg_walk_params *p, int32_t *status, float *conductance,
                                   uint32_t *rec_src, uint32_t *rec_dst, uint8_t *rec_kind,
                                   uint64_t rec_cap, uint64_t *n_rec, dyg_stream_t stream);
+
+/* Walk-list chunk of the mixed updater: 5% of |V|, at least 10000
+ * (dynamic_update/main.cu:86-87). */
+uint32_t dyg_stream_default_chunk(uint32_t n_vertices);
+/* One file of the mixed insert/delete stream (dynamic_update).
+ * op DYG_STREAM_INSERT, in file order: an edge already in G (or repeated
+ * earlier in the file) adds its weight to G and, if there, to H
+ * (status DYG_INS_MERGED); a new edge enters G at once.  The new edges are
+ * then walked on H from src to dst in chunks of `chunk` (0 =
+ * dyg_stream_default_chunk(|V|)); after each chunk its accepted edges
+ * (status -1) enter H with their stream weight; otherwise status = found_at.
+ * op DYG_STREAM_DELETE: the whole file is deleted from G and H first (status
+ * DYG_DEL_*), then the edges that were in H are walked on G from src to dst in
+ * chunks, recovering as dyg_decremental_batch does; w may be NULL.
+ * Update ids are first_update_id + file position.  Recovered edges (delete
+ * files) as in dyg_decremental_batch; *n_rec = 0 for insert files. */
+dyg_status dyg_stream_file(dyg_graph *G, dyg_graph *H, uint32_t op, const uint32_t *src,
+                           const uint32_t *dst, const float *w, uint32_t n,
+                           uint64_t first_update_id, uint32_t chunk, const dyg_walk_params *p,
+                           int32_t *status, float *conductance, uint32_t *rec_src,
+                           uint32_t *rec_dst, uint8_t *rec_kind, uint64_t rec_cap,
+                           uint64_t *n_rec, dyg_stream_t stream);
 
 /* No counterpart in the reference.  Incremental walk decision for one batch
  * (found_at / conductance / accepted exactly as dyg_incremental_batch reports

@@ -57,6 +57,22 @@ uint64_t dyg_synth_rmat(uint32_t scale, uint32_t edge_factor, double a, double b
 void dyg_synth_rmat_pairs(uint32_t scale, uint64_t count, double a, double b, double c,
                           uint64_t seed, uint32_t *src, uint32_t *dst);
 
+/* Mixed update stream on an R-MAT graph from dyg_synth_rmat (id_map, and
+ * its m edges src/dst): n_updates updates in files of file_size edges; file
+ * f deletes iff floor((f+1)*del_frac) > floor(f*del_frac), so a fraction
+ * del_frac of the files delete.  An insertion is a further R-MAT pair mapped
+ * through id_map (pairs leaving the component or self-loops are redrawn; an
+ * edge already present is kept: it merges its weight), weight U[wlo, whi).
+ * A deletion is an edge drawn uniformly from the edges present at that point
+ * (min, max order, weight 1).  Writes file_op[f] (0 insert, 1 delete) and
+ * the updates in order; returns the number of files. */
+uint64_t dyg_synth_rmat_stream(uint32_t scale, double a, double b, double c,
+                               const uint32_t *id_map, uint64_t m, const uint32_t *src,
+                               const uint32_t *dst, uint64_t n_updates, uint32_t file_size,
+                               double del_frac, float wlo, float whi, uint64_t seed,
+                               uint8_t *file_op, uint32_t *out_src, uint32_t *out_dst,
+                               float *out_w);
+
 /* k distinct indices of [0, m) in uniformly random order. */
 void dyg_synth_sample(uint64_t m, uint64_t k, uint64_t seed, uint64_t *out_idx);
 

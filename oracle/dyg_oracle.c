@@ -420,16 +420,13 @@ static void rec_add(orc_graph *H, rec_t *rc, uint32_t x, uint32_t y, float w, ui
     rc->n++;
 }
 
-uint64_t orc_decremental_batch(orc_graph *G, orc_graph *H, const uint32_t *src,
-                               const uint32_t *dst, uint32_t n, uint64_t first_uid,
-                               const orc_params *p, int threads, int32_t *status,
-                               float *cond, uint32_t *rec_src, uint32_t *rec_dst,
-                               uint8_t *rec_kind, uint64_t rec_cap, uint64_t *n_rec) {
-    uint64_t moves = 0;
-    uint32_t *filt = (uint32_t *)malloc((size_t)(n ? n : 1) * sizeof(uint32_t));
+/* Deletion stage: delete every edge from G (swap with the row's last slot),
+ * erase the ones also in H, and list those (gpu_graph.cuh:338-458;
+ * dynamic_update/gpu_graph.cuh:398-431).  Endpoints are ordered min -> max
+ * for the row operations (gpu_graph.cuh:342). */
+static uint32_t decr_delete(orc_graph *G, orc_graph *H, const uint32_t *src, const uint32_t *dst,
+                            uint32_t n, int32_t *status, float *cond, uint32_t *filt) {
     uint32_t nf = 0;
-    /* 1. delete from G, erase from H, filter (gpu_graph.cuh:338-458).
-          Endpoints are ordered min -> max (gpu_graph.cuh:342). */
     for (uint32_t e = 0; e < n; ++e) {
         uint32_t a = src[e], b = dst[e];
         if (a > b) { uint32_t t = a; a = b; b = t; }
@@ -451,30 +448,46 @@ uint64_t orc_decremental_batch(orc_graph *G, orc_graph *H, const uint32_t *src,
         if (status) status[e] = st;
         if (cond) cond[e] = 0.0f;
     }
-    /* 2. walks on the updated G (main.cu:392) */
+    return nf;
+}
+
+/* Walk endpoints of listed deletion e: min -> max for the standalone
+ * decremental updater (random_walk_decremental/gpu_graph.cuh:342), file
+ * orientation for stream files (dynamic_update/gpu_graph.cuh:874-875). */
+static void walk_ends(const uint32_t *src, const uint32_t *dst, uint32_t e, int file_orient,
+                      uint32_t *s, uint32_t *t) {
+    uint32_t a = src[e], b = dst[e];
+    if (!file_orient && a > b) { uint32_t x = a; a = b; b = x; }
+    *s = a;
+    *t = b;
+}
+
+/* Walk-and-recover stage for listed deletions filt[0..nf): walks on G, winner
+ * paths into H in order (gpu_graph.cuh:514-552), then the 2-step fallback
+ * walks from both walk endpoints (main.cu:243-290). */
+static uint64_t decr_walk(orc_graph *G, orc_graph *H, const uint32_t *src, const uint32_t *dst,
+                          const uint32_t *filt, uint32_t nf, uint64_t first_uid, int file_orient,
+                          const orc_params *p, int threads, int32_t *status, float *cond,
+                          rec_t *rc) {
+    uint64_t moves = 0;
     uint64_t *keys = (uint64_t *)malloc((size_t)(nf ? nf : 1) * sizeof(uint64_t));
     if (threads < 1) threads = 1;
 #pragma omp parallel for schedule(dynamic, 1) num_threads(threads) reduction(+ : moves)
     for (int64_t f = 0; f < (int64_t)nf; ++f) {
-        uint32_t e = filt[f];
-        uint32_t a = src[e], b = dst[e];
-        if (a > b) { uint32_t t = a; a = b; b = t; }
+        uint32_t e = filt[f], a, b;
+        walk_ends(src, dst, e, file_orient, &a, &b);
         uint64_t mv = 0;
         keys[f] = best_key(G, a, b, 0.0f, 0, p, first_uid + e, DOMAIN_DECR, &mv);
         moves += mv;
     }
-    /* 3. commit winner paths in order (gpu_graph.cuh:514-552) */
-    rec_t rc = {0};
-    rc.cap_out = rec_cap; rc.out_a = rec_src; rc.out_b = rec_dst; rc.out_kind = rec_kind;
     uint32_t pathlen = p->max_steps > 2 ? p->max_steps : 2;
     uint32_t *path = (uint32_t *)malloc((size_t)pathlen * sizeof(uint32_t));
     float *pathw = (float *)malloc((size_t)pathlen * sizeof(float));
     uint32_t *nop = (uint32_t *)malloc((size_t)(nf ? nf : 1) * sizeof(uint32_t));
     uint32_t nnop = 0;
     for (uint32_t f = 0; f < nf; ++f) {
-        uint32_t e = filt[f];
-        uint32_t a = src[e], b = dst[e];
-        if (a > b) { uint32_t t = a; a = b; b = t; }
+        uint32_t e = filt[f], a, b;
+        walk_ends(src, dst, e, file_orient, &a, &b);
         uint64_t k = keys[f];
         if (k) {
             uint32_t walker = 1023u - (uint32_t)((k >> 22) & 0x3FFu);
@@ -482,15 +495,15 @@ uint64_t orc_decremental_batch(orc_graph *G, orc_graph *H, const uint32_t *src,
             int32_t found = decr_walk_path(G, a, b, first_uid + e, walker, p, path, pathw, &R);
             if (status) status[e] = found;
             if (cond) cond[e] = key_cond(k);
-            for (int32_t j = 0; j < found; ++j) rec_add(H, &rc, path[j], path[j + 1], pathw[j + 1], 0);
+            for (int32_t j = 0; j < found; ++j) rec_add(H, rc, path[j], path[j + 1], pathw[j + 1], 0);
         } else {
             nop[nnop++] = f;
         }
     }
-    /* 4. fallback: 2-step walks from both endpoints (main.cu:243-290) */
     for (uint32_t q = 0; q < nnop; ++q) {
         uint32_t e = filt[nop[q]];
-        uint32_t ends[2] = {src[e] < dst[e] ? src[e] : dst[e], src[e] < dst[e] ? dst[e] : src[e]};
+        uint32_t ends[2];
+        walk_ends(src, dst, e, file_orient, &ends[0], &ends[1]);
         for (uint32_t side = 0; side < 2; ++side) {
             for (uint32_t j = 0; j < p->heuristic_walkers; ++j) {
                 rng_t rng;
@@ -510,13 +523,123 @@ uint64_t orc_decremental_batch(orc_graph *G, orc_graph *H, const uint32_t *src,
                     x2 = G->col[x1][i1];
                     w2 = G->w[x1][i1];
                 }
-                rec_add(H, &rc, s0, x1, w1, 1);
-                rec_add(H, &rc, x1, x2, w2, 1);
+                rec_add(H, rc, s0, x1, w1, 1);
+                rec_add(H, rc, x1, x2, w2, 1);
             }
         }
     }
+    free(path); free(pathw); free(nop); free(keys);
+    return moves;
+}
+
+uint64_t orc_decremental_batch(orc_graph *G, orc_graph *H, const uint32_t *src,
+                               const uint32_t *dst, uint32_t n, uint64_t first_uid,
+                               const orc_params *p, int threads, int32_t *status,
+                               float *cond, uint32_t *rec_src, uint32_t *rec_dst,
+                               uint8_t *rec_kind, uint64_t rec_cap, uint64_t *n_rec) {
+    uint32_t *filt = (uint32_t *)malloc((size_t)(n ? n : 1) * sizeof(uint32_t));
+    uint32_t nf = decr_delete(G, H, src, dst, n, status, cond, filt);
+    rec_t rc = {0};
+    rc.cap_out = rec_cap; rc.out_a = rec_src; rc.out_b = rec_dst; rc.out_kind = rec_kind;
+    uint64_t moves = decr_walk(G, H, src, dst, filt, nf, first_uid, 0, p, threads, status, cond, &rc);
     if (n_rec) *n_rec = rc.n;
-    free(path); free(pathw); free(nop); free(keys); free(filt);
+    free(filt);
+    return moves;
+}
+
+/* ----------------------------------------------------------- stream files */
+
+uint32_t orc_stream_default_chunk(uint32_t n_vertices) {
+    /* 5% of |V|, at least 10000 (dynamic_update/main.cu:86-87) */
+    uint32_t c = (uint32_t)((double)n_vertices * 0.05);
+    return c < 10000u ? 10000u : c;
+}
+
+/* Adds `w` to the weight of the first slot of row x holding y
+ * (dynamic_update/gpu_graph.cuh:452-465). */
+static void row_add_weight(orc_graph *g, uint32_t x, uint32_t y, float w) {
+    for (uint32_t j = 0; j < g->deg[x]; ++j)
+        if (g->col[x][j] == y) {
+            g->w[x][j] = g->w[x][j] + w;
+            return;
+        }
+}
+
+uint64_t orc_stream_file(orc_graph *G, orc_graph *H, uint32_t op, const uint32_t *src,
+                         const uint32_t *dst, const float *w, uint32_t n, uint64_t first_uid,
+                         uint32_t chunk, const orc_params *p, int threads, int32_t *status,
+                         float *cond, uint32_t *rec_src, uint32_t *rec_dst, uint8_t *rec_kind,
+                         uint64_t rec_cap, uint64_t *n_rec) {
+    uint64_t moves = 0;
+    uint32_t *list = (uint32_t *)malloc((size_t)(n ? n : 1) * sizeof(uint32_t));
+    uint32_t nl = 0;
+    if (chunk == 0) chunk = orc_stream_default_chunk(G->n);
+    if (threads < 1) threads = 1;
+    if (n_rec) *n_rec = 0;
+    if (op == ORC_STREAM_INSERT) {
+        /* preprocessing in file order (dynamic_update/gpu_graph.cuh:373-396):
+           an edge already in G adds its weight to G and, if there, to H; a
+           new edge enters G at once and is walked later */
+        for (uint32_t i = 0; i < n; ++i) {
+            uint32_t a = src[i] < dst[i] ? src[i] : dst[i];
+            uint32_t b = src[i] < dst[i] ? dst[i] : src[i];
+            if (cond) cond[i] = 0.0f;
+            if (a == b) {
+                if (status) status[i] = ORC_STREAM_SELF_LOOP;
+            } else if (orc_graph_has_edge(G, a, b)) {
+                row_add_weight(G, a, b, w[i]);
+                row_add_weight(G, b, a, w[i]);
+                if (orc_graph_has_edge(H, a, b)) {
+                    row_add_weight(H, a, b, w[i]);
+                    row_add_weight(H, b, a, w[i]);
+                }
+                if (status) status[i] = ORC_STREAM_MERGED;
+            } else {
+                row_append(G, a, b, w[i]);
+                row_append(G, b, a, w[i]);
+                list[nl++] = i;
+            }
+        }
+        /* walks on H in chunks, each chunk's accepted edges entering H with
+           their stream weight before the next chunk walks
+           (dynamic_update/main.cu:107-126, gpu_graph.cuh:629-640) */
+        uint64_t *keys = (uint64_t *)malloc((size_t)(nl ? nl : 1) * sizeof(uint64_t));
+        for (uint32_t c0 = 0; c0 < nl; c0 += chunk) {
+            uint32_t c1 = nl - c0 < chunk ? nl : c0 + chunk;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads) reduction(+ : moves)
+            for (int64_t k = c0; k < (int64_t)c1; ++k) {
+                uint32_t i = list[k];
+                uint64_t mv = 0;
+                keys[k] = best_key(H, src[i], dst[i], w[i], 1, p, first_uid + i, DOMAIN_INCR, &mv);
+                moves += mv;
+            }
+            for (uint32_t k = c0; k < c1; ++k) {
+                uint32_t i = list[k];
+                uint64_t kk = keys[k];
+                if (status) status[i] = kk ? (int32_t)(kk & 0x3FFFFFu) : -1;
+                if (cond) cond[i] = kk ? key_cond(kk) : 0.0f;
+                if (!kk) {
+                    row_append(H, src[i], dst[i], w[i]);
+                    row_append(H, dst[i], src[i], w[i]);
+                }
+            }
+        }
+        free(keys);
+    } else {
+        /* the whole file is deleted first (dynamic_update/gpu_graph.cuh:398-431),
+           then the listed edges are walked on G in chunks, each chunk's
+           recovered edges entering H before the next */
+        nl = decr_delete(G, H, src, dst, n, status, cond, list);
+        rec_t rc = {0};
+        rc.cap_out = rec_cap; rc.out_a = rec_src; rc.out_b = rec_dst; rc.out_kind = rec_kind;
+        for (uint32_t c0 = 0; c0 < nl; c0 += chunk) {
+            uint32_t c1 = nl - c0 < chunk ? nl : c0 + chunk;
+            moves += decr_walk(G, H, src, dst, list + c0, c1 - c0, first_uid, 1, p, threads,
+                               status, cond, &rc);
+        }
+        if (n_rec) *n_rec = rc.n;
+    }
+    free(list);
     return moves;
 }
 

@@ -94,6 +94,29 @@ uint64_t orc_decremental_stream(orc_graph *G, orc_graph *H, const uint32_t *src,
                                 float *cond, uint32_t *rec_src, uint32_t *rec_dst,
                                 uint8_t *rec_kind, uint64_t rec_cap, uint64_t *n_rec);
 
+/* One file of the mixed insert/delete stream
+ * (dynamic_update/main.cu:96-126, gpu_graph.cuh:361-465, 620-723).
+ * op ORC_STREAM_INSERT: in file order, an edge already in G adds its weight
+ * to G (and to H if H has it) and gets status ORC_STREAM_MERGED; a new edge
+ * enters G at once and is then walked on H from src to dst, in chunks of
+ * `chunk` walked edges (0 = orc_stream_default_chunk(|V|)); a chunk's
+ * accepted edges (status -1) enter H with their stream weight before the
+ * next chunk walks; found_at >= 0 otherwise.  A self-loop is ignored
+ * (ORC_STREAM_SELF_LOOP).
+ * op ORC_STREAM_DELETE: the whole file is deleted from G and H first, then
+ * the edges that were in H are walked on G from src to dst in chunks, with
+ * the status / conductance / recovered-edge outputs of the batch functions. */
+#define ORC_STREAM_INSERT 0u
+#define ORC_STREAM_DELETE 1u
+#define ORC_STREAM_MERGED (-4)
+#define ORC_STREAM_SELF_LOOP (-5)
+uint32_t orc_stream_default_chunk(uint32_t n_vertices);
+uint64_t orc_stream_file(orc_graph *G, orc_graph *H, uint32_t op, const uint32_t *src,
+                         const uint32_t *dst, const float *w, uint32_t n, uint64_t first_uid,
+                         uint32_t chunk, const orc_params *p, int threads, int32_t *status,
+                         float *cond, uint32_t *rec_src, uint32_t *rec_dst, uint8_t *rec_kind,
+                         uint64_t rec_cap, uint64_t *n_rec);
+
 /* Path of one walker of a decremental walk (for tests): returns found_at or
  * -1 and writes up to max_steps+1 vertices into path. */
 int32_t orc_decremental_walk_path(const orc_graph *G, uint32_t s, uint32_t t,

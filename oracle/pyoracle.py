@@ -60,6 +60,9 @@ def lib() -> C.CDLL:
                                         C.POINTER(u64)], u64),
             "orc_decremental_walk_path": ([vp, u32, u32, u64, u32, P, vp, C.POINTER(C.c_float)], C.c_int32),
             "orc_max_threads": ([], C.c_int),
+            "orc_stream_default_chunk": ([u32], u32),
+            "orc_stream_file": ([vp, vp, u32, vp, vp, vp, u32, u64, u32, P, C.c_int, vp, vp, vp, vp,
+                                 vp, u64, C.POINTER(u64)], u64),
         }
         for name, (a, r) in sig.items():
             f = getattr(L, name)
@@ -158,3 +161,30 @@ def decremental(G: OGraph, H: OGraph, src, dst, params, batch_size=0, threads=No
                                           _p(st), _p(cd), _p(rx), _p(ry), _p(rk), cap, C.byref(nr))
     k = nr.value
     return st, cd, rx[:k].copy(), ry[:k].copy(), rk[:k].copy(), int(mv)
+
+
+def stream_file(G: OGraph, H: OGraph, op, src, dst, w, params, first_uid=0, chunk=0,
+                threads=None):
+    """One stream file; returns (status, cond, rec_src, rec_dst, rec_kind, walker_moves)."""
+    src = np.ascontiguousarray(src, np.uint32)
+    dst = np.ascontiguousarray(dst, np.uint32)
+    w = None if w is None else np.ascontiguousarray(w, np.float32)
+    n = len(src)
+    cap = n * (params.max_steps + 4 * params.heuristic_walkers) + 16
+    st = np.empty(n, np.int32)
+    cd = np.empty(n, np.float32)
+    rx = np.empty(cap, np.uint32)
+    ry = np.empty(cap, np.uint32)
+    rk = np.empty(cap, np.uint8)
+    nr = C.c_uint64()
+    P = Params.from_walk_params(params)
+    th = threads or max_threads()
+    mv = lib().orc_stream_file(G.h, H.h, int(op), _p(src), _p(dst), _p(w), n, first_uid, chunk,
+                               C.byref(P), th, _p(st), _p(cd), _p(rx), _p(ry), _p(rk), cap,
+                               C.byref(nr))
+    k = nr.value
+    return st, cd, rx[:k].copy(), ry[:k].copy(), rk[:k].copy(), int(mv)
+
+
+def stream_default_chunk(n_vertices) -> int:
+    return int(lib().orc_stream_default_chunk(int(n_vertices)))
