@@ -15,6 +15,14 @@ with an L2 flush (a 256 MB write).  value = edge updates (insertions +
 deletions) per second over all ranks; the device-resident run keeps inputs
 and outputs in HBM, e2e passes host (pinned) buffers through the C ABI.
 
+Workload "rmat": the mixed-stream configuration -- R-MAT scale 20 (edge
+factor 16, a=0.57, b=c=0.19), symmetrised, deduplicated, largest connected
+component (645,911 vertices, 15.7 M edges at the default seed), weights
+U[0.1, 10], sparsifier = spanning tree + 5% off-tree; 500,000 updates in
+stream files of 4,096 (70% insertion files, 30% deletion files), threshold
+50, 256 walkers, max_steps 128.  One step = every file in order through
+dyg_stream_file from the initial graphs.
+
 N > 1 (torchrun): every rank runs an independent replica of the workload
 (weak scaling, no data-path collective); times are the max over ranks.
 
@@ -45,7 +53,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["mesh", "grid"], default="mesh")
+    ap.add_argument("--workload", choices=["mesh", "grid", "rmat"], default="mesh")
+    ap.add_argument("--rmat-scale", type=int, default=20)
+    ap.add_argument("--rmat-updates", type=int, default=500_000)
     ap.add_argument("--mesh-k", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -59,7 +69,13 @@ def parse():
 def make_workload(args, rank):
     import dygrass_b200.workloads as wl
     seed = wl.MASTER_SEED + 1000 * rank
-    W = wl.grid_2d(seed=seed) if args.workload == "grid" else wl.mesh_3d(k=args.mesh_k, seed=seed)
+    if args.workload == "rmat":
+        W = wl.rmat_mixed(scale=args.rmat_scale, n_updates=args.rmat_updates, seed=seed)
+        W.params = W.iparams
+    elif args.workload == "grid":
+        W = wl.grid_2d(seed=seed)
+    else:
+        W = wl.mesh_3d(k=args.mesh_k, seed=seed)
     if args.exhaustive:
         import dygrass_b200 as dyg
         W.params.flags |= dyg.FLAG_EXHAUSTIVE
@@ -68,6 +84,13 @@ def make_workload(args, rank):
 
 
 def workload_config(W, args):
+    if args.workload == "rmat":
+        nins = sum(len(f[1]) for f in W.files if f[0] == 0)
+        return {"workload": f"rmat scale {args.rmat_scale} mixed stream, files of 4,096 (70% insert / "
+                            f"30% delete), threshold 50, 256 walkers, max_steps 128",
+                "vertices": W.n, "edges": int(len(W.g_src)), "sparsifier_edges": int(len(W.h_src)),
+                "updates": W.n_updates, "insertions": nins, "deletions": W.n_updates - nins,
+                "files": len(W.files)}
     if args.workload == "grid":
         return {"workload": "grid_2d 100x100, 1,000 insertions, threshold 10, 512 walkers, max_steps 64",
                 "vertices": W.n, "edges": int(len(W.g_src)), "insertions": int(len(W.ins_src)),
@@ -291,7 +314,185 @@ def run_ours(args, rank, world, local_rank):
     return res
 
 
+def run_mixed(args, rank, world, local_rank):
+    """The mixed-stream workload: every stream file in order per step."""
+    import torch
+    import dygrass_b200 as dyg
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    W = make_workload(args, rank)
+    H0 = dyg.Graph.from_edges(W.n, W.h_src, W.h_dst, W.h_w, device=local_rank)
+    G0 = dyg.Graph.from_edges(W.n, W.g_src, W.g_dst, W.g_w, device=local_rank)
+    H, G = H0.clone(), G0.clone()
+    nmax = max(len(f[1]) for f in W.files)
+    rec_cap = nmax * (W.dparams.max_steps + 4 * W.dparams.heuristic_walkers) + 1024
+
+    def t(a, dt=None):
+        return torch.from_numpy(np.ascontiguousarray(a)).to(dev) if dt is None else \
+            torch.from_numpy(np.ascontiguousarray(a).view(dt)).to(dev)
+
+    dfiles = [(op, t(s_, np.int32), t(d_, np.int32), None if w_ is None else t(w_))
+              for op, s_, d_, w_ in W.files]
+    o_st = torch.empty(nmax, dtype=torch.int32, device=dev)
+    o_cd = torch.empty(nmax, dtype=torch.float32, device=dev)
+    o_rx = torch.empty(rec_cap, dtype=torch.int32, device=dev)
+    o_ry = torch.empty(rec_cap, dtype=torch.int32, device=dev)
+    o_rk = torch.empty(rec_cap, dtype=torch.uint8, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    n_upd = W.n_updates
+
+    def reset():
+        H.copy_from(H0, sp)
+        G.copy_from(G0, sp)
+        flush.fill_(rank + 1)
+
+    def apply(files, st, cd, rx, ry, rk):
+        uid, acc, nrec = 0, 0, 0
+        for op, s_, d_, w_ in files:
+            p = W.dparams if op else W.iparams
+            nrec += dyg.stream_file_into(G, H, op, s_, d_, w_, p, st, cd, rx, ry, rk, rec_cap,
+                                         first_update_id=uid, stream=sp)
+            uid += len(s_)
+        return nrec
+
+    if args.profile_only:
+        reset()
+        apply(dfiles, o_st, o_cd, o_rx, o_ry, o_rk)
+        torch.cuda.synchronize()
+        return None
+    for _ in range(args.warmup):
+        reset()
+        apply(dfiles, o_st, o_cd, o_rx, o_ry, o_rk)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    m0 = (H.counters()[0], G.counters()[0])
+    launches0 = dyg.kernel_launches()
+    dyg.profile_reset()
+    dyg.profile_enable(True)
+    times, nrec = [], 0
+    for _ in range(args.steps):
+        reset()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        nrec = apply(dfiles, o_st, o_cd, o_rx, o_ry, o_rk)
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    dyg.profile_enable(False)
+    prof = dyg.profile_read()
+    launches = dyg.kernel_launches() - launches0
+    m1 = (H.counters()[0], G.counters()[0])
+    clk = clocks.stop()
+    barrier()
+    ms = float(np.mean(times))
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    incr_moves = (m1[0] - m0[0]) / args.steps
+    decr_moves = (m1[1] - m0[1]) / args.steps
+
+    e2e = None
+    if not args.no_e2e:
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+        hfiles = [(op, pin(s_), pin(d_), None if w_ is None else pin(w_)) for op, s_, d_, w_ in W.files]
+        h_st, h_cd = pin(np.empty(nmax, np.int32)), pin(np.empty(nmax, np.float32))
+        h_rx, h_ry = pin(np.empty(rec_cap, np.uint32)), pin(np.empty(rec_cap, np.uint32))
+        h_rk = pin(np.empty(rec_cap, np.uint8))
+        barrier()
+        torch.cuda.synchronize()
+        et, nrec_h = [], 0
+        for _ in range(max(1, args.steps)):
+            reset()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            nrec_h = apply(hfiles, h_st, h_cd, h_rx, h_ry, h_rk)
+            e1.record(stream)
+            e1.synchronize()
+            et.append(e0.elapsed_time(e1))
+        barrier()
+        ems = float(np.mean(et))
+        if world > 1:
+            import torch.distributed as dist
+            tt = torch.tensor([ems], dtype=torch.float64, device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ems = float(tt.item())
+        nins = sum(len(f[1]) for f in W.files if f[0] == 0)
+        e2e = {"value": world * n_upd / (ems / 1e3), "unit": "edge_updates/s", "ms_per_step": ems,
+               "h2d_bytes_per_step": int(nins * 12 + (n_upd - nins) * 8),
+               "d2h_bytes_per_step": int(n_upd * 8 + nrec_h * 9)}
+
+    walk_ms = prof["incr_walk_ms"] + prof["decr_walk_ms"]
+    walk_launches = prof["incr_walk_launches"] + prof["decr_walk_launches"]
+    dom_decr = prof["decr_walk_ms"] >= prof["incr_walk_ms"]
+    res = {
+        "ms_per_step": ms, "steps_ms": times, "nin": n_upd, "ndel": 0, "accepted": None,
+        "recovered": nrec, "incr_moves": incr_moves, "decr_moves": decr_moves,
+        "walk_ms_per_step": walk_ms / args.steps, "walk_launches": walk_launches, "prof": prof,
+        "launches_per_step": launches / args.steps, "clocks": clk, "e2e": e2e,
+        "dom_kernel": "k_walk<0,0> (decremental walk on G)" if dom_decr
+        else "k_walk<1,0> (incremental walk on H)",
+        "dom_bytes_per_launch": (decr_moves if dom_decr else incr_moves) * args.steps * BYTES_PER_MOVE
+        / max(prof["decr_walk_launches"] if dom_decr else prof["incr_walk_launches"], 1),
+        "dom_ms_per_launch": (prof["decr_walk_ms"] / max(prof["decr_walk_launches"], 1)) if dom_decr
+        else (prof["incr_walk_ms"] / max(prof["incr_walk_launches"], 1)),
+        "W": W,
+    }
+    for g in (H, G, H0, G0):
+        g.close()
+    return res
+
+
 # --------------------------------------------------------- CPU baseline
+
+def cpu_baseline_mixed(W, threads=None):
+    """The oracle on a bounded sample of the mixed stream: the first insertion
+    file and the first deletion file (applied in stream order), per-update
+    costs extrapolated to the stream's insert/delete mix."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    th = threads or pyoracle.max_threads()
+    Ho = pyoracle.OGraph(W.n, W.h_src, W.h_dst, W.h_w)
+    Go = pyoracle.OGraph(W.n, W.g_src, W.g_dst, W.g_w)
+    t_op, n_op = [0.0, 0.0], [0, 0]
+    uid = 0
+    for op, s_, d_, w_ in W.files:
+        if n_op[0] and n_op[1]:
+            break
+        p = W.dparams if op else W.iparams
+        t0 = time.perf_counter()
+        pyoracle.stream_file(Go, Ho, op, s_, d_, w_, p, first_uid=uid, threads=th)
+        dt = time.perf_counter() - t0
+        uid += len(s_)
+        if not n_op[op]:
+            t_op[op] += dt
+            n_op[op] += len(s_)
+    nins = sum(len(f[1]) for f in W.files if f[0] == 0)
+    ndel = W.n_updates - nins
+    est = t_op[0] / max(n_op[0], 1) * nins + t_op[1] / max(n_op[1], 1) * ndel
+    return {"value": W.n_updates / est, "unit": "edge_updates/s", "cores": th, "kind": "port",
+            "seconds": sum(t_op),
+            "sample": f"oracle (C/OpenMP, {th} threads): the stream files up to the first deletion "
+                      f"file, timing the first insertion file ({n_op[0]} updates) and the first "
+                      f"deletion file ({n_op[1]} updates); per-update costs extrapolated to the "
+                      f"stream's mix ({nins} insertions, {ndel} deletions)"}
+
 
 def cpu_baseline(W, threads=None, max_incr=None):
     """The oracle (CPU port of the reference update loop) on a bounded sample:
@@ -338,15 +539,17 @@ def main():
         if rank != 0:
             return 0
         W = make_workload(args, 0)
+        base = cpu_baseline_mixed if args.workload == "rmat" else cpu_baseline
         vals = []
         for i in range(args.warmup + args.steps):
-            r = cpu_baseline(W)
+            r = base(W)
             if i >= args.warmup:
                 vals.append(r)
         v = float(np.mean([r["value"] for r in vals]))
         out = {"metric": "edge updates/sec (incr+decr)", "value": v, "unit": "edge_updates/s",
                "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-               "ms_per_step": (len(W.ins_src) + len(W.del_src)) / v * 1e3,
+               "ms_per_step": (W.n_updates if args.workload == "rmat"
+                               else len(W.ins_src) + len(W.del_src)) / v * 1e3,
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                "data": "synthetic (seeded)", "config": workload_config(W, args),
                "cpu_baseline": {k: vals[-1][k] for k in ("value", "unit", "cores", "kind", "sample")},
@@ -363,7 +566,7 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
-    res = run_ours(args, rank, world, local_rank)
+    res = (run_mixed if args.workload == "rmat" else run_ours)(args, rank, world, local_rank)
     if res is None:
         return 0
     W = res.pop("W")
@@ -398,7 +601,7 @@ def main():
     moves = res["incr_moves"] + res["decr_moves"]
     cpu = None
     if not args.no_cpu_baseline and world == 1:
-        cpu = cpu_baseline(W)
+        cpu = cpu_baseline_mixed(W) if args.workload == "rmat" else cpu_baseline(W)
     out = {
         "metric": "edge updates/sec (incr+decr)",
         "value": value, "unit": "edge_updates/s", "n_gpus": world, "steps": args.steps,

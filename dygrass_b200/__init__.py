@@ -374,7 +374,22 @@ def stream_file(G: Graph, H: Graph, op: int, src, dst, w, params: WalkParams,
     return DecrementalResult(st, cd, rx[:k].copy(), ry[:k].copy(), rk[:k].copy())
 
 
+def stream_file_into(G: Graph, H: Graph, op: int, src, dst, w, params: WalkParams, status,
+                     conductance, rec_src, rec_dst, rec_kind, rec_cap: int,
+                     first_update_id: int = 0, chunk: int = 0, stream: int | None = None) -> int:
+    """stream_file writing into caller buffers (numpy or torch, host or
+    device); returns the number of recovered edges."""
+    src, dst = _as(src, np.uint32), _as(dst, np.uint32)
+    w = None if w is None else _as(w, np.float32)
+    nrec = C.c_uint64()
+    _check(lib().dyg_stream_file(G.handle, H.handle, int(op), _ptr(src), _ptr(dst), _ptr(w), len(src),
+                                 int(first_update_id), int(chunk), C.byref(params), _ptr(status),
+                                 _ptr(conductance), _ptr(rec_src), _ptr(rec_dst), _ptr(rec_kind),
+                                 int(rec_cap), C.byref(nrec), stream), "dyg_stream_file")
+    return nrec.value
+
+
 __all__ = ["Graph", "WalkParams", "GraphOpts", "DygError", "incremental_batch",
            "incremental_stream", "decremental_batch", "decremental_stream", "lib", "version",
            "reference_batch_size", "IncrementalResult", "DecrementalResult", "stream_file",
-           "stream_default_chunk"]
+           "stream_file_into", "stream_default_chunk"]

@@ -170,7 +170,8 @@ void free_graph(dyg_graph *G) {
                    &ws.htab_v, &ws.nop, &ws.cub_tmp, &ws.s_src, &ws.s_dst, &ws.s_w, &ws.s_o1,
                    &ws.s_o2, &ws.s_o3, &ws.rx2, &ws.ry2, &ws.rk2, &ws.rank, &ws.lneed, &ws.dtmp,
                    &ws.rowcnt, &ws.rowtmp, &ws.tmask, &ws.del_hx, &ws.del_hy, &ws.nopos,
-                   &ws.st_key, &ws.st_val, &ws.st_pos, &ws.st_wapp, &ws.scalars, &ws.counts};
+                   &ws.st_key, &ws.st_val, &ws.st_pos, &ws.st_wapp, &ws.big, &ws.scalars,
+                   &ws.counts};
     for (Buf *b : bufs) free_buf(*b);
     if (ws.host_scalars) cudaFreeHost(ws.host_scalars);
     if (ws.host_counts) cudaFreeHost(ws.host_counts);
@@ -317,8 +318,11 @@ dyg_status dyg_graph_copy_from(dyg_graph *dst, const dyg_graph *src, dyg_stream_
                              cudaMemcpyDeviceToDevice, st));
     DYG_CUDA(cudaMemcpyAsync(dst->g.top, src->g.top, sizeof(unsigned long long),
                              cudaMemcpyDeviceToDevice, st));
+    DYG_CUDA(cudaMemsetAsync(ptr<unsigned long long>(dst->ws.scalars) + S_LONG, 0,
+                             sizeof(unsigned long long), st));
     dst->slack = src->slack;
     dst->headroom = src->headroom;
+    dst->long_rows = src->long_rows;
     return DYG_OK;
 }
 

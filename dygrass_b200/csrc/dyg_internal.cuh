@@ -100,6 +100,35 @@ __device__ __forceinline__ unsigned long long mul_hi32(uint32_t r, unsigned long
     return hi + (lo >> 32);
 }
 
+// ------------------------------------------------------------- long rows
+// Rows longer than kBigRow are scanned, moved and edited by a whole block
+// (kBigThreads threads) instead of one thread or one small lane group: on
+// power-law graphs a hub row holds tens of thousands of slots, and a serial
+// scan of it would bound the whole launch.
+constexpr uint32_t kBigRow = 256;
+constexpr uint32_t kBigThreads = 256;
+
+// First j < deg with slots[off + j].x == y, or ~0u.  Every thread of the block
+// calls it; s_best is one shared word.  Tiles of 4 * blockDim.x slots, so a
+// match near the front of a long row ends the scan early.
+__device__ __forceinline__ uint32_t block_find(const uint2 *slots, uint32_t off, uint32_t deg,
+                                               uint32_t y, uint32_t *s_best) {
+    for (uint32_t base = 0; base < deg; base += 4u * blockDim.x) {
+        if (threadIdx.x == 0) *s_best = ~0u;
+        __syncthreads();
+#pragma unroll
+        for (uint32_t u = 0; u < 4u; ++u) {
+            const uint32_t j = base + u * blockDim.x + threadIdx.x;
+            if (j < deg && slots[off + j].x == y) atomicMin(s_best, j);
+        }
+        __syncthreads();
+        const uint32_t b = *s_best;
+        __syncthreads();   // every thread has read it before the next reset
+        if (b != ~0u) return b;
+    }
+    return ~0u;
+}
+
 // ------------------------------------------------------------- workspace
 // Device scratch owned by a graph handle, grown on demand.
 struct Buf {
@@ -133,6 +162,7 @@ struct Workspace {
     Buf st_key, st_val;                       // stream file: (min, max) keys and indices, sorted
     Buf st_pos;                               // stream file: uint4 slot positions in G and H
     Buf st_wapp;                              // stream file: G weight of each new edge
+    Buf big;                                  // uint4 per long-row item (block-cooperative pass)
     Buf scalars;                              // u64 scalars (see Scalar)
     Buf counts;                               // u32 counts (see Count)
     unsigned long long *host_scalars = nullptr;   // pinned mirror
@@ -143,16 +173,18 @@ struct Workspace {
 enum Scalar : int {
     S_NEED = 0,       // arena slots a pending append needs (row moves)
     S_CURSOR = 1,     // arena cursor of the moves of that append (follows S_NEED)
-    S_ERR = 2,        // device error bits (kErr*)
-    S_MOVES = 3,      // walker moves (accumulating)
-    S_WALKS = 4,      // walks finished (accumulating)
-    S_TOP = 5,        // arena bump pointer of the owning graph
-    S_WORK = 6,       // work-chunk counter of the persistent walk kernel
-    S_OPRAN = 7,      // set when an append took its row ranks
-    S_TMPCUR = 8,     // scratch cursor of a delete
-    S_HALT = 9,       // halt code of a stream this handle drives (0 = running)
-    S_RECCNT = 10,    // recovered edges recorded so far in a decremental stream
-    S_RECCAP = 11,    // capacity of the record buffers
+    S_OPRAN = 2,      // set when an append took its row ranks
+    S_NBIG = 3,       // entries on the long-row list of the current row operation
+    S_TMPCUR = 4,     // scratch cursor of a delete (follows S_NBIG)
+    S_ERR = 5,        // device error bits (kErr*)
+    S_MOVES = 6,      // walker moves (accumulating)
+    S_WALKS = 7,      // walks finished (accumulating)
+    S_TOP = 8,        // arena bump pointer of the owning graph
+    S_WORK = 9,       // work-chunk counter of the persistent walk kernel
+    S_HALT = 10,      // halt code of a stream this handle drives (0 = running)
+    S_RECCNT = 11,    // recovered edges recorded so far in a decremental stream
+    S_RECCAP = 12,    // capacity of the record buffers (follows S_RECCNT)
+    S_LONG = 13,      // set by an append that made a row longer than kBigRow
     S_NSCALARS = 16
 };
 enum Count : int {
@@ -192,6 +224,10 @@ struct dyg_graph {
     double headroom = 0.5;
     dyg::Workspace ws;
     uint64_t moves_total = 0, walks_total = 0;
+    // The graph has (or may have) a row longer than kBigRow: row operations
+    // then send such rows to the block-cooperative kernels.  Without it every
+    // row takes the one-thread path (same results, no extra launches).
+    bool long_rows = false;
 };
 
 namespace dyg {

@@ -53,6 +53,7 @@ dyg_status read_scalars(dyg_graph *G, cudaStream_t st) {
     DYG_CUDA(cudaMemcpyAsync(ws.host_counts, ws.counts.p, C_NCOUNTS * sizeof(uint32_t),
                              cudaMemcpyDeviceToHost, st));
     DYG_CUDA(cudaStreamSynchronize(st));
+    if (ws.host_scalars[S_LONG]) G->long_rows = true;
     return DYG_OK;
 }
 
@@ -66,6 +67,8 @@ dyg_status read_scalars2(dyg_graph *A, dyg_graph *B, cudaStream_t st) {
                                  cudaMemcpyDeviceToHost, st));
     }
     DYG_CUDA(cudaStreamSynchronize(st));
+    for (dyg_graph *G : {A, B})
+        if (G->ws.host_scalars[S_LONG]) G->long_rows = true;
     return DYG_OK;
 }
 
@@ -87,6 +90,7 @@ dyg_status upload_graph(dyg_graph *G, uint32_t n, const uint64_t *row_ptr, const
     for (uint32_t v = 0; v < n; ++v) {
         const uint64_t deg = row_ptr[v + 1] - row_ptr[v];
         const uint64_t cap = deg + G->slack;
+        if (deg > kBigRow) G->long_rows = true;
         h_desc[v] = make_uint2((uint32_t)off, (uint32_t)deg);
         h_cap[v] = (uint32_t)cap;
         off += cap;

@@ -248,11 +248,14 @@ __global__ void k_hash_insert(const unsigned long long *halt, const uint32_t *cx
 
 // keep[i] = candidate i is the first occurrence of its edge and the edge is
 // not in H (gpu_graph.cuh:534-538 and 599-601 test sparse_map the same way);
-// zero for M <= i < M_host.
+// zero for M <= i < M_host.  H membership scans the shorter of the two rows;
+// when that row is longer than kBigRow the candidate goes to the big list and
+// k_keep_big decides.
 __global__ void k_hash_keep(const unsigned long long *halt, DevGraph h, const uint32_t *cx,
                             const uint32_t *cy, const uint32_t *M_dev, uint32_t M_host,
                             const unsigned long long *tk, const uint32_t *tv,
-                            const uint32_t *tmask, uint32_t *keep) {
+                            const uint32_t *tmask, uint32_t *keep, uint4 *big,
+                            unsigned long long *nbig, bool big_ok) {
     if (HALTED(halt)) return;
     const uint32_t M = dcount(M_dev, M_host), mask = *tmask;
     GSTRIDE(i, M_host) {
@@ -265,18 +268,39 @@ __global__ void k_hash_keep(const unsigned long long *halt, DevGraph h, const ui
                 while (tk[s] != k) s = (s + 1u) & mask;
                 if (tv[s] == i) {
                     kp = 1;
-                    if (x < h.n) {
-                        const uint2 d = h.desc[x];
-                        for (uint32_t j = 0; j < d.y; ++j)
-                            if (h.slots[d.x + j].x == y) {
-                                kp = 0;
-                                break;
-                            }
+                    if (x < h.n && y < h.n) {
+                        const uint2 dx = h.desc[x], dy = h.desc[y];
+                        const bool xs = dx.y <= dy.y;
+                        const uint2 d = xs ? dx : dy;
+                        const uint32_t other = xs ? y : x;
+                        if (big_ok && d.y > kBigRow) {
+                            big[atomicAdd(nbig, 1ull)] = make_uint4(i, xs ? x : y, other, 0u);
+                        } else {
+                            for (uint32_t j = 0; j < d.y; ++j)
+                                if (h.slots[d.x + j].x == other) {
+                                    kp = 0;
+                                    break;
+                                }
+                        }
                     }
                 }
             }
         }
         keep[i] = kp;
+    }
+}
+
+// One block per long-row candidate: {candidate, row, column}.
+__global__ void k_keep_big(const unsigned long long *halt, DevGraph h, const uint4 *big,
+                           const unsigned long long *nbig, uint32_t *keep) {
+    __shared__ uint32_t s_best;
+    if (HALTED(halt)) return;
+    const uint32_t nb = (uint32_t)*nbig;
+    for (uint32_t q = blockIdx.x; q < nb; q += gridDim.x) {
+        const uint4 e = big[q];
+        const uint2 d = h.desc[e.y];
+        const uint32_t j = block_find(h.slots, d.x, d.y, e.z, &s_best);
+        if (threadIdx.x == 0 && j != ~0u) keep[e.x] = 0;
     }
 }
 
@@ -337,6 +361,7 @@ dyg_status recover_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *cx, const
     DYG_TRY(ensure(ws.htab_v, sizeof(uint32_t) * T));
     DYG_TRY(ensure(ws.tmask, sizeof(uint32_t)));
     DYG_TRY(ensure(ws.keep, sizeof(uint32_t) * (size_t)M_host * 2));
+    DYG_TRY(ensure(ws.big, sizeof(uint4) * (size_t)M_host));
     DYG_TRY(ensure(ws.hx, sizeof(uint32_t) * (size_t)M_host * 2));
     DYG_TRY(ensure(ws.hy, sizeof(uint32_t) * (size_t)M_host * 2));
     DYG_TRY(ensure(ws.hw, sizeof(float) * (size_t)M_host * 2));
@@ -353,10 +378,18 @@ dyg_status recover_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *cx, const
     k_hash_insert<<<gr, 256, 0, st>>>(halt, cx, cy, M_dev, M_host, ptr<unsigned long long>(ws.htab_k),
                                       ptr<uint32_t>(ws.htab_v), ptr<uint32_t>(ws.tmask));
     count_launch();
+    const bool big_ok = H->long_rows;
+    if (big_ok) DYG_CUDA(cudaMemsetAsync(sc + S_NBIG, 0, sizeof(unsigned long long), st));
     k_hash_keep<<<gr, 256, 0, st>>>(halt, H->g, cx, cy, M_dev, M_host,
                                     ptr<unsigned long long>(ws.htab_k), ptr<uint32_t>(ws.htab_v),
-                                    ptr<uint32_t>(ws.tmask), keep);
+                                    ptr<uint32_t>(ws.tmask), keep, ptr<uint4>(ws.big), sc + S_NBIG,
+                                    big_ok);
     count_launch();
+    if (big_ok) {
+        k_keep_big<<<num_sms() * 2, kBigThreads, 0, st>>>(halt, H->g, ptr<uint4>(ws.big),
+                                                          sc + S_NBIG, keep);
+        count_launch();
+    }
     DYG_TRY(exclusive_scan_u32(ws, keep, kpos, M_host, st));
     k_rec_check<<<1, 1, 0, st>>>(halt, keep, kpos, M_dev, M_host, sc,
                                  halt_code(batch, (uint32_t)kHaltRecords, phase));

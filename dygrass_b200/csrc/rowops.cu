@@ -86,6 +86,7 @@ __global__ void k_reserve(unsigned long long *top1, uint64_t cap1, const unsigne
 
 __global__ void k_app_move(DevGraph g, const uint32_t *hx, const uint32_t *m_dev, uint32_t m_host,
                            const uint32_t *rank, const uint32_t *lneed, unsigned long long *cursor,
+                           uint4 *big, unsigned long long *nbig, bool big_ok,
                            const unsigned long long *halt) {
     if (*halt) return;
     const uint32_t m = dcount(m_dev, m_host);
@@ -94,12 +95,36 @@ __global__ void k_app_move(DevGraph g, const uint32_t *hx, const uint32_t *m_dev
         const uint32_t x = hx[i];
         const uint2 d = g.desc[x];
         const uint32_t off = (uint32_t)atomicAdd(cursor, (unsigned long long)lneed[i]);
+        if (big_ok && d.y > kBigRow) {   // copied by k_app_move_big
+            big[atomicAdd(nbig, 1ull)] = make_uint4(i, off, d.x, d.y);
+            continue;
+        }
         for (uint32_t j = 0; j < d.y; ++j) {
             g.slots[off + j] = g.slots[d.x + j];
             g.wts[off + j] = g.wts[d.x + j];
         }
         g.cap[x] = lneed[i];
         g.desc[x] = make_uint2(off, d.y);
+    }
+}
+
+// One block per long row to move: {leader, new offset, old offset, degree}.
+__global__ void k_app_move_big(DevGraph g, const uint32_t *hx, const uint32_t *lneed,
+                               const uint4 *big, const unsigned long long *nbig,
+                               const unsigned long long *halt) {
+    if (*halt) return;
+    const uint32_t nb = (uint32_t)*nbig;
+    for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
+        const uint4 e = big[b];
+        for (uint32_t j = threadIdx.x; j < e.w; j += blockDim.x) {
+            g.slots[e.y + j] = g.slots[e.z + j];
+            g.wts[e.y + j] = g.wts[e.z + j];
+        }
+        if (threadIdx.x == 0) {
+            const uint32_t x = hx[e.x];
+            g.cap[x] = lneed[e.x];
+            g.desc[x] = make_uint2(e.y, e.w);
+        }
     }
 }
 
@@ -123,7 +148,8 @@ __global__ void k_app_write(DevGraph g, const uint32_t *hx, const uint32_t *hy, 
 // this operation's ranks were taken).
 __global__ void k_app_finish(DevGraph g, const uint32_t *hx, const uint32_t *m_dev,
                              uint32_t m_host, const uint32_t *rank, uint32_t *rowcnt,
-                             const unsigned long long *halt, const unsigned long long *ran) {
+                             const unsigned long long *halt, const unsigned long long *ran,
+                             unsigned long long *long_flag) {
     const bool halted = *halt != 0ull;
     if (halted && !*ran) return;
     const uint32_t m = dcount(m_dev, m_host);
@@ -150,6 +176,7 @@ __global__ void k_app_finish(DevGraph g, const uint32_t *hx, const uint32_t *m_d
         for (uint32_t a = 0; a < cnt; ++a)
             g.slots[base + a].y = __float_as_uint(__frcp_rn(g.wts[base + a]));
         g.desc[x] = make_uint2(d.x, d.y + cnt);
+        if (d.y + cnt > kBigRow && d.y <= kBigRow) *long_flag = 1ull;
     }
 }
 
@@ -197,14 +224,22 @@ __global__ void k_del_scatter(DevGraph g, const uint32_t *hx, uint32_t m, const 
 
 // Leaders remove their row's entries in list order.  With `mask`, entry
 // i = 2e + side is applied only if edge e was found on both sides of `mask`.
+// With big_ok, rows longer than kBigRow go to the big list for
+// k_del_apply_big.
 __global__ void k_del_apply(DevGraph g, const uint32_t *hx, const uint32_t *hy, uint32_t m,
                             const uint32_t *rank, uint32_t *rowcnt, const uint32_t *rowtmp,
-                            uint32_t *tmp, const uint8_t *mask, uint8_t *found,
+                            uint32_t *tmp, const uint8_t *mask, uint8_t *found, uint4 *big,
+                            unsigned long long *nbig, bool big_ok,
                             const unsigned long long *halt) {
     if (*halt) return;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
         if (rank[i] != 0u) continue;
         const uint32_t x = hx[i];
+        const uint2 d = g.desc[x];
+        if (big_ok && d.y > kBigRow) {
+            big[atomicAdd(nbig, 1ull)] = make_uint4(i, 0u, 0u, 0u);
+            continue;
+        }
         const uint32_t cnt = rowcnt[x];
         rowcnt[x] = 0u;
         uint32_t *run = tmp + rowtmp[x];
@@ -217,7 +252,6 @@ __global__ void k_del_apply(DevGraph g, const uint32_t *hx, const uint32_t *hy, 
             }
             run[b] = v;
         }
-        const uint2 d = g.desc[x];
         uint32_t deg = d.y;
         for (uint32_t a = 0; a < cnt; ++a) {
             const uint32_t k = run[a];
@@ -237,6 +271,53 @@ __global__ void k_del_apply(DevGraph g, const uint32_t *hx, const uint32_t *hy, 
     }
 }
 
+// One block per long row: the row's run is ordered by list index (each
+// entry placed at its rank, into the second half of the scratch), then the
+// deletions are applied one by one, each search a block-wide scan.  The
+// result is the same as the one-thread path's.
+__global__ void k_del_apply_big(DevGraph g, const uint32_t *hx, const uint32_t *hy, uint32_t m,
+                                uint32_t *rowcnt, const uint32_t *rowtmp, uint32_t *tmp,
+                                const uint8_t *mask, uint8_t *found, const uint4 *big,
+                                const unsigned long long *nbig, const unsigned long long *halt) {
+    __shared__ uint32_t s_best;
+    if (*halt) return;
+    const uint32_t nb = (uint32_t)*nbig;
+    for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
+        const uint32_t x = hx[big[b].x];
+        const uint32_t cnt = rowcnt[x];
+        const uint32_t *run = tmp + rowtmp[x];
+        uint32_t *sorted = tmp + m + rowtmp[x];
+        for (uint32_t a = threadIdx.x; a < cnt; a += blockDim.x) {
+            const uint32_t v = run[a];
+            uint32_t r = 0;
+            for (uint32_t c = 0; c < cnt; ++c) r += run[c] < v;
+            sorted[r] = v;
+        }
+        __syncthreads();
+        const uint2 d = g.desc[x];
+        uint32_t deg = d.y;
+        for (uint32_t a = 0; a < cnt; ++a) {
+            const uint32_t k = sorted[a];
+            if (mask && !(mask[k & ~1u] && mask[k | 1u])) continue;
+            const uint32_t j = block_find(g.slots, d.x, deg, hy[k], &s_best);
+            if (j != ~0u) {
+                if (threadIdx.x == 0) {
+                    g.slots[d.x + j] = g.slots[d.x + deg - 1u];
+                    g.wts[d.x + j] = g.wts[d.x + deg - 1u];
+                    found[k] = 1;
+                }
+                --deg;
+                __syncthreads();   // the moved slot is visible to the next search
+            }
+        }
+        if (threadIdx.x == 0) {
+            rowcnt[x] = 0u;
+            g.desc[x] = make_uint2(d.x, deg);
+        }
+        __syncthreads();
+    }
+}
+
 int grid_for(uint64_t m) {
     const uint64_t b = (m + 255) / 256;
     const uint64_t cap = (uint64_t)num_sms() * 8;
@@ -249,7 +330,8 @@ dyg_status rowops_ensure(dyg_graph *G, uint32_t m_host) {
     Workspace &ws = G->ws;
     DYG_TRY(ensure(ws.rank, sizeof(uint32_t) * (size_t)(m_host ? m_host : 1)));
     DYG_TRY(ensure(ws.lneed, sizeof(uint32_t) * (size_t)(m_host ? m_host : 1)));
-    DYG_TRY(ensure(ws.dtmp, sizeof(uint32_t) * (size_t)(m_host ? m_host : 1)));
+    DYG_TRY(ensure(ws.dtmp, sizeof(uint32_t) * (size_t)(m_host ? m_host : 1) * 2));
+    DYG_TRY(ensure(ws.big, sizeof(uint4) * (size_t)(m_host ? m_host : 1)));
     if (!ws.rowcnt.p) {
         DYG_TRY(ensure(ws.rowcnt, sizeof(uint32_t) * (size_t)(G->g.n ? G->g.n : 1)));
         DYG_TRY(ensure(ws.rowtmp, sizeof(uint32_t) * (size_t)(G->g.n ? G->g.n : 1)));
@@ -270,8 +352,9 @@ dyg_status append_enqueue(dyg_graph *GA, const AppendList &A, dyg_graph *GB, con
         if (!G) continue;
         DYG_TRY(rowops_ensure(G, ls[k]->m_host));
         unsigned long long *sc = ptr<unsigned long long>(G->ws.scalars);
-        DYG_CUDA(cudaMemsetAsync(sc + S_NEED, 0, sizeof(unsigned long long) * 2, st));  // need, cursor
-        DYG_CUDA(cudaMemsetAsync(sc + S_OPRAN, 0, sizeof(unsigned long long), st));
+        // need, cursor, ran [, long-row count]
+        DYG_CUDA(cudaMemsetAsync(sc + S_NEED, 0, sizeof(unsigned long long) * (G->long_rows ? 4 : 3),
+                                 st));
         if (ls[k]->m_host == 0) continue;
         const int gr = grid_for(ls[k]->m_host);
         k_rank<<<gr, 256, 0, st>>>(G->g, ls[k]->hx, ls[k]->m_dev, ls[k]->m_host,
@@ -296,14 +379,21 @@ dyg_status append_enqueue(dyg_graph *GA, const AppendList &A, dyg_graph *GB, con
         const int gr = grid_for(ls[k]->m_host);
         k_app_move<<<gr, 256, 0, st>>>(G->g, ls[k]->hx, ls[k]->m_dev, ls[k]->m_host,
                                        ptr<uint32_t>(G->ws.rank), ptr<uint32_t>(G->ws.lneed),
-                                       sc + S_CURSOR, halt);
+                                       sc + S_CURSOR, ptr<uint4>(G->ws.big), sc + S_NBIG,
+                                       G->long_rows, halt);
         count_launch();
+        if (G->long_rows) {
+            k_app_move_big<<<num_sms() * 2, kBigThreads, 0, st>>>(
+                G->g, ls[k]->hx, ptr<uint32_t>(G->ws.lneed), ptr<uint4>(G->ws.big), sc + S_NBIG,
+                halt);
+            count_launch();
+        }
         k_app_write<<<gr, 256, 0, st>>>(G->g, ls[k]->hx, ls[k]->hy, ls[k]->hw, ls[k]->m_dev,
                                         ls[k]->m_host, ptr<uint32_t>(G->ws.rank), halt);
         count_launch();
         k_app_finish<<<gr, 256, 0, st>>>(G->g, ls[k]->hx, ls[k]->m_dev, ls[k]->m_host,
                                          ptr<uint32_t>(G->ws.rank), ptr<uint32_t>(G->ws.rowcnt),
-                                         halt, sc + S_OPRAN);
+                                         halt, sc + S_OPRAN, sc + S_LONG);
         count_launch();
     }
     DYG_CUDA(cudaGetLastError());
@@ -317,7 +407,11 @@ dyg_status delete_enqueue(dyg_graph *G, const uint32_t *hx, const uint32_t *hy, 
     if (m == 0) return DYG_OK;
     DYG_TRY(rowops_ensure(G, m));
     unsigned long long *sc = ptr<unsigned long long>(G->ws.scalars);
-    DYG_CUDA(cudaMemsetAsync(sc + S_TMPCUR, 0, sizeof(unsigned long long), st));
+    // [long-row count,] scratch cursor
+    if (G->long_rows)
+        DYG_CUDA(cudaMemsetAsync(sc + S_NBIG, 0, sizeof(unsigned long long) * 2, st));
+    else
+        DYG_CUDA(cudaMemsetAsync(sc + S_TMPCUR, 0, sizeof(unsigned long long), st));
     DYG_CUDA(cudaMemsetAsync(found, 0, m, st));
     const int gr = grid_for(m);
     k_rank<<<gr, 256, 0, st>>>(G->g, hx, nullptr, m, ptr<uint32_t>(G->ws.rank),
@@ -332,8 +426,15 @@ dyg_status delete_enqueue(dyg_graph *G, const uint32_t *hx, const uint32_t *hy, 
     count_launch();
     k_del_apply<<<gr, 256, 0, st>>>(G->g, hx, hy, m, ptr<uint32_t>(G->ws.rank),
                                     ptr<uint32_t>(G->ws.rowcnt), ptr<uint32_t>(G->ws.rowtmp),
-                                    ptr<uint32_t>(G->ws.dtmp), mask, found, halt);
+                                    ptr<uint32_t>(G->ws.dtmp), mask, found, ptr<uint4>(G->ws.big),
+                                    sc + S_NBIG, G->long_rows, halt);
     count_launch();
+    if (G->long_rows) {
+        k_del_apply_big<<<num_sms() * 2, kBigThreads, 0, st>>>(
+            G->g, hx, hy, m, ptr<uint32_t>(G->ws.rowcnt), ptr<uint32_t>(G->ws.rowtmp),
+            ptr<uint32_t>(G->ws.dtmp), mask, found, ptr<uint4>(G->ws.big), sc + S_NBIG, halt);
+        count_launch();
+    }
     DYG_CUDA(cudaGetLastError());
     return DYG_OK;
 }

@@ -60,13 +60,19 @@ __device__ __forceinline__ uint2 group_edge(const DevGraph &g, uint32_t a, uint3
     return a_short ? make_uint2(ps, pl) : make_uint2(pl, ps);
 }
 
+__device__ __forceinline__ bool long_rows(const DevGraph &g, uint32_t a, uint32_t b) {
+    return g.desc[a].y > kBigRow || g.desc[b].y > kBigRow;
+}
+
 // One group of kProbeLanes lanes per edge: slot positions in G and H, the
 // sort key (min << nb | max) and index; self-loops and invalid endpoints get
-// key ~0 (sorted last, never merged or walked).
+// key ~0 (sorted last, never merged or walked).  An edge with a row longer
+// than kBigRow in G or H goes to the big list for k_st_probe_big.
 __global__ void k_st_probe(const unsigned long long *halt, DevGraph G, DevGraph H,
                            const uint32_t *src, const uint32_t *dst, uint32_t n, uint32_t nb,
                            unsigned long long *key, uint32_t *val, uint4 *pos, uint32_t *nflag,
-                           int32_t *status, float *cond, unsigned long long *err) {
+                           int32_t *status, float *cond, uint4 *big, unsigned long long *nbig,
+                           bool big_ok, unsigned long long *err) {
     if (HALTED(halt)) return;
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t i = t / kProbeLanes;
@@ -92,13 +98,44 @@ __global__ void k_st_probe(const unsigned long long *halt, DevGraph G, DevGraph 
         }
         return;
     }
-    const uint2 pg = group_edge(G, a, b, lane, gbase, gmask);
-    const uint2 ph = group_edge(H, a, b, lane, gbase, gmask);
     if (lane == 0) {
         key[i] = ((unsigned long long)a << nb) | b;
         val[i] = i;
-        pos[i] = make_uint4(pg.x, pg.y, ph.x, ph.y);
         nflag[i] = 0;
+    }
+    if (big_ok && (long_rows(G, a, b) || long_rows(H, a, b))) {
+        if (lane == 0) big[atomicAdd(nbig, 1ull)] = make_uint4(i, a, b, 0u);
+        return;
+    }
+    const uint2 pg = group_edge(G, a, b, lane, gbase, gmask);
+    const uint2 ph = group_edge(H, a, b, lane, gbase, gmask);
+    if (lane == 0) pos[i] = make_uint4(pg.x, pg.y, ph.x, ph.y);
+}
+
+// Slots of edge {a, b} in g by block-wide scans, the shorter row first.
+__device__ uint2 block_edge(const DevGraph &g, uint32_t a, uint32_t b, uint32_t *s_best) {
+    const uint2 da = g.desc[a], db = g.desc[b];
+    const bool a_short = da.y <= db.y;
+    const uint2 ds = a_short ? da : db, dl = a_short ? db : da;
+    const uint32_t s = a_short ? a : b, l = a_short ? b : a;
+    const uint32_t js = block_find(g.slots, ds.x, ds.y, l, s_best);
+    if (js == ~0u) return make_uint2(~0u, ~0u);
+    const uint32_t jl = block_find(g.slots, dl.x, dl.y, s, s_best);
+    const uint32_t ps = ds.x + js, pl = jl == ~0u ? ~0u : dl.x + jl;
+    return a_short ? make_uint2(ps, pl) : make_uint2(pl, ps);
+}
+
+// One block per edge on the big list.
+__global__ void k_st_probe_big(const unsigned long long *halt, DevGraph G, DevGraph H,
+                               const uint4 *big, const unsigned long long *nbig, uint4 *pos) {
+    __shared__ uint32_t s_best;
+    if (HALTED(halt)) return;
+    const uint32_t nbl = (uint32_t)*nbig;
+    for (uint32_t q = blockIdx.x; q < nbl; q += gridDim.x) {
+        const uint4 e = big[q];
+        const uint2 pg = block_edge(G, e.y, e.z, &s_best);
+        const uint2 ph = block_edge(H, e.y, e.z, &s_best);
+        if (threadIdx.x == 0) pos[e.x] = make_uint4(pg.x, pg.y, ph.x, ph.y);
     }
 }
 
@@ -262,10 +299,17 @@ dyg_status insert_prep_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src,
     uint32_t *nflag = ptr<uint32_t>(ws.flags), *npos = ptr<uint32_t>(ws.pos);
     uint32_t *counts = ptr<uint32_t>(ws.counts);
     unsigned long long *sc = ptr<unsigned long long>(ws.scalars);
+    const bool big_ok = G->long_rows || H->long_rows;
+    if (big_ok) DYG_CUDA(cudaMemsetAsync(sc + S_NBIG, 0, sizeof(unsigned long long), st));
     k_st_probe<<<blocks((uint64_t)n * kProbeLanes, 256), 256, 0, st>>>(
         halt, G->g, H->g, src, dst, n, nb, key, val, ptr<uint4>(ws.st_pos), nflag, status, cond,
-        sc + S_ERR);
+        ptr<uint4>(ws.big), sc + S_NBIG, big_ok, sc + S_ERR);
     count_launch();
+    if (big_ok) {
+        k_st_probe_big<<<num_sms() * 2, kBigThreads, 0, st>>>(halt, G->g, H->g, ptr<uint4>(ws.big),
+                                                              sc + S_NBIG, ptr<uint4>(ws.st_pos));
+        count_launch();
+    }
     size_t tmp = 0;
     DYG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, key, skey, val, sval, (int)n, 0,
                                              (int)(2 * nb), st));
@@ -357,6 +401,10 @@ dyg_status insert_file_run(dyg_graph *G, dyg_graph *H, const uint32_t *src, cons
     DYG_TRY(ensure(wg.st_val, sizeof(uint32_t) * (size_t)n * 2));
     DYG_TRY(ensure(wg.st_pos, sizeof(uint4) * (size_t)n));
     DYG_TRY(ensure(wg.st_wapp, sizeof(float) * (size_t)n));
+    DYG_TRY(ensure(wg.big, sizeof(uint4) * (size_t)n * 2));   // probe, then the G append
+    DYG_TRY(ensure(wg.dtmp, sizeof(uint32_t) * (size_t)n * 4));
+    DYG_TRY(ensure(wg.rank, sizeof(uint32_t) * (size_t)n * 2));
+    DYG_TRY(ensure(wg.lneed, sizeof(uint32_t) * (size_t)n * 2));
     DYG_TRY(ensure(wg.flags, sizeof(uint32_t) * (size_t)n));
     DYG_TRY(ensure(wg.pos, sizeof(uint32_t) * (size_t)n));
     DYG_TRY(ensure(wg.f_src, sizeof(uint32_t) * (size_t)n));

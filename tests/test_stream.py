@@ -226,3 +226,53 @@ def test_gpu_rmat_mixed_sequence(dyg, oracle, slack, headroom, chunk):
         p = wl.dparams if op else wl.iparams
         apply_both(dyg, oracle, G, H, Go, Ho, op, s, d, w, p, uid0=uid, chunk=chunk)
         uid += len(s)
+
+
+def two_hubs(N=600):
+    """Hubs 0 and 1 joined to every leaf 2..N-1 (weight 1) in G and H; the
+    hub-hub edge (0,1) (weight 100) in G only.  Every hub row is longer than
+    the one-thread limit, so deletions, probes, moves and H-membership tests
+    on them take the block-cooperative paths."""
+    leaves = np.arange(2, N, dtype=np.uint32)
+    hs = np.concatenate([np.zeros(N - 2, np.uint32), np.ones(N - 2, np.uint32)])
+    hd = np.concatenate([leaves, leaves])
+    hw = np.ones(len(hs), np.float32)
+    gs = np.concatenate([hs, np.array([0], np.uint32)])
+    gd = np.concatenate([hd, np.array([1], np.uint32)])
+    gw = np.concatenate([hw, np.array([100.0], np.float32)])
+    return N, (gs, gd, gw), (hs, hd, hw)
+
+
+@pytest.mark.gpu
+def test_gpu_long_rows(dyg, oracle):
+    N, g, h = two_hubs()
+    G, H, Go, Ho = both(dyg, oracle, N, g, h, slack=0, headroom=0.02)
+    rng = np.random.default_rng(5)
+    a = np.arange(2, 202, dtype=np.uint32)
+    # deletions of hub edges: walks a -> 0 go through hub 1; a walker that
+    # steps 1 -> 0 makes (1,0) a recovery candidate with two long H rows
+    r = apply_both(dyg, oracle, G, H, Go, Ho, DEL, a, np.zeros(200, np.uint32), None,
+                   params(walkers=64), uid0=0)
+    assert (r.status >= 1).all()
+    assert any((x, y) in ((0, 1), (1, 0)) for x, y in zip(r.rec_src, r.rec_dst))
+    # insertions: the deleted hub edges come back (new in G: long-row G append),
+    # existing hub edges merge (long-row probes), repeats fold; a low
+    # threshold makes the walks fail so the hub row of H grows past its
+    # capacity (long-row move)
+    s = np.concatenate([a[:100], np.full(50, 1, np.uint32), a[:20]])
+    d = np.concatenate([np.zeros(100, np.uint32), a[100:150], np.zeros(20, np.uint32)])
+    w = rng.uniform(0.5, 2.0, len(s)).astype(np.float32)
+    perm = rng.permutation(len(s))
+    r = apply_both(dyg, oracle, G, H, Go, Ho, INS, s[perm], d[perm], w[perm],
+                   params(threshold=0.5, walkers=64), uid0=1000, chunk=64)
+    assert (r.status == -1).sum() >= 50 and (r.status == MERGED).sum() >= 70
+    # the standalone decremental batch on the same long rows
+    db = dyg.decremental_batch(G, H, a[100:180], np.zeros(80, np.uint32), params(walkers=64),
+                               first_update_id=5000)
+    st, cd, rx, ry, rk, _ = oracle.decremental(Go, Ho, a[100:180], np.zeros(80, np.uint32),
+                                               params(walkers=64), first_uid=5000,
+                                               single_batch=True)
+    assert np.array_equal(db.status, st)
+    assert np.array_equal(db.rec_src, rx) and np.array_equal(db.rec_dst, ry)
+    same_graph(G, Go)
+    same_graph(H, Ho)
