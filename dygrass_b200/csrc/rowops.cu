@@ -84,27 +84,55 @@ __global__ void k_reserve(unsigned long long *top1, uint64_t cap1, const unsigne
     }
 }
 
+// Leaders that must move their row take a new offset; a row of up to 32
+// slots is copied by its leader's lane, a longer one by the whole warp (rows
+// longer than kBigRow, with big_ok, by k_app_move_big instead).  Every lane of a warp runs the same
+// iterations.
 __global__ void k_app_move(DevGraph g, const uint32_t *hx, const uint32_t *m_dev, uint32_t m_host,
                            const uint32_t *rank, const uint32_t *lneed, unsigned long long *cursor,
                            uint4 *big, unsigned long long *nbig, bool big_ok,
                            const unsigned long long *halt) {
     if (*halt) return;
     const uint32_t m = dcount(m_dev, m_host);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
-        if (rank[i] != 0u || lneed[i] == 0u) continue;
-        const uint32_t x = hx[i];
-        const uint2 d = g.desc[x];
-        const uint32_t off = (uint32_t)atomicAdd(cursor, (unsigned long long)lneed[i]);
-        if (big_ok && d.y > kBigRow) {   // copied by k_app_move_big
-            big[atomicAdd(nbig, 1ull)] = make_uint4(i, off, d.x, d.y);
-            continue;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t first = blockIdx.x * blockDim.x + threadIdx.x;
+    for (uint32_t wb = first - lane; wb < m; wb += gridDim.x * blockDim.x) {
+        const uint32_t i = wb + lane;
+        bool mv = i < m && rank[i] == 0u && lneed[i] != 0u;
+        uint32_t x = 0, off = 0;
+        uint2 d = make_uint2(0u, 0u);
+        if (mv) {
+            x = hx[i];
+            d = g.desc[x];
+            off = (uint32_t)atomicAdd(cursor, (unsigned long long)lneed[i]);
+            if (big_ok && d.y > kBigRow) {
+                big[atomicAdd(nbig, 1ull)] = make_uint4(i, off, d.x, d.y);
+                mv = false;
+            }
         }
-        for (uint32_t j = 0; j < d.y; ++j) {
-            g.slots[off + j] = g.slots[d.x + j];
-            g.wts[off + j] = g.wts[d.x + j];
+        // rows of up to 32 slots are copied by their own lane
+        if (mv && d.y <= 32u) {
+            for (uint32_t j = 0; j < d.y; ++j) {
+                g.slots[off + j] = g.slots[d.x + j];
+                g.wts[off + j] = g.wts[d.x + j];
+            }
         }
-        g.cap[x] = lneed[i];
-        g.desc[x] = make_uint2(off, d.y);
+        unsigned todo = __ballot_sync(kFull, mv && d.y > 32u);
+        while (todo) {
+            const int src = __ffs(todo) - 1;
+            todo &= todo - 1u;
+            const uint32_t so = __shfl_sync(kFull, off, src);
+            const uint32_t sx = __shfl_sync(kFull, d.x, src);
+            const uint32_t sy = __shfl_sync(kFull, d.y, src);
+            for (uint32_t j = lane; j < sy; j += 32u) {
+                g.slots[so + j] = g.slots[sx + j];
+                g.wts[so + j] = g.wts[sx + j];
+            }
+        }
+        if (mv) {
+            g.cap[x] = lneed[i];
+            g.desc[x] = make_uint2(off, d.y);
+        }
     }
 }
 
@@ -143,9 +171,14 @@ __global__ void k_app_write(DevGraph g, const uint32_t *hx, const uint32_t *hy, 
     }
 }
 
+constexpr uint32_t kTailWarp = 256;   // new tails up to this length are ordered by a warp
+constexpr uint32_t kTailLane = 8;     // ... and from this length on (shorter: by the leader)
+
 // Leaders order their row's new tail by list index, store 1/w in place of the
 // index, publish the degree and clear the row counter (also after a halt, if
-// this operation's ranks were taken).
+// this operation's ranks were taken).  A tail of kTailLane+1..kTailWarp
+// entries is ordered by the whole warp (each entry placed at its rank among
+// the tail's list indices, which are distinct); other tails by the leader.
 __global__ void k_app_finish(DevGraph g, const uint32_t *hx, const uint32_t *m_dev,
                              uint32_t m_host, const uint32_t *rank, uint32_t *rowcnt,
                              const unsigned long long *halt, const unsigned long long *ran,
@@ -153,30 +186,80 @@ __global__ void k_app_finish(DevGraph g, const uint32_t *hx, const uint32_t *m_d
     const bool halted = *halt != 0ull;
     if (halted && !*ran) return;
     const uint32_t m = dcount(m_dev, m_host);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
-        if (rank[i] != 0u) continue;
-        const uint32_t x = hx[i];
-        const uint32_t cnt = rowcnt[x];
-        rowcnt[x] = 0u;
-        if (halted) continue;
-        const uint2 d = g.desc[x];
-        const uint32_t base = d.x + d.y;
-        for (uint32_t a = 1; a < cnt; ++a) {   // insertion sort by list index
-            const uint2 s = g.slots[base + a];
-            const float w = g.wts[base + a];
-            uint32_t b = a;
-            while (b > 0 && g.slots[base + b - 1].y > s.y) {
-                g.slots[base + b] = g.slots[base + b - 1];
-                g.wts[base + b] = g.wts[base + b - 1];
-                --b;
-            }
-            g.slots[base + b] = s;
-            g.wts[base + b] = w;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t first = blockIdx.x * blockDim.x + threadIdx.x;
+    for (uint32_t wb = first - lane; wb < m; wb += gridDim.x * blockDim.x) {
+        const uint32_t i = wb + lane;
+        const bool lead = i < m && rank[i] == 0u;
+        uint32_t x = 0, cnt = 0;
+        if (lead) {
+            x = hx[i];
+            cnt = rowcnt[x];
+            rowcnt[x] = 0u;
         }
-        for (uint32_t a = 0; a < cnt; ++a)
-            g.slots[base + a].y = __float_as_uint(__frcp_rn(g.wts[base + a]));
-        g.desc[x] = make_uint2(d.x, d.y + cnt);
-        if (d.y + cnt > kBigRow && d.y <= kBigRow) *long_flag = 1ull;
+        if (halted) continue;
+        const uint2 d = lead ? g.desc[x] : make_uint2(0u, 0u);
+        const uint32_t base = d.x + d.y;
+        const bool coop = lead && cnt > kTailLane && cnt <= kTailWarp;
+        if (lead && !coop) {
+            for (uint32_t a = 1; a < cnt; ++a) {   // insertion sort by list index
+                const uint2 sl = g.slots[base + a];
+                const float w = g.wts[base + a];
+                uint32_t b = a;
+                while (b > 0 && g.slots[base + b - 1].y > sl.y) {
+                    g.slots[base + b] = g.slots[base + b - 1];
+                    g.wts[base + b] = g.wts[base + b - 1];
+                    --b;
+                }
+                g.slots[base + b] = sl;
+                g.wts[base + b] = w;
+            }
+            for (uint32_t a = 0; a < cnt; ++a)
+                g.slots[base + a].y = __float_as_uint(__frcp_rn(g.wts[base + a]));
+        }
+        unsigned todo = __ballot_sync(kFull, coop);
+        while (todo) {
+            const int src = __ffs(todo) - 1;
+            todo &= todo - 1u;
+            const uint32_t tb = __shfl_sync(kFull, base, src);
+            const uint32_t c = __shfl_sync(kFull, cnt, src);
+            uint32_t col[kTailWarp / 32], key[kTailWarp / 32], r[kTailWarp / 32];
+            float w[kTailWarp / 32];
+#pragma unroll
+            for (uint32_t u = 0; u < kTailWarp / 32; ++u) {
+                const uint32_t a = lane + 32u * u;
+                key[u] = 0xFFFFFFFFu;
+                r[u] = 0u;
+                if (a < c) {
+                    const uint2 sl = g.slots[tb + a];
+                    col[u] = sl.x;
+                    key[u] = sl.y;
+                    w[u] = g.wts[tb + a];
+                }
+            }
+#pragma unroll
+            for (uint32_t cu = 0; cu < kTailWarp / 32; ++cu) {
+                if (32u * cu >= c) break;
+                for (uint32_t j = 0; j < 32u; ++j) {
+                    const uint32_t kj = __shfl_sync(kFull, key[cu], j);
+#pragma unroll
+                    for (uint32_t u = 0; u < kTailWarp / 32; ++u) r[u] += kj < key[u] ? 1u : 0u;
+                }
+            }
+            __syncwarp();
+#pragma unroll
+            for (uint32_t u = 0; u < kTailWarp / 32; ++u) {
+                if (lane + 32u * u < c) {
+                    g.slots[tb + r[u]] = make_uint2(col[u], __float_as_uint(__frcp_rn(w[u])));
+                    g.wts[tb + r[u]] = w[u];
+                }
+            }
+            __syncwarp();
+        }
+        if (lead) {
+            g.desc[x] = make_uint2(d.x, d.y + cnt);
+            if (d.y + cnt > kBigRow && d.y <= kBigRow) *long_flag = 1ull;
+        }
     }
 }
 
@@ -271,15 +354,21 @@ __global__ void k_del_apply(DevGraph g, const uint32_t *hx, const uint32_t *hy, 
     }
 }
 
-// One block per long row: the row's run is ordered by list index (each
-// entry placed at its rank, into the second half of the scratch), then the
-// deletions are applied one by one, each search a block-wide scan.  The
-// result is the same as the one-thread path's.
+constexpr uint32_t kTrackMax = 128;   // deletions per long row tracked in shared memory
+
+// One block per long row.  The row's run is ordered by list index (each
+// entry placed at its rank, into the second half of the scratch).  Then, if
+// the row has at most kTrackMax deletions whose columns are distinct and each
+// occur once in the row, one pass over the row finds every target's slot and
+// one thread applies the swaps in order, following the single slot each swap
+// moves (the row's last); otherwise every deletion is a block-wide search.
+// Both give the one-thread path's result.
 __global__ void k_del_apply_big(DevGraph g, const uint32_t *hx, const uint32_t *hy, uint32_t m,
                                 uint32_t *rowcnt, const uint32_t *rowtmp, uint32_t *tmp,
                                 const uint8_t *mask, uint8_t *found, const uint4 *big,
                                 const unsigned long long *nbig, const unsigned long long *halt) {
-    __shared__ uint32_t s_best;
+    __shared__ uint32_t s_best, s_ok;
+    __shared__ uint32_t s_y[kTrackMax], s_pos[kTrackMax], s_occ[kTrackMax];
     if (*halt) return;
     const uint32_t nb = (uint32_t)*nbig;
     for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
@@ -293,28 +382,72 @@ __global__ void k_del_apply_big(DevGraph g, const uint32_t *hx, const uint32_t *
             for (uint32_t c = 0; c < cnt; ++c) r += run[c] < v;
             sorted[r] = v;
         }
+        if (threadIdx.x == 0) s_ok = cnt <= kTrackMax ? 1u : 0u;
         __syncthreads();
         const uint2 d = g.desc[x];
         uint32_t deg = d.y;
-        for (uint32_t a = 0; a < cnt; ++a) {
-            const uint32_t k = sorted[a];
-            if (mask && !(mask[k & ~1u] && mask[k | 1u])) continue;
-            const uint32_t j = block_find(g.slots, d.x, deg, hy[k], &s_best);
-            if (j != ~0u) {
-                if (threadIdx.x == 0) {
-                    g.slots[d.x + j] = g.slots[d.x + deg - 1u];
-                    g.wts[d.x + j] = g.wts[d.x + deg - 1u];
-                    found[k] = 1;
+        if (s_ok) {
+            for (uint32_t a = threadIdx.x; a < cnt; a += blockDim.x) {
+                const uint32_t k = sorted[a];
+                const bool on = !mask || (mask[k & ~1u] && mask[k | 1u]);
+                s_y[a] = on ? hy[k] : ~0u;
+                s_pos[a] = ~0u;
+                s_occ[a] = 0u;
+            }
+            __syncthreads();
+            for (uint32_t a = threadIdx.x; a < cnt; a += blockDim.x)
+                for (uint32_t c = 0; c < a; ++c)
+                    if (s_y[a] != ~0u && s_y[c] == s_y[a]) s_ok = 0u;
+            for (uint32_t j = threadIdx.x; j < deg; j += blockDim.x) {
+                const uint32_t col = g.slots[d.x + j].x;
+                for (uint32_t a = 0; a < cnt; ++a)
+                    if (s_y[a] == col) {
+                        atomicMin(&s_pos[a], j);
+                        atomicAdd(&s_occ[a], 1u);
+                    }
+            }
+            __syncthreads();
+            for (uint32_t a = threadIdx.x; a < cnt; a += blockDim.x)
+                if (s_occ[a] > 1u) s_ok = 0u;
+            __syncthreads();
+        }
+        if (s_ok) {
+            if (threadIdx.x == 0) {
+                for (uint32_t a = 0; a < cnt; ++a) {
+                    const uint32_t p = s_pos[a];
+                    if (s_y[a] == ~0u || p == ~0u) continue;
+                    const uint32_t last = deg - 1u;
+                    g.slots[d.x + p] = g.slots[d.x + last];
+                    g.wts[d.x + p] = g.wts[d.x + last];
+                    --deg;
+                    found[sorted[a]] = 1;
+                    if (p != last)   // the slot from `last` now sits at p
+                        for (uint32_t c = a + 1; c < cnt; ++c)
+                            if (s_pos[c] == last) s_pos[c] = p;
                 }
-                --deg;
-                __syncthreads();   // the moved slot is visible to the next search
+                g.desc[x] = make_uint2(d.x, deg);
+            }
+        } else {
+            for (uint32_t a = 0; a < cnt; ++a) {
+                const uint32_t k = sorted[a];
+                if (mask && !(mask[k & ~1u] && mask[k | 1u])) continue;
+                const uint32_t j = block_find(g.slots, d.x, deg, hy[k], &s_best);
+                if (j != ~0u) {
+                    if (threadIdx.x == 0) {
+                        g.slots[d.x + j] = g.slots[d.x + deg - 1u];
+                        g.wts[d.x + j] = g.wts[d.x + deg - 1u];
+                        found[k] = 1;
+                    }
+                    --deg;
+                    __syncthreads();   // the moved slot is visible to the next search
+                }
             }
         }
         if (threadIdx.x == 0) {
             rowcnt[x] = 0u;
-            g.desc[x] = make_uint2(d.x, deg);
+            if (!s_ok) g.desc[x] = make_uint2(d.x, deg);
         }
-        __syncthreads();
+        __syncthreads();   // s_ok and the shared arrays are reused by the next row
     }
 }
 

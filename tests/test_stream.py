@@ -276,3 +276,30 @@ def test_gpu_long_rows(dyg, oracle):
     assert np.array_equal(db.rec_src, rx) and np.array_equal(db.rec_dst, ry)
     same_graph(G, Go)
     same_graph(H, Ho)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("slack", [0, 2])
+def test_gpu_long_tails(dyg, oracle, slack):
+    """Appends of 100 and 300 edges to one row in one batch: the new tail is
+    ordered by a warp (100) and by the leader alone (300); a threshold this
+    low rejects every path longer than one step, so all are accepted."""
+    N = 420
+    ps = np.arange(N - 1, dtype=np.uint32)
+    pd = ps + 1
+    pw = np.ones(N - 1, np.float32)
+    H = dyg.Graph.from_edges(N, ps, pd, pw, slack_per_row=slack, arena_headroom=0.1)
+    Ho = oracle.OGraph(N, ps, pd, pw)
+    p = params(threshold=1e-3, walkers=32)
+    uid = 0
+    for s, d in [(np.zeros(100, np.uint32), np.arange(2, 102, dtype=np.uint32)),
+                 (np.arange(102, 402, dtype=np.uint32), np.zeros(300, np.uint32)),
+                 (np.full(36, 1, np.uint32), np.arange(404, 440, dtype=np.uint32) % N),
+                 (np.full(6, 3, np.uint32), np.arange(300, 306, dtype=np.uint32))]:
+        w = np.linspace(0.5, 2.0, len(s)).astype(np.float32)
+        r = dyg.incremental_batch(H, s, d, w, p, first_update_id=uid)
+        fa, cd, ac, _ = oracle.incremental(Ho, s, d, w, p, first_uid=uid, single_batch=True)
+        assert np.array_equal(r.found_at, fa) and np.array_equal(r.accepted, ac)
+        same_graph(H, Ho)
+        uid += len(s)
+    assert rows(H.export())[0][0] == (1, 1.0) and len(rows(H.export())[0]) == 401
