@@ -37,6 +37,17 @@ INS_MERGED = -4
 INS_SELF_LOOP = -5
 
 
+class MtxInfo(C.Structure):
+    """dyg_mtx_info: the mixed updater's format detection of a graph file."""
+    _fields_ = [("skip_lines", C.c_int64), ("has_header", C.c_int32),
+                ("has_dimensions", C.c_int32), ("weighted", C.c_int32), ("laplacian", C.c_int32),
+                ("triangular", C.c_int32), ("base", C.c_int32), ("v_max", C.c_uint32),
+                ("v_min", C.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
 class DygError(RuntimeError):
     def __init__(self, status: int, what: str, msg: str):
         super().__init__(f"{what}: {STATUS_NAMES.get(status, status)}: {msg}")
@@ -112,6 +123,9 @@ def lib() -> C.CDLL:
         "dyg_mtx_read": ([C.c_char_p, u32, C.c_int, C.POINTER(u64), C.POINTER(vp), C.POINTER(vp),
                           C.POINTER(vp), C.POINTER(u32)], C.c_int),
         "dyg_mtx_free": ([vp], None),
+        "dyg_mtx_detect": ([C.c_char_p, C.POINTER(MtxInfo)], C.c_int),
+        "dyg_mtx_read_auto": ([C.c_char_p, C.POINTER(MtxInfo), C.POINTER(u64), C.POINTER(vp),
+                               C.POINTER(vp), C.POINTER(vp)], C.c_int),
         "dyg_mtx_write": ([C.c_char_p, C.c_int, u64, vp, vp, vp, u32], C.c_int),
         "dyg_synth_lattice_edges": ([u32, u32, u32], u64),
         "dyg_synth_lattice": ([u32, u32, u32, u32, C.c_float, C.c_float, u64, vp, vp, vp], None),
@@ -340,6 +354,32 @@ def decremental_stream(G: Graph, H: Graph, src, dst, params: WalkParams, batch_s
                        stream: int | None = None, rec_cap: int | None = None) -> DecrementalResult:
     return _decremental(lib().dyg_decremental_stream, G, H, src, dst, params, batch_size, stream,
                         rec_cap)
+
+
+def mtx_detect(path: str) -> dict:
+    """Format detection of a graph file with the mixed updater's rules."""
+    info = MtxInfo()
+    _check(lib().dyg_mtx_detect(os.fsencode(path), C.byref(info)), "dyg_mtx_detect")
+    return info.as_dict()
+
+
+def mtx_read_auto(path: str):
+    """Returns (info dict, src, dst, w): the records as the mixed updater's
+    graph loader reads them (0-based)."""
+    info = MtxInfo()
+    m = C.c_uint64()
+    ps, pd, pw = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    _check(lib().dyg_mtx_read_auto(os.fsencode(path), C.byref(info), C.byref(m), C.byref(ps),
+                                   C.byref(pd), C.byref(pw)), "dyg_mtx_read_auto")
+    k = m.value
+    try:
+        src = np.ctypeslib.as_array(C.cast(ps, C.POINTER(C.c_uint32)), (max(k, 1),))[:k].copy()
+        dst = np.ctypeslib.as_array(C.cast(pd, C.POINTER(C.c_uint32)), (max(k, 1),))[:k].copy()
+        w = np.ctypeslib.as_array(C.cast(pw, C.POINTER(C.c_float)), (max(k, 1),))[:k].copy()
+    finally:
+        for p in (ps, pd, pw):
+            lib().dyg_mtx_free(p)
+    return info.as_dict(), src, dst, w
 
 
 def stream_default_chunk(n_vertices: int) -> int:

@@ -9,6 +9,7 @@
 #include <sys/stat.h>
 #include <unistd.h>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -21,6 +22,68 @@ void set_error(const std::string &msg);
 namespace {
 
 inline bool is_ws(char c) { return c == ' ' || c == '\t' || c == '\n' || c == '\r'; }
+
+// A read-only mapping of a whole file (empty files map to nothing).
+struct Mapped {
+    const char *p = nullptr;
+    size_t n = 0;
+    int fd = -1;
+    ~Mapped() {
+        if (p) munmap((void *)p, n);
+        if (fd >= 0) close(fd);
+    }
+    dyg_status open_file(const char *path) {
+        fd = open(path, O_RDONLY);
+        if (fd < 0) {
+            dyg::set_error(std::string("cannot open ") + path + ": " + strerror(errno));
+            return DYG_EIO;
+        }
+        struct stat stt;
+        if (fstat(fd, &stt) != 0) {
+            dyg::set_error(std::string("cannot stat ") + path);
+            return DYG_EIO;
+        }
+        n = (size_t)stt.st_size;
+        if (n) {
+            void *m = mmap(nullptr, n, PROT_READ, MAP_PRIVATE, fd, 0);
+            if (m == MAP_FAILED) {
+                n = 0;
+                dyg::set_error(std::string("cannot mmap ") + path);
+                return DYG_EIO;
+            }
+            p = (const char *)m;
+        }
+        return DYG_OK;
+    }
+};
+
+// Parses the line at [b, e) (at most 254 characters, like the reference's
+// 256-byte line buffer) with sscanf("%lf %lf %lf"); returns the count parsed,
+// 0 for a longer line.
+int scan3(const char *b, const char *e, double *x) {
+    const size_t len = (size_t)(e - b);
+    if (len >= 255) return 0;
+    char line[256];
+    memcpy(line, b, len);
+    line[len] = 0;
+    return sscanf(line, "%lf %lf %lf", &x[0], &x[1], &x[2]);
+}
+
+// Advances past a "line" the way the detector's first two steps do: to the
+// next newline or tab, then past every newline and tab that follows.
+size_t skip_record(const char *d, size_t i, size_t n) {
+    while (i < n && d[i] != '\n' && d[i] != '\t') ++i;
+    while (i < n && (d[i] == '\n' || d[i] == '\t')) ++i;
+    return i;
+}
+
+const char *line_end(const char *d, size_t i, size_t n) {
+    while (i < n && d[i] != '\n') ++i;
+    return d + i;
+}
+
+// Vertex ids go through the reference's (vertex_t)double conversion.
+inline uint32_t as_vertex(double v) { return (uint32_t)(long long)v; }
 
 }  // namespace
 
@@ -161,6 +224,218 @@ dyg_status dyg_mtx_write(const char *path, int append, uint64_t n_edges, const u
         dyg::set_error(std::string("close failed: ") + path);
         return DYG_EIO;
     }
+    return DYG_OK;
+}
+
+// Restates auto_detect_graph_info (dynamic_update/functions.cpp:35-291):
+//  - leading lines starting with '%' are header lines (each ends at a newline
+//    or a tab, functions.cpp:59-70);
+//  - the first other line is a dimensions line when it holds three numbers
+//    "n n m" with m an integer > 1, n*n > m and m >= n - 1 (96-110); it is
+//    skipped even if its n later disagrees with the ids (246-258);
+//  - the next line decides weighted (three numbers) or not (two) (139-170);
+//  - a later line with a negative third number marks a Laplacian (207-211);
+//  - the file is triangular unless the first off-diagonal edge after the
+//    first line appears again, in either orientation, on a later line (214-226);
+//  - the smallest id (0 or 1) is the base (237-244).
+dyg_status dyg_mtx_detect(const char *path, dyg_mtx_info *info) {
+    if (!path || !info) {
+        dyg::set_error("dyg_mtx_detect: NULL argument");
+        return DYG_EINVAL;
+    }
+    Mapped f;
+    dyg_status rc = f.open_file(path);
+    if (rc != DYG_OK) return rc;
+    const char *d = f.p;
+    const size_t n = f.n;
+    dyg_mtx_info r;
+    memset(&r, 0, sizeof r);
+    uint32_t vmax = 0, vmin = 1u << 30;
+    size_t pos = 0;
+    while (pos < n && d[pos] == '%') {
+        r.has_header = 1;
+        r.skip_lines++;
+        pos = skip_record(d, pos, n);
+    }
+    // first non-header line
+    double x[3] = {0, 0, 0};
+    size_t cur = pos;
+    pos = skip_record(d, pos, n);
+    int k = scan3(d + cur, line_end(d, cur, n), x);
+    double dims = 0;
+    if (k == 3 && x[2] == (double)(long)x[2] && x[2] > 1 && x[0] == x[1] && x[0] * x[1] > x[2] &&
+        x[2] >= x[0] - 1) {
+        r.has_dimensions = 1;
+        dims = x[0];
+        r.skip_lines++;
+    }
+    if (!r.has_dimensions) {
+        if (k < 2) {
+            dyg::set_error(std::string(path) + ": the first data line does not hold two numbers");
+            return DYG_EIO;
+        }
+        vmax = std::max(vmax, as_vertex(x[0]));
+        vmin = std::min(vmin, as_vertex(x[0]));
+        vmax = std::max(vmax, as_vertex(x[1]));
+        vmin = std::min(vmin, as_vertex(x[1]));
+    }
+    // the line that decides the weight column
+    bool loaded = false, checked = false;
+    double ea = 0, eb = 0;
+    r.triangular = 1;
+    cur = pos;
+    pos = skip_record(d, pos, n);
+    k = scan3(d + cur, line_end(d, cur, n), x);
+    if (k == 3) {
+        r.weighted = 1;
+        if (x[0] != x[1]) {
+            ea = std::max(x[0], x[1]);
+            eb = std::min(x[0], x[1]);
+            loaded = true;
+        }
+    } else if (k != 2) {
+        dyg::set_error(std::string(path) + ": invalid line format (expected 2 or 3 numbers)");
+        return DYG_EIO;
+    }
+    vmax = std::max(vmax, as_vertex(x[0]));
+    vmin = std::min(vmin, as_vertex(x[0]));
+    vmax = std::max(vmax, as_vertex(x[1]));
+    vmin = std::min(vmin, as_vertex(x[1]));
+    // every later line
+    while (pos < n) {
+        size_t c = pos;
+        while (c < n && (d[c] == ' ' || d[c] == '\t')) ++c;
+        if (c >= n) break;
+        {
+            // ids of the line's first two numbers (strtod, as the reference)
+            char *e1 = nullptr, *e2 = nullptr;
+            const double a = strtod(d + c, &e1);
+            if (e1 > d + c) {
+                const double b = strtod(e1, &e2);
+                if (e2 > e1) {
+                    vmax = std::max(vmax, as_vertex(a));
+                    vmin = std::min(vmin, as_vertex(a));
+                    vmax = std::max(vmax, as_vertex(b));
+                    vmin = std::min(vmin, as_vertex(b));
+                }
+            }
+        }
+        const char *le = line_end(d, c, n);
+        const size_t len = (size_t)(le - (d + c));
+        if (len > 0 && len < 255) {
+            char line[256];
+            memcpy(line, d + c, len);
+            line[len] = 0;
+            if (r.weighted) {
+                k = sscanf(line, "%lf %lf %lf", &x[0], &x[1], &x[2]);
+                if (k >= 3 && x[2] < 0) r.laplacian = 1;
+            } else {
+                k = sscanf(line, "%lf %lf", &x[0], &x[1]);
+            }
+            if (k >= 2) {
+                if (!loaded && x[0] != x[1]) {
+                    ea = std::max(x[0], x[1]);
+                    eb = std::min(x[0], x[1]);
+                    loaded = true;
+                } else if (!checked && loaded) {
+                    if (std::max(x[0], x[1]) == ea && std::min(x[0], x[1]) == eb) {
+                        r.triangular = 0;
+                        checked = true;
+                    }
+                }
+            }
+        }
+        while (pos < n && d[pos] != '\n') ++pos;
+        ++pos;
+        while (pos < n && d[pos] == '\n') ++pos;
+    }
+    if (vmin == 1) {
+        r.base = 1;
+    } else if (vmin == 0) {
+        r.base = 0;
+    } else {
+        dyg::set_error(std::string(path) + ": vertex ids are neither 0- nor 1-based");
+        return DYG_EIO;
+    }
+    if (r.has_dimensions && (double)vmax + (r.base ? 0.0 : 1.0) != dims) r.has_dimensions = 0;
+    r.v_max = vmax;
+    r.v_min = vmin;
+    *info = r;
+    return DYG_OK;
+}
+
+// Reads the records the way the mixed updater's CSRGraph constructor does
+// (dynamic_update/functions.cpp:308-587): skip info.skip_lines lines, then
+// whitespace-separated "src dst [w]" records (w = 1 without a weight column),
+// ids minus the base; a Laplacian's diagonal records are dropped and its
+// weights negated.
+dyg_status dyg_mtx_read_auto(const char *path, dyg_mtx_info *info, uint64_t *n_records,
+                             uint32_t **src, uint32_t **dst, float **w) {
+    if (!path || !info || !n_records || !src || !dst || !w) {
+        dyg::set_error("dyg_mtx_read_auto: NULL argument");
+        return DYG_EINVAL;
+    }
+    *n_records = 0;
+    *src = *dst = nullptr;
+    *w = nullptr;
+    dyg_status rc = dyg_mtx_detect(path, info);
+    if (rc != DYG_OK) return rc;
+    Mapped f;
+    rc = f.open_file(path);
+    if (rc != DYG_OK) return rc;
+    const char *d = f.p;
+    const size_t n = f.n;
+    size_t pos = 0;
+    for (int64_t skipped = 0; skipped < info->skip_lines && pos < n;)
+        if (d[pos++] == '\n') ++skipped;
+    auto is_sep = [](char c) { return c == ' ' || c == '\n' || c == '\t'; };
+    std::vector<uint32_t> vs, vd;
+    std::vector<float> vw;
+    std::string tok;
+    auto next_token = [&](size_t &i) -> const char * {
+        const char *t = d + i;
+        size_t j = i;
+        while (j < n && !is_sep(d[j])) ++j;
+        tok.assign(t, j - i);
+        while (j < n && is_sep(d[j])) ++j;
+        i = j;
+        return tok.c_str();
+    };
+    while (pos < n) {
+        const long a = atol(next_token(pos)) - info->base;
+        const long b = pos < n ? atol(next_token(pos)) - info->base : -1;
+        float wt = 1.0f;
+        if (info->weighted && pos < n) {
+            wt = (float)atof(next_token(pos));
+            if (info->laplacian) wt = -wt;
+        }
+        if (a < 0 || b < 0) {
+            dyg::set_error(std::string(path) + ": record " + std::to_string(vs.size() + 1) +
+                           " has an id below the base");
+            return DYG_EIO;
+        }
+        if (info->laplacian && a == b) continue;
+        vs.push_back((uint32_t)a);
+        vd.push_back((uint32_t)b);
+        vw.push_back(wt);
+    }
+    const size_t m = vs.size();
+    *src = (uint32_t *)malloc(sizeof(uint32_t) * (m ? m : 1));
+    *dst = (uint32_t *)malloc(sizeof(uint32_t) * (m ? m : 1));
+    *w = (float *)malloc(sizeof(float) * (m ? m : 1));
+    if (!*src || !*dst || !*w) {
+        free(*src); free(*dst); free(*w);
+        *src = *dst = nullptr;
+        *w = nullptr;
+        dyg::set_error("host allocation failed");
+        return DYG_ENOMEM;
+    }
+    if (m) {
+        memcpy(*src, vs.data(), sizeof(uint32_t) * m);
+        memcpy(*dst, vd.data(), sizeof(uint32_t) * m);
+        memcpy(*w, vw.data(), sizeof(float) * m);
+    }
+    *n_records = m;
     return DYG_OK;
 }
 

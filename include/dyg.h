@@ -186,7 +186,7 @@ dyg_status dyg_decremental_stream(dyg_graph *G, dyg_graph *H, const uint32_t *sr
                                   uint64_t rec_cap, uint64_t *n_rec, dyg_stream_t stream);
 
 /* Walk-list chunk of the mixed updater: 5% of |V|, at least 10000
- * (dynamic_update/main.cu:86-87). */
+ * (dynamic_update/main.cu:83-84). */
 uint32_t dyg_stream_default_chunk(uint32_t n_vertices);
 /* One file of the mixed insert/delete stream (dynamic_update).
  * op DYG_STREAM_INSERT, in file order: an edge already in G (or repeated

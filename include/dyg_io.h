@@ -30,6 +30,34 @@ void dyg_mtx_free(void *p);
 dyg_status dyg_mtx_write(const char *path, int append, uint64_t n_edges, const uint32_t *src,
                          const uint32_t *dst, const float *w, uint32_t id_offset);
 
+/* What the mixed updater's format detection finds in a graph file
+ * (auto_detect_graph_info, dynamic_update/functions.cpp:35-291). */
+typedef struct dyg_mtx_info {
+    int64_t skip_lines;        /* leading lines that are not records            */
+    int32_t has_header;        /* leading '%' lines                             */
+    int32_t has_dimensions;    /* an "n n m" line that matches the ids          */
+    int32_t weighted;          /* records have a third (weight) column          */
+    int32_t laplacian;         /* some weight is negative                       */
+    int32_t triangular;        /* each undirected edge is listed once           */
+    int32_t base;              /* smallest id: 0 or 1                           */
+    uint32_t v_max, v_min;     /* largest / smallest id as written              */
+} dyg_mtx_info;
+
+/* Format detection with the reference's rules.  DYG_EIO (message in
+ * dyg_last_error_string) where the reference exits: a line that is neither
+ * 2 nor 3 numbers where the weight column is decided, ids neither 0- nor
+ * 1-based. */
+dyg_status dyg_mtx_detect(const char *path, dyg_mtx_info *info);
+/* Detects, then reads the records as the mixed updater's graph loader does
+ * (dynamic_update/functions.cpp:308-587): 0-based ids, weight 1 without a
+ * weight column, a Laplacian's diagonal dropped and its weights negated.
+ * Arrays are malloc'ed (free with dyg_mtx_free).  A triangular file lists
+ * each undirected edge once (build with dyg_graph_create_from_edges); a full
+ * one lists both directions (each record fills its source's row only:
+ * dyg_graph_create_from_csr). */
+dyg_status dyg_mtx_read_auto(const char *path, dyg_mtx_info *info, uint64_t *n_records,
+                             uint32_t **src, uint32_t **dst, float **w);
+
 #ifdef __cplusplus
 }
 #endif

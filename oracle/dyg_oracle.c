@@ -550,7 +550,7 @@ uint64_t orc_decremental_batch(orc_graph *G, orc_graph *H, const uint32_t *src,
 /* ----------------------------------------------------------- stream files */
 
 uint32_t orc_stream_default_chunk(uint32_t n_vertices) {
-    /* 5% of |V|, at least 10000 (dynamic_update/main.cu:86-87) */
+    /* 5% of |V|, at least 10000 (dynamic_update/main.cu:83-84) */
     uint32_t c = (uint32_t)((double)n_vertices * 0.05);
     return c < 10000u ? 10000u : c;
 }
@@ -602,7 +602,7 @@ uint64_t orc_stream_file(orc_graph *G, orc_graph *H, uint32_t op, const uint32_t
         }
         /* walks on H in chunks, each chunk's accepted edges entering H with
            their stream weight before the next chunk walks
-           (dynamic_update/main.cu:107-126, gpu_graph.cuh:629-640) */
+           (dynamic_update/main.cu:107-126, gpu_graph.cuh:632-636) */
         uint64_t *keys = (uint64_t *)malloc((size_t)(nl ? nl : 1) * sizeof(uint64_t));
         for (uint32_t c0 = 0; c0 < nl; c0 += chunk) {
             uint32_t c1 = nl - c0 < chunk ? nl : c0 + chunk;
