@@ -98,6 +98,7 @@ def lib() -> C.CDLL:
         "dyg_graph_opts_default": ([C.POINTER(GraphOpts)], None),
         "dyg_reference_batch_size": ([u32], u32),
         "dyg_graph_create_from_edges": ([u32, u64, vp, vp, vp, C.POINTER(GraphOpts), C.POINTER(vp)], C.c_int),
+        "dyg_graph_create_from_csr": ([u32, vp, vp, vp, C.POINTER(GraphOpts), C.POINTER(vp)], C.c_int),
         "dyg_graph_clone": ([vp, C.POINTER(vp)], C.c_int),
         "dyg_graph_copy_from": ([vp, vp, vp], C.c_int),
         "dyg_graph_destroy": ([vp], C.c_int),
@@ -124,6 +125,9 @@ def lib() -> C.CDLL:
                           C.POINTER(vp), C.POINTER(u32)], C.c_int),
         "dyg_mtx_free": ([vp], None),
         "dyg_mtx_detect": ([C.c_char_p, C.POINTER(MtxInfo)], C.c_int),
+        "dyg_stream_read": ([C.c_char_p, u32, C.POINTER(u64), C.POINTER(vp), C.POINTER(vp),
+                             C.POINTER(vp), C.POINTER(C.c_int32)], C.c_int),
+        "dyg_stream_op_from_name": ([C.c_char_p, u32], u32),
         "dyg_mtx_read_auto": ([C.c_char_p, C.POINTER(MtxInfo), C.POINTER(u64), C.POINTER(vp),
                                C.POINTER(vp), C.POINTER(vp)], C.c_int),
         "dyg_mtx_write": ([C.c_char_p, C.c_int, u64, vp, vp, vp, u32], C.c_int),
@@ -215,6 +219,20 @@ class Graph:
         _check(lib().dyg_graph_create_from_edges(int(n_vertices), len(src), _ptr(src), _ptr(dst),
                                                  _ptr(w), C.byref(opts), C.byref(h)),
                "dyg_graph_create_from_edges")
+        return cls(h.value)
+
+    @classmethod
+    def from_csr(cls, n_vertices: int, row_ptr, col, w, slack_per_row: int = 2,
+                 arena_headroom: float = 0.5, device: int = -1) -> "Graph":
+        """Rows as given (no reverse slots added)."""
+        rp = np.ascontiguousarray(row_ptr, np.uint64)
+        col = _as(col, np.uint32)
+        w = _as(w, np.float32)
+        opts = GraphOpts(int(slack_per_row), 0, float(arena_headroom), int(device), 0)
+        h = C.c_void_p()
+        _check(lib().dyg_graph_create_from_csr(int(n_vertices), _ptr(rp), _ptr(col), _ptr(w),
+                                               C.byref(opts), C.byref(h)),
+               "dyg_graph_create_from_csr")
         return cls(h.value)
 
     def clone(self) -> "Graph":
@@ -380,6 +398,28 @@ def mtx_read_auto(path: str):
         for p in (ps, pd, pw):
             lib().dyg_mtx_free(p)
     return info.as_dict(), src, dst, w
+
+
+def stream_read(path: str, base: int):
+    """Returns (src, dst, w, weighted) of one stream file, ids minus base."""
+    m = C.c_uint64()
+    ps, pd, pw = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    wt = C.c_int32()
+    _check(lib().dyg_stream_read(os.fsencode(path), int(base), C.byref(m), C.byref(ps),
+                                 C.byref(pd), C.byref(pw), C.byref(wt)), "dyg_stream_read")
+    k = m.value
+    try:
+        src = np.ctypeslib.as_array(C.cast(ps, C.POINTER(C.c_uint32)), (max(k, 1),))[:k].copy()
+        dst = np.ctypeslib.as_array(C.cast(pd, C.POINTER(C.c_uint32)), (max(k, 1),))[:k].copy()
+        w = np.ctypeslib.as_array(C.cast(pw, C.POINTER(C.c_float)), (max(k, 1),))[:k].copy()
+    finally:
+        for p in (ps, pd, pw):
+            lib().dyg_mtx_free(p)
+    return src, dst, w, bool(wt.value)
+
+
+def stream_op_from_name(name: str, prev_op: int = 0) -> int:
+    return int(lib().dyg_stream_op_from_name(os.fsencode(name), int(prev_op)))
 
 
 def stream_default_chunk(n_vertices: int) -> int:

@@ -18,6 +18,7 @@ CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libdygrass.so")
 BIN_INCR = os.path.join(PKG, "bin", "incremental_update")
 BIN_DECR = os.path.join(PKG, "bin", "decremental_update")
+BIN_DYN = os.path.join(PKG, "bin", "dynamic_update")
 
 CUDA_SOURCES = ["walk.cu", "graph.cu", "rowops.cu", "pipeline.cu", "capi.cu", "noalloc.cu", "stream.cu"]
 HOST_SOURCES = ["synth.cpp", "mtx_io.cpp"]
@@ -66,7 +67,8 @@ def build_library(force: bool = False) -> str:
 
 def build_tools(force: bool = False) -> None:
     os.makedirs(os.path.dirname(BIN_INCR), exist_ok=True)
-    for target, main in ((BIN_INCR, "cli_incremental.cpp"), (BIN_DECR, "cli_decremental.cpp")):
+    for target, main in ((BIN_INCR, "cli_incremental.cpp"), (BIN_DECR, "cli_decremental.cpp"),
+                         (BIN_DYN, "cli_dynamic.cpp")):
         src = os.path.join(CSRC, main)
         if not os.path.exists(src):
             continue

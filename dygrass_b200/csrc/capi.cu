@@ -282,6 +282,51 @@ dyg_status dyg_graph_create_from_edges(uint32_t n_vertices, uint64_t n_edges, co
     return DYG_OK;
 }
 
+dyg_status dyg_graph_create_from_csr(uint32_t n_vertices, const uint64_t *row_ptr,
+                                     const uint32_t *col, const float *w,
+                                     const dyg_graph_opts *opts, dyg_graph **out) {
+    set_error("");
+    if (!out || !row_ptr) {
+        set_error("NULL argument");
+        return DYG_EINVAL;
+    }
+    *out = nullptr;
+    const uint64_t m = row_ptr[n_vertices];
+    if (m && (!col || !w)) {
+        set_error("NULL argument");
+        return DYG_EINVAL;
+    }
+    if (row_ptr[0] != 0 || m > 0xFFFFFFFFull) {
+        set_error("row_ptr must start at 0 and hold at most 2^32 - 1 slots");
+        return DYG_EINVAL;
+    }
+    for (uint32_t v = 0; v < n_vertices; ++v)
+        if (row_ptr[v + 1] < row_ptr[v]) {
+            set_error("row_ptr must be non-decreasing");
+            return DYG_EINVAL;
+        }
+    DYG_TRY(check_host_ids(col, m, n_vertices, "col"));
+    DYG_TRY(check_host_weights(w, m));
+    dyg_graph_opts o;
+    dyg_graph_opts_default(&o);
+    if (opts) o = *opts;
+    int dev = o.device;
+    if (dev < 0) DYG_CUDA(cudaGetDevice(&dev));
+    DeviceGuard dg(dev);
+    dyg_graph *G = new dyg_graph();
+    G->device = dev;
+    G->slack = o.slack_per_row;
+    G->headroom = o.arena_headroom > 0 ? o.arena_headroom : 0.0;
+    dyg_status rc = graph_alloc_scalars(G);
+    if (rc == DYG_OK) rc = upload_graph(G, n_vertices, row_ptr, col, w);
+    if (rc != DYG_OK) {
+        free_graph(G);
+        return rc;
+    }
+    *out = G;
+    return DYG_OK;
+}
+
 dyg_status dyg_graph_copy_from(dyg_graph *dst, const dyg_graph *src, dyg_stream_t stream) {
     set_error("");
     if (!dst || !src || dst->g.n != src->g.n || dst->device != src->device) {

@@ -439,4 +439,88 @@ dyg_status dyg_mtx_read_auto(const char *path, dyg_mtx_info *info, uint64_t *n_r
     return DYG_OK;
 }
 
+// Restates EdgeStream::autoDetectWeightExist and loadBatchFromFile
+// (dynamic_update/functions.cpp:717-838): the first line decides the weight
+// column (three numbers: weighted, two: not; a '%' line or anything else is
+// an error); then whitespace-separated records "src dst [w]", ids minus
+// `base`, weight 1 without the column.
+dyg_status dyg_stream_read(const char *path, uint32_t base, uint64_t *n_records,
+                           uint32_t **src, uint32_t **dst, float **w, int32_t *weighted) {
+    if (!path || !n_records || !src || !dst || !w) {
+        dyg::set_error("dyg_stream_read: NULL argument");
+        return DYG_EINVAL;
+    }
+    *n_records = 0;
+    *src = *dst = nullptr;
+    *w = nullptr;
+    Mapped f;
+    dyg_status rc = f.open_file(path);
+    if (rc != DYG_OK) return rc;
+    const char *d = f.p;
+    const size_t n = f.n;
+    if (n == 0) {
+        dyg::set_error(std::string(path) + ": cannot read the first line");
+        return DYG_EIO;
+    }
+    if (d[0] == '%') {
+        dyg::set_error(std::string(path) + ": comment lines are not supported in stream files");
+        return DYG_EIO;
+    }
+    const std::string first(d, line_end(d, 0, n));
+    double x[3];
+    const int k = sscanf(first.c_str(), "%lf %lf %lf", &x[0], &x[1], &x[2]);
+    if (k != 2 && k != 3) {
+        dyg::set_error(std::string(path) + ": invalid first line (expected 2 or 3 numbers)");
+        return DYG_EIO;
+    }
+    const bool wt = k == 3;
+    if (weighted) *weighted = wt ? 1 : 0;
+    auto is_sep = [](char c) { return c == ' ' || c == '\n' || c == '\t'; };
+    std::vector<std::string> toks;
+    for (size_t i = 0; i < n;) {
+        while (i < n && is_sep(d[i])) ++i;
+        if (i >= n) break;
+        size_t j = i;
+        while (j < n && !is_sep(d[j])) ++j;
+        toks.emplace_back(d + i, j - i);
+        i = j;
+    }
+    const size_t per = wt ? 3 : 2;
+    const size_t m = toks.size() / per;
+    *src = (uint32_t *)malloc(sizeof(uint32_t) * (m ? m : 1));
+    *dst = (uint32_t *)malloc(sizeof(uint32_t) * (m ? m : 1));
+    *w = (float *)malloc(sizeof(float) * (m ? m : 1));
+    if (!*src || !*dst || !*w) {
+        free(*src); free(*dst); free(*w);
+        *src = *dst = nullptr;
+        *w = nullptr;
+        dyg::set_error("host allocation failed");
+        return DYG_ENOMEM;
+    }
+    for (size_t r = 0; r < m; ++r) {
+        const long a = atol(toks[r * per].c_str()) - (long)base;
+        const long b = atol(toks[r * per + 1].c_str()) - (long)base;
+        if (a < 0 || b < 0) {
+            free(*src); free(*dst); free(*w);
+            *src = *dst = nullptr;
+            *w = nullptr;
+            dyg::set_error(std::string(path) + ": record " + std::to_string(r + 1) +
+                           " has an id below the base");
+            return DYG_EIO;
+        }
+        (*src)[r] = (uint32_t)a;
+        (*dst)[r] = (uint32_t)b;
+        (*w)[r] = wt ? (float)atof(toks[r * per + 2].c_str()) : 1.0f;
+    }
+    *n_records = m;
+    return DYG_OK;
+}
+
+uint32_t dyg_stream_op_from_name(const char *name, uint32_t prev_op) {
+    if (!name) return prev_op;
+    if (strstr(name, "insert") || strstr(name, "inc")) return DYG_STREAM_INSERT;
+    if (strstr(name, "delete") || strstr(name, "dec")) return DYG_STREAM_DELETE;
+    return prev_op;
+}
+
 }  // extern "C"

@@ -6,6 +6,9 @@
  * executables do between reading the .mtx files and writing the result:
  *
  *   dyg_graph_create_from_edges  <- read_graph + gpu_graph ctor + copyToDevice
+ *   dyg_graph_create_from_csr       (and CSRGraph ctor + GPU_Dual_Graph ctor,
+ *                                    dynamic_update/functions.cpp:308-587,
+ *                                    dynamic_update/gpu_graph.cuh:283-333)
  *                                   (random_walk_incremental/functions.cpp:58-239,
  *                                    random_walk_incremental/gpu_graph.cuh:123-162, 205-275;
  *                                    random_walk_decremental/functions.cpp:69-281,
@@ -130,6 +133,14 @@ dyg_status dyg_graph_create_from_edges(uint32_t n_vertices, uint64_t n_edges,
                                        const uint32_t *src, const uint32_t *dst,
                                        const float *w, const dyg_graph_opts *opts,
                                        dyg_graph **out);
+/* A graph from rows as given: row v holds col/w[row_ptr[v] .. row_ptr[v+1]),
+ * in that order; no reverse slots are added.  This is how the mixed
+ * updater's loader fills rows from a full (both-direction) matrix file, each
+ * record filling its source's row only (dynamic_update/functions.cpp:525-562).
+ * Weights must be finite and > 0.  Host pointers only. */
+dyg_status dyg_graph_create_from_csr(uint32_t n_vertices, const uint64_t *row_ptr,
+                                     const uint32_t *col, const float *w,
+                                     const dyg_graph_opts *opts, dyg_graph **out);
 /* Deep copy on the same device (used to restore a snapshot). */
 dyg_status dyg_graph_clone(const dyg_graph *g, dyg_graph **out);
 /* Overwrite dst's rows with src's (same vertex count); stream-ordered. */

@@ -58,6 +58,18 @@ dyg_status dyg_mtx_detect(const char *path, dyg_mtx_info *info);
 dyg_status dyg_mtx_read_auto(const char *path, dyg_mtx_info *info, uint64_t *n_records,
                              uint32_t **src, uint32_t **dst, float **w);
 
+/* One stream file of the mixed updater (EdgeStream::loadBatchFromFile,
+ * dynamic_update/functions.cpp:717-838): its first line decides the weight
+ * column (3 numbers: weighted; 2: not; a '%' line or anything else is
+ * DYG_EIO); records "src dst [w]" with `base` subtracted (the dense graph's
+ * base), weight 1 without the column.  Arrays are malloc'ed. */
+dyg_status dyg_stream_read(const char *path, uint32_t base, uint64_t *n_records,
+                           uint32_t **src, uint32_t **dst, float **w, int32_t *weighted);
+/* Operation of a stream file from its name (functions.cpp:688-692): a name
+ * containing "insert" or "inc" inserts, else one containing "delete" or "dec"
+ * deletes, else the previous file's operation (prev_op). */
+uint32_t dyg_stream_op_from_name(const char *name, uint32_t prev_op);
+
 #ifdef __cplusplus
 }
 #endif

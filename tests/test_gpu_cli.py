@@ -49,3 +49,69 @@ def test_decremental_cli(tmp_path, name):
     lines = (tmp_path / "dataset" / name / "added_edges.mtx").read_text().split("\n")
     got = sorted(tuple(int(x) for x in ln.split()) for ln in lines if ln.strip())
     assert got == sorted(case["expect_added"])
+
+
+def _write_graph(path, n, s, d, w):
+    with open(path, "w") as f:
+        f.write("%%MatrixMarket matrix coordinate real symmetric\n% written by the test\n")
+        f.write(f"{n} {n} {len(s)}\n")
+        for a, b, x in zip(s, d, w):
+            f.write(f"{a + 1} {b + 1} {float(x):.9g}\n")
+
+
+def _graph_lines(g, oracle_graph):
+    rp, col, w = oracle_graph.export()
+    out = []
+    for u in range(len(rp) - 1):
+        for j in range(int(rp[u]), int(rp[u + 1])):
+            if int(col[j]) >= u:
+                out.append((u, int(col[j]), float(w[j])))
+    out.sort(key=lambda t: (t[0], t[1]))
+    lines, last = [], None
+    for u, v, x in out:
+        if (u, v) != last:
+            lines.append(f"{u + 1} {v + 1} {x:g}")
+        last = (u, v)
+    return lines
+
+
+def test_dynamic_update_cli(tmp_path, oracle):
+    """dynamic_update on a folder of insertion and deletion stream files:
+    both output graphs equal the oracle's after the same files."""
+    import dygrass_b200 as dyg
+    from dygrass_b200 import workloads as W
+    wl = W.rmat_mixed(scale=10, n_updates=4000, file_size=700, walkers=64)
+    ds = tmp_path / "dataset" / "rmat10"
+    (ds / "stream_edges" / "sub").mkdir(parents=True)
+    _write_graph(ds / "new_adj_dense.mtx", wl.n, wl.g_src, wl.g_dst, wl.g_w)
+    _write_graph(ds / "new_adj_sparse.mtx", wl.n, wl.h_src, wl.h_dst, wl.h_w)
+    (ds / "stream_edges" / "notes.txt").write_text("not a stream file\n")
+    for i, (op, s, d, w) in enumerate(wl.files):
+        kind = "decremental" if op else "incremental"
+        with open(ds / "stream_edges" / f"stream_{i:04d}_{kind}.mtx", "w") as f:
+            for k in range(len(s)):
+                f.write(f"{s[k] + 1} {d[k] + 1}" + ("\n" if op else f" {float(w[k]):.9g}\n"))
+    cp = subprocess.run([os.path.join(BIN, "dynamic_update"), "rmat10", "50", "128", "128", "64",
+                         "64", "--timestamp=T"], cwd=tmp_path, capture_output=True, text=True,
+                        timeout=300)
+    assert cp.returncode == 0, cp.stdout[-2000:] + cp.stderr
+    assert f"Found {len(wl.files)} stream updates files" in cp.stdout
+
+    info, gs, gd, gw = dyg.mtx_read_auto(str(ds / "new_adj_dense.mtx"))
+    _, hs, hd, hw = dyg.mtx_read_auto(str(ds / "new_adj_sparse.mtx"))
+    assert info["triangular"] and info["has_dimensions"] and info["base"] == 1
+    G, H = oracle.OGraph(wl.n, gs, gd, gw), oracle.OGraph(wl.n, hs, hd, hw)
+    ip = dyg.WalkParams.make(threshold=50.0, walkers=64, max_steps=128)
+    dp = dyg.WalkParams.make(threshold=50.0, walkers=64, max_steps=128)
+    names = sorted(os.listdir(ds / "stream_edges"))
+    uid, op = 0, 0
+    for nm in names:
+        if not (nm.startswith("stream_") and ".mtx" in nm):
+            continue
+        op = dyg.stream_op_from_name(nm, op)
+        s, d, w, _ = dyg.stream_read(str(ds / "stream_edges" / nm), 1)
+        oracle.stream_file(G, H, op, s, d, w if op == 0 else None, dp if op else ip, first_uid=uid)
+        uid += len(s)
+    out = tmp_path / "output" / "rmat10" / "T"
+    assert (out / "adj_dense.mtx").read_text().split("\n")[:-1] == _graph_lines(None, G)
+    assert (out / "adj_sparse.mtx").read_text().split("\n")[:-1] == _graph_lines(None, H)
