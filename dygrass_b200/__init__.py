@@ -48,6 +48,18 @@ class MtxInfo(C.Structure):
         return {k: int(getattr(self, k)) for k, _ in self._fields_}
 
 
+class KappaOpts(C.Structure):
+    """Mirror of dyg_kappa_opts (include/dyg_eval.h)."""
+    _fields_ = [("offset", C.c_double), ("tol", C.c_double), ("max_iter", C.c_uint32),
+                ("pcg_max_iter", C.c_uint32), ("pcg_rtol", C.c_double), ("seed", C.c_uint64)]
+
+
+class KappaResult(C.Structure):
+    """Mirror of dyg_kappa_result (include/dyg_eval.h)."""
+    _fields_ = [("kappa", C.c_double), ("density", C.c_double), ("lanczos_iters", C.c_uint32),
+                ("pcg_iters", C.c_uint32), ("pcg_relres", C.c_double), ("factor_nnz", C.c_uint64)]
+
+
 class DygError(RuntimeError):
     def __init__(self, status: int, what: str, msg: str):
         super().__init__(f"{what}: {STATUS_NAMES.get(status, status)}: {msg}")
@@ -128,6 +140,9 @@ def lib() -> C.CDLL:
         "dyg_stream_read": ([C.c_char_p, u32, C.POINTER(u64), C.POINTER(vp), C.POINTER(vp),
                              C.POINTER(vp), C.POINTER(C.c_int32)], C.c_int),
         "dyg_stream_op_from_name": ([C.c_char_p, u32], u32),
+        "dyg_kappa_opts_default": ([C.POINTER(KappaOpts)], None),
+        "dyg_kappa": ([u32, u64, vp, vp, vp, u64, vp, vp, vp, C.POINTER(KappaOpts),
+                       C.POINTER(KappaResult)], C.c_int),
         "dyg_mtx_read_auto": ([C.c_char_p, C.POINTER(MtxInfo), C.POINTER(u64), C.POINTER(vp),
                                C.POINTER(vp), C.POINTER(vp)], C.c_int),
         "dyg_mtx_write": ([C.c_char_p, C.c_int, u64, vp, vp, vp, u32], C.c_int),
@@ -422,6 +437,36 @@ def stream_op_from_name(name: str, prev_op: int = 0) -> int:
     return int(lib().dyg_stream_op_from_name(os.fsencode(name), int(prev_op)))
 
 
+def kappa(n: int, g_src, g_dst, g_w, h_src, h_dst, h_w, **opts) -> dict:
+    """kappa(L_G, L_H), density and the PCG iteration count (dyg_kappa).
+    Edge lists give each undirected edge once; opts override dyg_kappa_opts."""
+    o = KappaOpts()
+    lib().dyg_kappa_opts_default(C.byref(o))
+    for k, v in opts.items():
+        setattr(o, k, v)
+    gs, gd, gw = (np.ascontiguousarray(a, t) for a, t in
+                  ((g_src, np.uint32), (g_dst, np.uint32), (g_w, np.float32)))
+    hs, hd, hw = (np.ascontiguousarray(a, t) for a, t in
+                  ((h_src, np.uint32), (h_dst, np.uint32), (h_w, np.float32)))
+    r = KappaResult()
+    _check(lib().dyg_kappa(int(n), len(gs), _ptr(gs), _ptr(gd), _ptr(gw), len(hs), _ptr(hs),
+                           _ptr(hd), _ptr(hw), C.byref(o), C.byref(r)), "dyg_kappa")
+    return {k: getattr(r, k) for k, _ in r._fields_}
+
+
+def graph_edges(g: "Graph"):
+    """(src, dst, w) of a device graph, each undirected edge once (u <= v,
+    the weight of u's first slot holding v)."""
+    rp, col, w = g.export()
+    rows = np.repeat(np.arange(len(rp) - 1, dtype=np.uint32), np.diff(rp).astype(np.int64))
+    keep = col >= rows
+    u, v, x = rows[keep], col[keep], w[keep]
+    key = u.astype(np.uint64) << np.uint64(32) | v.astype(np.uint64)
+    _, first = np.unique(key, return_index=True)
+    first.sort()
+    return u[first], v[first], x[first]
+
+
 def stream_default_chunk(n_vertices: int) -> int:
     """Walk-list chunk of the mixed updater: 5% of |V|, at least 10000."""
     return int(lib().dyg_stream_default_chunk(int(n_vertices)))
@@ -472,4 +517,4 @@ def stream_file_into(G: Graph, H: Graph, op: int, src, dst, w, params: WalkParam
 __all__ = ["Graph", "WalkParams", "GraphOpts", "DygError", "incremental_batch",
            "incremental_stream", "decremental_batch", "decremental_stream", "lib", "version",
            "reference_batch_size", "IncrementalResult", "DecrementalResult", "stream_file",
-           "stream_file_into", "stream_default_chunk"]
+           "stream_file_into", "stream_default_chunk", "kappa", "graph_edges"]

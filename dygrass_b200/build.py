@@ -21,7 +21,7 @@ BIN_DECR = os.path.join(PKG, "bin", "decremental_update")
 BIN_DYN = os.path.join(PKG, "bin", "dynamic_update")
 
 CUDA_SOURCES = ["walk.cu", "graph.cu", "rowops.cu", "pipeline.cu", "capi.cu", "noalloc.cu", "stream.cu"]
-HOST_SOURCES = ["synth.cpp", "mtx_io.cpp"]
+HOST_SOURCES = ["synth.cpp", "mtx_io.cpp", "kappa.cpp"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",

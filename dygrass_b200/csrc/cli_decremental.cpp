@@ -13,7 +13,10 @@
 // them out of the file, gpu_graph.cuh:599-601, so its final sparsifier
 // loses them).
 // Options: --dataset-dir=DIR, --max-steps=N, --walkers=N, --seed=S, --batch=B,
-// --fallback-walkers=N, --path-edges-only.
+// --fallback-walkers=N, --path-edges-only, --snapshot-dir=DIR (also write
+// the final G and H there as adj_dense.mtx / adj_sparse.mtx, the format of
+// dyg_graph_save: what the reference's evaluation rebuilds from
+// added_edges.mtx, dyGRASS.jl:516-541).
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -43,6 +46,7 @@ int main(int argc, char **argv) {
     p.heuristic_walkers = 16;
     uint32_t batch = 0;
     bool path_only = false;
+    std::string snapshot;
     for (int i = 2; i < argc; ++i) {
         const char *a = argv[i];
         if (!strncmp(a, "--dataset-dir=", 14)) dir = a + 14;
@@ -52,6 +56,7 @@ int main(int argc, char **argv) {
         else if (!strncmp(a, "--batch=", 8)) batch = (uint32_t)atoi(a + 8);
         else if (!strncmp(a, "--fallback-walkers=", 19)) p.heuristic_walkers = (uint32_t)atoi(a + 19);
         else if (!strcmp(a, "--path-edges-only")) path_only = true;
+        else if (!strncmp(a, "--snapshot-dir=", 15)) snapshot = a + 15;
         else {
             fprintf(stderr, "unknown option %s\n", a);
             return 2;
@@ -117,6 +122,12 @@ int main(int argc, char **argv) {
     s = dyg_mtx_write(output_file.c_str(), 0, ox.size(), ox.data(), oy.data(), nullptr, 1);
     if (s) return fail("writing added_edges.mtx", s);
     printf("Added edges saved to: %s\n", output_file.c_str());
+    if (!snapshot.empty()) {
+        s = dyg_graph_save(G, (snapshot + "/adj_dense.mtx").c_str());
+        if (s) return fail("writing adj_dense.mtx", s);
+        s = dyg_graph_save(H, (snapshot + "/adj_sparse.mtx").c_str());
+        if (s) return fail("writing adj_sparse.mtx", s);
+    }
     dyg_graph_destroy(G);
     dyg_graph_destroy(H);
     dyg_mtx_free(gs); dyg_mtx_free(gd); dyg_mtx_free(gw);

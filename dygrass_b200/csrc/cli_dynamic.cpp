@@ -31,7 +31,6 @@
 #include <algorithm>
 #include <chrono>
 #include <string>
-#include <tuple>
 #include <vector>
 
 #include "dyg.h"
@@ -75,38 +74,6 @@ dyg_status build_graph(const Loaded &L, uint32_t n, dyg_graph **out) {
         w[p] = L.w[i];
     }
     return dyg_graph_create_from_csr(n, rp.data(), col.data(), w.data(), nullptr, out);
-}
-
-// Writes one line per undirected edge {u, v}, u <= v, with the weight of
-// u's first slot holding v.
-dyg_status save_graph(dyg_graph *g, uint32_t n, const std::string &path) {
-    uint64_t slots = 0;
-    dyg_status s = dyg_graph_info(g, nullptr, &slots, nullptr, nullptr);
-    if (s) return s;
-    std::vector<uint64_t> rp((size_t)n + 1);
-    std::vector<uint32_t> col(slots ? slots : 1);
-    std::vector<float> w(slots ? slots : 1);
-    s = dyg_graph_export(g, rp.data(), col.data(), w.data(), slots);
-    if (s) return s;
-    std::vector<std::tuple<uint32_t, uint32_t, float>> e;
-    for (uint32_t u = 0; u < n; ++u)
-        for (uint64_t j = rp[u]; j < rp[u + 1]; ++j)
-            if (col[j] >= u) e.emplace_back(u, col[j], w[j]);
-    std::stable_sort(e.begin(), e.end(), [](const auto &a, const auto &b) {
-        return std::get<0>(a) != std::get<0>(b) ? std::get<0>(a) < std::get<0>(b)
-                                                : std::get<1>(a) < std::get<1>(b);
-    });
-    std::vector<uint32_t> ou, ov;
-    std::vector<float> ow;
-    for (size_t i = 0; i < e.size(); ++i) {
-        if (i && std::get<0>(e[i]) == std::get<0>(e[i - 1]) &&
-            std::get<1>(e[i]) == std::get<1>(e[i - 1]))
-            continue;   // a self-loop holds two slots; an edge is written once
-        ou.push_back(std::get<0>(e[i]));
-        ov.push_back(std::get<1>(e[i]));
-        ow.push_back(std::get<2>(e[i]));
-    }
-    return dyg_mtx_write(path.c_str(), 0, ou.size(), ou.data(), ov.data(), ow.data(), 1);
 }
 
 void mkdirs(const std::string &path) {
@@ -261,9 +228,9 @@ int main(int argc, char **argv) {
     printf("Update time: %.3f milliseconds\n", total_ms);
     const std::string out = output + "/" + name + "/" + stamp;
     mkdirs(out);
-    s = save_graph(G, n, out + "/adj_dense.mtx");
+    s = dyg_graph_save(G, (out + "/adj_dense.mtx").c_str());
     if (s) return fail("writing adj_dense.mtx", s);
-    s = save_graph(H, n, out + "/adj_sparse.mtx");
+    s = dyg_graph_save(H, (out + "/adj_sparse.mtx").c_str());
     if (s) return fail("writing adj_sparse.mtx", s);
     printf("Results saved to: %s\n", out.c_str());
     dyg_graph_destroy(G);

@@ -523,4 +523,45 @@ uint32_t dyg_stream_op_from_name(const char *name, uint32_t prev_op) {
     return prev_op;
 }
 
+// Snapshot of a device graph in the mixed updater's save format
+// (GPU_Dual_Graph::save_result, dynamic_update/gpu_graph.cuh:725-763): one
+// line "u+1 v+1 w" per undirected edge, here sorted by (u, v) with u <= v and
+// the weight of u's first slot holding v (the reference writes its hash map
+// in iteration order).
+dyg_status dyg_graph_save(dyg_graph *g, const char *path) {
+    if (!g || !path) {
+        dyg::set_error("dyg_graph_save: NULL argument");
+        return DYG_EINVAL;
+    }
+    uint32_t n = 0;
+    uint64_t slots = 0;
+    dyg_status s = dyg_graph_info(g, &n, &slots, nullptr, nullptr);
+    if (s) return s;
+    std::vector<uint64_t> rp((size_t)n + 1);
+    std::vector<uint32_t> col(slots ? slots : 1);
+    std::vector<float> w(slots ? slots : 1);
+    s = dyg_graph_export(g, rp.data(), col.data(), w.data(), slots);
+    if (s) return s;
+    struct E {
+        uint32_t u, v;
+        float w;
+    };
+    std::vector<E> e;
+    for (uint32_t u = 0; u < n; ++u)
+        for (uint64_t j = rp[u]; j < rp[u + 1]; ++j)
+            if (col[j] >= u) e.push_back({u, col[j], w[j]});
+    std::stable_sort(e.begin(), e.end(), [](const E &a, const E &b) {
+        return a.u != b.u ? a.u < b.u : a.v < b.v;
+    });
+    std::vector<uint32_t> ou, ov;
+    std::vector<float> ow;
+    for (size_t i = 0; i < e.size(); ++i) {
+        if (i && e[i].u == e[i - 1].u && e[i].v == e[i - 1].v) continue;   // self-loop: 2 slots
+        ou.push_back(e[i].u);
+        ov.push_back(e[i].v);
+        ow.push_back(e[i].w);
+    }
+    return dyg_mtx_write(path, 0, ou.size(), ou.data(), ov.data(), ow.data(), 1);
+}
+
 }  // extern "C"

@@ -70,6 +70,13 @@ dyg_status dyg_stream_read(const char *path, uint32_t base, uint64_t *n_records,
  * deletes, else the previous file's operation (prev_op). */
 uint32_t dyg_stream_op_from_name(const char *name, uint32_t prev_op);
 
+/* Writes a device graph as the mixed updater saves adj_dense.mtx /
+ * adj_sparse.mtx (GPU_Dual_Graph::save_result,
+ * dynamic_update/gpu_graph.cuh:725-763): one line "u+1 v+1 w" per undirected
+ * edge, sorted by (u, v), u <= v, with the weight of u's first slot holding
+ * v (the reference's order is its hash map's). */
+dyg_status dyg_graph_save(dyg_graph *g, const char *path);
+
 #ifdef __cplusplus
 }
 #endif

@@ -115,3 +115,40 @@ def test_dynamic_update_cli(tmp_path, oracle):
     out = tmp_path / "output" / "rmat10" / "T"
     assert (out / "adj_dense.mtx").read_text().split("\n")[:-1] == _graph_lines(None, G)
     assert (out / "adj_sparse.mtx").read_text().split("\n")[:-1] == _graph_lines(None, H)
+
+
+def test_decremental_snapshot_matches_reconstruction(tmp_path):
+    """The final H that the reference's evaluation rebuilds from the files
+    (updated graphs minus del.mtx plus added_edges.mtx, dyGRASS.jl:478-541)
+    is the device H that decremental_update snapshots."""
+    from dygrass_b200 import workloads as W
+    from dygrass_b200.evaluate import _read, reconstruct_final
+    wl = W.mesh_3d(10, inserts=400)
+    gs = np.concatenate([wl.g_src, wl.ins_src])
+    gd = np.concatenate([wl.g_dst, wl.ins_dst])
+    gw = np.concatenate([wl.g_w, wl.ins_w])
+    ds = tmp_path / "dataset" / "mesh10"
+    ds.mkdir(parents=True)
+    for name, (s, d, w) in (("updated_dense.mtx", (gs, gd, gw)),
+                            ("updated_adj_sparse.mtx", (wl.h_src, wl.h_dst, wl.h_w))):
+        (ds / name).write_text("".join(f"{a + 1} {b + 1} {float(x):.9g}\n" for a, b, x in zip(s, d, w)))
+    (ds / "del.mtx").write_text("".join(f"{a + 1} {b + 1}\n" for a, b in zip(wl.del_src, wl.del_dst)))
+    snap = tmp_path / "snap"
+    snap.mkdir()
+    run = tmp_path / "run"
+    run.mkdir()
+    cp = subprocess.run([os.path.join(BIN, "decremental_update"), "mesh10", f"--snapshot-dir={snap}"],
+                        cwd=run, capture_output=True, text=True, timeout=300)
+    assert cp.returncode == 0, cp.stderr
+    g = _read(str(ds / "updated_dense.mtx"), 1, True)
+    h = _read(str(ds / "updated_adj_sparse.mtx"), 1, True)
+    dl = _read(str(ds / "del.mtx"), 1, False)
+    ad = _read(str(ds / "added_edges.mtx"), 1, False)
+    assert len(ad[0]) > 0
+    (fgs, fgd, fgw), (fhs, fhd, fhw) = reconstruct_final(g, h, dl, ad)
+
+    def lines(s, d, w):
+        return sorted(f"{min(a, b) + 1} {max(a, b) + 1} {float(x):g}"
+                      for a, b, x in zip(s.tolist(), d.tolist(), w.tolist()))
+    assert sorted((snap / "adj_sparse.mtx").read_text().split("\n")[:-1]) == lines(fhs, fhd, fhw)
+    assert sorted((snap / "adj_dense.mtx").read_text().split("\n")[:-1]) == lines(fgs, fgd, fgw)
