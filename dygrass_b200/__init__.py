@@ -141,6 +141,14 @@ def lib() -> C.CDLL:
                              C.POINTER(vp), C.POINTER(C.c_int32)], C.c_int),
         "dyg_stream_op_from_name": ([C.c_char_p, u32], u32),
         "dyg_kappa_opts_default": ([C.POINTER(KappaOpts)], None),
+        "dyg_synth_rgg": ([u32, C.c_double, u32, u64, C.POINTER(u32), C.POINTER(vp), C.POINTER(vp),
+                           C.POINTER(vp), C.POINTER(u32), C.POINTER(vp), C.POINTER(vp),
+                           C.POINTER(vp)], u64),
+        "dyg_incremental_batch_ids": ([vp, vp, vp, vp, vp, vp, u32, C.POINTER(WalkParams), vp, vp,
+                                       vp, vp], C.c_int),
+        "dyg_decremental_batch_ids": ([vp, vp, vp, vp, vp, u32, C.POINTER(WalkParams), vp, vp, vp,
+                                       vp, vp, u64, C.POINTER(u64), vp], C.c_int),
+        "dyg_tune_set": ([u32, u32], None),
         "dyg_kappa": ([u32, u64, vp, vp, vp, u64, vp, vp, vp, C.POINTER(KappaOpts),
                        C.POINTER(KappaResult)], C.c_int),
         "dyg_mtx_read_auto": ([C.c_char_p, C.POINTER(MtxInfo), C.POINTER(u64), C.POINTER(vp),
@@ -465,6 +473,51 @@ def graph_edges(g: "Graph"):
     _, first = np.unique(key, return_index=True)
     first.sort()
     return u[first], v[first], x[first]
+
+
+def incremental_batch_ids(H: Graph, src, dst, w, update_ids, params: WalkParams,
+                          G: Graph | None = None, stream: int | None = None,
+                          out: IncrementalResult | None = None) -> IncrementalResult:
+    """One incremental batch with an update id per edge (dyg_incremental_batch_ids)."""
+    src, dst, w = _as(src, np.uint32), _as(dst, np.uint32), _as(w, np.float32)
+    ids = _as(update_ids, np.uint64)
+    n = len(src)
+    if out is None:
+        out = IncrementalResult(np.empty(n, np.int32), np.empty(n, np.float32),
+                                np.empty(n, np.uint8))
+    _check(lib().dyg_incremental_batch_ids(H.handle, G.handle if G else None, _ptr(src), _ptr(dst),
+                                           _ptr(w), _ptr(ids), n, C.byref(params),
+                                           _ptr(out.found_at), _ptr(out.conductance),
+                                           _ptr(out.accepted), stream),
+           "dyg_incremental_batch_ids")
+    return out
+
+
+def decremental_batch_ids(G: Graph, H: Graph, src, dst, update_ids, params: WalkParams,
+                          stream: int | None = None, rec_cap: int | None = None) -> DecrementalResult:
+    """One decremental batch with an update id per edge (dyg_decremental_batch_ids)."""
+    src, dst = _as(src, np.uint32), _as(dst, np.uint32)
+    ids = _as(update_ids, np.uint64)
+    n = len(src)
+    if rec_cap is None:
+        rec_cap = n * (params.max_steps + 4 * params.heuristic_walkers) + 16
+    st = np.empty(n, np.int32)
+    cd = np.empty(n, np.float32)
+    rx = np.empty(max(rec_cap, 1), np.uint32)
+    ry = np.empty(max(rec_cap, 1), np.uint32)
+    rk = np.empty(max(rec_cap, 1), np.uint8)
+    nrec = C.c_uint64()
+    _check(lib().dyg_decremental_batch_ids(G.handle, H.handle, _ptr(src), _ptr(dst), _ptr(ids), n,
+                                           C.byref(params), _ptr(st), _ptr(cd), _ptr(rx), _ptr(ry),
+                                           _ptr(rk), rec_cap, C.byref(nrec), stream),
+           "dyg_decremental_batch_ids")
+    k = nrec.value
+    return DecrementalResult(st, cd, rx[:k].copy(), ry[:k].copy(), rk[:k].copy())
+
+
+def tune_set(walk_chunk: int = 0, blocks_per_sm: int = 0) -> None:
+    """Walk-kernel launch shape for this process (results do not depend on it)."""
+    lib().dyg_tune_set(int(walk_chunk), int(blocks_per_sm))
 
 
 def stream_default_chunk(n_vertices: int) -> int:

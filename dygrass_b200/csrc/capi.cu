@@ -170,7 +170,7 @@ void free_graph(dyg_graph *G) {
                    &ws.htab_v, &ws.nop, &ws.cub_tmp, &ws.s_src, &ws.s_dst, &ws.s_w, &ws.s_o1,
                    &ws.s_o2, &ws.s_o3, &ws.rx2, &ws.ry2, &ws.rk2, &ws.rank, &ws.lneed, &ws.dtmp,
                    &ws.rowcnt, &ws.rowtmp, &ws.tmask, &ws.del_hx, &ws.del_hy, &ws.nopos,
-                   &ws.st_key, &ws.st_val, &ws.st_pos, &ws.st_wapp, &ws.big, &ws.scalars,
+                   &ws.st_key, &ws.st_val, &ws.st_pos, &ws.st_wapp, &ws.big, &ws.s_uid, &ws.scalars,
                    &ws.counts};
     for (Buf *b : bufs) free_buf(*b);
     if (ws.host_scalars) cudaFreeHost(ws.host_scalars);
@@ -522,7 +522,7 @@ dyg_status dyg_graph_counters(const dyg_graph *g, uint64_t *walker_moves, uint64
 
 static dyg_status incremental_common(dyg_graph *H, dyg_graph *G, const uint32_t *src,
                                      const uint32_t *dst, const float *w, uint32_t n,
-                                     uint32_t batch_size, uint64_t uid_base,
+                                     uint32_t batch_size, uint64_t uid_base, const uint64_t *uids,
                                      const dyg_walk_params *p, int32_t *found_at,
                                      float *conductance, uint8_t *accepted, dyg_stream_t stream) {
     set_error("");
@@ -547,6 +547,8 @@ static dyg_status incremental_common(dyg_graph *H, dyg_graph *G, const uint32_t 
     DYG_TRY(stage_in(ws.s_src, src, n, st, &d_src));
     DYG_TRY(stage_in(ws.s_dst, dst, n, st, &d_dst));
     DYG_TRY(stage_in(ws.s_w, w, n, st, &d_w));
+    const uint64_t *d_uid = nullptr;
+    DYG_TRY(stage_in(ws.s_uid, uids, n, st, &d_uid));
     // device outputs are written in place; host outputs go through staging
     int32_t *o_found = found_at && on_device(found_at) ? found_at : nullptr;
     float *o_cond = conductance && on_device(conductance) ? conductance : nullptr;
@@ -564,7 +566,8 @@ static dyg_status incremental_common(dyg_graph *H, dyg_graph *G, const uint32_t 
         o_acc = ptr<uint8_t>(ws.s_o3);
     }
     const uint32_t B = batch_size ? batch_size : dyg_reference_batch_size(n);
-    DYG_TRY(incremental_run(H, G, d_src, d_dst, d_w, n, B, uid_base, *p, o_found, o_cond, o_acc,
+    DYG_TRY(incremental_run(H, G, d_src, d_dst, d_w, n, B, uid_base,
+                            (const unsigned long long *)d_uid, *p, o_found, o_cond, o_acc,
                             st));
     if (H->ws.host_scalars[S_ERR]) DYG_TRY(check_device_errors(H, st));
     bool host_out = false;
@@ -580,8 +583,8 @@ dyg_status dyg_incremental_batch(dyg_graph *H, dyg_graph *G, const uint32_t *src
                                  uint64_t first_update_id, const dyg_walk_params *p,
                                  int32_t *found_at, float *conductance, uint8_t *accepted,
                                  dyg_stream_t stream) {
-    return incremental_common(H, G, src, dst, w, n, n ? n : 1, first_update_id, p, found_at,
-                              conductance, accepted, stream);
+    return incremental_common(H, G, src, dst, w, n, n ? n : 1, first_update_id, nullptr, p,
+                              found_at, conductance, accepted, stream);
 }
 
 dyg_status dyg_incremental_stream(dyg_graph *H, dyg_graph *G, const uint32_t *src,
@@ -589,13 +592,14 @@ dyg_status dyg_incremental_stream(dyg_graph *H, dyg_graph *G, const uint32_t *sr
                                   uint32_t batch_size, const dyg_walk_params *p,
                                   int32_t *found_at, float *conductance, uint8_t *accepted,
                                   dyg_stream_t stream) {
-    return incremental_common(H, G, src, dst, w, n, batch_size, 0, p, found_at, conductance,
-                              accepted, stream);
+    return incremental_common(H, G, src, dst, w, n, batch_size, 0, nullptr, p, found_at,
+                              conductance, accepted, stream);
 }
 
 static dyg_status decremental_common(dyg_graph *G, dyg_graph *H, const uint32_t *src,
                                      const uint32_t *dst, uint32_t n, uint32_t batch_size,
-                                     uint64_t uid_base, const dyg_walk_params *p, int32_t *status,
+                                     uint64_t uid_base, const uint64_t *uids,
+                                     const dyg_walk_params *p, int32_t *status,
                                      float *conductance, uint32_t *rec_src, uint32_t *rec_dst,
                                      uint8_t *rec_kind, uint64_t rec_cap, uint64_t *n_rec,
                                      dyg_stream_t stream) {
@@ -619,6 +623,8 @@ static dyg_status decremental_common(dyg_graph *G, dyg_graph *H, const uint32_t 
     const uint32_t *d_src, *d_dst;
     DYG_TRY(stage_in(ws.s_src, src, n, st, &d_src));
     DYG_TRY(stage_in(ws.s_dst, dst, n, st, &d_dst));
+    const uint64_t *d_uid = nullptr;
+    DYG_TRY(stage_in(ws.s_uid, uids, n, st, &d_uid));
     int32_t *o_st = status && on_device(status) ? status : nullptr;
     float *o_cd = conductance && on_device(conductance) ? conductance : nullptr;
     if (!o_st) {
@@ -631,7 +637,8 @@ static dyg_status decremental_common(dyg_graph *G, dyg_graph *H, const uint32_t 
     }
     const uint32_t B = batch_size ? batch_size : dyg_reference_batch_size(n);
     uint64_t total = 0;
-    DYG_TRY(decremental_run(G, H, d_src, d_dst, n, B, uid_base, *p, o_st, o_cd, &total, st));
+    DYG_TRY(decremental_run(G, H, d_src, d_dst, n, B, uid_base, (const unsigned long long *)d_uid,
+                            *p, o_st, o_cd, &total, st));
     if (G->ws.host_scalars[S_ERR]) DYG_TRY(check_device_errors(G, st));
     bool host_out = false;
     if (status && o_st != status) DYG_TRY(copy_out(status, (const int32_t *)o_st, n, st, &host_out));
@@ -654,8 +661,8 @@ dyg_status dyg_decremental_batch(dyg_graph *G, dyg_graph *H, const uint32_t *src
                                  const dyg_walk_params *p, int32_t *status, float *conductance,
                                  uint32_t *rec_src, uint32_t *rec_dst, uint8_t *rec_kind,
                                  uint64_t rec_cap, uint64_t *n_rec, dyg_stream_t stream) {
-    return decremental_common(G, H, src, dst, n, n ? n : 1, first_update_id, p, status, conductance,
-                              rec_src, rec_dst, rec_kind, rec_cap, n_rec, stream);
+    return decremental_common(G, H, src, dst, n, n ? n : 1, first_update_id, nullptr, p, status,
+                              conductance, rec_src, rec_dst, rec_kind, rec_cap, n_rec, stream);
 }
 
 dyg_status dyg_decremental_stream(dyg_graph *G, dyg_graph *H, const uint32_t *src,
@@ -663,8 +670,35 @@ dyg_status dyg_decremental_stream(dyg_graph *G, dyg_graph *H, const uint32_t *sr
                                   const dyg_walk_params *p, int32_t *status, float *conductance,
                                   uint32_t *rec_src, uint32_t *rec_dst, uint8_t *rec_kind,
                                   uint64_t rec_cap, uint64_t *n_rec, dyg_stream_t stream) {
-    return decremental_common(G, H, src, dst, n, batch_size, 0, p, status, conductance, rec_src,
-                              rec_dst, rec_kind, rec_cap, n_rec, stream);
+    return decremental_common(G, H, src, dst, n, batch_size, 0, nullptr, p, status, conductance,
+                              rec_src, rec_dst, rec_kind, rec_cap, n_rec, stream);
+}
+
+dyg_status dyg_incremental_batch_ids(dyg_graph *H, dyg_graph *G, const uint32_t *src,
+                                     const uint32_t *dst, const float *w,
+                                     const uint64_t *update_ids, uint32_t n,
+                                     const dyg_walk_params *p, int32_t *found_at,
+                                     float *conductance, uint8_t *accepted, dyg_stream_t stream) {
+    if (n && !update_ids) {
+        set_error("NULL update_ids");
+        return DYG_EINVAL;
+    }
+    return incremental_common(H, G, src, dst, w, n, n ? n : 1, 0, update_ids, p, found_at,
+                              conductance, accepted, stream);
+}
+
+dyg_status dyg_decremental_batch_ids(dyg_graph *G, dyg_graph *H, const uint32_t *src,
+                                     const uint32_t *dst, const uint64_t *update_ids, uint32_t n,
+                                     const dyg_walk_params *p, int32_t *status,
+                                     float *conductance, uint32_t *rec_src, uint32_t *rec_dst,
+                                     uint8_t *rec_kind, uint64_t rec_cap, uint64_t *n_rec,
+                                     dyg_stream_t stream) {
+    if (n && !update_ids) {
+        set_error("NULL update_ids");
+        return DYG_EINVAL;
+    }
+    return decremental_common(G, H, src, dst, n, n ? n : 1, 0, update_ids, p, status, conductance,
+                              rec_src, rec_dst, rec_kind, rec_cap, n_rec, stream);
 }
 
 uint32_t dyg_stream_default_chunk(uint32_t n_vertices) {

@@ -163,6 +163,7 @@ struct Workspace {
     Buf st_pos;                               // stream file: uint4 slot positions in G and H
     Buf st_wapp;                              // stream file: G weight of each new edge
     Buf big;                                  // uint4 per long-row item (block-cooperative pass)
+    Buf s_uid;                                // staged per-edge update ids
     Buf scalars;                              // u64 scalars (see Scalar)
     Buf counts;                               // u32 counts (see Count)
     unsigned long long *host_scalars = nullptr;   // pinned mirror
@@ -282,16 +283,19 @@ dyg_status launch_fallback_walks(dyg_graph *G, const unsigned long long *halt,
                                  cudaStream_t st);
 
 // --- pipeline.cu
+// uids (device, may be null): per-edge update ids instead of uid_base + e.
 dyg_status incremental_run(dyg_graph *H, dyg_graph *G, const uint32_t *src, const uint32_t *dst,
                            const float *w, uint32_t n, uint32_t B, uint64_t uid_base,
-                           const dyg_walk_params &p, int32_t *found, float *cond, uint8_t *acc,
+                           const unsigned long long *uids, const dyg_walk_params &p, int32_t *found, float *cond, uint8_t *acc,
                            cudaStream_t st);
 dyg_status decremental_run(dyg_graph *G, dyg_graph *H, const uint32_t *src, const uint32_t *dst,
-                           uint32_t n, uint32_t B, uint64_t uid_base, const dyg_walk_params &p,
+                           uint32_t n, uint32_t B, uint64_t uid_base,
+                           const unsigned long long *uids, const dyg_walk_params &p,
                            int32_t *status, float *cond, uint64_t *n_rec, cudaStream_t st);
 
 dyg_status decr_delete_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src,
-                               const uint32_t *dst, uint32_t n, uint64_t uid0, bool file_orient,
+                               const uint32_t *dst, uint32_t n, uint64_t uid0,
+                               const unsigned long long *uids, bool file_orient,
                                unsigned long long *halt, int32_t *status, float *cond,
                                cudaStream_t st);
 dyg_status decr_walk_enqueue(dyg_graph *G, dyg_graph *H, uint32_t f0, uint32_t nf,

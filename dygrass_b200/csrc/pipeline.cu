@@ -120,8 +120,9 @@ __global__ void k_del_filter(const unsigned long long *halt, const uint8_t *fG, 
 __global__ void k_del_compact(const unsigned long long *halt, const uint32_t *hx,
                               const uint32_t *hy, const uint32_t *osrc, const uint32_t *odst,
                               uint32_t n, const uint32_t *flags, const uint32_t *pos,
-                              unsigned long long uid0, uint32_t *f_src, uint32_t *f_dst,
-                              unsigned long long *f_uid, uint32_t *f_idx, uint32_t *count) {
+                              unsigned long long uid0, const unsigned long long *uids,
+                              uint32_t *f_src, uint32_t *f_dst, unsigned long long *f_uid,
+                              uint32_t *f_idx, uint32_t *count) {
     if (HALTED(halt)) return;
     const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n) return;
@@ -130,7 +131,7 @@ __global__ void k_del_compact(const unsigned long long *halt, const uint32_t *hx
     const uint32_t f = pos[e];
     f_src[f] = osrc ? osrc[e] : hx[2 * e];
     f_dst[f] = odst ? odst[e] : hy[2 * e];
-    f_uid[f] = uid0 + e;
+    f_uid[f] = uids ? uids[e] : uid0 + e;
     f_idx[f] = e;
 }
 
@@ -430,7 +431,8 @@ dyg_status grow_keep(Buf &b, size_t bytes, size_t used, cudaStream_t st) {
 // Enqueues incremental batch `batch` (edges src/dst/w[0, n), update ids
 // uid0 + e).  Outputs go to found/cond/acc (device, may be null).
 dyg_status incr_enqueue(dyg_graph *H, dyg_graph *G, const uint32_t *src, const uint32_t *dst,
-                        const float *w, uint32_t n, uint64_t uid0, const dyg_walk_params &p,
+                        const float *w, uint32_t n, uint64_t uid0,
+                        const unsigned long long *uids, const dyg_walk_params &p,
                         unsigned long long *halt, uint32_t batch, int32_t *found, float *cond,
                         uint8_t *acc, cudaStream_t st) {
     Workspace &ws = H->ws;
@@ -443,7 +445,7 @@ dyg_status incr_enqueue(dyg_graph *H, dyg_graph *G, const uint32_t *src, const u
     unsigned long long *keys = ptr<unsigned long long>(ws.keys);
     DYG_CUDA(cudaMemsetAsync(keys, 0, sizeof(unsigned long long) * n, st));
     DYG_CUDA(cudaMemsetAsync(ws.hx.p, 0xFF, sizeof(uint32_t) * (size_t)n * 2, st));
-    WalkJob job{halt, src, dst, w, nullptr, (unsigned long long)uid0, nullptr, n, kDomainIncr};
+    WalkJob job{halt, src, dst, w, uids, (unsigned long long)uid0, nullptr, n, kDomainIncr};
     DYG_TRY(launch_walk(H, job, p, true, keys, st));
     k_incr_decode<<<blocks(n, 256), 256, 0, st>>>(halt, keys, n, found, cond, acc,
                                                    ptr<uint32_t>(ws.flags));
@@ -479,7 +481,8 @@ dyg_status incr_enqueue(dyg_graph *H, dyg_graph *G, const uint32_t *src, const u
 // file_orient, src -> dst (dynamic_update/gpu_graph.cuh:874-875).
 // status/cond (device, length n) get the per-deletion codes.
 dyg_status decr_delete_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src,
-                               const uint32_t *dst, uint32_t n, uint64_t uid0, bool file_orient,
+                               const uint32_t *dst, uint32_t n, uint64_t uid0,
+                               const unsigned long long *uids, bool file_orient,
                                unsigned long long *halt, int32_t *status, float *cond,
                                cudaStream_t st) {
     Workspace &ws = G->ws;
@@ -508,7 +511,7 @@ dyg_status decr_delete_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src,
     DYG_TRY(exclusive_scan_u32(ws, ptr<uint32_t>(ws.flags), ptr<uint32_t>(ws.pos), n, st));
     k_del_compact<<<blocks(n, 256), 256, 0, st>>>(
         halt, hx, hy, file_orient ? src : nullptr, file_orient ? dst : nullptr, n,
-        ptr<uint32_t>(ws.flags), ptr<uint32_t>(ws.pos), uid0,
+        ptr<uint32_t>(ws.flags), ptr<uint32_t>(ws.pos), uid0, uids,
         ptr<uint32_t>(ws.f_src), ptr<uint32_t>(ws.f_dst), ptr<unsigned long long>(ws.f_uid),
         ptr<uint32_t>(ws.f_idx), counts + C_FILTERED);
     count_launch();
@@ -598,11 +601,12 @@ dyg_status decr_walk_enqueue(dyg_graph *G, dyg_graph *H, uint32_t f0, uint32_t n
 // Decremental batch `batch` of the standalone updater: deletion stage, then
 // walks over the batch's whole walk list.
 dyg_status decr_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src, const uint32_t *dst,
-                        uint32_t n, uint64_t uid0, const dyg_walk_params &p,
+                        uint32_t n, uint64_t uid0, const unsigned long long *uids,
+                        const dyg_walk_params &p,
                         unsigned long long *halt, uint32_t batch, uint32_t phase0,
                         int32_t *status, float *cond, cudaStream_t st) {
     if (phase0 <= 0)
-        DYG_TRY(decr_delete_enqueue(G, H, src, dst, n, uid0, false, halt, status, cond, st));
+        DYG_TRY(decr_delete_enqueue(G, H, src, dst, n, uid0, uids, false, halt, status, cond, st));
     return decr_walk_enqueue(G, H, 0, n, ptr<uint32_t>(G->ws.counts) + C_FILTERED, p, halt, batch,
                              phase0, status, cond, st);
 }
@@ -635,7 +639,7 @@ dyg_status grow_for_halt(dyg_graph *A, dyg_graph *B, cudaStream_t st) {
 
 dyg_status incremental_run(dyg_graph *H, dyg_graph *G, const uint32_t *src, const uint32_t *dst,
                            const float *w, uint32_t n, uint32_t B, uint64_t uid_base,
-                           const dyg_walk_params &p, int32_t *found, float *cond, uint8_t *acc,
+                           const unsigned long long *uids, const dyg_walk_params &p, int32_t *found, float *cond, uint8_t *acc,
                            cudaStream_t st) {
     unsigned long long *halt = ptr<unsigned long long>(H->ws.scalars) + S_HALT;
     DYG_TRY(clear_halt(H, st));
@@ -643,7 +647,8 @@ dyg_status incremental_run(dyg_graph *H, dyg_graph *G, const uint32_t *src, cons
     for (int round = 0; round < 64; ++round) {
         for (uint32_t b = b_start; (uint64_t)b * B < n; ++b) {
             const uint32_t b0 = b * B, nb = (n - b0 < B) ? n - b0 : B;
-            DYG_TRY(incr_enqueue(H, G, src + b0, dst + b0, w + b0, nb, uid_base + b0, p, halt, b,
+            DYG_TRY(incr_enqueue(H, G, src + b0, dst + b0, w + b0, nb, uid_base + b0,
+                                 uids ? uids + b0 : nullptr, p, halt, b,
                                  found ? found + b0 : nullptr, cond ? cond + b0 : nullptr,
                                  acc ? acc + b0 : nullptr, st));
         }
@@ -660,7 +665,8 @@ dyg_status incremental_run(dyg_graph *H, dyg_graph *G, const uint32_t *src, cons
 }
 
 dyg_status decremental_run(dyg_graph *G, dyg_graph *H, const uint32_t *src, const uint32_t *dst,
-                           uint32_t n, uint32_t B, uint64_t uid_base, const dyg_walk_params &p,
+                           uint32_t n, uint32_t B, uint64_t uid_base,
+                           const unsigned long long *uids, const dyg_walk_params &p,
                            int32_t *status, float *cond, uint64_t *n_rec, cudaStream_t st) {
     Workspace &ws = G->ws;
     unsigned long long *sc = ptr<unsigned long long>(ws.scalars);
@@ -680,7 +686,8 @@ dyg_status decremental_run(dyg_graph *G, dyg_graph *H, const uint32_t *src, cons
     for (int round = 0; round < 64; ++round) {
         for (uint32_t b = b_start; (uint64_t)b * B < n; ++b) {
             const uint32_t b0 = b * B, nb = (n - b0 < B) ? n - b0 : B;
-            DYG_TRY(decr_enqueue(G, H, src + b0, dst + b0, nb, uid_base + b0, p, halt, b,
+            DYG_TRY(decr_enqueue(G, H, src + b0, dst + b0, nb, uid_base + b0,
+                                 uids ? uids + b0 : nullptr, p, halt, b,
                                  b == b_start ? ph_start : 0, status + b0, cond + b0, st));
         }
         DYG_TRY(read_scalars2(G, H, st));

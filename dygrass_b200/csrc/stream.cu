@@ -462,7 +462,7 @@ dyg_status delete_file_run(dyg_graph *G, dyg_graph *H, const uint32_t *src, cons
     unsigned long long init[2] = {0ull, cap};   // S_RECCNT, S_RECCAP
     DYG_CUDA(cudaMemcpyAsync(sc + S_RECCNT, init, sizeof(init), cudaMemcpyHostToDevice, st));
     DYG_TRY(clear_halt(G, st));
-    DYG_TRY(decr_delete_enqueue(G, H, src, dst, n, uid0, true, halt, status, cond, st));
+    DYG_TRY(decr_delete_enqueue(G, H, src, dst, n, uid0, nullptr, true, halt, status, cond, st));
     const uint32_t nchunks = (uint32_t)(((uint64_t)n + chunk - 1) / chunk);
     uint32_t c_start = 0, ph_start = 0;
     for (int round = 0; round < 64; ++round) {

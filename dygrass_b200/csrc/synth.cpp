@@ -2,6 +2,7 @@
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
+#include <string.h>
 
 #include <algorithm>
 #include <numeric>
@@ -291,6 +292,111 @@ uint64_t dyg_synth_rmat_stream(uint32_t scale, double a, double b, double c,
         }
     }
     return nfiles;
+}
+
+uint64_t dyg_synth_rgg(uint32_t n, double avg_deg, uint32_t n_ins, uint64_t seed,
+                       uint32_t *n_out, uint32_t **src, uint32_t **dst, float **w,
+                       uint32_t *n_ins_out, uint32_t **isrc, uint32_t **idst, float **iw) {
+    SplitMix r(seed);
+    std::vector<double> px(n), py(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        px[i] = r.unit();
+        py[i] = r.unit();
+    }
+    const double rad = sqrt(avg_deg / (3.141592653589793 * (double)(n ? n : 1)));
+    const uint32_t gdim = std::max<uint32_t>(1, (uint32_t)(1.0 / rad));
+    auto cell = [&](double x) { return std::min<uint32_t>(gdim - 1, (uint32_t)(x * gdim)); };
+    std::vector<std::vector<uint32_t>> grid((size_t)gdim * gdim);
+    for (uint32_t i = 0; i < n; ++i) grid[(size_t)cell(py[i]) * gdim + cell(px[i])].push_back(i);
+    // cells are at least rad wide, so neighbours lie in the 3x3 block
+    std::vector<std::pair<uint32_t, uint32_t>> e;
+    for (uint32_t i = 0; i < n; ++i) {
+        const int cx = (int)cell(px[i]), cy = (int)cell(py[i]);
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx) {
+                const int x = cx + dx, y = cy + dy;
+                if (x < 0 || y < 0 || x >= (int)gdim || y >= (int)gdim) continue;
+                for (uint32_t j : grid[(size_t)y * gdim + x]) {
+                    if (j <= i) continue;
+                    const double d = hypot(px[i] - px[j], py[i] - py[j]);
+                    if (d < rad && d > 0) e.emplace_back(i, j);
+                }
+            }
+    }
+    std::sort(e.begin(), e.end());
+    DSU dsu(n);
+    for (auto &p : e) dsu.unite(p.first, p.second);
+    std::vector<uint32_t> size(n, 0);
+    for (uint32_t i = 0; i < n; ++i) size[dsu.find(i)]++;
+    uint32_t best = 0;
+    for (uint32_t i = 0; i < n; ++i)
+        if (size[i] > size[best]) best = i;
+    std::vector<uint32_t> map(n, 0xFFFFFFFFu);
+    uint32_t nn = 0;
+    for (uint32_t i = 0; i < n; ++i)
+        if (dsu.find(i) == best) map[i] = nn++;
+    std::vector<uint32_t> vs, vd;
+    std::vector<float> vw;
+    std::unordered_set<uint64_t> present;
+    for (auto &p : e) {
+        if (map[p.first] == 0xFFFFFFFFu) continue;
+        vs.push_back(map[p.first]);
+        vd.push_back(map[p.second]);
+        vw.push_back((float)(1.0 / hypot(px[p.first] - px[p.second], py[p.first] - py[p.second])));
+        present.insert(pair_key(map[p.first], map[p.second]));
+    }
+    std::vector<uint32_t> back(nn);
+    for (uint32_t i = 0; i < n; ++i)
+        if (map[i] != 0xFFFFFFFFu) back[map[i]] = i;
+    // insertions: pairs of component points at distance in [rad, 3 rad)
+    std::vector<uint32_t> is, id;
+    std::vector<float> iwv;
+    std::vector<uint32_t> cand;
+    uint64_t tries = 0;
+    while (is.size() < n_ins && nn > 1 && tries < (uint64_t)n_ins * 1000 + 1000) {
+        ++tries;
+        const uint32_t u = (uint32_t)r.below(nn);
+        const uint32_t pu = back[u];
+        const int cx = (int)cell(px[pu]), cy = (int)cell(py[pu]);
+        cand.clear();
+        for (int dy = -3; dy <= 3; ++dy)
+            for (int dx = -3; dx <= 3; ++dx) {
+                const int x = cx + dx, y = cy + dy;
+                if (x < 0 || y < 0 || x >= (int)gdim || y >= (int)gdim) continue;
+                for (uint32_t j : grid[(size_t)y * gdim + x]) {
+                    if (map[j] == 0xFFFFFFFFu || j == pu) continue;
+                    const double d = hypot(px[pu] - px[j], py[pu] - py[j]);
+                    if (d >= rad && d < 3 * rad && !present.count(pair_key(u, map[j])))
+                        cand.push_back(j);
+                }
+            }
+        if (cand.empty()) continue;
+        const uint32_t pv = cand[r.below(cand.size())];
+        const uint32_t v = map[pv];
+        present.insert(pair_key(u, v));
+        is.push_back(u);
+        id.push_back(v);
+        iwv.push_back((float)(1.0 / hypot(px[pu] - px[pv], py[pu] - py[pv])));
+    }
+    auto out_u32 = [](const std::vector<uint32_t> &v) {
+        uint32_t *p = (uint32_t *)malloc(sizeof(uint32_t) * (v.size() ? v.size() : 1));
+        if (p && !v.empty()) memcpy(p, v.data(), sizeof(uint32_t) * v.size());
+        return p;
+    };
+    auto out_f32 = [](const std::vector<float> &v) {
+        float *p = (float *)malloc(sizeof(float) * (v.size() ? v.size() : 1));
+        if (p && !v.empty()) memcpy(p, v.data(), sizeof(float) * v.size());
+        return p;
+    };
+    *n_out = nn;
+    *src = out_u32(vs);
+    *dst = out_u32(vd);
+    *w = out_f32(vw);
+    *n_ins_out = (uint32_t)is.size();
+    *isrc = out_u32(is);
+    *idst = out_u32(id);
+    *iw = out_f32(iwv);
+    return vs.size();
 }
 
 void dyg_synth_sample(uint64_t m, uint64_t k, uint64_t seed, uint64_t *out_idx) {

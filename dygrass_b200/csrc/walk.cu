@@ -21,6 +21,8 @@
 #include <mutex>
 #include <vector>
 
+#include <atomic>
+
 #include "dyg_internal.cuh"
 
 namespace dyg {
@@ -388,27 +390,32 @@ __global__ void k_fallback(DevGraph g, const unsigned long long *halt, const uin
 // of an edge nobody connects spread over 16 warps instead of running as 16
 // waves on one.  DYG_WALK_CHUNK (a multiple of 32 dividing the walker count)
 // overrides it for tuning sweeps.
+// Launch shape of the walk kernel, process-wide (dyg_tune_set); 0 = default.
+static std::atomic<uint32_t> g_tune_chunk{0}, g_tune_bpsm{0};
+
 static uint32_t chunk_for(uint32_t walkers) {
     static int env = -1;
     if (env < 0) {
         const char *v = getenv("DYG_WALK_CHUNK");
         env = v ? atoi(v) : 0;
     }
+    const uint32_t want = g_tune_chunk.load() ? g_tune_chunk.load() : (uint32_t)(env > 0 ? env : 0);
     uint32_t c = 32u;
-    if (env > 0 && env % 32 == 0 && walkers % (uint32_t)env == 0) c = (uint32_t)env;
+    if (want > 0 && want % 32 == 0 && walkers % want == 0) c = want;
     return c;
 }
 
 template <typename K>
 static int persistent_blocks(K kernel) {
-    static int cached = 0;
-    if (!cached) {
+    static int per_sm = 0;
+    if (!per_sm) {
         int nb = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, kWalkThreads, 0);
-        if (nb < 1) nb = 1;
-        cached = nb * num_sms();
+        per_sm = nb < 1 ? 1 : nb;
     }
-    return cached;
+    const uint32_t t = g_tune_bpsm.load();
+    const int b = (t && (int)t < per_sm) ? (int)t : per_sm;
+    return b * num_sms();
 }
 
 dyg_status launch_walk(dyg_graph *G, const WalkJob &job, const dyg_walk_params &p, bool incremental,
@@ -558,3 +565,8 @@ dyg_status dyg_profile_read(dyg_profile *out) {
 }
 
 }  // extern "C"
+
+extern "C" void dyg_tune_set(uint32_t walk_chunk, uint32_t blocks_per_sm) {
+    dyg::g_tune_chunk.store(walk_chunk);
+    dyg::g_tune_bpsm.store(blocks_per_sm);
+}

@@ -23,6 +23,13 @@ private drive by datasetdownload.py), so every workload here is generated:
                merge their weight) and 30% deletions (uniform over the edges
                present); threshold 50, 256 walkers, max_steps 128.  At
                scale 20: 2^20 ids, 500,000 updates in 123 files.
+  rgg_many   -- independent random geometric graphs in the unit square (n
+               log-uniform, radius for mean degree 8, weights 1/distance,
+               largest component), each with sparsifier = maximum spanning tree
+               + 10% off-tree and 0.05 n insertions at distance [r, 3r);
+               threshold 100 (the configuration leaves it open; 100 is the
+               reference's example bound), 512 walkers, max_steps 100.  The
+               full configuration is 256 graphs with n in [1e3, 2e5].
 """
 from __future__ import annotations
 
@@ -105,6 +112,54 @@ def rmat_stream(scale, a, b, c, id_map, src, dst, n_updates, file_size, del_frac
         files.append((int(ops[f]), os_[lo:hi].copy(), od[lo:hi].copy(),
                       None if ops[f] else ow[lo:hi].copy()))
     return files
+
+
+def rgg(n: int, avg_deg: float, n_ins: int, seed: int):
+    """Returns (n, src, dst, w, ins_src, ins_dst, ins_w)."""
+    no, ni = C.c_uint32(), C.c_uint32()
+    ptrs = [C.c_void_p() for _ in range(6)]
+    m = int(lib().dyg_synth_rgg(int(n), float(avg_deg), int(n_ins), int(seed), C.byref(no),
+                                C.byref(ptrs[0]), C.byref(ptrs[1]), C.byref(ptrs[2]), C.byref(ni),
+                                C.byref(ptrs[3]), C.byref(ptrs[4]), C.byref(ptrs[5])))
+    k = ni.value
+    try:
+        def arr(p, cnt, t):
+            return np.ctypeslib.as_array(C.cast(p, C.POINTER(t)), (max(cnt, 1),))[:cnt].copy()
+        out = (int(no.value), arr(ptrs[0], m, C.c_uint32), arr(ptrs[1], m, C.c_uint32),
+               arr(ptrs[2], m, C.c_float), arr(ptrs[3], k, C.c_uint32), arr(ptrs[4], k, C.c_uint32),
+               arr(ptrs[5], k, C.c_float))
+    finally:
+        for p in ptrs:
+            lib().dyg_mtx_free(p)
+    return out
+
+
+@dataclass
+class GraphCase:
+    n: int
+    g_src: np.ndarray
+    g_dst: np.ndarray
+    g_w: np.ndarray
+    h_src: np.ndarray
+    h_dst: np.ndarray
+    h_w: np.ndarray
+    ins_src: np.ndarray
+    ins_dst: np.ndarray
+    ins_w: np.ndarray
+
+
+def rgg_many(k: int = 256, n_lo: int = 1000, n_hi: int = 200_000, seed: int = MASTER_SEED,
+             walkers: int = 512, max_steps: int = 100, threshold: float = 100.0):
+    """Returns (list of GraphCase, WalkParams)."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(n_lo), np.log(n_hi), k)).astype(np.int64)
+    cases = []
+    for i, n0 in enumerate(sizes):
+        n, s, d, w, is_, id_, iw = rgg(int(n0), 8.0, int(0.05 * n0), seed + 101 + i)
+        idx = sparsifier(n, s, d, w, 0.10, seed + 7001 + i)
+        cases.append(GraphCase(n, s, d, w, s[idx], d[idx], w[idx], is_, id_, iw))
+    return cases, WalkParams.make(threshold=threshold, walkers=walkers, max_steps=max_steps,
+                                  seed=seed)
 
 
 @dataclass

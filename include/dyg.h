@@ -196,6 +196,32 @@ dyg_status dyg_decremental_stream(dyg_graph *G, dyg_graph *H, const uint32_t *sr
                                   uint32_t *rec_src, uint32_t *rec_dst, uint8_t *rec_kind,
                                   uint64_t rec_cap, uint64_t *n_rec, dyg_stream_t stream);
 
+/* dyg_incremental_batch / dyg_decremental_batch with an explicit update id
+ * per edge (update_ids[e] in place of first_update_id + e; host or device
+ * array).  With a union of independent graphs (each graph's vertices at its
+ * own offset), one call tests the current batch of every graph in a single
+ * launch and gives each graph exactly what its own call with those ids would
+ * (walks never leave a graph; rows are updated in list order per row).
+ * Extends the batch entry points (random_walk_incremental/main.cu:301-328,
+ * random_walk_decremental/main.cu:392-408) to many graphs at once. */
+dyg_status dyg_incremental_batch_ids(dyg_graph *H, dyg_graph *G, const uint32_t *src,
+                                     const uint32_t *dst, const float *w,
+                                     const uint64_t *update_ids, uint32_t n,
+                                     const dyg_walk_params *p, int32_t *found_at,
+                                     float *conductance, uint8_t *accepted, dyg_stream_t stream);
+dyg_status dyg_decremental_batch_ids(dyg_graph *G, dyg_graph *H, const uint32_t *src,
+                                     const uint32_t *dst, const uint64_t *update_ids, uint32_t n,
+                                     const dyg_walk_params *p, int32_t *status,
+                                     float *conductance, uint32_t *rec_src, uint32_t *rec_dst,
+                                     uint8_t *rec_kind, uint64_t rec_cap, uint64_t *n_rec,
+                                     dyg_stream_t stream);
+/* Launch shape of the walk kernel for this process (an autotuner's knobs;
+ * results do not depend on them): walkers each warp takes per fetch (a
+ * multiple of 32 dividing the walker count; 0 = 32) and resident blocks per
+ * SM (0 or more than fit = as many as fit).  Replaces the reference's fixed
+ * one-block-per-edge launch (random_walk_incremental/main.cu:316). */
+void dyg_tune_set(uint32_t walk_chunk, uint32_t blocks_per_sm);
+
 /* Walk-list chunk of the mixed updater: 5% of |V|, at least 10000
  * (dynamic_update/main.cu:83-84). */
 uint32_t dyg_stream_default_chunk(uint32_t n_vertices);

@@ -73,6 +73,18 @@ uint64_t dyg_synth_rmat_stream(uint32_t scale, double a, double b, double c,
                                uint8_t *file_op, uint32_t *out_src, uint32_t *out_dst,
                                float *out_w);
 
+/* Random geometric graph: n points uniform in the unit square, an edge
+ * between two points closer than r = sqrt(avg_deg / (pi n)) (mean degree
+ * avg_deg), weight 1/distance; restricted to the largest connected component,
+ * relabelled in point order (*n_out vertices).  Then n_ins new edges: u
+ * uniform over the component, v uniform among its points at distance in
+ * [r, 3r) from u not yet adjacent to u, weight 1/distance (*n_ins_out may fall
+ * short on tiny graphs).  Arrays are malloc'ed (free with dyg_mtx_free).
+ * Returns the edge count. */
+uint64_t dyg_synth_rgg(uint32_t n, double avg_deg, uint32_t n_ins, uint64_t seed,
+                       uint32_t *n_out, uint32_t **src, uint32_t **dst, float **w,
+                       uint32_t *n_ins_out, uint32_t **isrc, uint32_t **idst, float **iw);
+
 /* k distinct indices of [0, m) in uniformly random order. */
 void dyg_synth_sample(uint64_t m, uint64_t k, uint64_t seed, uint64_t *out_idx);
 
