@@ -23,6 +23,14 @@ stream files of 4,096 (70% insertion files, 30% deletion files), threshold
 50, 256 walkers, max_steps 128.  One step = every file in order through
 dyg_stream_file from the initial graphs.
 
+Workload "rgg_many": the batched many-graph configuration -- 256 random
+geometric graphs (n log-uniform in [1e3, 2e5], mean degree 8, weights
+1/distance), each with sparsifier = spanning tree + 10% off-tree and 0.05 n
+insertions; threshold 100, 512 walkers, max_steps 100.  The graphs form one
+union graph and a step is the 10 rounds that carry batch r of every graph
+(dygrass_b200/multi.py), after an autotune of the walk launch shape.  The
+plain per-graph loop on the same updates is timed beside it.
+
 N > 1 (torchrun): every rank runs an independent replica of the workload
 (weak scaling, no data-path collective); times are the max over ranks.
 
@@ -53,12 +61,18 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["mesh", "grid", "rmat"], default="mesh")
+    ap.add_argument("--workload", choices=["mesh", "grid", "rmat", "rgg_many"], default="mesh")
+    ap.add_argument("--rgg-graphs", type=int, default=256)
+    ap.add_argument("--rgg-n-hi", type=int, default=200_000)
+    ap.add_argument("--tune-walkers", action="store_true",
+                    help="let the autotuner lower the walker count at equal kappa")
     ap.add_argument("--rmat-scale", type=int, default=20)
     ap.add_argument("--rmat-updates", type=int, default=500_000)
     ap.add_argument("--mesh-k", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-plain", action="store_true",
+                    help="rgg_many: skip timing the plain per-graph loop")
     ap.add_argument("--exhaustive", action="store_true",
                     help="run every walker to its natural end (no pruning)")
     ap.add_argument("--profile-only", action="store_true",
@@ -69,6 +83,16 @@ def parse():
 def make_workload(args, rank):
     import dygrass_b200.workloads as wl
     seed = wl.MASTER_SEED + 1000 * rank
+    if args.workload == "rgg_many":
+        cases, p = wl.rgg_many(k=args.rgg_graphs, n_hi=args.rgg_n_hi, seed=seed)
+
+        class Many:
+            pass
+        W = Many()
+        W.cases, W.params, W.dparams = cases, p, p
+        W.n_updates = sum(len(c.ins_src) for c in cases)
+        W.n = sum(c.n for c in cases)
+        return W
     if args.workload == "rmat":
         W = wl.rmat_mixed(scale=args.rmat_scale, n_updates=args.rmat_updates, seed=seed)
         W.params = W.iparams
@@ -84,6 +108,15 @@ def make_workload(args, rank):
 
 
 def workload_config(W, args):
+    if args.workload == "rgg_many":
+        return {"workload": f"rgg_many {len(W.cases)} random geometric graphs, n log-uniform "
+                            f"[1,000, {args.rgg_n_hi:,}], mean degree 8, 0.05 n insertions each, "
+                            f"threshold 100, {W.params.walkers} walkers, max_steps 100, "
+                            f"one launch per round over all graphs",
+                "graphs": len(W.cases), "vertices": W.n,
+                "edges": int(sum(len(c.g_src) for c in W.cases)),
+                "sparsifier_edges": int(sum(len(c.h_src) for c in W.cases)),
+                "insertions": W.n_updates}
     if args.workload == "rmat":
         nins = sum(len(f[1]) for f in W.files if f[0] == 0)
         return {"workload": f"rmat scale {args.rmat_scale} mixed stream, files of 4,096 (70% insert / "
@@ -478,7 +511,186 @@ def run_mixed(args, rank, world, local_rank):
     return res
 
 
+def run_many(args, rank, world, local_rank):
+    """Many graphs: union rounds (timed) and the plain per-graph loop."""
+    import torch
+    import dygrass_b200 as dyg
+    from dygrass_b200.multi import ManyGraphs, autotune
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    W = make_workload(args, rank)
+    p = W.params
+    best, trials = autotune(W.cases, params=p, chunks=(32, 64), blocks=(0, 4),
+                            walkers=(128, 256) if args.tune_walkers else (), repeats=2,
+                            device=local_rank, sync=torch.cuda.synchronize)
+    if best["walkers"] != p.walkers:
+        p = dyg.WalkParams.make(threshold=p.threshold, walkers=best["walkers"],
+                                max_steps=p.max_steps, seed=p.seed)
+    M = ManyGraphs(W.cases, device=local_rank)
+    plan = M.plan()
+    H0, G0 = M.H.clone(), M.G.clone()
+    t = lambda a, dt=None: torch.from_numpy(np.ascontiguousarray(a if dt is None else a.view(dt))).to(dev)
+    for rd in plan.rounds:
+        rd.src, rd.dst, rd.w, rd.uid = (t(rd.src, np.int32), t(rd.dst, np.int32), t(rd.w),
+                                        t(rd.uid, np.int64))
+    outs = [dyg.IncrementalResult(torch.empty(len(rd.graph), dtype=torch.int32, device=dev),
+                                  torch.empty(len(rd.graph), dtype=torch.float32, device=dev),
+                                  torch.empty(len(rd.graph), dtype=torch.uint8, device=dev))
+            for rd in plan.rounds]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+
+    def reset():
+        M.H.copy_from(H0, sp)
+        M.G.copy_from(G0, sp)
+        flush.fill_(rank + 1)
+
+    if args.profile_only:
+        reset()
+        M.run(plan, p, stream=sp, outs=outs)
+        torch.cuda.synchronize()
+        return None
+    for _ in range(args.warmup):
+        reset()
+        M.run(plan, p, stream=sp, outs=outs)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    m0 = M.H.counters()[0]
+    launches0 = dyg.kernel_launches()
+    dyg.profile_reset()
+    dyg.profile_enable(True)
+    times = []
+    for _ in range(args.steps):
+        reset()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        M.run(plan, p, stream=sp, outs=outs)
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    dyg.profile_enable(False)
+    prof = dyg.profile_read()
+    launches = dyg.kernel_launches() - launches0
+    incr_moves = (M.H.counters()[0] - m0) / args.steps
+    clk = clocks.stop()
+    barrier()
+    ms = float(np.mean(times))
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    accepted = int(sum(int(o.accepted.sum().item()) for o in outs))
+
+    # the plain path: every graph its own handles and its own update loop
+    plain_ms = None
+    if not args.no_plain:
+        per = []
+        for c in W.cases:
+            Hg = dyg.Graph.from_edges(c.n, c.h_src, c.h_dst, c.h_w, device=local_rank)
+            Gg = dyg.Graph.from_edges(c.n, c.g_src, c.g_dst, c.g_w, device=local_rank)
+            per.append((Hg, Gg, Hg.clone(), Gg.clone(), t(c.ins_src, np.int32), t(c.ins_dst, np.int32),
+                        t(c.ins_w), dyg.IncrementalResult(
+                            torch.empty(len(c.ins_src), dtype=torch.int32, device=dev),
+                            torch.empty(len(c.ins_src), dtype=torch.float32, device=dev),
+                            torch.empty(len(c.ins_src), dtype=torch.uint8, device=dev))))
+        pt = []
+        for it in range(2):
+            for Hg, Gg, H0g, G0g, *_ in per:
+                Hg.copy_from(H0g, sp)
+                Gg.copy_from(G0g, sp)
+            flush.fill_(rank + 2)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for Hg, Gg, _, _, s_, d_, w_, o_ in per:
+                dyg.incremental_stream(Hg, s_, d_, w_, p, G=Gg, stream=sp, out=o_)
+            e1.record(stream)
+            e1.synchronize()
+            if it:
+                pt.append(e0.elapsed_time(e1))
+        plain_ms = float(np.mean(pt))
+        plain_acc = int(sum(int(x[-1].accepted.sum().item()) for x in per))
+        assert plain_acc == accepted, "union rounds and per-graph loops disagree"
+        for x in per:
+            for g in x[:4]:
+                g.close()
+
+    e2e = None
+    if not args.no_e2e:
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+        hplan = M.plan()
+        for rd in hplan.rounds:
+            rd.src, rd.dst, rd.w, rd.uid = pin(rd.src), pin(rd.dst), pin(rd.w), pin(rd.uid)
+        houts = [dyg.IncrementalResult(pin(np.empty(len(rd.graph), np.int32)),
+                                       pin(np.empty(len(rd.graph), np.float32)),
+                                       pin(np.empty(len(rd.graph), np.uint8))) for rd in hplan.rounds]
+        et = []
+        for _ in range(max(1, args.steps)):
+            reset()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            M.run(hplan, p, stream=sp, outs=houts)
+            e1.record(stream)
+            e1.synchronize()
+            et.append(e0.elapsed_time(e1))
+        ems = float(np.mean(et))
+        e2e = {"value": world * plan.n_edges / (ems / 1e3), "unit": "edge_updates/s",
+               "ms_per_step": ems, "h2d_bytes_per_step": int(plan.n_edges * 20),
+               "d2h_bytes_per_step": int(plan.n_edges * 9)}
+
+    res = {
+        "ms_per_step": ms, "steps_ms": times, "nin": plan.n_edges, "ndel": 0,
+        "accepted": accepted, "recovered": 0, "incr_moves": incr_moves, "decr_moves": 0.0,
+        "walk_ms_per_step": prof["incr_walk_ms"] / args.steps,
+        "walk_launches": prof["incr_walk_launches"], "prof": prof,
+        "launches_per_step": launches / args.steps, "clocks": clk, "e2e": e2e,
+        "dom_kernel": "k_walk<1,0>",
+        "dom_bytes_per_launch": dom_bytes(prof, incr_moves, 0.0, args.steps),
+        "dom_ms_per_launch": dom_ms(prof),
+        "plain_ms_per_step": plain_ms, "tuned": best, "tune_trials": trials, "W": W,
+    }
+    for g in (H0, G0):
+        g.close()
+    M.close()
+    return res
+
+
 # --------------------------------------------------------- CPU baseline
+
+def cpu_baseline_many(W, threads=None):
+    """The oracle's per-graph update loop on every 16th graph (a spread of
+    sizes), per-insertion cost extrapolated to all graphs' insertions."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    th = threads or pyoracle.max_threads()
+    sample = W.cases[::16] or W.cases[:1]
+    t0 = time.perf_counter()
+    for c in sample:
+        Ho = pyoracle.OGraph(c.n, c.h_src, c.h_dst, c.h_w)
+        Go = pyoracle.OGraph(c.n, c.g_src, c.g_dst, c.g_w)
+        pyoracle.incremental(Ho, c.ins_src, c.ins_dst, c.ins_w, W.params, G=Go, threads=th)
+    dt = time.perf_counter() - t0
+    ns = sum(len(c.ins_src) for c in sample)
+    return {"value": ns / dt, "unit": "edge_updates/s", "cores": th, "kind": "port", "seconds": dt,
+            "sample": f"oracle (C/OpenMP, {th} threads): the update loops of {len(sample)} of the "
+                      f"{len(W.cases)} graphs (every 16th), {ns} insertions; per-insertion cost "
+                      f"extrapolated to all {W.n_updates}"}
+
 
 def cpu_baseline_mixed(W, threads=None):
     """The oracle on a bounded sample of the mixed stream: the first insertion
@@ -558,7 +770,8 @@ def main():
         if rank != 0:
             return 0
         W = make_workload(args, 0)
-        base = cpu_baseline_mixed if args.workload == "rmat" else cpu_baseline
+        base = {"rmat": cpu_baseline_mixed, "rgg_many": cpu_baseline_many}.get(args.workload,
+                                                                               cpu_baseline)
         vals = []
         for i in range(args.warmup + args.steps):
             r = base(W)
@@ -567,7 +780,7 @@ def main():
         v = float(np.mean([r["value"] for r in vals]))
         out = {"metric": "edge updates/sec (incr+decr)", "value": v, "unit": "edge_updates/s",
                "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-               "ms_per_step": (W.n_updates if args.workload == "rmat"
+               "ms_per_step": (W.n_updates if args.workload in ("rmat", "rgg_many")
                                else len(W.ins_src) + len(W.del_src)) / v * 1e3,
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                "data": "synthetic (seeded)", "config": workload_config(W, args),
@@ -585,7 +798,8 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
-    res = (run_mixed if args.workload == "rmat" else run_ours)(args, rank, world, local_rank)
+    runner = {"rmat": run_mixed, "rgg_many": run_many}.get(args.workload, run_ours)
+    res = runner(args, rank, world, local_rank)
     if res is None:
         return 0
     W = res.pop("W")
@@ -623,7 +837,8 @@ def main():
     moves = res["incr_moves"] + res["decr_moves"]
     cpu = None
     if not args.no_cpu_baseline and world == 1:
-        cpu = cpu_baseline_mixed(W) if args.workload == "rmat" else cpu_baseline(W)
+        cpu = {"rmat": cpu_baseline_mixed, "rgg_many": cpu_baseline_many}.get(
+            args.workload, cpu_baseline)(W)
     out = {
         "metric": "edge updates/sec (incr+decr)",
         "value": value, "unit": "edge_updates/s", "n_gpus": world, "steps": args.steps,
@@ -651,6 +866,11 @@ def main():
         "e2e": res["e2e"],
         "gpu_launches": int(round(res["launches_per_step"] * args.steps)),
         "pruning": not args.exhaustive,
+        **({"batched": {"plain_per_graph_ms_per_step": res["plain_ms_per_step"],
+                        "speedup_vs_plain": (res["plain_ms_per_step"] / ms
+                                             if res["plain_ms_per_step"] else None),
+                        "tuned": res["tuned"], "rounds": 10}}
+           if args.workload == "rgg_many" else {}),
         "cpu_baseline": cpu,
     }
     print(json.dumps(out))

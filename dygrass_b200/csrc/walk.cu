@@ -168,6 +168,18 @@ __device__ __forceinline__ int step_once(Walker &s, const uint2 *__restrict__ de
     return kContinue;
 }
 
+// RN(1/R) < c for positive finite R, c, decided by one product where it can
+// be: p = RN(R*c) is within 2^-24 of R*c, so p > 1 + 2^-21 gives
+// 1/R < c (1 - 7 * 2^-24), below c by more than half an ulp of c, hence
+// RN(1/R) < c; p < 1 - 2^-21 gives RN(1/R) > c the same way.  Only products
+// inside that band take the correctly rounded reciprocal.
+__device__ __forceinline__ bool below_best(float R, float c) {
+    const float p = __fmul_rn(R, c);
+    if (p > 1.0000004768371582f) return true;    // 1 + 2^-21
+    if (p < 0.9999995231628418f) return false;   // 1 - 2^-21
+    return __frcp_rn(R) < c;
+}
+
 template <bool INCR, bool WEIGHTED>
 __global__ void __launch_bounds__(kWalkThreads) k_walk(WalkArgs a) {
     if (a.job.halt && *a.job.halt) return;
@@ -279,7 +291,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(WalkArgs a) {
                     gbest = max(gbest, (uint32_t)(*(volatile unsigned long long *)(a.keys + my_e) >> 32));
                 const uint32_t known = max(gbest, (my_e == ce) ? ce_best
                                                   : (my_e == pe ? pe_best : 0u));
-                if (known && __frcp_rn(s.R) < __uint_as_float(known)) {
+                if (known && below_best(s.R, __uint_as_float(known))) {
                     active = false;
                     ++walks;
                 }
