@@ -31,6 +31,15 @@ union graph and a step is the 10 rounds that carry batch r of every graph
 (dygrass_b200/multi.py), after an autotune of the walk launch shape.  The
 plain per-graph loop on the same updates is timed beside it.
 
+Workload "serve": the serving configuration -- 64 resident graphs mixed from
+the mesh, R-MAT and random-geometric generators, update requests of log-
+uniform size in [1, 4096], 60% insertions / 40% deletions.  value = the
+continuous-batching server's throughput replaying a fixed request set that
+is all pending at once (saturation), timed with CUDA events from a restored
+snapshot; then p50/p99 latency at Poisson arrival rates swept around that
+capacity, for the server and for the plain sequential path (every request
+alone on its graph's own handles).
+
 N > 1 (torchrun): every rank runs an independent replica of the workload
 (weak scaling, no data-path collective); times are the max over ranks.
 
@@ -61,7 +70,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["mesh", "grid", "rmat", "rgg_many"], default="mesh")
+    ap.add_argument("--workload", choices=["mesh", "grid", "rmat", "rgg_many", "serve"],
+                    default="mesh")
+    ap.add_argument("--serve-requests", type=int, default=2000)
     ap.add_argument("--rgg-graphs", type=int, default=256)
     ap.add_argument("--rgg-n-hi", type=int, default=200_000)
     ap.add_argument("--tune-walkers", action="store_true",
@@ -83,6 +94,19 @@ def parse():
 def make_workload(args, rank):
     import dygrass_b200.workloads as wl
     seed = wl.MASTER_SEED + 1000 * rank
+    if args.workload == "serve":
+        from dygrass_b200.serve import footprint_bytes, poisson_requests
+        cases, ip, dp = wl.serving_mix(seed=seed)
+
+        class Serve:
+            pass
+        W = Serve()
+        W.cases, W.params, W.dparams = cases, ip, dp
+        W.requests = poisson_requests(cases, 1.0, args.serve_requests, seed + 5)
+        W.n_updates = sum(len(r.src) for r in W.requests)
+        W.n = sum(c.n for c in cases)
+        W.footprint = sum(footprint_bytes(c.n, len(c.g_src), len(c.h_src)) for c in cases)
+        return W
     if args.workload == "rgg_many":
         cases, p = wl.rgg_many(k=args.rgg_graphs, n_hi=args.rgg_n_hi, seed=seed)
 
@@ -108,6 +132,15 @@ def make_workload(args, rank):
 
 
 def workload_config(W, args):
+    if args.workload == "serve":
+        ins = sum(len(r.src) for r in W.requests if r.op == 0)
+        return {"workload": f"serve {len(W.cases)} resident graphs (meshes, R-MAT, random geometric), "
+                            f"{len(W.requests)} requests of log-uniform size [1, 4096], 60% insert / "
+                            f"40% delete, threshold 100, 512 walkers, max_steps 100",
+                "graphs": len(W.cases), "vertices": W.n,
+                "edges": int(sum(len(c.g_src) for c in W.cases)),
+                "footprint_bytes_estimate": W.footprint, "requests": len(W.requests),
+                "updates": W.n_updates, "insertions": ins, "deletions": W.n_updates - ins}
     if args.workload == "rgg_many":
         return {"workload": f"rgg_many {len(W.cases)} random geometric graphs, n log-uniform "
                             f"[1,000, {args.rgg_n_hi:,}], mean degree 8, 0.05 n insertions each, "
@@ -670,7 +703,141 @@ def run_many(args, rank, world, local_rank):
     return res
 
 
+def _arrive(reqs, rate):
+    """Copies of the requests with Poisson arrival times at `rate` per
+    second (the request set's own exponential draws, rescaled; rate None:
+    all pending at once)."""
+    import dataclasses
+    out = [dataclasses.replace(r) for r in reqs]
+    for r in out:
+        r.arrival = 0.0 if rate is None else r.arrival / rate
+    return out
+
+
+def run_serve(args, rank, world, local_rank):
+    import torch
+    import dygrass_b200 as dyg
+    from dygrass_b200.serve import PlainServer, Server, latency_stats
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    W = make_workload(args, rank)
+    S = Server(W.cases, W.params, W.dparams, device=local_rank)
+    S.snapshot()
+    stream = torch.cuda.current_stream(dev)
+    sync = torch.cuda.synchronize
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    n_upd = W.n_updates
+
+    def replay(server, rate):
+        server.restore()
+        flush.fill_(rank + 1)
+        sync()
+        return server.serve(_arrive(W.requests, rate), sync=sync)
+
+    if args.profile_only:
+        replay(S, None)
+        return None
+    for _ in range(args.warmup):
+        replay(S, None)
+    sync()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    m0 = S.H.counters()[0] + S.G.counters()[0]
+    launches0 = dyg.kernel_launches()
+    dyg.profile_reset()
+    dyg.profile_enable(True)
+    times, steps = [], 0
+    for _ in range(args.steps):
+        S.restore()
+        flush.fill_(rank + 1)
+        sync()
+        reqs = _arrive(W.requests, None)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        S.serve(reqs)
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+        steps = S.steps
+    dyg.profile_enable(False)
+    prof = dyg.profile_read()
+    launches = dyg.kernel_launches() - launches0
+    moves = (S.H.counters()[0] + S.G.counters()[0] - m0) / args.steps
+    clk = clocks.stop()
+    ms = float(np.mean(times))
+    capacity = len(W.requests) / (ms / 1e3)      # requests per second at saturation
+
+    # latency at swept arrival rates, server and plain path
+    P = PlainServer(W.cases, W.params, W.dparams, device=local_rank)
+    P.snapshot()
+    sweep = []
+    for frac in (0.25, 0.5, 0.9):
+        rate = capacity * frac
+        row = {"rate_req_per_s": rate, "fraction_of_capacity": frac,
+               "server": latency_stats(replay(S, rate))}
+        row["plain"] = latency_stats(replay(P, rate))
+        sweep.append(row)
+    sync()
+    plain_sat = latency_stats(replay(P, None))
+    P.close()
+    S.close()
+    res = {
+        "ms_per_step": ms, "steps_ms": times, "nin": n_upd, "ndel": 0, "accepted": None,
+        "recovered": 0, "incr_moves": moves, "decr_moves": 0.0,
+        "walk_ms_per_step": (prof["incr_walk_ms"] + prof["decr_walk_ms"]) / args.steps,
+        "walk_launches": prof["incr_walk_launches"] + prof["decr_walk_launches"], "prof": prof,
+        "launches_per_step": launches / args.steps, "clocks": clk,
+        "e2e": {"value": n_upd / (ms / 1e3), "unit": "edge_updates/s", "ms_per_step": ms,
+                "h2d_bytes_per_step": int(sum(len(r.src) * (20 if r.op == 0 else 16)
+                                              for r in W.requests)),
+                "d2h_bytes_per_step": int(sum(len(r.src) * (9 if r.op == 0 else 8)
+                                              for r in W.requests)),
+                "note": "the server takes host arrays: its device-timed run is end to end"},
+        "dom_kernel": dom_name(prof),
+        "dom_bytes_per_launch": BYTES_PER_MOVE * moves * args.steps / max(
+            prof["decr_walk_launches"] + prof["incr_walk_launches"], 1),
+        "dom_ms_per_launch": (prof["incr_walk_ms"] + prof["decr_walk_ms"]) / max(
+            prof["decr_walk_launches"] + prof["incr_walk_launches"], 1),
+        "serving": {"server_steps_per_replay": steps, "capacity_req_per_s": capacity,
+                    "sweep": sweep, "plain_saturated": plain_sat},
+        "W": W,
+    }
+    return res
+
+
 # --------------------------------------------------------- CPU baseline
+
+def cpu_baseline_serve(W, threads=None, max_requests=300):
+    """The oracle applying the first requests one by one on their graphs."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    th = threads or pyoracle.max_threads()
+    reqs = W.requests[:max_requests]
+    gs, uid = {}, {}
+    for r in reqs:
+        if r.graph not in gs:
+            c = W.cases[r.graph]
+            gs[r.graph] = (pyoracle.OGraph(c.n, c.g_src, c.g_dst, c.g_w),
+                           pyoracle.OGraph(c.n, c.h_src, c.h_dst, c.h_w))
+            uid[r.graph] = 0
+    t0 = time.perf_counter()
+    for r in reqs:
+        Go, Ho = gs[r.graph]
+        if r.op == 0:
+            pyoracle.incremental(Ho, r.src, r.dst, r.w, W.params, G=Go, threads=th,
+                                 first_uid=uid[r.graph], single_batch=True)
+        else:
+            pyoracle.decremental(Go, Ho, r.src, r.dst, W.dparams, threads=th,
+                                 first_uid=uid[r.graph], single_batch=True)
+        uid[r.graph] += len(r.src)
+    dt = time.perf_counter() - t0
+    nu = sum(len(r.src) for r in reqs)
+    return {"value": nu / dt, "unit": "edge_updates/s", "cores": th, "kind": "port", "seconds": dt,
+            "sample": f"oracle (C/OpenMP, {th} threads): the first {len(reqs)} requests ({nu} "
+                      f"updates) one by one on their graphs (graph loading not timed)"}
+
 
 def cpu_baseline_many(W, threads=None):
     """The oracle's per-graph update loop on every 16th graph (a spread of
@@ -770,8 +937,8 @@ def main():
         if rank != 0:
             return 0
         W = make_workload(args, 0)
-        base = {"rmat": cpu_baseline_mixed, "rgg_many": cpu_baseline_many}.get(args.workload,
-                                                                               cpu_baseline)
+        base = {"rmat": cpu_baseline_mixed, "rgg_many": cpu_baseline_many,
+                "serve": cpu_baseline_serve}.get(args.workload, cpu_baseline)
         vals = []
         for i in range(args.warmup + args.steps):
             r = base(W)
@@ -780,7 +947,7 @@ def main():
         v = float(np.mean([r["value"] for r in vals]))
         out = {"metric": "edge updates/sec (incr+decr)", "value": v, "unit": "edge_updates/s",
                "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-               "ms_per_step": (W.n_updates if args.workload in ("rmat", "rgg_many")
+               "ms_per_step": (W.n_updates if args.workload in ("rmat", "rgg_many", "serve")
                                else len(W.ins_src) + len(W.del_src)) / v * 1e3,
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                "data": "synthetic (seeded)", "config": workload_config(W, args),
@@ -798,7 +965,8 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
-    runner = {"rmat": run_mixed, "rgg_many": run_many}.get(args.workload, run_ours)
+    runner = {"rmat": run_mixed, "rgg_many": run_many, "serve": run_serve}.get(args.workload,
+                                                                                run_ours)
     res = runner(args, rank, world, local_rank)
     if res is None:
         return 0
@@ -837,8 +1005,8 @@ def main():
     moves = res["incr_moves"] + res["decr_moves"]
     cpu = None
     if not args.no_cpu_baseline and world == 1:
-        cpu = {"rmat": cpu_baseline_mixed, "rgg_many": cpu_baseline_many}.get(
-            args.workload, cpu_baseline)(W)
+        cpu = {"rmat": cpu_baseline_mixed, "rgg_many": cpu_baseline_many,
+               "serve": cpu_baseline_serve}.get(args.workload, cpu_baseline)(W)
     out = {
         "metric": "edge updates/sec (incr+decr)",
         "value": value, "unit": "edge_updates/s", "n_gpus": world, "steps": args.steps,
@@ -866,6 +1034,7 @@ def main():
         "e2e": res["e2e"],
         "gpu_launches": int(round(res["launches_per_step"] * args.steps)),
         "pruning": not args.exhaustive,
+        **({"serving": res["serving"]} if args.workload == "serve" else {}),
         **({"batched": {"plain_per_graph_ms_per_step": res["plain_ms_per_step"],
                         "speedup_vs_plain": (res["plain_ms_per_step"] / ms
                                              if res["plain_ms_per_step"] else None),

@@ -307,50 +307,106 @@ __global__ void k_del_scatter(DevGraph g, const uint32_t *hx, uint32_t m, const 
 
 // Leaders remove their row's entries in list order.  With `mask`, entry
 // i = 2e + side is applied only if edge e was found on both sides of `mask`.
-// With big_ok, rows longer than kBigRow go to the big list for
-// k_del_apply_big.
+// A row of up to 32 slots is edited by its leader's lane; a longer one by the
+// whole warp (each search 32 slots at a time); with big_ok, rows longer than
+// kBigRow go to the big list for k_del_apply_big.  Every lane of a warp runs
+// the same iterations.
 __global__ void k_del_apply(DevGraph g, const uint32_t *hx, const uint32_t *hy, uint32_t m,
                             const uint32_t *rank, uint32_t *rowcnt, const uint32_t *rowtmp,
                             uint32_t *tmp, const uint8_t *mask, uint8_t *found, uint4 *big,
                             unsigned long long *nbig, bool big_ok,
                             const unsigned long long *halt) {
     if (*halt) return;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
-        if (rank[i] != 0u) continue;
-        const uint32_t x = hx[i];
-        const uint2 d = g.desc[x];
-        if (big_ok && d.y > kBigRow) {
-            big[atomicAdd(nbig, 1ull)] = make_uint4(i, 0u, 0u, 0u);
-            continue;
-        }
-        const uint32_t cnt = rowcnt[x];
-        rowcnt[x] = 0u;
-        uint32_t *run = tmp + rowtmp[x];
-        for (uint32_t a = 1; a < cnt; ++a) {
-            const uint32_t v = run[a];
-            uint32_t b = a;
-            while (b > 0 && run[b - 1] > v) {
-                run[b] = run[b - 1];
-                --b;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t first = blockIdx.x * blockDim.x + threadIdx.x;
+    for (uint32_t wb = first - lane; wb < m; wb += gridDim.x * blockDim.x) {
+        const uint32_t i = wb + lane;
+        bool lead = i < m && rank[i] == 0u;
+        uint32_t x = 0u, cnt = 0u;
+        uint2 d = make_uint2(0u, 0u);
+        if (lead) {
+            x = hx[i];
+            d = g.desc[x];
+            if (big_ok && d.y > kBigRow) {
+                big[atomicAdd(nbig, 1ull)] = make_uint4(i, 0u, 0u, 0u);
+                lead = false;
+            } else {
+                cnt = rowcnt[x];
+                rowcnt[x] = 0u;
             }
-            run[b] = v;
         }
-        uint32_t deg = d.y;
-        for (uint32_t a = 0; a < cnt; ++a) {
-            const uint32_t k = run[a];
-            if (mask && !(mask[k & ~1u] && mask[k | 1u])) continue;
-            const uint32_t y = hy[k];
-            for (uint32_t j = 0; j < deg; ++j) {
-                if (g.slots[d.x + j].x == y) {
-                    g.slots[d.x + j] = g.slots[d.x + deg - 1u];
-                    g.wts[d.x + j] = g.wts[d.x + deg - 1u];
-                    --deg;
-                    found[k] = 1;
-                    break;
+        const bool coop = lead && d.y > 32u;
+        if (lead && !coop) {
+            uint32_t *run = tmp + rowtmp[x];
+            for (uint32_t a = 1; a < cnt; ++a) {
+                const uint32_t v = run[a];
+                uint32_t b = a;
+                while (b > 0 && run[b - 1] > v) {
+                    run[b] = run[b - 1];
+                    --b;
+                }
+                run[b] = v;
+            }
+            uint32_t deg = d.y;
+            for (uint32_t a = 0; a < cnt; ++a) {
+                const uint32_t k = run[a];
+                if (mask && !(mask[k & ~1u] && mask[k | 1u])) continue;
+                const uint32_t y = hy[k];
+                for (uint32_t j = 0; j < deg; ++j) {
+                    if (g.slots[d.x + j].x == y) {
+                        g.slots[d.x + j] = g.slots[d.x + deg - 1u];
+                        g.wts[d.x + j] = g.wts[d.x + deg - 1u];
+                        --deg;
+                        found[k] = 1;
+                        break;
+                    }
                 }
             }
+            g.desc[x] = make_uint2(d.x, deg);
         }
-        g.desc[x] = make_uint2(d.x, deg);
+        unsigned todo = __ballot_sync(kFull, coop);
+        while (todo) {
+            const int src = __ffs(todo) - 1;
+            todo &= todo - 1u;
+            const uint32_t sx = __shfl_sync(kFull, x, src);
+            const uint32_t sc = __shfl_sync(kFull, cnt, src);
+            const uint32_t off = __shfl_sync(kFull, d.x, src);
+            uint32_t deg = __shfl_sync(kFull, d.y, src);
+            uint32_t *run = tmp + rowtmp[sx];
+            uint32_t *sorted = tmp + m + rowtmp[sx];
+            for (uint32_t a = lane; a < sc; a += 32u) {   // each entry to its rank
+                const uint32_t v = run[a];
+                uint32_t r = 0;
+                for (uint32_t c = 0; c < sc; ++c) r += run[c] < v;
+                sorted[r] = v;
+            }
+            __syncwarp();
+            for (uint32_t a = 0; a < sc; ++a) {
+                const uint32_t k = sorted[a];
+                if (mask && !(mask[k & ~1u] && mask[k | 1u])) continue;
+                const uint32_t y = hy[k];
+                uint32_t pos = ~0u;
+                for (uint32_t j0 = 0; j0 < deg; j0 += 32u) {
+                    const uint32_t j = j0 + lane;
+                    const unsigned hit = __ballot_sync(kFull, j < deg && g.slots[off + j].x == y);
+                    if (hit) {
+                        pos = j0 + (uint32_t)(__ffs(hit) - 1);
+                        break;
+                    }
+                }
+                if (pos != ~0u) {
+                    if (lane == 0u) {
+                        g.slots[off + pos] = g.slots[off + deg - 1u];
+                        g.wts[off + pos] = g.wts[off + deg - 1u];
+                        found[k] = 1;
+                    }
+                    --deg;
+                    __syncwarp();   // the moved slot is visible to the next search
+                }
+            }
+            if (lane == 0u) g.desc[sx] = make_uint2(off, deg);
+            __syncwarp();
+        }
     }
 }
 

@@ -1,0 +1,292 @@
+"""Serving many resident graphs with continuous batching.
+
+Requests are update batches for one graph (insertions or deletions, any
+size).  The server keeps every admitted graph resident in one union graph
+(each at its own vertex offset, as in multi.py) with its update counter on
+the host, so a graph's random streams depend only on its own history.  Each
+scheduler step takes the oldest pending request of every graph that has one,
+runs all insertion requests of the step as one dyg_incremental_batch_ids
+launch and all deletion requests as one dyg_decremental_batch_ids launch, and
+completes them; requests that arrive meanwhile join the next step.  Graphs
+are disjoint and a graph's requests run in arrival order, one per step, so
+every request gets exactly the result it gets when run alone on its graph's
+own handles (tested).
+
+Admission: graphs are admitted in the given order while their estimated
+device footprint (dense graph and sparsifier arenas and descriptors, plus
+the per-request workspace) fits the HBM budget; requests for other graphs
+are refused.
+"""
+from __future__ import annotations
+
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import (DecrementalResult, Graph, IncrementalResult, WalkParams, decremental_batch_ids,
+               incremental_batch_ids)
+
+INSERT, DELETE = 0, 1
+
+
+@dataclass
+class Request:
+    graph: int
+    op: int                       # INSERT or DELETE
+    src: np.ndarray               # local vertex ids
+    dst: np.ndarray
+    w: np.ndarray | None = None   # insertions only
+    arrival: float = 0.0          # seconds on the server's clock
+    # filled on completion
+    done: float = 0.0
+    first_update_id: int = 0
+    found_at: np.ndarray | None = None      # insertions
+    conductance: np.ndarray | None = None
+    accepted: np.ndarray | None = None
+    status: np.ndarray | None = None        # deletions
+    recovered: list = field(default_factory=list)   # (x, y, kind), local ids
+
+    @property
+    def latency(self) -> float:
+        return self.done - self.arrival
+
+
+def footprint_bytes(n: int, g_edges: int, h_edges: int, headroom: float = 0.5,
+                    slack: int = 2) -> int:
+    """Estimated device bytes of one graph in the union: per slot 12 B
+    (slot + weight) with arena headroom, per vertex 12 B (descriptor +
+    capacity) for G and H each."""
+    slots = lambda m: (2 * m + slack * n) * (1 + headroom)
+    return int(12 * (slots(g_edges) + slots(h_edges)) + 24 * n)
+
+
+class Server:
+    def __init__(self, cases, iparams: WalkParams, dparams: WalkParams,
+                 hbm_budget: float = float("inf"), device: int = -1):
+        self.iparams, self.dparams = iparams, dparams
+        self.admitted, offs, used = [], [0], 0
+        for i, c in enumerate(cases):
+            fp = footprint_bytes(c.n, len(c.g_src), len(c.h_src))
+            if used + fp > hbm_budget:
+                continue
+            used += fp
+            self.admitted.append(i)
+            offs.append(offs[-1] + c.n)
+        self.footprint = used
+        self.slot = {g: k for k, g in enumerate(self.admitted)}
+        self.offsets = np.array(offs, np.int64)
+        cat = lambda xs, t: np.concatenate(xs).astype(t) if xs else np.empty(0, t)
+        sel = [cases[g] for g in self.admitted]
+        n = int(self.offsets[-1])
+        self.H = Graph.from_edges(n, cat([c.h_src + o for c, o in zip(sel, offs)], np.uint32),
+                                  cat([c.h_dst + o for c, o in zip(sel, offs)], np.uint32),
+                                  cat([c.h_w for c in sel], np.float32), device=device)
+        self.G = Graph.from_edges(n, cat([c.g_src + o for c, o in zip(sel, offs)], np.uint32),
+                                  cat([c.g_dst + o for c, o in zip(sel, offs)], np.uint32),
+                                  cat([c.g_w for c in sel], np.float32), device=device)
+        self.queues = {g: deque() for g in self.admitted}
+        self.uid_next = {g: 0 for g in self.admitted}
+        self.steps = 0
+        self.t0 = time.perf_counter()
+
+    def now(self) -> float:
+        return time.perf_counter() - self.t0
+
+    def snapshot(self):
+        """Keeps a device copy of the graphs for restore()."""
+        self._snap = (self.H.clone(), self.G.clone())
+
+    def restore(self, stream: int | None = None):
+        """Back to the snapshot: graphs, update counters, empty queues."""
+        self.H.copy_from(self._snap[0], stream)
+        self.G.copy_from(self._snap[1], stream)
+        self.uid_next = {g: 0 for g in self.admitted}
+        for q in self.queues.values():
+            q.clear()
+        self.steps = 0
+
+    def submit(self, r: Request) -> bool:
+        """Queues a request; False if its graph was not admitted."""
+        if r.graph not in self.queues:
+            return False
+        self.queues[r.graph].append(r)
+        return True
+
+    def pending(self) -> bool:
+        return any(self.queues.values())
+
+    def _batch(self, reqs):
+        src, dst, w, uid = [], [], [], []
+        for r in reqs:
+            off = self.offsets[self.slot[r.graph]]
+            r.first_update_id = self.uid_next[r.graph]
+            src.append(np.asarray(r.src, np.int64) + off)
+            dst.append(np.asarray(r.dst, np.int64) + off)
+            if r.op == INSERT:
+                w.append(np.asarray(r.w, np.float32))
+            uid.append(np.arange(len(r.src), dtype=np.uint64) + np.uint64(r.first_update_id))
+            self.uid_next[r.graph] += len(r.src)
+        return (np.concatenate(src).astype(np.uint32), np.concatenate(dst).astype(np.uint32),
+                np.concatenate(w) if w else None, np.concatenate(uid))
+
+    def step(self) -> list:
+        """Runs the oldest pending request of every graph; returns them."""
+        heads = [q.popleft() for q in self.queues.values() if q]
+        for r in heads:
+            r.first_update_id = self.uid_next[r.graph]
+        ins = [r for r in heads if r.op == INSERT and len(r.src)]
+        dels = [r for r in heads if r.op == DELETE and len(r.src)]
+        if ins:
+            s, d, w, u = self._batch(ins)
+            res = incremental_batch_ids(self.H, s, d, w, u, self.iparams, G=self.G)
+            k = 0
+            for r in ins:
+                m = len(r.src)
+                r.found_at = res.found_at[k:k + m].copy()
+                r.conductance = res.conductance[k:k + m].copy()
+                r.accepted = res.accepted[k:k + m].copy()
+                k += m
+        if dels:
+            s, d, _, u = self._batch(dels)
+            res = decremental_batch_ids(self.G, self.H, s, d, u, self.dparams)
+            k = 0
+            # recovered edges come in commit order: edge by edge, so each
+            # belongs to the request whose vertex range holds it
+            owner = np.searchsorted(self.offsets, res.rec_src, side="right") - 1
+            for r in dels:
+                m = len(r.src)
+                r.status = res.status[k:k + m].copy()
+                k += m
+                sl = self.slot[r.graph]
+                sel = owner == sl
+                off = self.offsets[sl]
+                r.recovered = list(zip((res.rec_src[sel] - off).tolist(),
+                                       (res.rec_dst[sel] - off).tolist(), res.rec_kind[sel].tolist()))
+        t = self.now()
+        for r in heads:
+            r.done = t
+            if r.op == INSERT and r.found_at is None:
+                r.found_at = np.empty(0, np.int32)
+                r.conductance = np.empty(0, np.float32)
+                r.accepted = np.empty(0, np.uint8)
+            if r.op == DELETE and r.status is None:
+                r.status = np.empty(0, np.int32)
+        self.steps += 1
+        return heads
+
+    def serve(self, requests, sync=lambda: None) -> list:
+        """Replays requests at their arrival times (seconds from now) with
+        continuous batching; returns the completed requests."""
+        order = sorted(requests, key=lambda r: r.arrival)
+        self.t0 = time.perf_counter()
+        i, done = 0, []
+        while i < len(order) or self.pending():
+            t = self.now()
+            while i < len(order) and order[i].arrival <= t:
+                if not self.submit(order[i]):
+                    order[i].done = -1.0
+                i += 1
+            if self.pending():
+                done += self.step()
+                sync()
+            elif i < len(order):
+                time.sleep(max(0.0, min(order[i].arrival - self.now(), 0.001)))
+        return done
+
+    def close(self):
+        for x in (self.H, self.G) + tuple(getattr(self, "_snap", ())):
+            x.close()
+
+
+class PlainServer:
+    """The plain sequential path: every graph its own handles, requests one
+    at a time in arrival order."""
+
+    def __init__(self, cases, iparams: WalkParams, dparams: WalkParams, device: int = -1):
+        self.iparams, self.dparams = iparams, dparams
+        self.H = [Graph.from_edges(c.n, c.h_src, c.h_dst, c.h_w, device=device) for c in cases]
+        self.G = [Graph.from_edges(c.n, c.g_src, c.g_dst, c.g_w, device=device) for c in cases]
+        self.uid_next = [0] * len(cases)
+
+    def snapshot(self):
+        self._snap = ([h.clone() for h in self.H], [g.clone() for g in self.G])
+
+    def restore(self, stream: int | None = None):
+        for x, y in zip(self.H + self.G, self._snap[0] + self._snap[1]):
+            x.copy_from(y, stream)
+        self.uid_next = [0] * len(self.H)
+
+    def run_one(self, r: Request):
+        from . import decremental_batch, incremental_batch
+        g = r.graph
+        r.first_update_id = self.uid_next[g]
+        if r.op == INSERT:
+            res = incremental_batch(self.H[g], r.src, r.dst, r.w, self.iparams,
+                                    first_update_id=r.first_update_id, G=self.G[g])
+            r.found_at, r.conductance, r.accepted = res.found_at, res.conductance, res.accepted
+        else:
+            res = decremental_batch(self.G[g], self.H[g], r.src, r.dst, self.dparams,
+                                    first_update_id=r.first_update_id)
+            r.status = res.status
+            r.recovered = list(zip(res.rec_src.tolist(), res.rec_dst.tolist(),
+                                   res.rec_kind.tolist()))
+        self.uid_next[g] += len(r.src)
+
+    def serve(self, requests, sync=lambda: None) -> list:
+        order = sorted(requests, key=lambda r: r.arrival)
+        t0 = time.perf_counter()
+        for r in order:
+            wait = r.arrival - (time.perf_counter() - t0)
+            if wait > 0:
+                time.sleep(wait)
+            self.run_one(r)
+            sync()
+            r.done = time.perf_counter() - t0
+        return order
+
+    def close(self):
+        snap = getattr(self, "_snap", ([], []))
+        for x in self.H + self.G + snap[0] + snap[1]:
+            x.close()
+
+
+def poisson_requests(cases, rate: float, count: int, seed: int, ins_frac: float = 0.6,
+                     size_lo: int = 1, size_hi: int = 4096):
+    """Requests with exponential inter-arrival times (mean 1/rate), sizes
+    log-uniform in [size_lo, size_hi], insertions with probability ins_frac.
+    An insertion takes the next edges of its graph's insertion pool (the
+    case's ins_*), a deletion edges of its dense graph not deleted before
+    (uniform).  Sizes are capped by what the graph has left."""
+    rng = np.random.default_rng(seed)
+    nxt = [0] * len(cases)
+    alive = [rng.permutation(len(c.g_src)) for c in cases]
+    dpos = [0] * len(cases)
+    t, out = 0.0, []
+    for _ in range(count):
+        t += rng.exponential(1.0 / rate)
+        g = int(rng.integers(len(cases)))
+        c = cases[g]
+        size = int(np.exp(rng.uniform(np.log(size_lo), np.log(size_hi + 1))))
+        if rng.random() < ins_frac:
+            k = min(size, len(c.ins_src) - nxt[g])
+            sl = slice(nxt[g], nxt[g] + k)
+            nxt[g] += k
+            out.append(Request(g, INSERT, c.ins_src[sl], c.ins_dst[sl], c.ins_w[sl], arrival=t))
+        else:
+            k = min(size, len(alive[g]) - dpos[g])
+            idx = alive[g][dpos[g]:dpos[g] + k]
+            dpos[g] += k
+            out.append(Request(g, DELETE, c.g_src[idx], c.g_dst[idx], arrival=t))
+    return out
+
+
+def latency_stats(done) -> dict:
+    lat = np.array([r.latency for r in done if r.done >= 0]) * 1e3
+    upd = sum(len(r.src) for r in done if r.done >= 0)
+    span = max(r.done for r in done) if done else 0.0
+    return {"requests": int(len(lat)), "updates": int(upd),
+            "p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
+            "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
+            "throughput_updates_per_s": upd / span if span > 0 else None}

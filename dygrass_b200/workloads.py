@@ -162,6 +162,51 @@ def rgg_many(k: int = 256, n_lo: int = 1000, n_hi: int = 200_000, seed: int = MA
                                   seed=seed)
 
 
+def rmat_case(scale: int, seed: int, n_ins: int, edge_factor: int = 16) -> GraphCase:
+    """An R-MAT graph (largest component, weights U[0.1, 10]) with sparsifier
+    = spanning tree + 5% off-tree and n_ins further R-MAT pairs inside the
+    component (repeats of existing edges included)."""
+    a, b, c = 0.57, 0.19, 0.19
+    n, s, d, w, idm = rmat(scale, edge_factor, a, b, c, 0.1, 10.0, seed)
+    idx = sparsifier(n, s, d, w, 0.05, seed + 1)
+    ps = np.empty(n_ins * 4, np.uint32)
+    pd = np.empty(n_ins * 4, np.uint32)
+    lib().dyg_synth_rmat_pairs(scale, n_ins * 4, a, b, c, seed + 2, _ptr(ps), _ptr(pd))
+    u, v = idm[ps], idm[pd]
+    ok = (u != 0xFFFFFFFF) & (v != 0xFFFFFFFF) & (u != v)
+    u, v = u[ok][:n_ins], v[ok][:n_ins]
+    rng = np.random.default_rng(seed + 3)
+    iw = rng.uniform(0.1, 10.0, len(u)).astype(np.float32)
+    return GraphCase(n, s, d, w, s[idx], d[idx], w[idx], u.astype(np.uint32), v.astype(np.uint32), iw)
+
+
+def serving_mix(k: int = 64, seed: int = MASTER_SEED):
+    """k resident graphs drawn in turn from the three generators: 3-D meshes
+    (k^3, k in [12, 48]), R-MAT (scale 10..16) and random geometric graphs
+    (n log-uniform in [1e3, 2e5]); each with an insertion pool of 0.5 n edges.
+    Returns (cases, insertion params, deletion params): threshold 100, 512
+    walkers, max_steps 100."""
+    rng = np.random.default_rng(seed)
+    cases = []
+    for i in range(k):
+        kind = i % 3
+        if kind == 0:
+            m = int(rng.integers(12, 49))
+            wl = mesh_3d(m, inserts=max(1, m ** 3 // 2), seed=seed + 31 * i)
+            cases.append(GraphCase(wl.n, wl.g_src, wl.g_dst, wl.g_w, wl.h_src, wl.h_dst, wl.h_w,
+                                   wl.ins_src, wl.ins_dst, wl.ins_w))
+        elif kind == 1:
+            sc = int(rng.integers(10, 17))
+            cases.append(rmat_case(sc, seed + 31 * i, n_ins=(1 << sc) // 2))
+        else:
+            n0 = int(np.exp(rng.uniform(np.log(1e3), np.log(2e5))))
+            n, s, d, w, is_, id_, iw = rgg(n0, 8.0, n0 // 2, seed + 31 * i)
+            idx = sparsifier(n, s, d, w, 0.10, seed + 31 * i + 1)
+            cases.append(GraphCase(n, s, d, w, s[idx], d[idx], w[idx], is_, id_, iw))
+    p = WalkParams.make(threshold=100.0, walkers=512, max_steps=100, seed=seed)
+    return cases, p, WalkParams.make(walkers=512, max_steps=100, seed=seed)
+
+
 @dataclass
 class MixedWorkload:
     name: str
