@@ -82,6 +82,9 @@ def parse():
     ap.add_argument("--mesh-k", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--shard", action="store_true",
+                    help="mesh: one graph, every batch split over the ranks (keys all-reduced), "
+                         "strong scaling; default N > 1 runs independent replicas")
     ap.add_argument("--no-plain", action="store_true",
                     help="rgg_many: skip timing the plain per-graph loop")
     ap.add_argument("--exhaustive", action="store_true",
@@ -280,7 +283,30 @@ def run_ours(args, rank, world, local_rank):
         G.copy_from(G0, sp)
         flush.fill_(rank + 1)
 
+    shard_back = None
+    if args.shard:
+        from dygrass_b200.shard import GpuBackend, allreduce_max, decremental_sharded, incremental_sharded
+        shard_back = GpuBackend(dev, stream=sp)
+        combine = allreduce_max() if world > 1 else (lambda k: k)
+        Bi, Bd = dyg.reference_batch_size(nin), dyg.reference_batch_size(max(ndel, 1))
+
+    def step_sharded():
+        for b0 in range(0, nin, Bi):
+            sl = slice(b0, min(b0 + Bi, nin))
+            fa, cd, ac = incremental_sharded(shard_back, H, G, d_is[sl], d_id[sl], d_iw[sl], b0,
+                                             W.params, rank, world, combine)
+            o_inc.accepted[sl] = ac
+        nrec = 0
+        for b0 in range(0, ndel, Bd):
+            sl = slice(b0, min(b0 + Bd, ndel))
+            st, cd, rx, ry, rk = decremental_sharded(shard_back, G, H, d_ds[sl], d_dd[sl], b0,
+                                                     W.dparams, rank, world, combine)
+            nrec += len(rx)
+        return nrec
+
     def step_device():
+        if shard_back is not None:
+            return step_sharded()
         dyg.incremental_stream(H, d_is, d_id, d_iw, W.params, G=G, stream=sp, out=o_inc)
         nrec = 0
         if ndel:
@@ -344,7 +370,7 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- end-to-end through host buffers (pinned), copies inside the region
     e2e = None
-    if not args.no_e2e:
+    if not args.no_e2e and not args.shard:
         pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
         h_is, h_id, h_iw = pin(W.ins_src), pin(W.ins_dst), pin(W.ins_w)
         h_ds, h_dd = pin(W.del_src), pin(W.del_dst)
@@ -1001,7 +1027,7 @@ def main():
                               "(profiles/roofline_traffic.json)"
     nin, ndel = res["nin"], res["ndel"]
     ms = res["ms_per_step"]
-    value = world * (nin + ndel) / (ms / 1e3)
+    value = (1 if args.shard else world) * (nin + ndel) / (ms / 1e3)
     moves = res["incr_moves"] + res["decr_moves"]
     cpu = None
     if not args.no_cpu_baseline and world == 1:
@@ -1012,8 +1038,10 @@ def main():
         "value": value, "unit": "edge_updates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators, dygrass_b200/workloads.py)",
+        **({"scaling": "strong"} if args.shard else {}),
         "config": dict(workload_config(W, args), l2="flushed between steps (256 MB write)",
-                       parallelism=f"replicas x{world}"),
+                       parallelism=(f"one graph, batches sharded x{world} (winner keys all-reduced)"
+                                    if args.shard else f"replicas x{world}")),
         "walker_steps_per_s": world * moves / (ms / 1e3),
         "breakdown": {"insertions_added": res["accepted"], "edges_recovered": res["recovered"],
                       "incr_walker_moves": res["incr_moves"], "decr_walker_moves": res["decr_moves"],

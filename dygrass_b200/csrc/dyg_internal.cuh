@@ -298,10 +298,18 @@ dyg_status decr_delete_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src,
                                const unsigned long long *uids, bool file_orient,
                                unsigned long long *halt, int32_t *status, float *cond,
                                cudaStream_t st);
+// keys_given (device, may be null): the walk list's winner keys, computed
+// elsewhere (a sharded batch); the walks are then skipped.
 dyg_status decr_walk_enqueue(dyg_graph *G, dyg_graph *H, uint32_t f0, uint32_t nf,
                              const uint32_t *F_dev, const dyg_walk_params &p,
                              unsigned long long *halt, uint32_t batch, uint32_t phase0,
-                             int32_t *status, float *cond, cudaStream_t st);
+                             int32_t *status, float *cond, cudaStream_t st,
+                             const unsigned long long *keys_given = nullptr);
+dyg_status incr_commit_enqueue(dyg_graph *H, dyg_graph *G, const uint32_t *src,
+                               const uint32_t *dst, const float *w, uint32_t n,
+                               const unsigned long long *keys, unsigned long long *halt,
+                               uint32_t batch, int32_t *found, float *cond, uint8_t *acc,
+                               cudaStream_t st);
 // Grows b to `bytes`, keeping its first `used` bytes.
 dyg_status grow_keep(Buf &b, size_t bytes, size_t used, cudaStream_t st);
 

@@ -430,23 +430,21 @@ dyg_status grow_keep(Buf &b, size_t bytes, size_t used, cudaStream_t st) {
 
 // Enqueues incremental batch `batch` (edges src/dst/w[0, n), update ids
 // uid0 + e).  Outputs go to found/cond/acc (device, may be null).
-dyg_status incr_enqueue(dyg_graph *H, dyg_graph *G, const uint32_t *src, const uint32_t *dst,
-                        const float *w, uint32_t n, uint64_t uid0,
-                        const unsigned long long *uids, const dyg_walk_params &p,
-                        unsigned long long *halt, uint32_t batch, int32_t *found, float *cond,
-                        uint8_t *acc, cudaStream_t st) {
+// Commit half of an incremental batch from its winner keys (keys[e] = 0: no
+// walker connected edge e): decode, scan of the accept flags in input order,
+// accepted half-edges to H [and every half-edge to G], reserved together.
+dyg_status incr_commit_enqueue(dyg_graph *H, dyg_graph *G, const uint32_t *src,
+                               const uint32_t *dst, const float *w, uint32_t n,
+                               const unsigned long long *keys, unsigned long long *halt,
+                               uint32_t batch, int32_t *found, float *cond, uint8_t *acc,
+                               cudaStream_t st) {
     Workspace &ws = H->ws;
-    DYG_TRY(ensure(ws.keys, sizeof(unsigned long long) * n));
     DYG_TRY(ensure(ws.flags, sizeof(uint32_t) * n));
     DYG_TRY(ensure(ws.pos, sizeof(uint32_t) * n));
     DYG_TRY(ensure(ws.hx, sizeof(uint32_t) * (size_t)n * 2));
     DYG_TRY(ensure(ws.hy, sizeof(uint32_t) * (size_t)n * 2));
     DYG_TRY(ensure(ws.hw, sizeof(float) * (size_t)n * 2));
-    unsigned long long *keys = ptr<unsigned long long>(ws.keys);
-    DYG_CUDA(cudaMemsetAsync(keys, 0, sizeof(unsigned long long) * n, st));
     DYG_CUDA(cudaMemsetAsync(ws.hx.p, 0xFF, sizeof(uint32_t) * (size_t)n * 2, st));
-    WalkJob job{halt, src, dst, w, uids, (unsigned long long)uid0, nullptr, n, kDomainIncr};
-    DYG_TRY(launch_walk(H, job, p, true, keys, st));
     k_incr_decode<<<blocks(n, 256), 256, 0, st>>>(halt, keys, n, found, cond, acc,
                                                    ptr<uint32_t>(ws.flags));
     count_launch();
@@ -472,6 +470,20 @@ dyg_status incr_enqueue(dyg_graph *H, dyg_graph *G, const uint32_t *src, const u
     DYG_CUDA(cudaGetLastError());
     return append_enqueue(H, LH, G, G ? &LG : nullptr, halt,
                           halt_code(batch, (uint32_t)kHaltArena, 0), st);
+}
+
+dyg_status incr_enqueue(dyg_graph *H, dyg_graph *G, const uint32_t *src, const uint32_t *dst,
+                        const float *w, uint32_t n, uint64_t uid0,
+                        const unsigned long long *uids, const dyg_walk_params &p,
+                        unsigned long long *halt, uint32_t batch, int32_t *found, float *cond,
+                        uint8_t *acc, cudaStream_t st) {
+    Workspace &ws = H->ws;
+    DYG_TRY(ensure(ws.keys, sizeof(unsigned long long) * n));
+    unsigned long long *keys = ptr<unsigned long long>(ws.keys);
+    DYG_CUDA(cudaMemsetAsync(keys, 0, sizeof(unsigned long long) * n, st));
+    WalkJob job{halt, src, dst, w, uids, (unsigned long long)uid0, nullptr, n, kDomainIncr};
+    DYG_TRY(launch_walk(H, job, p, true, keys, st));
+    return incr_commit_enqueue(H, G, src, dst, w, n, keys, halt, batch, found, cond, acc, st);
 }
 
 // Deletion stage of a decremental batch: delete every edge from G (swap with
@@ -525,7 +537,8 @@ dyg_status decr_delete_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src,
 dyg_status decr_walk_enqueue(dyg_graph *G, dyg_graph *H, uint32_t f0, uint32_t nf,
                              const uint32_t *F_dev, const dyg_walk_params &p,
                              unsigned long long *halt, uint32_t batch, uint32_t phase0,
-                             int32_t *status, float *cond, cudaStream_t st) {
+                             int32_t *status, float *cond, cudaStream_t st,
+                             const unsigned long long *keys_given) {
     if (nf == 0) return DYG_OK;
     Workspace &ws = G->ws;
     const uint32_t n = nf;
@@ -557,9 +570,13 @@ dyg_status decr_walk_enqueue(dyg_graph *G, dyg_graph *H, uint32_t f0, uint32_t n
 
     if (phase0 <= 0) {
         // walks on the updated G (main.cu:392, 420)
-        unsigned long long *keys = ptr<unsigned long long>(ws.keys);
-        DYG_CUDA(cudaMemsetAsync(keys, 0, sizeof(unsigned long long) * n, st));
-        DYG_TRY(launch_walk(G, job, p, false, keys, st));
+        const unsigned long long *keys = keys_given;
+        if (!keys) {
+            unsigned long long *k = ptr<unsigned long long>(ws.keys);
+            DYG_CUDA(cudaMemsetAsync(k, 0, sizeof(unsigned long long) * n, st));
+            DYG_TRY(launch_walk(G, job, p, false, k, st));
+            keys = k;
+        }
         DYG_TRY(launch_winner_paths(G, job, p, keys, n, stride, ptr<uint32_t>(ws.path_v),
                                     ptr<float>(ws.path_w), ptr<int32_t>(ws.path_len), st));
         k_decr_results<<<blocks(n, 256), 256, 0, st>>>(halt, keys, ptr<int32_t>(ws.path_len),

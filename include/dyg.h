@@ -215,6 +215,43 @@ dyg_status dyg_decremental_batch_ids(dyg_graph *G, dyg_graph *H, const uint32_t 
                                      float *conductance, uint32_t *rec_src, uint32_t *rec_dst,
                                      uint8_t *rec_kind, uint64_t rec_cap, uint64_t *n_rec,
                                      dyg_stream_t stream);
+/* A batch sharded over processes holding replicas of G and H (one per GPU):
+ * each rank computes the winner keys of a contiguous range of the batch, the
+ * ranks combine their key arrays (element-wise max; entries outside a rank's
+ * range are left as they were, so arrays that start at zero combine
+ * exactly), and every rank commits the whole batch.  Together they give what
+ * dyg_incremental_batch / dyg_decremental_batch give for the same ids.  Keys
+ * are device arrays of n (incremental) or n_walk (decremental) u64.
+ * Incremental: dyg_walk_keys on H (incremental = 1) for [lo, hi), then
+ * dyg_incremental_commit_keys (outputs device arrays).  Decremental:
+ * dyg_decremental_delete (status / conductance device arrays, kept for the
+ * commit; *n_walk = edges to walk), dyg_decremental_walk_keys for [lo, hi) of
+ * that walk list, then dyg_decremental_commit_keys with the same status /
+ * conductance arrays; no other call on G may come in between.  Splits
+ * random_walk_incremental/main.cu:301-328 and random_walk_decremental/main.cu:
+ * 392-408 at the point where the reference reads the kernel's results back. */
+dyg_status dyg_walk_keys(dyg_graph *X, const uint32_t *src, const uint32_t *dst, const float *w,
+                         const uint64_t *update_ids, uint64_t first_update_id, uint32_t n,
+                         uint32_t lo, uint32_t hi, uint32_t incremental,
+                         const dyg_walk_params *p, uint64_t *keys, dyg_stream_t stream);
+dyg_status dyg_incremental_commit_keys(dyg_graph *H, dyg_graph *G, const uint32_t *src,
+                                       const uint32_t *dst, const float *w, uint32_t n,
+                                       const uint64_t *keys, int32_t *found_at,
+                                       float *conductance, uint8_t *accepted,
+                                       dyg_stream_t stream);
+dyg_status dyg_decremental_delete(dyg_graph *G, dyg_graph *H, const uint32_t *src,
+                                  const uint32_t *dst, const uint64_t *update_ids,
+                                  uint64_t first_update_id, uint32_t n, int32_t *status,
+                                  float *conductance, uint32_t *n_walk, dyg_stream_t stream);
+dyg_status dyg_decremental_walk_keys(dyg_graph *G, uint32_t lo, uint32_t hi,
+                                     const dyg_walk_params *p, uint64_t *keys,
+                                     dyg_stream_t stream);
+dyg_status dyg_decremental_commit_keys(dyg_graph *G, dyg_graph *H, const dyg_walk_params *p,
+                                       const uint64_t *keys, uint32_t n_walk, int32_t *status,
+                                       float *conductance, uint32_t *rec_src, uint32_t *rec_dst,
+                                       uint8_t *rec_kind, uint64_t rec_cap, uint64_t *n_rec,
+                                       dyg_stream_t stream);
+
 /* Launch shape of the walk kernel for this process (an autotuner's knobs;
  * results do not depend on them): walkers each warp takes per fetch (a
  * multiple of 32 dividing the walker count; 0 = 32) and resident blocks per

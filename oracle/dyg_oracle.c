@@ -321,20 +321,26 @@ static uint64_t best_key(const orc_graph *g, uint32_t s, uint32_t t, float we, i
 
 /* ------------------------------------------------------------- incremental */
 
-uint64_t orc_incremental_batch(orc_graph *H, orc_graph *G, const uint32_t *src,
-                               const uint32_t *dst, const float *w, uint32_t n,
-                               uint64_t first_uid, const orc_params *p, int threads,
-                               int32_t *found_at, float *cond, uint8_t *accepted) {
-    uint64_t moves = 0;
-    uint64_t *keys = (uint64_t *)malloc((size_t)(n ? n : 1) * sizeof(uint64_t));
+void orc_walk_keys(const orc_graph *g, const uint32_t *src, const uint32_t *dst, const float *w,
+                   uint64_t first_uid, uint32_t lo, uint32_t hi, int incr, const orc_params *p,
+                   int threads, uint64_t *keys, uint64_t *moves) {
+    uint64_t mv_total = 0;
     if (threads < 1) threads = 1;
-#pragma omp parallel for schedule(dynamic, 1) num_threads(threads) reduction(+ : moves)
-    for (int64_t e = 0; e < (int64_t)n; ++e) {
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads) reduction(+ : mv_total)
+    for (int64_t e = lo; e < (int64_t)hi; ++e) {
         uint64_t mv = 0;
-        keys[e] = best_key(H, src[e], dst[e], w[e], 1, p, first_uid + (uint64_t)e, DOMAIN_INCR, &mv);
-        moves += mv;
+        keys[e] = best_key(g, src[e], dst[e], incr ? w[e] : 0.0f, incr, p, first_uid + (uint64_t)e,
+                           incr ? DOMAIN_INCR : DOMAIN_DECR, &mv);
+        mv_total += mv;
     }
-    /* commit in input order (gpu_graph.cuh:297-329): add iff no path */
+    if (moves) *moves = mv_total;
+}
+
+/* commit in input order (gpu_graph.cuh:297-329): add iff no path */
+void orc_incremental_commit_keys(orc_graph *H, orc_graph *G, const uint32_t *src,
+                                 const uint32_t *dst, const float *w, uint32_t n,
+                                 const uint64_t *keys, int32_t *found_at, float *cond,
+                                 uint8_t *accepted) {
     for (uint32_t e = 0; e < n; ++e) {
         uint64_t k = keys[e];
         if (found_at) found_at[e] = k ? (int32_t)(k & 0x3FFFFFu) : -1;
@@ -351,6 +357,16 @@ uint64_t orc_incremental_batch(orc_graph *H, orc_graph *G, const uint32_t *src,
             row_append(G, dst[e], src[e], w[e]);
         }
     }
+}
+
+uint64_t orc_incremental_batch(orc_graph *H, orc_graph *G, const uint32_t *src,
+                               const uint32_t *dst, const float *w, uint32_t n,
+                               uint64_t first_uid, const orc_params *p, int threads,
+                               int32_t *found_at, float *cond, uint8_t *accepted) {
+    uint64_t moves = 0;
+    uint64_t *keys = (uint64_t *)malloc((size_t)(n ? n : 1) * sizeof(uint64_t));
+    orc_walk_keys(H, src, dst, w, first_uid, 0, n, 1, p, threads, keys, &moves);
+    orc_incremental_commit_keys(H, G, src, dst, w, n, keys, found_at, cond, accepted);
     free(keys);
     return moves;
 }
@@ -468,12 +484,13 @@ static void walk_ends(const uint32_t *src, const uint32_t *dst, uint32_t e, int 
 static uint64_t decr_walk(orc_graph *G, orc_graph *H, const uint32_t *src, const uint32_t *dst,
                           const uint32_t *filt, uint32_t nf, uint64_t first_uid, int file_orient,
                           const orc_params *p, int threads, int32_t *status, float *cond,
-                          rec_t *rc) {
+                          rec_t *rc, const uint64_t *keys_in) {
     uint64_t moves = 0;
     uint64_t *keys = (uint64_t *)malloc((size_t)(nf ? nf : 1) * sizeof(uint64_t));
     if (threads < 1) threads = 1;
+    if (keys_in) memcpy(keys, keys_in, (size_t)nf * sizeof(uint64_t));
 #pragma omp parallel for schedule(dynamic, 1) num_threads(threads) reduction(+ : moves)
-    for (int64_t f = 0; f < (int64_t)nf; ++f) {
+    for (int64_t f = 0; f < (int64_t)(keys_in ? 0 : nf); ++f) {
         uint32_t e = filt[f], a, b;
         walk_ends(src, dst, e, file_orient, &a, &b);
         uint64_t mv = 0;
@@ -541,7 +558,8 @@ uint64_t orc_decremental_batch(orc_graph *G, orc_graph *H, const uint32_t *src,
     uint32_t nf = decr_delete(G, H, src, dst, n, status, cond, filt);
     rec_t rc = {0};
     rc.cap_out = rec_cap; rc.out_a = rec_src; rc.out_b = rec_dst; rc.out_kind = rec_kind;
-    uint64_t moves = decr_walk(G, H, src, dst, filt, nf, first_uid, 0, p, threads, status, cond, &rc);
+    uint64_t moves = decr_walk(G, H, src, dst, filt, nf, first_uid, 0, p, threads, status, cond, &rc,
+                               NULL);
     if (n_rec) *n_rec = rc.n;
     free(filt);
     return moves;
@@ -635,12 +653,43 @@ uint64_t orc_stream_file(orc_graph *G, orc_graph *H, uint32_t op, const uint32_t
         for (uint32_t c0 = 0; c0 < nl; c0 += chunk) {
             uint32_t c1 = nl - c0 < chunk ? nl : c0 + chunk;
             moves += decr_walk(G, H, src, dst, list + c0, c1 - c0, first_uid, 1, p, threads,
-                               status, cond, &rc);
+                               status, cond, &rc, NULL);
         }
         if (n_rec) *n_rec = rc.n;
     }
     free(list);
     return moves;
+}
+
+uint32_t orc_decremental_delete(orc_graph *G, orc_graph *H, const uint32_t *src,
+                                const uint32_t *dst, uint32_t n, int32_t *status, float *cond,
+                                uint32_t *walk_list) {
+    return decr_delete(G, H, src, dst, n, status, cond, walk_list);
+}
+
+void orc_decremental_walk_list_keys(const orc_graph *G, const uint32_t *src, const uint32_t *dst,
+                                    const uint32_t *walk_list, uint32_t lo, uint32_t hi,
+                                    uint64_t first_uid, const orc_params *p, int threads,
+                                    uint64_t *keys) {
+    if (threads < 1) threads = 1;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
+    for (int64_t f = lo; f < (int64_t)hi; ++f) {
+        uint32_t e = walk_list[f], a, b;
+        walk_ends(src, dst, e, 0, &a, &b);
+        uint64_t mv = 0;
+        keys[f] = best_key(G, a, b, 0.0f, 0, p, first_uid + e, DOMAIN_DECR, &mv);
+    }
+}
+
+void orc_decremental_commit_keys(orc_graph *G, orc_graph *H, const uint32_t *src,
+                                 const uint32_t *dst, const uint32_t *walk_list, uint32_t nf,
+                                 uint64_t first_uid, const orc_params *p, const uint64_t *keys,
+                                 int32_t *status, float *cond, uint32_t *rec_src, uint32_t *rec_dst,
+                                 uint8_t *rec_kind, uint64_t rec_cap, uint64_t *n_rec) {
+    rec_t rc = {0};
+    rc.cap_out = rec_cap; rc.out_a = rec_src; rc.out_b = rec_dst; rc.out_kind = rec_kind;
+    decr_walk(G, H, src, dst, walk_list, nf, first_uid, 0, p, 1, status, cond, &rc, keys);
+    if (n_rec) *n_rec = rc.n;
 }
 
 uint64_t orc_decremental_stream(orc_graph *G, orc_graph *H, const uint32_t *src,

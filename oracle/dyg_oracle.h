@@ -117,6 +117,32 @@ uint64_t orc_stream_file(orc_graph *G, orc_graph *H, uint32_t op, const uint32_t
                          float *cond, uint32_t *rec_src, uint32_t *rec_dst, uint8_t *rec_kind,
                          uint64_t rec_cap, uint64_t *n_rec);
 
+/* The batch functions in two halves, for a batch sharded over processes:
+ * winner keys of edges [lo, hi) (incr: walks on H with the distortion test,
+ * else on the graph given, endpoints as given), then the commit from a full
+ * key array.  Decremental: the deletion stage lists the edges to walk
+ * (returns their count), keys for [lo, hi) of that list (min -> max), then
+ * the commit (winner paths, recovery, fallback) from the full key array. */
+void orc_walk_keys(const orc_graph *g, const uint32_t *src, const uint32_t *dst, const float *w,
+                   uint64_t first_uid, uint32_t lo, uint32_t hi, int incr, const orc_params *p,
+                   int threads, uint64_t *keys, uint64_t *moves);
+void orc_incremental_commit_keys(orc_graph *H, orc_graph *G, const uint32_t *src,
+                                 const uint32_t *dst, const float *w, uint32_t n,
+                                 const uint64_t *keys, int32_t *found_at, float *cond,
+                                 uint8_t *accepted);
+uint32_t orc_decremental_delete(orc_graph *G, orc_graph *H, const uint32_t *src,
+                                const uint32_t *dst, uint32_t n, int32_t *status, float *cond,
+                                uint32_t *walk_list);
+void orc_decremental_walk_list_keys(const orc_graph *G, const uint32_t *src, const uint32_t *dst,
+                                    const uint32_t *walk_list, uint32_t lo, uint32_t hi,
+                                    uint64_t first_uid, const orc_params *p, int threads,
+                                    uint64_t *keys);
+void orc_decremental_commit_keys(orc_graph *G, orc_graph *H, const uint32_t *src,
+                                 const uint32_t *dst, const uint32_t *walk_list, uint32_t nf,
+                                 uint64_t first_uid, const orc_params *p, const uint64_t *keys,
+                                 int32_t *status, float *cond, uint32_t *rec_src, uint32_t *rec_dst,
+                                 uint8_t *rec_kind, uint64_t rec_cap, uint64_t *n_rec);
+
 /* Path of one walker of a decremental walk (for tests): returns found_at or
  * -1 and writes up to max_steps+1 vertices into path. */
 int32_t orc_decremental_walk_path(const orc_graph *G, uint32_t s, uint32_t t,

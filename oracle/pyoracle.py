@@ -61,6 +61,12 @@ def lib() -> C.CDLL:
             "orc_decremental_walk_path": ([vp, u32, u32, u64, u32, P, vp, C.POINTER(C.c_float)], C.c_int32),
             "orc_max_threads": ([], C.c_int),
             "orc_stream_default_chunk": ([u32], u32),
+            "orc_walk_keys": ([vp, vp, vp, vp, u64, u32, u32, C.c_int, P, C.c_int, vp, vp], None),
+            "orc_incremental_commit_keys": ([vp, vp, vp, vp, vp, u32, vp, vp, vp, vp], None),
+            "orc_decremental_delete": ([vp, vp, vp, vp, u32, vp, vp, vp], u32),
+            "orc_decremental_walk_list_keys": ([vp, vp, vp, vp, u32, u32, u64, P, C.c_int, vp], None),
+            "orc_decremental_commit_keys": ([vp, vp, vp, vp, vp, u32, u64, P, vp, vp, vp, vp, vp, vp,
+                                             u64, C.POINTER(u64)], None),
             "orc_stream_file": ([vp, vp, u32, vp, vp, vp, u32, u64, u32, P, C.c_int, vp, vp, vp, vp,
                                  vp, u64, C.POINTER(u64)], u64),
         }
@@ -188,3 +194,67 @@ def stream_file(G: OGraph, H: OGraph, op, src, dst, w, params, first_uid=0, chun
 
 def stream_default_chunk(n_vertices) -> int:
     return int(lib().orc_stream_default_chunk(int(n_vertices)))
+
+
+class ShardBackend:
+    """The oracle behind dygrass_b200.shard's backend interface (keys are
+    torch CPU int64 tensors, exchanged with gloo in tests)."""
+
+    def __init__(self, threads=None):
+        self.th = threads or max_threads()
+        self._last = None
+
+    def zeros_keys(self, n):
+        import torch
+        return torch.zeros(max(n, 1), dtype=torch.int64)
+
+    @staticmethod
+    def _u64(keys):
+        return keys.numpy().view(np.uint64)
+
+    def walk_keys(self, H, src, dst, w, first_uid, lo, hi, p, keys):
+        src = np.ascontiguousarray(src, np.uint32)
+        dst = np.ascontiguousarray(dst, np.uint32)
+        w = np.ascontiguousarray(w, np.float32)
+        P = Params.from_walk_params(p)
+        lib().orc_walk_keys(H.h, _p(src), _p(dst), _p(w), first_uid, lo, hi, 1, C.byref(P), self.th,
+                            _p(self._u64(keys)), None)
+
+    def incr_commit(self, H, G, src, dst, w, keys):
+        src = np.ascontiguousarray(src, np.uint32)
+        dst = np.ascontiguousarray(dst, np.uint32)
+        w = np.ascontiguousarray(w, np.float32)
+        n = len(src)
+        fa, cd, ac = np.empty(n, np.int32), np.empty(n, np.float32), np.empty(n, np.uint8)
+        lib().orc_incremental_commit_keys(H.h, G.h if G else None, _p(src), _p(dst), _p(w), n,
+                                          _p(self._u64(keys)), _p(fa), _p(cd), _p(ac))
+        return fa, cd, ac
+
+    def decr_delete(self, G, H, src, dst, first_uid):
+        src = np.ascontiguousarray(src, np.uint32)
+        dst = np.ascontiguousarray(dst, np.uint32)
+        n = len(src)
+        st, cd = np.empty(n, np.int32), np.empty(n, np.float32)
+        wl = np.empty(max(n, 1), np.uint32)
+        nf = lib().orc_decremental_delete(G.h, H.h, _p(src), _p(dst), n, _p(st), _p(cd), _p(wl))
+        self._last = (src, dst, wl, first_uid)
+        return nf, (st, cd)
+
+    def decr_walk_keys(self, G, lo, hi, p, keys):
+        src, dst, wl, first_uid = self._last
+        P = Params.from_walk_params(p)
+        lib().orc_decremental_walk_list_keys(G.h, _p(src), _p(dst), _p(wl), lo, hi, first_uid,
+                                             C.byref(P), self.th, _p(self._u64(keys)))
+
+    def decr_commit(self, G, H, p, keys, n_walk, state, rec_cap):
+        src, dst, wl, first_uid = self._last
+        st, cd = state
+        P = Params.from_walk_params(p)
+        rx, ry, rk = (np.empty(max(rec_cap, 1), np.uint32), np.empty(max(rec_cap, 1), np.uint32),
+                      np.empty(max(rec_cap, 1), np.uint8))
+        nr = C.c_uint64()
+        lib().orc_decremental_commit_keys(G.h, H.h, _p(src), _p(dst), _p(wl), n_walk, first_uid,
+                                          C.byref(P), _p(self._u64(keys)), _p(st), _p(cd), _p(rx),
+                                          _p(ry), _p(rk), rec_cap, C.byref(nr))
+        k = nr.value
+        return st, cd, rx[:k].copy(), ry[:k].copy(), rk[:k].copy()
