@@ -183,14 +183,27 @@ class ClockSampler:
         self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device_index}.csv")
 
     def start(self):
+        """Starts nvidia-smi and returns once its first sample is written, so
+        that the samples after it fall inside the timed region."""
+        self.n0 = 0
         try:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
-                 "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+                 "-lms", "50"], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        t0 = time.time()
+        while time.time() - t0 < 10.0 and self.proc.poll() is None:
+            self.f.flush()
+            with open(self.path) as g:
+                n = sum(1 for _ in g)
+            if n:
+                self.n0 = n
+                return
+            time.sleep(0.01)
 
     def stop(self):
         if self.proc is None:
@@ -203,7 +216,9 @@ class ClockSampler:
         self.f.close()
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        lines = open(self.path).read().splitlines()
+        inside = lines[self.n0:]
+        for line in inside or lines:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -216,7 +231,8 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm) if inside else 0,
+                "when": "during the timed region" if inside else "just before the timed region"}
 
 
 # ------------------------------------------------------------- our arm

@@ -10,7 +10,8 @@
 // edge, and the warp pulls a new edge from a global counter when the current
 // one is handed out.  The per-edge winner (max 1/R, lowest walker id) is a
 // 64-bit key reduced with atomicMax, so no barrier and no global scratch
-// arrays are needed.
+// arrays are needed.  Lanes refill in step with one another (every fourth
+// warp iteration), so the random-number blocks are drawn by whole warps.
 //
 // Draw d of walker k of update u is word d&3 of
 // Philox4x32-10({d>>2, k, u_lo, u_hi | domain<<24}, seed): any walker can be
@@ -131,9 +132,16 @@ __device__ __forceinline__ int step_once(Walker &s, const uint2 *__restrict__ de
         const uint32_t idx = first ? (r % deg) : (r % (deg - 1u));
         at = d.x + idx;
         sl = __ldg(slots + at);
-        if (!first && sl.x == s.prev) {
-            at = d.x + deg - 1u;
-            sl = __ldg(slots + at);
+        if (!first) {
+            // the row's last slot is loaded beside the drawn one, not after
+            // it: some lane of a warp lands on its previous vertex in almost
+            // every step, and a dependent reload would hold the whole warp
+            const uint32_t at_last = d.x + deg - 1u;
+            const uint2 sl_last = __ldg(slots + at_last);
+            if (sl.x == s.prev) {
+                at = at_last;
+                sl = sl_last;
+            }
         }
     } else {
         unsigned long long total = 0ull;
@@ -209,9 +217,19 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(WalkArgs a) {
     s.we = 0.f;
     uint32_t moves = 0u, walks = 0u;
 
+    // Walkers start only on warp iterations T = 0 mod 4.  Every walker moves
+    // once per iteration, so all of a warp's walkers then stand at steps
+    // 1 mod 4 together and draw their next Philox block in the same
+    // iteration: the block (a quarter of the kernel's instructions when
+    // computed) is run once per four iterations by the whole warp instead of
+    // in almost every iteration for a few lanes, and refills are batched.
+    // A lane waits at most three iterations; an empty warp refills at once.
+    uint32_t T = 0u;
     while (true) {
         uint32_t free_mask = __ballot_sync(kFull, !active);
-        while (free_mask != 0u && !exhausted) {
+        if (free_mask == kFull) T = 0u;
+        const bool refill = (T & 3u) == 0u;
+        while (free_mask != 0u && !exhausted && refill) {
             if (c_next >= c_end) {
                 unsigned long long c = 0ull;
                 if (lane == 0u) c = atomicAdd(work, 1ull);
@@ -297,6 +315,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(WalkArgs a) {
                 }
             }
         }
+        ++T;
     }
     const uint32_t wm = __reduce_add_sync(kFull, moves);
     const uint32_t ww = __reduce_add_sync(kFull, walks);
