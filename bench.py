@@ -1035,9 +1035,10 @@ def main():
     tpath = os.path.join(ROOT, "profiles", "roofline_traffic.json")
     if os.path.exists(tpath):
         for t in json.load(open(tpath)).get("entries", []):
-            if t.get("workload") == args.workload and t.get("mesh_k", args.mesh_k) == args.mesh_k \
+            opts = ("mesh_k", "rgg_graphs", "rgg_n_hi", "rmat_scale", "rmat_updates", "serve_requests")
+            if t.get("workload") == args.workload and t.get("kernel") == res["dom_kernel"] \
                     and t.get("exhaustive", False) == args.exhaustive \
-                    and t.get("kernel") == res["dom_kernel"]:
+                    and all(t[o] == getattr(args, o) for o in opts if o in t):
                 traffic = t.get("dram_bytes_per_launch")
                 traffic_src = "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch " \
                               "(profiles/roofline_traffic.json)"
