@@ -825,6 +825,22 @@ def run_serve(args, rank, world, local_rank):
     plain_sat = latency_stats(replay(P, None))
     P.close()
     S.close()
+    # the same steps scheduled from Python (per-step library calls), for comparison
+    Sp = Server(W.cases, W.params, W.dparams, device=local_rank, native=False)
+    Sp.snapshot()
+    py_ms = []
+    for _ in range(2):
+        Sp.restore()
+        flush.fill_(rank + 1)
+        sync()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        Sp.serve(_arrive(W.requests, None))
+        e1.record(stream)
+        e1.synchronize()
+        py_ms.append(e0.elapsed_time(e1))
+    Sp.close()
     res = {
         "ms_per_step": ms, "steps_ms": times, "nin": n_upd, "ndel": 0, "accepted": None,
         "recovered": 0, "incr_moves": moves, "decr_moves": 0.0,
@@ -843,7 +859,9 @@ def run_serve(args, rank, world, local_rank):
         "dom_ms_per_launch": (prof["incr_walk_ms"] + prof["decr_walk_ms"]) / max(
             prof["decr_walk_launches"] + prof["incr_walk_launches"], 1),
         "serving": {"server_steps_per_replay": steps, "capacity_req_per_s": capacity,
-                    "sweep": sweep, "plain_saturated": plain_sat},
+                    "sweep": sweep, "plain_saturated": plain_sat,
+                    "python_scheduler_ms_per_replay": float(np.mean(py_ms)),
+                    "scheduler": "native (include/dyg_serve.h): loop thread, pinned staging"},
         "W": W,
     }
     return res

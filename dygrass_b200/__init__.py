@@ -21,6 +21,7 @@ _PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_PKG, "libdygrass.so")
 
 DYG_OK = 0
+DYG_EINVAL, DYG_ENOMEM, DYG_ECUDA, DYG_ERANGE, DYG_ESTATE = 1, 2, 3, 4, 5
 STATUS_NAMES = {0: "DYG_OK", 1: "DYG_EINVAL", 2: "DYG_ENOMEM", 3: "DYG_ECUDA", 4: "DYG_ERANGE",
                 5: "DYG_ESTATE", 6: "DYG_ENOTSUP", 7: "DYG_EIO"}
 TRANSITION_UNIFORM = 0
@@ -84,6 +85,14 @@ class Profile(C.Structure):
     _fields_ = [("incr_walk_ms", C.c_double), ("decr_walk_ms", C.c_double),
                 ("other_walk_ms", C.c_double), ("incr_walk_launches", C.c_uint64),
                 ("decr_walk_launches", C.c_uint64), ("other_walk_launches", C.c_uint64)]
+
+
+class ServerDone(C.Structure):
+    """A completed server request (dyg_server_done, include/dyg_serve.h)."""
+    _fields_ = [("tag", C.c_uint64), ("graph", C.c_uint32), ("op", C.c_uint32), ("n", C.c_uint32),
+                ("status", C.c_int32), ("first_update_id", C.c_uint64), ("n_rec", C.c_uint64),
+                ("step", C.c_uint64), ("t_submit_ns", C.c_uint64), ("t_start_ns", C.c_uint64),
+                ("t_done_ns", C.c_uint64)]
 
 
 class GraphOpts(C.Structure):
@@ -166,6 +175,22 @@ def lib() -> C.CDLL:
         "dyg_kernel_launches": ([], u64),
         "dyg_incremental_walk_noalloc": ([vp, vp, vp, vp, u32, u64, C.POINTER(WalkParams), vp, vp, vp, vp],
                                          C.c_int),
+        "dyg_server_create": ([vp, vp, u32, vp, C.POINTER(WalkParams), C.POINTER(WalkParams), vp,
+                               C.POINTER(vp)], C.c_int),
+        "dyg_server_destroy": ([vp], C.c_int),
+        "dyg_server_submit": ([vp, u64, u32, u32, vp, vp, vp, u32], C.c_int),
+        "dyg_server_submit_many": ([vp, u32, vp, vp, vp, vp, vp, vp, vp], C.c_int),
+        "dyg_server_step": ([vp, C.POINTER(u32)], C.c_int),
+        "dyg_server_start": ([vp], C.c_int),
+        "dyg_server_stop": ([vp], C.c_int),
+        "dyg_server_drain": ([vp, C.c_double], C.c_int),
+        "dyg_server_pending": ([vp], u32),
+        "dyg_server_poll": ([vp, C.POINTER(ServerDone), u32, C.POINTER(u32)], C.c_int),
+        "dyg_server_fetch": ([vp, u64, vp, vp, vp, vp, vp, vp, u64], C.c_int),
+        "dyg_server_reset": ([vp], C.c_int),
+        "dyg_server_steps": ([vp], u64),
+        "dyg_server_now_ns": ([vp], u64),
+        "dyg_server_last_error": ([vp], C.c_char_p),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -20,7 +20,8 @@ BIN_INCR = os.path.join(PKG, "bin", "incremental_update")
 BIN_DECR = os.path.join(PKG, "bin", "decremental_update")
 BIN_DYN = os.path.join(PKG, "bin", "dynamic_update")
 
-CUDA_SOURCES = ["walk.cu", "graph.cu", "rowops.cu", "pipeline.cu", "capi.cu", "noalloc.cu", "stream.cu", "shard.cu"]
+CUDA_SOURCES = ["walk.cu", "graph.cu", "rowops.cu", "pipeline.cu", "capi.cu", "noalloc.cu", "stream.cu", "shard.cu",
+                "server.cu"]
 HOST_SOURCES = ["synth.cpp", "mtx_io.cpp", "kappa.cpp"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -184,6 +184,13 @@ void free_graph(dyg_graph *G) {
 }
 
 }  // namespace
+
+dyg_status check_walk_params(const dyg_walk_params *p) { return check_params(p); }
+
+dyg_status device_errors(dyg_graph *G, cudaStream_t st) {
+    return G->ws.host_scalars[S_ERR] ? check_device_errors(G, st) : DYG_OK;
+}
+
 }  // namespace dyg
 
 using namespace dyg;

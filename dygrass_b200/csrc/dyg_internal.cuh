@@ -282,6 +282,13 @@ dyg_status launch_fallback_walks(dyg_graph *G, const unsigned long long *halt,
                                  const dyg_walk_params &p, uint32_t *cx, uint32_t *cy, float *cw,
                                  cudaStream_t st);
 
+// --- capi.cu
+// After a run: DYG_OK, or the error the kernels flagged in G's scalars (last
+// read by the run), which are cleared.
+dyg_status device_errors(dyg_graph *G, cudaStream_t st);
+// DYG_OK, or DYG_EINVAL with the message set, for walk parameters.
+dyg_status check_walk_params(const dyg_walk_params *p);
+
 // --- pipeline.cu
 // uids (device, may be null): per-edge update ids instead of uid_base + e.
 dyg_status incremental_run(dyg_graph *H, dyg_graph *G, const uint32_t *src, const uint32_t *dst,

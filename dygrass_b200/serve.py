@@ -2,15 +2,21 @@
 
 Requests are update batches for one graph (insertions or deletions, any
 size).  The server keeps every admitted graph resident in one union graph
-(each at its own vertex offset, as in multi.py) with its update counter on
-the host, so a graph's random streams depend only on its own history.  Each
-scheduler step takes the oldest pending request of every graph that has one,
-runs all insertion requests of the step as one dyg_incremental_batch_ids
-launch and all deletion requests as one dyg_decremental_batch_ids launch, and
-completes them; requests that arrive meanwhile join the next step.  Graphs
-are disjoint and a graph's requests run in arrival order, one per step, so
-every request gets exactly the result it gets when run alone on its graph's
-own handles (tested).
+(each at its own vertex offset, as in multi.py) with its own update counter,
+so a graph's random streams depend only on its own history.  Each scheduler
+step takes the oldest pending request of every graph that has one, runs all
+insertion requests of the step as one incremental batch and all deletion
+requests as one decremental batch, and completes them; requests that arrive
+meanwhile join the next step.  Graphs are disjoint and a graph's requests run
+in arrival order, one per step, so every request gets exactly the result it
+gets when run alone on its graph's own handles (tested).
+
+The scheduler is native (include/dyg_serve.h, csrc/server.cu): requests are
+copied into its per-graph queues, its loop thread runs a step whenever one is
+pending, stages each step through page-locked memory and splits the results
+per request, and this module submits, polls and fetches.  Server(native=False)
+runs the same steps from Python over dyg_incremental_batch_ids /
+dyg_decremental_batch_ids (kept to measure the scheduler against).
 
 Admission: graphs are admitted in the given order while their estimated
 device footprint (dense graph and sparsifier arenas and descriptors, plus
@@ -19,14 +25,15 @@ are refused.
 """
 from __future__ import annotations
 
+import ctypes as C
 import time
 from collections import deque
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 
 import numpy as np
 
-from . import (DecrementalResult, Graph, IncrementalResult, WalkParams, decremental_batch_ids,
-               incremental_batch_ids)
+from . import (DygError, Graph, ServerDone, WalkParams, _check, _ptr, decremental_batch_ids,
+               incremental_batch_ids, lib)
 
 INSERT, DELETE = 0, 1
 
@@ -46,11 +53,20 @@ class Request:
     conductance: np.ndarray | None = None
     accepted: np.ndarray | None = None
     status: np.ndarray | None = None        # deletions
-    recovered: list = field(default_factory=list)   # (x, y, kind), local ids
+    rec_src: np.ndarray | None = None       # recovered edges, local ids, commit order
+    rec_dst: np.ndarray | None = None
+    rec_kind: np.ndarray | None = None
 
     @property
     def latency(self) -> float:
         return self.done - self.arrival
+
+    @property
+    def recovered(self) -> list:
+        """[(x, y, kind), ...] of the recovered edges."""
+        if self.rec_src is None:
+            return []
+        return list(zip(self.rec_src.tolist(), self.rec_dst.tolist(), self.rec_kind.tolist()))
 
 
 def footprint_bytes(n: int, g_edges: int, h_edges: int, headroom: float = 0.5,
@@ -64,7 +80,7 @@ def footprint_bytes(n: int, g_edges: int, h_edges: int, headroom: float = 0.5,
 
 class Server:
     def __init__(self, cases, iparams: WalkParams, dparams: WalkParams,
-                 hbm_budget: float = float("inf"), device: int = -1):
+                 hbm_budget: float = float("inf"), device: int = -1, native: bool = True):
         self.iparams, self.dparams = iparams, dparams
         self.admitted, offs, used = [], [0], 0
         for i, c in enumerate(cases):
@@ -86,12 +102,32 @@ class Server:
         self.G = Graph.from_edges(n, cat([c.g_src + o for c, o in zip(sel, offs)], np.uint32),
                                   cat([c.g_dst + o for c, o in zip(sel, offs)], np.uint32),
                                   cat([c.g_w for c in sel], np.float32), device=device)
-        self.queues = {g: deque() for g in self.admitted}
-        self.uid_next = {g: 0 for g in self.admitted}
-        self.steps = 0
+        self.native = native
+        self._srv = None
+        if native:
+            h = C.c_void_p()
+            o32 = np.ascontiguousarray(self.offsets, np.uint32)
+            _check(lib().dyg_server_create(self.G.handle, self.H.handle, len(self.admitted), _ptr(o32),
+                                           C.byref(iparams), C.byref(dparams), None, C.byref(h)),
+                   "dyg_server_create")
+            self._srv = h
+            self._tags = {}          # tag -> Request, submitted and not yet collected
+            self._next_tag = 0
+            self._poll = (ServerDone * 1024)()
+            self._t0_ns = 0
+        else:
+            self.queues = {g: deque() for g in self.admitted}
+            self.uid_next = {g: 0 for g in self.admitted}
+            self._steps = 0
         self.t0 = time.perf_counter()
 
+    @property
+    def steps(self) -> int:
+        return int(lib().dyg_server_steps(self._srv)) if self.native else self._steps
+
     def now(self) -> float:
+        if self.native:
+            return (lib().dyg_server_now_ns(self._srv) - self._t0_ns) * 1e-9
         return time.perf_counter() - self.t0
 
     def snapshot(self):
@@ -102,20 +138,102 @@ class Server:
         """Back to the snapshot: graphs, update counters, empty queues."""
         self.H.copy_from(self._snap[0], stream)
         self.G.copy_from(self._snap[1], stream)
-        self.uid_next = {g: 0 for g in self.admitted}
-        for q in self.queues.values():
-            q.clear()
-        self.steps = 0
+        if self.native:
+            _check(lib().dyg_server_reset(self._srv), "dyg_server_reset")
+            self._tags.clear()
+        else:
+            self.uid_next = {g: 0 for g in self.admitted}
+            for q in self.queues.values():
+                q.clear()
+            self._steps = 0
 
     def submit(self, r: Request) -> bool:
         """Queues a request; False if its graph was not admitted."""
-        if r.graph not in self.queues:
+        if r.graph not in self.slot:
             return False
-        self.queues[r.graph].append(r)
+        if not self.native:
+            self.queues[r.graph].append(r)
+            return True
+        src = np.ascontiguousarray(r.src, np.uint32)
+        dst = np.ascontiguousarray(r.dst, np.uint32)
+        w = np.ascontiguousarray(r.w, np.float32) if r.op == INSERT else None
+        tag = self._next_tag
+        self._next_tag += 1
+        _check(lib().dyg_server_submit(self._srv, tag, self.slot[r.graph], r.op, _ptr(src), _ptr(dst),
+                                       _ptr(w), len(src)), "dyg_server_submit")
+        self._tags[tag] = r
         return True
 
+    def submit_many(self, reqs) -> None:
+        """Queues requests in order, with one call for the native server;
+        requests of graphs not admitted get done = -1."""
+        ok = []
+        for r in reqs:
+            if r.graph in self.slot:
+                ok.append(r)
+            else:
+                r.done = -1.0
+        if not self.native:
+            for r in ok:
+                self.queues[r.graph].append(r)
+            return
+        if not ok:
+            return
+        lens = np.fromiter((len(r.src) for r in ok), np.uint64, len(ok))
+        offs = np.zeros(len(ok) + 1, np.uint64)
+        np.cumsum(lens, out=offs[1:])
+        src = np.concatenate([np.asarray(r.src, np.uint32) for r in ok])
+        dst = np.concatenate([np.asarray(r.dst, np.uint32) for r in ok])
+        w = np.concatenate([np.asarray(r.w, np.float32) if r.op == INSERT
+                            else np.zeros(len(r.src), np.float32) for r in ok])
+        tags = np.arange(self._next_tag, self._next_tag + len(ok), dtype=np.uint64)
+        graphs = np.fromiter((self.slot[r.graph] for r in ok), np.uint32, len(ok))
+        ops = np.fromiter((r.op for r in ok), np.uint32, len(ok))
+        _check(lib().dyg_server_submit_many(self._srv, len(ok), _ptr(tags), _ptr(graphs), _ptr(ops),
+                                            _ptr(offs), _ptr(src), _ptr(dst), _ptr(w)),
+               "dyg_server_submit_many")
+        self._next_tag += len(ok)
+        for t, r in zip(tags.tolist(), ok):
+            self._tags[t] = r
+
     def pending(self) -> bool:
+        if self.native:
+            return lib().dyg_server_pending(self._srv) > 0
         return any(self.queues.values())
+
+    def _collect(self) -> list:
+        """Completed requests of the native server, with their results."""
+        L = lib()
+        out = []
+        while True:
+            k = C.c_uint32()
+            _check(L.dyg_server_poll(self._srv, self._poll, len(self._poll), C.byref(k)),
+                   "dyg_server_poll")
+            for i in range(k.value):
+                d = self._poll[i]
+                r = self._tags.pop(d.tag)
+                if d.status != 0:
+                    raise DygError(d.status, "server step", L.dyg_server_last_error(self._srv).decode())
+                m = d.n
+                r.first_update_id = d.first_update_id
+                r.done = (d.t_done_ns - self._t0_ns) * 1e-9
+                cd = np.empty(m, np.float32)
+                if r.op == INSERT:
+                    fa, ac = np.empty(m, np.int32), np.empty(m, np.uint8)
+                    _check(L.dyg_server_fetch(self._srv, d.tag, _ptr(fa), _ptr(cd), _ptr(ac), None, None,
+                                              None, 0), "dyg_server_fetch")
+                    r.found_at, r.conductance, r.accepted = fa, cd, ac
+                else:
+                    st = np.empty(m, np.int32)
+                    nr = d.n_rec
+                    rx, ry, rk = np.empty(nr, np.uint32), np.empty(nr, np.uint32), np.empty(nr, np.uint8)
+                    _check(L.dyg_server_fetch(self._srv, d.tag, _ptr(st), _ptr(cd), None, _ptr(rx),
+                                              _ptr(ry), _ptr(rk), nr), "dyg_server_fetch")
+                    r.status, r.conductance = st, cd
+                    r.rec_src, r.rec_dst, r.rec_kind = rx, ry, rk
+                out.append(r)
+            if k.value < len(self._poll):
+                return out
 
     def _batch(self, reqs):
         src, dst, w, uid = [], [], [], []
@@ -133,6 +251,9 @@ class Server:
 
     def step(self) -> list:
         """Runs the oldest pending request of every graph; returns them."""
+        if self.native:
+            _check(lib().dyg_server_step(self._srv, None), "dyg_server_step")
+            return self._collect()
         heads = [q.popleft() for q in self.queues.values() if q]
         for r in heads:
             r.first_update_id = self.uid_next[r.graph]
@@ -158,12 +279,14 @@ class Server:
             for r in dels:
                 m = len(r.src)
                 r.status = res.status[k:k + m].copy()
+                r.conductance = res.conductance[k:k + m].copy()
                 k += m
                 sl = self.slot[r.graph]
                 sel = owner == sl
                 off = self.offsets[sl]
-                r.recovered = list(zip((res.rec_src[sel] - off).tolist(),
-                                       (res.rec_dst[sel] - off).tolist(), res.rec_kind[sel].tolist()))
+                r.rec_src = (res.rec_src[sel] - off).astype(np.uint32)
+                r.rec_dst = (res.rec_dst[sel] - off).astype(np.uint32)
+                r.rec_kind = res.rec_kind[sel].copy()
         t = self.now()
         for r in heads:
             r.done = t
@@ -173,13 +296,18 @@ class Server:
                 r.accepted = np.empty(0, np.uint8)
             if r.op == DELETE and r.status is None:
                 r.status = np.empty(0, np.int32)
-        self.steps += 1
+                r.conductance = np.empty(0, np.float32)
+                r.rec_src = r.rec_dst = np.empty(0, np.uint32)
+                r.rec_kind = np.empty(0, np.uint8)
+        self._steps += 1
         return heads
 
     def serve(self, requests, sync=lambda: None) -> list:
         """Replays requests at their arrival times (seconds from now) with
         continuous batching; returns the completed requests."""
         order = sorted(requests, key=lambda r: r.arrival)
+        if self.native:
+            return self._serve_native(order, sync)
         self.t0 = time.perf_counter()
         i, done = 0, []
         while i < len(order) or self.pending():
@@ -195,7 +323,40 @@ class Server:
                 time.sleep(max(0.0, min(order[i].arrival - self.now(), 0.001)))
         return done
 
+    def _serve_native(self, order, sync) -> list:
+        L = lib()
+        self._t0_ns = L.dyg_server_now_ns(self._srv)
+        i = 0
+        while i < len(order) and order[i].arrival <= 0.0:   # pending at once
+            i += 1
+        self.submit_many(order[:i])
+        done = []
+        _check(L.dyg_server_start(self._srv), "dyg_server_start")
+        try:
+            while i < len(order):
+                t = self.now()
+                j = i
+                while j < len(order) and order[j].arrival <= t:
+                    j += 1
+                if j > i:
+                    self.submit_many(order[i:j])
+                    i = j
+                done += self._collect()
+                if i < len(order):
+                    time.sleep(max(0.0, min(order[i].arrival - self.now(), 0.001)))
+            # results are fetched while the last steps run
+            while L.dyg_server_drain(self._srv, 0.001) != 0:
+                done += self._collect()
+        finally:
+            _check(L.dyg_server_stop(self._srv), "dyg_server_stop")
+        done += self._collect()
+        sync()
+        return done
+
     def close(self):
+        if self._srv is not None:
+            lib().dyg_server_destroy(self._srv)
+            self._srv = None
         for x in (self.H, self.G) + tuple(getattr(self, "_snap", ())):
             x.close()
 
@@ -229,9 +390,8 @@ class PlainServer:
         else:
             res = decremental_batch(self.G[g], self.H[g], r.src, r.dst, self.dparams,
                                     first_update_id=r.first_update_id)
-            r.status = res.status
-            r.recovered = list(zip(res.rec_src.tolist(), res.rec_dst.tolist(),
-                                   res.rec_kind.tolist()))
+            r.status, r.conductance = res.status, res.conductance
+            r.rec_src, r.rec_dst, r.rec_kind = res.rec_src, res.rec_dst, res.rec_kind
         self.uid_next[g] += len(r.src)
 
     def serve(self, requests, sync=lambda: None) -> list:

@@ -1,6 +1,7 @@
-"""Continuous-batching server (dygrass_b200/serve.py): every request gets the
-result it gets alone on its graph's own handles, and admission respects the
-HBM budget."""
+"""Continuous-batching server (include/dyg_serve.h, dygrass_b200/serve.py):
+every request gets the result it gets alone on its graph's own handles, in
+the native scheduler (stepped or in its loop thread) and in the Python one,
+admission respects the HBM budget, and the C ABI reports misuse."""
 import dataclasses
 
 import numpy as np
@@ -44,14 +45,15 @@ def rows_of(server, which, k):
     return rp[lo:hi + 1] - rp[lo], col[a:b] - lo, w[a:b]
 
 
-def test_mixed_requests_match_alone(dyg):
+@pytest.mark.parametrize("native", [True, False])
+def test_mixed_requests_match_alone(dyg, native):
     import torch
     from dygrass_b200.serve import PlainServer, Server, poisson_requests
     cases = mixed_cases()
     p = dyg.WalkParams.make(threshold=100.0, walkers=128)
     reqs = poisson_requests(cases, rate=1e7, count=80, seed=3, size_hi=200)
     alone = [dataclasses.replace(r) for r in reqs]
-    S = Server(cases, p, p)
+    S = Server(cases, p, p, native=native)
     done = S.serve(reqs, sync=torch.cuda.synchronize)
     assert len(done) == len(reqs) and S.steps < len(reqs)   # requests were batched
     P = PlainServer(cases, p, p)
@@ -88,4 +90,95 @@ def test_admission_by_footprint(dyg):
     refused = [r for r in reqs if r.done < 0]
     assert refused and all(r.graph not in S.admitted for r in refused)
     assert all(r.graph in S.admitted for r in done)
+    S.close()
+
+
+def test_native_loop_with_arrivals_matches_alone(dyg):
+    """Requests arriving while steps run (the loop thread) still get their
+    results alone; latencies are measured on the server clock."""
+    from dygrass_b200.serve import PlainServer, Server, poisson_requests
+    cases = mixed_cases()
+    p = dyg.WalkParams.make(threshold=100.0, walkers=64)
+    reqs = poisson_requests(cases, rate=4000.0, count=60, seed=5, size_hi=100)
+    alone = [dataclasses.replace(r) for r in reqs]
+    S = Server(cases, p, p)
+    S.snapshot()
+    done = S.serve(reqs)
+    assert len(done) == len(reqs)
+    assert all(r.done >= r.arrival - 1e-3 for r in reqs)
+    P = PlainServer(cases, p, p)
+    P.serve(alone)
+    for a, b in zip(reqs, alone):
+        same_request(a, b)
+    # the same replay again after restore: identical results
+    again = [dataclasses.replace(r, found_at=None, status=None, rec_src=None) for r in reqs]
+    S.restore()
+    S.serve(again)
+    for a, b in zip(again, alone):
+        same_request(a, b)
+    S.close()
+    P.close()
+
+
+def test_native_server_errors(dyg):
+    import ctypes as C
+    from dygrass_b200.serve import Server
+    cases = mixed_cases()[:2]
+    p = dyg.WalkParams.make(walkers=32)
+    S = Server(cases, p, p)
+    L, h = dyg.lib(), S._srv
+    n0 = cases[0].n
+    src = np.array([0, n0], np.uint32)          # n0 is outside graph 0
+    dst = np.array([1, 2], np.uint32)
+    w = np.ones(2, np.float32)
+    assert L.dyg_server_submit(h, 1, 0, 0, dyg._ptr(src), dyg._ptr(dst), dyg._ptr(w), 2) == dyg.DYG_EINVAL
+    assert b"outside graph 0" in L.dyg_server_last_error(h)
+    assert L.dyg_server_submit(h, 1, 7, 0, dyg._ptr(src), dyg._ptr(dst), dyg._ptr(w), 1) == dyg.DYG_EINVAL
+    bad_w = np.array([0.0], np.float32)
+    assert L.dyg_server_submit(h, 1, 0, 0, dyg._ptr(src), dyg._ptr(dst), dyg._ptr(bad_w), 1) == dyg.DYG_EINVAL
+    assert L.dyg_server_pending(h) == 0
+    # a good deletion request; its tag cannot be reused until fetched
+    c = cases[0]
+    ds, dd = np.ascontiguousarray(c.g_src[:5], np.uint32), np.ascontiguousarray(c.g_dst[:5], np.uint32)
+    assert L.dyg_server_submit(h, 9, 0, 1, dyg._ptr(ds), dyg._ptr(dd), None, 5) == 0
+    assert L.dyg_server_submit(h, 9, 1, 1, dyg._ptr(ds), dyg._ptr(dd), None, 0) == dyg.DYG_EINVAL
+    assert L.dyg_server_fetch(h, 9, None, None, None, None, None, None, 0) == dyg.DYG_EINVAL  # not run yet
+    assert L.dyg_server_reset(h) == dyg.DYG_ESTATE            # not idle
+    assert L.dyg_server_drain(h, 0.0) == dyg.DYG_ESTATE       # pending, no loop
+    k = C.c_uint32()
+    assert L.dyg_server_step(h, C.byref(k)) == 0 and k.value == 1
+    buf = (dyg.ServerDone * 4)()
+    assert L.dyg_server_poll(h, buf, 4, C.byref(k)) == 0 and k.value == 1
+    d = buf[0]
+    assert (d.tag, d.graph, d.op, d.n, d.status, d.first_update_id) == (9, 0, 1, 5, 0, 0)
+    st = np.empty(5, np.int32)
+    if d.n_rec:
+        rx = np.empty(d.n_rec, np.uint32)
+        assert L.dyg_server_fetch(h, 9, dyg._ptr(st), None, None, dyg._ptr(rx), None, None,
+                                  d.n_rec - 1) == dyg.DYG_ERANGE   # kept
+    assert L.dyg_server_fetch(h, 9, dyg._ptr(st), None, None, None, None, None, 0) == 0
+    assert L.dyg_server_fetch(h, 9, None, None, None, None, None, None, 0) == dyg.DYG_EINVAL  # released
+    assert L.dyg_server_step(h, C.byref(k)) == 0 and k.value == 0
+    # bulk submission is all or nothing: a bad request or a repeated tag queues none
+    tags = np.array([20, 21], np.uint64)
+    graphs = np.array([0, 1], np.uint32)
+    ops = np.array([1, 1], np.uint32)
+    offs = np.array([0, 2, 4], np.uint64)
+    bs = np.array([0, 1, 0, cases[1].n], np.uint32)
+    bd = np.array([1, 2, 1, 0], np.uint32)
+    args = lambda t, sr: (h, 2, dyg._ptr(t), dyg._ptr(graphs), dyg._ptr(ops), dyg._ptr(offs),
+                          dyg._ptr(sr), dyg._ptr(bd), None)
+    assert L.dyg_server_submit_many(*args(tags, bs)) == dyg.DYG_EINVAL
+    assert b"request 1" in L.dyg_server_last_error(h) and L.dyg_server_pending(h) == 0
+    bs[3] = 1
+    assert L.dyg_server_submit_many(*args(np.array([20, 20], np.uint64), bs)) == dyg.DYG_EINVAL
+    assert L.dyg_server_pending(h) == 0
+    assert L.dyg_server_submit_many(*args(tags, bs)) == 0 and L.dyg_server_pending(h) == 2
+    assert L.dyg_server_step(h, C.byref(k)) == 0 and k.value == 2      # one per graph, one step
+    assert L.dyg_server_poll(h, buf, 4, C.byref(k)) == 0 and k.value == 2
+    assert sorted((buf[i].tag, buf[i].graph, buf[i].first_update_id) for i in range(2)) == \
+        [(20, 0, 5), (21, 1, 0)]
+    for t in (20, 21):
+        assert L.dyg_server_fetch(h, t, None, None, None, None, None, None, 0) == 0
+    assert L.dyg_server_reset(h) == 0 and L.dyg_server_steps(h) == 0
     S.close()
