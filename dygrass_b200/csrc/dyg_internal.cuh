@@ -109,18 +109,29 @@ constexpr uint32_t kBigRow = 256;
 constexpr uint32_t kBigThreads = 256;
 
 // First j < deg with slots[off + j].x == y, or ~0u.  Every thread of the block
-// calls it; s_best is one shared word.  Tiles of 4 * blockDim.x slots, so a
-// match near the front of a long row ends the scan early.
+// calls it; s_best is one shared word.  Tiles of kFindUnroll * blockDim.x
+// slots whose loads are all issued before any compare, so a hub row costs a
+// few dependent round trips instead of one per 4 * blockDim.x slots, and a
+// match ends the scan at the end of its tile.
+constexpr uint32_t kFindUnroll = 16;
 __device__ __forceinline__ uint32_t block_find(const uint2 *slots, uint32_t off, uint32_t deg,
                                                uint32_t y, uint32_t *s_best) {
-    for (uint32_t base = 0; base < deg; base += 4u * blockDim.x) {
+    const uint32_t *cols = reinterpret_cast<const uint32_t *>(slots + off);
+    for (uint32_t base = 0; base < deg; base += kFindUnroll * blockDim.x) {
         if (threadIdx.x == 0) *s_best = ~0u;
         __syncthreads();
+        uint32_t v[kFindUnroll];
 #pragma unroll
-        for (uint32_t u = 0; u < 4u; ++u) {
+        for (uint32_t u = 0; u < kFindUnroll; ++u) {
             const uint32_t j = base + u * blockDim.x + threadIdx.x;
-            if (j < deg && slots[off + j].x == y) atomicMin(s_best, j);
+            v[u] = j < deg ? cols[2u * j] : ~0u;   // vertex ids are never ~0u
         }
+#pragma unroll
+        for (uint32_t u = 0; u < kFindUnroll; ++u)
+            if (v[u] == y) {   // this thread's first match is its smallest j
+                atomicMin(s_best, base + u * blockDim.x + threadIdx.x);
+                break;
+            }
         __syncthreads();
         const uint32_t b = *s_best;
         __syncthreads();   // every thread has read it before the next reset

@@ -423,8 +423,9 @@ __global__ void k_del_apply_big(DevGraph g, const uint32_t *hx, const uint32_t *
                                 uint32_t *rowcnt, const uint32_t *rowtmp, uint32_t *tmp,
                                 const uint8_t *mask, uint8_t *found, const uint4 *big,
                                 const unsigned long long *nbig, const unsigned long long *halt) {
-    __shared__ uint32_t s_best, s_ok;
+    __shared__ uint32_t s_best, s_ok, s_n;
     __shared__ uint32_t s_y[kTrackMax], s_pos[kTrackMax], s_occ[kTrackMax];
+    __shared__ unsigned long long s_key[kTrackMax];   // (column << 8 | a), ascending
     if (*halt) return;
     const uint32_t nb = (uint32_t)*nbig;
     for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
@@ -451,16 +452,39 @@ __global__ void k_del_apply_big(DevGraph g, const uint32_t *hx, const uint32_t *
                 s_occ[a] = 0u;
             }
             __syncthreads();
-            for (uint32_t a = threadIdx.x; a < cnt; a += blockDim.x)
-                for (uint32_t c = 0; c < a; ++c)
-                    if (s_y[a] != ~0u && s_y[c] == s_y[a]) s_ok = 0u;
+            // the tracked columns sorted (rank by count, ties by index), so
+            // each slot of the row finds its deletion by binary search instead
+            // of comparing against all of them
+            for (uint32_t a = threadIdx.x; a < cnt; a += blockDim.x) {
+                const unsigned long long ka = ((unsigned long long)s_y[a] << 8) | a;
+                uint32_t r = 0;
+                for (uint32_t c = 0; c < cnt; ++c) {
+                    const unsigned long long kc = ((unsigned long long)s_y[c] << 8) | c;
+                    r += kc < ka;
+                    if (c < a && s_y[a] != ~0u && s_y[c] == s_y[a]) s_ok = 0u;
+                }
+                s_key[r] = ka;
+            }
+            if (threadIdx.x == 0) {
+                uint32_t live = 0;
+                for (uint32_t a = 0; a < cnt; ++a) live += s_y[a] != ~0u;
+                s_n = live;   // masked-off entries (column ~0u) sort last
+            }
+            __syncthreads();
+            const uint32_t nlive = s_n;
             for (uint32_t j = threadIdx.x; j < deg; j += blockDim.x) {
                 const uint32_t col = g.slots[d.x + j].x;
-                for (uint32_t a = 0; a < cnt; ++a)
-                    if (s_y[a] == col) {
-                        atomicMin(&s_pos[a], j);
-                        atomicAdd(&s_occ[a], 1u);
-                    }
+                uint32_t lo = 0, hi = nlive;
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if ((uint32_t)(s_key[mid] >> 8) < col) lo = mid + 1u;
+                    else hi = mid;
+                }
+                if (lo < nlive && (uint32_t)(s_key[lo] >> 8) == col) {
+                    const uint32_t a = (uint32_t)(s_key[lo] & 0xFFu);
+                    atomicMin(&s_pos[a], j);
+                    atomicAdd(&s_occ[a], 1u);
+                }
             }
             __syncthreads();
             for (uint32_t a = threadIdx.x; a < cnt; a += blockDim.x)
