@@ -144,9 +144,28 @@ __global__ void k_app_move_big(DevGraph g, const uint32_t *hx, const uint32_t *l
     const uint32_t nb = (uint32_t)*nbig;
     for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
         const uint4 e = big[b];
-        for (uint32_t j = threadIdx.x; j < e.w; j += blockDim.x) {
-            g.slots[e.y + j] = g.slots[e.z + j];
-            g.wts[e.y + j] = g.wts[e.z + j];
+        // the old and new ranges never overlap (the row moves to fresh arena
+        // space), so a tile's loads are all issued before its stores
+        constexpr uint32_t U = 8;
+        for (uint32_t base = 0; base < e.w; base += U * blockDim.x) {
+            uint2 sv[U];
+            float wv[U];
+#pragma unroll
+            for (uint32_t u = 0; u < U; ++u) {
+                const uint32_t j = base + u * blockDim.x + threadIdx.x;
+                if (j < e.w) {
+                    sv[u] = g.slots[e.z + j];
+                    wv[u] = g.wts[e.z + j];
+                }
+            }
+#pragma unroll
+            for (uint32_t u = 0; u < U; ++u) {
+                const uint32_t j = base + u * blockDim.x + threadIdx.x;
+                if (j < e.w) {
+                    g.slots[e.y + j] = sv[u];
+                    g.wts[e.y + j] = wv[u];
+                }
+            }
         }
         if (threadIdx.x == 0) {
             const uint32_t x = hx[e.x];
@@ -472,18 +491,29 @@ __global__ void k_del_apply_big(DevGraph g, const uint32_t *hx, const uint32_t *
             }
             __syncthreads();
             const uint32_t nlive = s_n;
-            for (uint32_t j = threadIdx.x; j < deg; j += blockDim.x) {
-                const uint32_t col = g.slots[d.x + j].x;
-                uint32_t lo = 0, hi = nlive;
-                while (lo < hi) {
-                    const uint32_t mid = (lo + hi) >> 1;
-                    if ((uint32_t)(s_key[mid] >> 8) < col) lo = mid + 1u;
-                    else hi = mid;
+            const uint32_t *cols = reinterpret_cast<const uint32_t *>(g.slots + d.x);
+            for (uint32_t base = 0; base < deg; base += kFindUnroll * blockDim.x) {
+                uint32_t v[kFindUnroll];   // a tile's loads are issued before any search
+#pragma unroll
+                for (uint32_t u = 0; u < kFindUnroll; ++u) {
+                    const uint32_t j = base + u * blockDim.x + threadIdx.x;
+                    v[u] = j < deg ? cols[2u * j] : ~0u;
                 }
-                if (lo < nlive && (uint32_t)(s_key[lo] >> 8) == col) {
-                    const uint32_t a = (uint32_t)(s_key[lo] & 0xFFu);
-                    atomicMin(&s_pos[a], j);
-                    atomicAdd(&s_occ[a], 1u);
+#pragma unroll
+                for (uint32_t u = 0; u < kFindUnroll; ++u) {
+                    const uint32_t col = v[u];
+                    if (col == ~0u) continue;
+                    uint32_t lo = 0, hi = nlive;
+                    while (lo < hi) {
+                        const uint32_t mid = (lo + hi) >> 1;
+                        if ((uint32_t)(s_key[mid] >> 8) < col) lo = mid + 1u;
+                        else hi = mid;
+                    }
+                    if (lo < nlive && (uint32_t)(s_key[lo] >> 8) == col) {
+                        const uint32_t a = (uint32_t)(s_key[lo] & 0xFFu);
+                        atomicMin(&s_pos[a], base + u * blockDim.x + threadIdx.x);
+                        atomicAdd(&s_occ[a], 1u);
+                    }
                 }
             }
             __syncthreads();
