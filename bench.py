@@ -34,11 +34,13 @@ plain per-graph loop on the same updates is timed beside it.
 Workload "serve": the serving configuration -- 64 resident graphs mixed from
 the mesh, R-MAT and random-geometric generators, update requests of log-
 uniform size in [1, 4096], 60% insertions / 40% deletions.  value = the
-continuous-batching server's throughput replaying a fixed request set that
-is all pending at once (saturation), timed with CUDA events from a restored
-snapshot; then p50/p99 latency at Poisson arrival rates swept around that
-capacity, for the server and for the plain sequential path (every request
-alone on its graph's own handles).
+continuous-batching server's throughput (the native scheduler of
+include/dyg_serve.h, driven by dygrass_b200/serve.py) replaying a fixed
+request set that is all pending at once (saturation), timed with CUDA events
+from a restored snapshot; then p50/p99 latency at Poisson arrival rates
+swept around that capacity, for the server and for the plain sequential path
+(every request alone on its graph's own handles), and the same steps
+scheduled from Python for comparison.
 
 N > 1 (torchrun): every rank runs an independent replica of the workload
 (weak scaling, no data-path collective); times are the max over ranks.
