@@ -1092,9 +1092,13 @@ def main():
                      "bytes_model": f"{BYTES_PER_MOVE} B per walker move (row descriptor sector + slot sector)",
                      "algorithmic_bytes_per_launch": res["dom_bytes_per_launch"],
                      "ms_per_launch": res["dom_ms_per_launch"],
+                     "useful_bytes_per_move": 16,
+                     "sector_efficiency": 16 / BYTES_PER_MOVE,
                      "note": "the graphs are largely L2-resident: traffic (ncu DRAM bytes per launch) "
                              "is well below the algorithmic bytes, so frac is an equivalent-bandwidth "
-                             "figure; the walk is bound by dependent-load latency"},
+                             "figure; the walk is bound by instruction issue and L1 gathers "
+                             "(profiles/k_walk_mesh100.md); of each move's two sectors, 16 B "
+                             "(descriptor + slot) are payload"},
         "clocks": res["clocks"],
         "e2e": res["e2e"],
         "gpu_launches": int(round(res["launches_per_step"] * args.steps)),
