@@ -26,9 +26,11 @@
 #include <condition_variable>
 #include <deque>
 #include <mutex>
+#include <new>
 #include <string>
 #include <thread>
 #include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 #include "dyg_internal.cuh"
@@ -266,7 +268,13 @@ dyg_status run_step(dyg_server *s, uint32_t *n_done) {
         if (r->rec.op == DYG_STREAM_INSERT) ni += r->rec.n;
         else nd += r->rec.n;
     }
-    const dyg_status rc = stage_and_run(s, heads, ni, nd);
+    dyg_status rc;
+    try {
+        rc = stage_and_run(s, heads, ni, nd);
+    } catch (const std::bad_alloc &) {
+        dyg::set_error("host allocation failed in a server step");
+        rc = DYG_ENOMEM;
+    }
     const std::string msg = rc == DYG_OK ? std::string() : std::string(dyg_last_error_string());
     const uint64_t t_done = now_ns(s);
     {
@@ -419,36 +427,57 @@ dyg_status dyg_server_submit_many(dyg_server *s, uint32_t n_req, const uint64_t 
     if (n_req && (!tags || !graphs || !ops || !offsets))
         return fail(s, DYG_EINVAL, "NULL request arrays");
     std::vector<Request *> made;
-    made.reserve(n_req);
     auto drop = [&made] {
         for (Request *r : made) delete r;
     };
-    for (uint32_t j = 0; j < n_req; ++j) {
-        const uint64_t a = offsets[j], b = offsets[j + 1];
-        if (b < a) {
-            drop();
-            return fail(s, DYG_EINVAL, "request offsets must ascend");
+    try {
+        made.reserve(n_req);
+        for (uint32_t j = 0; j < n_req; ++j) {
+            const uint64_t a = offsets[j], b = offsets[j + 1];
+            if (b < a) {
+                drop();
+                return fail(s, DYG_EINVAL, "request offsets must ascend");
+            }
+            const uint32_t *sj = src ? src + a : nullptr, *dj = dst ? dst + a : nullptr;
+            const float *wj = (w && ops[j] == DYG_STREAM_INSERT) ? w + a : nullptr;
+            const std::string e = check_request(s, graphs[j], ops[j], sj, dj, wj, b - a);
+            if (!e.empty()) {
+                drop();
+                return fail(s, DYG_EINVAL, "request " + std::to_string(j) + ": " + e);
+            }
+            made.push_back(make_request(s, tags[j], graphs[j], ops[j], sj, dj, wj, (uint32_t)(b - a)));
         }
-        const uint32_t *sj = src ? src + a : nullptr, *dj = dst ? dst + a : nullptr;
-        const float *wj = (w && ops[j] == DYG_STREAM_INSERT) ? w + a : nullptr;
-        const std::string e = check_request(s, graphs[j], ops[j], sj, dj, wj, b - a);
-        if (!e.empty()) {
-            drop();
-            return fail(s, DYG_EINVAL, "request " + std::to_string(j) + ": " + e);
-        }
-        made.push_back(make_request(s, tags[j], graphs[j], ops[j], sj, dj, wj, (uint32_t)(b - a)));
+    } catch (const std::bad_alloc &) {
+        drop();
+        return fail(s, DYG_ENOMEM, "host allocation failed while copying requests");
+    }
+    std::unordered_set<uint64_t> seen;   // tags repeated within this call
+    uint32_t rep = n_req;
+    try {
+        seen.reserve(n_req);
+        for (uint32_t j = 0; j < n_req && rep == n_req; ++j)
+            if (!seen.insert(tags[j]).second) rep = j;
+    } catch (const std::bad_alloc &) {
+        drop();
+        return fail(s, DYG_ENOMEM, "host allocation failed while checking tags");
     }
     {
         std::lock_guard<std::mutex> lk(s->mu);
         for (uint32_t j = 0; j < n_req; ++j) {
-            bool dup = s->by_tag.count(tags[j]) != 0;
-            for (uint32_t i = 0; i < j && !dup; ++i) dup = tags[i] == tags[j];
-            if (dup) {
+            if (j == rep || s->by_tag.count(tags[j]) != 0) {
                 drop();
                 s->err = "tag " + std::to_string(tags[j]) + " is held by an unfetched request";
                 dyg::set_error(s->err);
                 return DYG_EINVAL;
             }
+        }
+        try {
+            s->by_tag.reserve(s->by_tag.size() + n_req);
+        } catch (const std::bad_alloc &) {
+            drop();
+            s->err = "host allocation failed while queueing requests";
+            dyg::set_error(s->err);
+            return DYG_ENOMEM;
         }
         for (uint32_t j = 0; j < n_req; ++j) {
             s->by_tag[tags[j]] = made[j];

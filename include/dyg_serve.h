@@ -60,13 +60,14 @@ dyg_status dyg_server_create(dyg_graph *G, dyg_graph *H, uint32_t n_graphs,
                              dyg_server **out);
 
 /* Stops the loop thread (after its current step) and frees the server; the
- * graphs stay the caller's. */
+ * graphs stay the caller's and must outlive the server (destroy it first). */
 dyg_status dyg_server_destroy(dyg_server *s);
 
 /* Queues a request: op DYG_STREAM_INSERT (w required, finite and > 0) or
  * DYG_STREAM_DELETE (w ignored); n may be 0.  Host arrays, copied.  tag must
  * not be held by an unfetched request.  DYG_EINVAL for a bad graph, op, tag,
- * vertex id or weight (nothing is queued then). */
+ * vertex id or weight, DYG_ENOMEM if the copy cannot be allocated (nothing is
+ * queued then). */
 dyg_status dyg_server_submit(dyg_server *s, uint64_t tag, uint32_t graph, uint32_t op,
                              const uint32_t *src, const uint32_t *dst, const float *w,
                              uint32_t n);
