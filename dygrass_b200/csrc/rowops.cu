@@ -110,11 +110,25 @@ __global__ void k_app_move(DevGraph g, const uint32_t *hx, const uint32_t *m_dev
                 mv = false;
             }
         }
-        // rows of up to 32 slots are copied by their own lane
+        // rows of up to 32 slots are copied by their own lane, eight slots
+        // loaded before they are stored (the new range is fresh arena space,
+        // so it never overlaps a row being read)
         if (mv && d.y <= 32u) {
-            for (uint32_t j = 0; j < d.y; ++j) {
-                g.slots[off + j] = g.slots[d.x + j];
-                g.wts[off + j] = g.wts[d.x + j];
+            for (uint32_t j0 = 0; j0 < d.y; j0 += 8u) {
+                uint2 sv[8];
+                float wv[8];
+#pragma unroll
+                for (uint32_t u = 0; u < 8u; ++u)
+                    if (j0 + u < d.y) {
+                        sv[u] = g.slots[d.x + j0 + u];
+                        wv[u] = g.wts[d.x + j0 + u];
+                    }
+#pragma unroll
+                for (uint32_t u = 0; u < 8u; ++u)
+                    if (j0 + u < d.y) {
+                        g.slots[off + j0 + u] = sv[u];
+                        g.wts[off + j0 + u] = wv[u];
+                    }
             }
         }
         unsigned todo = __ballot_sync(kFull, mv && d.y > 32u);
@@ -124,9 +138,25 @@ __global__ void k_app_move(DevGraph g, const uint32_t *hx, const uint32_t *m_dev
             const uint32_t so = __shfl_sync(kFull, off, src);
             const uint32_t sx = __shfl_sync(kFull, d.x, src);
             const uint32_t sy = __shfl_sync(kFull, d.y, src);
-            for (uint32_t j = lane; j < sy; j += 32u) {
-                g.slots[so + j] = g.slots[sx + j];
-                g.wts[so + j] = g.wts[sx + j];
+            for (uint32_t j0 = 0; j0 < sy; j0 += 256u) {
+                uint2 sv[8];
+                float wv[8];
+#pragma unroll
+                for (uint32_t u = 0; u < 8u; ++u) {
+                    const uint32_t j = j0 + lane + 32u * u;
+                    if (j < sy) {
+                        sv[u] = g.slots[sx + j];
+                        wv[u] = g.wts[sx + j];
+                    }
+                }
+#pragma unroll
+                for (uint32_t u = 0; u < 8u; ++u) {
+                    const uint32_t j = j0 + lane + 32u * u;
+                    if (j < sy) {
+                        g.slots[so + j] = sv[u];
+                        g.wts[so + j] = wv[u];
+                    }
+                }
             }
         }
         if (mv) {
@@ -220,7 +250,29 @@ __global__ void k_app_finish(DevGraph g, const uint32_t *hx, const uint32_t *m_d
         const uint2 d = lead ? g.desc[x] : make_uint2(0u, 0u);
         const uint32_t base = d.x + d.y;
         const bool coop = lead && cnt > kTailLane && cnt <= kTailWarp;
-        if (lead && !coop) {
+        if (lead && !coop && cnt <= kTailLane) {
+            // a short tail: loaded at once, each entry written at its rank
+            // among the tail's (distinct) list indices, with 1/w in place of
+            // the index
+            uint2 sv[kTailLane];
+            float wv[kTailLane];
+#pragma unroll
+            for (uint32_t u = 0; u < kTailLane; ++u)
+                if (u < cnt) {
+                    sv[u] = g.slots[base + u];
+                    wv[u] = g.wts[base + u];
+                }
+#pragma unroll
+            for (uint32_t u = 0; u < kTailLane; ++u)
+                if (u < cnt) {
+                    uint32_t r = 0;
+#pragma unroll
+                    for (uint32_t v = 0; v < kTailLane; ++v)
+                        if (v < cnt) r += sv[v].y < sv[u].y ? 1u : 0u;
+                    g.slots[base + r] = make_uint2(sv[u].x, __float_as_uint(__frcp_rn(wv[u])));
+                    g.wts[base + r] = wv[u];
+                }
+        } else if (lead && !coop) {
             for (uint32_t a = 1; a < cnt; ++a) {   // insertion sort by list index
                 const uint2 sl = g.slots[base + a];
                 const float w = g.wts[base + a];
@@ -371,14 +423,23 @@ __global__ void k_del_apply(DevGraph g, const uint32_t *hx, const uint32_t *hy, 
                 const uint32_t k = run[a];
                 if (mask && !(mask[k & ~1u] && mask[k | 1u])) continue;
                 const uint32_t y = hy[k];
-                for (uint32_t j = 0; j < deg; ++j) {
-                    if (g.slots[d.x + j].x == y) {
-                        g.slots[d.x + j] = g.slots[d.x + deg - 1u];
-                        g.wts[d.x + j] = g.wts[d.x + deg - 1u];
-                        --deg;
-                        found[k] = 1;
-                        break;
-                    }
+                // first slot holding y, eight columns loaded before they are
+                // compared (vertex ids are never ~0u)
+                uint32_t pos = ~0u;
+                for (uint32_t j0 = 0; j0 < deg && pos == ~0u; j0 += 8u) {
+                    uint32_t cv[8];
+#pragma unroll
+                    for (uint32_t u = 0; u < 8u; ++u)
+                        cv[u] = j0 + u < deg ? g.slots[d.x + j0 + u].x : ~0u;
+#pragma unroll
+                    for (uint32_t u = 0; u < 8u; ++u)
+                        if (pos == ~0u && cv[u] == y) pos = j0 + u;
+                }
+                if (pos != ~0u) {
+                    g.slots[d.x + pos] = g.slots[d.x + deg - 1u];
+                    g.wts[d.x + pos] = g.wts[d.x + deg - 1u];
+                    --deg;
+                    found[k] = 1;
                 }
             }
             g.desc[x] = make_uint2(d.x, deg);
