@@ -277,11 +277,16 @@ __global__ void k_hash_keep(const unsigned long long *halt, DevGraph h, const ui
                         if (big_ok && d.y > kBigRow) {
                             big[atomicAdd(nbig, 1ull)] = make_uint4(i, xs ? x : y, other, 0u);
                         } else {
-                            for (uint32_t j = 0; j < d.y; ++j)
-                                if (h.slots[d.x + j].x == other) {
-                                    kp = 0;
-                                    break;
-                                }
+                            // eight columns loaded before they are compared
+                            for (uint32_t j0 = 0; j0 < d.y && kp; j0 += 8u) {
+                                uint32_t cv[8];
+#pragma unroll
+                                for (uint32_t u = 0; u < 8u; ++u)
+                                    cv[u] = j0 + u < d.y ? h.slots[d.x + j0 + u].x : ~0u;
+#pragma unroll
+                                for (uint32_t u = 0; u < 8u; ++u)
+                                    if (cv[u] == other) kp = 0;
+                            }
                         }
                     }
                 }

@@ -40,11 +40,20 @@ inline int blocks(uint64_t n, int th) { return (int)((n + th - 1) / th); }
 __device__ __forceinline__ uint32_t group_find(const DevGraph &g, uint32_t x, uint32_t y,
                                                uint32_t lane, uint32_t gbase, uint32_t gmask) {
     const uint2 d = g.desc[x];
-    for (uint32_t j0 = 0; j0 < d.y; j0 += kProbeLanes) {
-        const uint32_t j = j0 + lane;
-        const bool hit = j < d.y && g.slots[d.x + j].x == y;
-        const uint32_t bits = (__ballot_sync(gmask, hit) >> gbase) & ((1u << kProbeLanes) - 1u);
-        if (bits) return d.x + j0 + (uint32_t)(__ffs(bits) - 1);
+    constexpr uint32_t U = 4;   // a group's tile: U loads per lane issued before any compare
+    for (uint32_t t0 = 0; t0 < d.y; t0 += U * kProbeLanes) {
+        uint32_t cv[U];
+#pragma unroll
+        for (uint32_t u = 0; u < U; ++u) {
+            const uint32_t j = t0 + u * kProbeLanes + lane;
+            cv[u] = j < d.y ? g.slots[d.x + j].x : ~0u;   // vertex ids are never ~0u
+        }
+#pragma unroll
+        for (uint32_t u = 0; u < U; ++u) {
+            const uint32_t bits =
+                (__ballot_sync(gmask, cv[u] == y) >> gbase) & ((1u << kProbeLanes) - 1u);
+            if (bits) return d.x + t0 + u * kProbeLanes + (uint32_t)(__ffs(bits) - 1);
+        }
     }
     return ~0u;
 }
