@@ -42,6 +42,39 @@ class Plan:
     counts: list = field(default_factory=list)   # insertions per graph
 
 
+def plan_rounds(offsets, streams, batch_sizes=None) -> Plan:
+    """Rounds over graphs at vertex offsets[g]: round r holds batch r of every
+    graph's stream (src, dst, w local ids), with global ids, the edge's
+    position in its graph's stream as its update id, and its graph index.
+    Batch sizes are ceil(n_g/10) (random_walk_incremental/gpu_graph.cuh:135)
+    unless given per graph."""
+    per = []
+    for g, (s, d, w) in enumerate(streams):
+        m = len(s)
+        B = (batch_sizes[g] if batch_sizes else reference_batch_size(m)) or 1
+        per.append((g, np.asarray(s, np.uint32), np.asarray(d, np.uint32),
+                    np.asarray(w, np.float32), m, B))
+    nrounds = max((-(-m // B) for *_, m, B in per if m), default=0)
+    rounds = []
+    for r in range(nrounds):
+        cs, cd, cw, cu, cg, cp = [], [], [], [], [], []
+        for g, s, d, w, m, B in per:
+            lo, hi = r * B, min((r + 1) * B, m)
+            if lo >= hi:
+                continue
+            off = offsets[g]
+            cs.append(s[lo:hi] + off)
+            cd.append(d[lo:hi] + off)
+            cw.append(w[lo:hi])
+            cu.append(np.arange(lo, hi, dtype=np.uint64))
+            cg.append(np.full(hi - lo, g, np.int32))
+            cp.append(np.arange(lo, hi, dtype=np.int64))
+        rounds.append(Round(np.concatenate(cs).astype(np.uint32), np.concatenate(cd).astype(np.uint32),
+                            np.concatenate(cw), np.concatenate(cu), np.concatenate(cg),
+                            np.concatenate(cp)))
+    return Plan(rounds, sum(m for *_, m, _ in per), [m for *_, m, _ in per])
+
+
 class ManyGraphs:
     """Union of independent graphs: H (and optionally G) on the device."""
 
@@ -74,31 +107,7 @@ class ManyGraphs:
         given."""
         if streams is None:
             streams = [(c.ins_src, c.ins_dst, c.ins_w) for c in self.cases]
-        per = []
-        for g, (s, d, w) in enumerate(streams):
-            m = len(s)
-            B = (batch_sizes[g] if batch_sizes else reference_batch_size(m)) or 1
-            per.append((g, np.asarray(s, np.uint32), np.asarray(d, np.uint32),
-                        np.asarray(w, np.float32), m, B))
-        nrounds = max((-(-m // B) for *_, m, B in per if m), default=0)
-        rounds = []
-        for r in range(nrounds):
-            cs, cd, cw, cu, cg, cp = [], [], [], [], [], []
-            for g, s, d, w, m, B in per:
-                lo, hi = r * B, min((r + 1) * B, m)
-                if lo >= hi:
-                    continue
-                off = self.offsets[g]
-                cs.append(s[lo:hi] + off)
-                cd.append(d[lo:hi] + off)
-                cw.append(w[lo:hi])
-                cu.append(np.arange(lo, hi, dtype=np.uint64))
-                cg.append(np.full(hi - lo, g, np.int32))
-                cp.append(np.arange(lo, hi, dtype=np.int64))
-            rounds.append(Round(np.concatenate(cs).astype(np.uint32), np.concatenate(cd).astype(np.uint32),
-                                np.concatenate(cw), np.concatenate(cu), np.concatenate(cg),
-                                np.concatenate(cp)))
-        return Plan(rounds, sum(m for *_, m, _ in per), [m for *_, m, _ in per])
+        return plan_rounds(self.offsets, streams, batch_sizes)
 
     def run(self, plan: Plan, params: WalkParams, stream: int | None = None, outs=None):
         """Applies every round; returns the per-round IncrementalResults."""

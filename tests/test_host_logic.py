@@ -1,0 +1,147 @@
+"""Host-side logic of the batched and serving modes, on the CPU: the rounds
+that carry batch r of every graph (multi.plan_rounds), the request generator,
+latency statistics and footprint estimate of the server (serve.py)."""
+from types import SimpleNamespace
+
+import numpy as np
+
+from dygrass_b200.multi import plan_rounds
+from dygrass_b200.serve import DELETE, INSERT, Request, footprint_bytes, latency_stats, poisson_requests
+
+
+def streams_of(lengths, seed=0):
+    rng = np.random.default_rng(seed)
+    out = []
+    for m in lengths:
+        out.append((rng.integers(0, 50, m).astype(np.uint32), rng.integers(0, 50, m).astype(np.uint32),
+                    rng.uniform(0.5, 2.0, m).astype(np.float32)))
+    return out
+
+
+def check_plan(plan, offsets, streams, sizes):
+    # every graph's edges appear once, batch r of graph g in round r, in stream
+    # order, with global ids, update id = position in the graph's stream
+    assert plan.counts == [len(s) for s, _, _ in streams]
+    assert plan.n_edges == sum(plan.counts)
+    seen = {g: [] for g in range(len(streams))}
+    for r, rd in enumerate(plan.rounds):
+        for g in np.unique(rd.graph):
+            sel = rd.graph == g
+            pos = rd.pos[sel]
+            B = sizes[g]
+            assert np.array_equal(pos, np.arange(r * B, min((r + 1) * B, len(streams[g][0]))))
+            s, d, w = streams[g]
+            assert np.array_equal(rd.src[sel], s[pos] + offsets[g])
+            assert np.array_equal(rd.dst[sel], d[pos] + offsets[g])
+            assert np.array_equal(rd.w[sel].view(np.uint32), w[pos].view(np.uint32))
+            assert np.array_equal(rd.uid[sel], pos.astype(np.uint64))
+            seen[g] += pos.tolist()
+        # graphs appear in index order within a round
+        assert np.all(np.diff(rd.graph) >= 0)
+    for g, (s, _, _) in enumerate(streams):
+        assert seen[g] == list(range(len(s)))
+    assert len(plan.rounds) == max(-(-len(s) // sizes[g]) for g, (s, _, _) in enumerate(streams) if len(s))
+
+
+def test_plan_reference_batches():
+    lengths = [0, 7, 25, 100, 1]
+    streams = streams_of(lengths)
+    offsets = np.array([0, 50, 100, 150, 200, 250], np.int64)
+    plan = plan_rounds(offsets, streams)
+    sizes = [max(1, -(-m // 10)) for m in lengths]     # ceil(m/10)
+    check_plan(plan, offsets, streams, sizes)
+    assert len(plan.rounds) == 10
+
+
+def test_plan_given_batch_sizes():
+    lengths = [13, 4, 9]
+    streams = streams_of(lengths, seed=1)
+    offsets = np.array([0, 50, 100, 150], np.int64)
+    sizes = [5, 1, 9]
+    plan = plan_rounds(offsets, streams, sizes)
+    check_plan(plan, offsets, streams, sizes)
+    assert len(plan.rounds) == 4
+
+
+def test_plan_empty():
+    plan = plan_rounds(np.array([0, 10], np.int64), streams_of([0]))
+    assert plan.rounds == [] and plan.n_edges == 0
+
+
+def fake_cases(k=3, n=40, seed=2):
+    rng = np.random.default_rng(seed)
+    cases = []
+    for g in range(k):
+        m = 60 + 10 * g
+        iu, ju = np.triu_indices(n, 1)                  # distinct pairs
+        pick = rng.choice(len(iu), m, replace=False)
+        src, dst = iu[pick].astype(np.uint32), ju[pick].astype(np.uint32)
+        cases.append(SimpleNamespace(n=n, g_src=src, g_dst=dst, h_src=src[:10], h_dst=dst[:10],
+                                     ins_src=rng.integers(0, n, 300).astype(np.uint32),
+                                     ins_dst=rng.integers(0, n, 300).astype(np.uint32),
+                                     ins_w=rng.uniform(1, 2, 300).astype(np.float32)))
+    return cases
+
+
+def test_poisson_requests():
+    cases = fake_cases()
+    a = poisson_requests(cases, rate=1000.0, count=200, seed=7, size_hi=40)
+    b = poisson_requests(cases, rate=1000.0, count=200, seed=7, size_hi=40)
+    assert [(r.graph, r.op, r.arrival, r.src.tolist()) for r in a] == \
+        [(r.graph, r.op, r.arrival, r.src.tolist()) for r in b]            # seeded
+    arr = np.array([r.arrival for r in a])
+    assert np.all(np.diff(arr) > 0)
+    assert 0.1 < arr[-1] < 0.4                                            # mean gap 1/rate
+    ins = {g: 0 for g in range(len(cases))}
+    dels = {g: set() for g in range(len(cases))}
+    for r in a:
+        c = cases[r.graph]
+        assert len(r.src) == len(r.dst) <= 40
+        if r.op == INSERT:
+            # the next edges of the graph's insertion pool, in order
+            k = ins[r.graph]
+            assert np.array_equal(r.src, c.ins_src[k:k + len(r.src)])
+            assert np.array_equal(r.w, c.ins_w[k:k + len(r.src)])
+            ins[r.graph] += len(r.src)
+        else:
+            assert r.op == DELETE and r.w is None
+            pairs = set(zip(r.src.tolist(), r.dst.tolist()))
+            g_pairs = set(zip(c.g_src.tolist(), c.g_dst.tolist()))
+            assert pairs <= g_pairs
+            # deletions of a graph never repeat an edge of its dense graph
+            idx = [i for i in range(len(c.g_src)) if (c.g_src[i], c.g_dst[i]) in pairs]
+            assert not (dels[r.graph] & set(idx))
+            dels[r.graph] |= set(idx)
+    assert any(r.op == INSERT for r in a) and any(r.op == DELETE for r in a)
+
+
+def test_latency_stats_and_recovered():
+    reqs = []
+    for i in range(100):
+        r = Request(0, INSERT, np.arange(i % 5 + 1, dtype=np.uint32), np.arange(i % 5 + 1, dtype=np.uint32),
+                    arrival=0.01 * i)
+        r.done = r.arrival + 0.001 * (i + 1)
+        reqs.append(r)
+    refused = Request(1, DELETE, np.zeros(3, np.uint32), np.ones(3, np.uint32))
+    refused.done = -1.0
+    st = latency_stats(reqs + [refused])
+    assert st["requests"] == 100
+    assert st["updates"] == sum(i % 5 + 1 for i in range(100))
+    assert abs(st["p50_ms"] - np.percentile(np.arange(1, 101), 50)) < 1e-9
+    assert abs(st["p99_ms"] - np.percentile(np.arange(1, 101), 99)) < 1e-9
+    r = Request(0, DELETE, np.zeros(1, np.uint32), np.ones(1, np.uint32))
+    assert r.recovered == []
+    r.rec_src = np.array([3, 4], np.uint32)
+    r.rec_dst = np.array([5, 6], np.uint32)
+    r.rec_kind = np.array([0, 1], np.uint8)
+    assert r.recovered == [(3, 5, 0), (4, 6, 1)]
+
+
+def test_footprint_grows_with_the_graph():
+    base = footprint_bytes(1000, 4000, 1500)
+    assert base > 0
+    assert footprint_bytes(2000, 4000, 1500) > base
+    assert footprint_bytes(1000, 8000, 1500) > base
+    assert footprint_bytes(1000, 4000, 3000) > base
+    # slots (12 B each) of both graphs with headroom, plus descriptors
+    assert base >= 12 * 2 * (4000 + 1500)
