@@ -336,6 +336,20 @@ void orc_walk_keys(const orc_graph *g, const uint32_t *src, const uint32_t *dst,
     if (moves) *moves = mv_total;
 }
 
+void orc_walk_keys_ids(const orc_graph *g, const uint32_t *src, const uint32_t *dst,
+                       const float *w, const uint64_t *uids, uint32_t n, const orc_params *p,
+                       int threads, uint64_t *keys, uint64_t *moves) {
+    uint64_t mv_total = 0;
+    if (threads < 1) threads = 1;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads) reduction(+ : mv_total)
+    for (int64_t e = 0; e < (int64_t)n; ++e) {
+        uint64_t mv = 0;
+        keys[e] = best_key(g, src[e], dst[e], w[e], 1, p, uids[e], DOMAIN_INCR, &mv);
+        mv_total += mv;
+    }
+    if (moves) *moves = mv_total;
+}
+
 /* commit in input order (gpu_graph.cuh:297-329): add iff no path */
 void orc_incremental_commit_keys(orc_graph *H, orc_graph *G, const uint32_t *src,
                                  const uint32_t *dst, const float *w, uint32_t n,

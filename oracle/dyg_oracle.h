@@ -126,6 +126,12 @@ uint64_t orc_stream_file(orc_graph *G, orc_graph *H, uint32_t op, const uint32_t
 void orc_walk_keys(const orc_graph *g, const uint32_t *src, const uint32_t *dst, const float *w,
                    uint64_t first_uid, uint32_t lo, uint32_t hi, int incr, const orc_params *p,
                    int threads, uint64_t *keys, uint64_t *moves);
+/* orc_walk_keys with each edge's update id read from uids[e] (the batched
+ * many-graph mode: a union of graphs at vertex offsets, every edge carrying
+ * its position in its own graph's stream), incremental walks on g. */
+void orc_walk_keys_ids(const orc_graph *g, const uint32_t *src, const uint32_t *dst,
+                       const float *w, const uint64_t *uids, uint32_t n, const orc_params *p,
+                       int threads, uint64_t *keys, uint64_t *moves);
 void orc_incremental_commit_keys(orc_graph *H, orc_graph *G, const uint32_t *src,
                                  const uint32_t *dst, const float *w, uint32_t n,
                                  const uint64_t *keys, int32_t *found_at, float *cond,

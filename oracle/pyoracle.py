@@ -63,6 +63,7 @@ def lib() -> C.CDLL:
             "orc_stream_default_chunk": ([u32], u32),
             "orc_walk_keys": ([vp, vp, vp, vp, u64, u32, u32, C.c_int, P, C.c_int, vp, vp], None),
             "orc_incremental_commit_keys": ([vp, vp, vp, vp, vp, u32, vp, vp, vp, vp], None),
+            "orc_walk_keys_ids": ([vp, vp, vp, vp, vp, u32, P, C.c_int, vp, vp], None),
             "orc_decremental_delete": ([vp, vp, vp, vp, u32, vp, vp, vp], u32),
             "orc_decremental_walk_list_keys": ([vp, vp, vp, vp, u32, u32, u64, P, C.c_int, vp], None),
             "orc_decremental_commit_keys": ([vp, vp, vp, vp, vp, u32, u64, P, vp, vp, vp, vp, vp, vp,
@@ -142,6 +143,26 @@ def incremental(H: OGraph, src, dst, w, params, batch_size=0, G: OGraph | None =
         mv = lib().orc_incremental_stream(H.h, G.h if G else None, _p(src), _p(dst), _p(w), n,
                                           batch_size, C.byref(P), th, _p(fa), _p(cd), _p(ac))
     return fa, cd, ac, int(mv)
+
+
+def incremental_ids(H: OGraph, src, dst, w, uids, params, G: OGraph | None = None, threads=None):
+    """One incremental batch whose edge e walks with update id uids[e]
+    (the batched many-graph mode).  Returns (found_at, cond, accepted)."""
+    src = np.ascontiguousarray(src, np.uint32)
+    dst = np.ascontiguousarray(dst, np.uint32)
+    w = np.ascontiguousarray(w, np.float32)
+    uids = np.ascontiguousarray(uids, np.uint64)
+    n = len(src)
+    keys = np.empty(max(n, 1), np.uint64)
+    fa = np.empty(n, np.int32)
+    cd = np.empty(n, np.float32)
+    ac = np.empty(n, np.uint8)
+    P = Params.from_walk_params(params)
+    th = threads or max_threads()
+    lib().orc_walk_keys_ids(H.h, _p(src), _p(dst), _p(w), _p(uids), n, C.byref(P), th, _p(keys), None)
+    lib().orc_incremental_commit_keys(H.h, G.h if G else None, _p(src), _p(dst), _p(w), n, _p(keys),
+                                      _p(fa), _p(cd), _p(ac))
+    return fa, cd, ac
 
 
 def decremental(G: OGraph, H: OGraph, src, dst, params, batch_size=0, threads=None,
