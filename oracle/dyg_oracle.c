@@ -12,7 +12,7 @@
  *                                   random_walk_decremental/gpu_graph.cuh:577-615
  * with cuRAND's per-thread XORWOW stream replaced by Philox4x32-10 keyed by
  * (seed; draw block, walker, update id, domain).  Deviations from the
- * reference are the ones the CUDA path makes too (documented in DESIGN.md):
+ * reference are the ones the CUDA path makes too:
  * a walker whose source has degree 0 fails instead of computing `x % 0`,
  * the winner is (max 1/R, lowest walker id) for every walker count, and the
  * fallback walk's second step reads the row of the vertex it stands on.

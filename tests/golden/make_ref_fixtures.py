@@ -3,9 +3,9 @@ updaters on the known-answer cases of kat_cases.py.
 
 The reference (random_walk_incremental/, random_walk_decremental/) is built
 unmodified from its sources by `make -C oracle ref-gpu` into oracle/_ref/;
-it needs a GPU, so this script runs on the B200 box:
+it needs a GPU, so this script runs on a machine with a B200:
 
-    python tests/golden/make_ref_fixtures.py gpurun_out/ref_kat.json
+    python tests/golden/make_ref_fixtures.py out/ref_kat.json
 
 It writes each case as ../dataset/<case>/ (the reference's fixed relative
 layout, main.cu:247-249, 326-329) under a scratch directory, runs the
