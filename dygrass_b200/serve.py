@@ -90,6 +90,8 @@ class Server:
             used += fp
             self.admitted.append(i)
             offs.append(offs[-1] + c.n)
+        if not self.admitted:
+            raise ValueError("no graph fits the HBM budget")
         self.footprint = used
         self.slot = {g: k for k, g in enumerate(self.admitted)}
         self.offsets = np.array(offs, np.int64)

@@ -145,3 +145,11 @@ def test_footprint_grows_with_the_graph():
     assert footprint_bytes(1000, 4000, 3000) > base
     # slots (12 B each) of both graphs with headroom, plus descriptors
     assert base >= 12 * 2 * (4000 + 1500)
+
+
+def test_server_needs_an_admitted_graph():
+    import pytest
+    from dygrass_b200.serve import Server
+    cases = fake_cases(k=2)
+    with pytest.raises(ValueError, match="HBM budget"):
+        Server(cases, None, None, hbm_budget=10.0)
