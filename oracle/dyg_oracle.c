@@ -498,7 +498,8 @@ static void walk_ends(const uint32_t *src, const uint32_t *dst, uint32_t e, int 
 static uint64_t decr_walk(orc_graph *G, orc_graph *H, const uint32_t *src, const uint32_t *dst,
                           const uint32_t *filt, uint32_t nf, uint64_t first_uid, int file_orient,
                           const orc_params *p, int threads, int32_t *status, float *cond,
-                          rec_t *rc, const uint64_t *keys_in) {
+                          rec_t *rc, const uint64_t *keys_in, const uint64_t *uids) {
+#define DECR_UID(e) (uids ? uids[e] : first_uid + (e))
     uint64_t moves = 0;
     uint64_t *keys = (uint64_t *)malloc((size_t)(nf ? nf : 1) * sizeof(uint64_t));
     if (threads < 1) threads = 1;
@@ -508,7 +509,7 @@ static uint64_t decr_walk(orc_graph *G, orc_graph *H, const uint32_t *src, const
         uint32_t e = filt[f], a, b;
         walk_ends(src, dst, e, file_orient, &a, &b);
         uint64_t mv = 0;
-        keys[f] = best_key(G, a, b, 0.0f, 0, p, first_uid + e, DOMAIN_DECR, &mv);
+        keys[f] = best_key(G, a, b, 0.0f, 0, p, DECR_UID(e), DOMAIN_DECR, &mv);
         moves += mv;
     }
     uint32_t pathlen = p->max_steps > 2 ? p->max_steps : 2;
@@ -523,7 +524,7 @@ static uint64_t decr_walk(orc_graph *G, orc_graph *H, const uint32_t *src, const
         if (k) {
             uint32_t walker = 1023u - (uint32_t)((k >> 22) & 0x3FFu);
             float R;
-            int32_t found = decr_walk_path(G, a, b, first_uid + e, walker, p, path, pathw, &R);
+            int32_t found = decr_walk_path(G, a, b, DECR_UID(e), walker, p, path, pathw, &R);
             if (status) status[e] = found;
             if (cond) cond[e] = key_cond(k);
             for (int32_t j = 0; j < found; ++j) rec_add(H, rc, path[j], path[j + 1], pathw[j + 1], 0);
@@ -538,7 +539,7 @@ static uint64_t decr_walk(orc_graph *G, orc_graph *H, const uint32_t *src, const
         for (uint32_t side = 0; side < 2; ++side) {
             for (uint32_t j = 0; j < p->heuristic_walkers; ++j) {
                 rng_t rng;
-                rng_init(&rng, p->seed, first_uid + e, DOMAIN_HEUR, side * p->heuristic_walkers + j);
+                rng_init(&rng, p->seed, DECR_UID(e), DOMAIN_HEUR, side * p->heuristic_walkers + j);
                 uint32_t s0 = ends[side];
                 uint32_t d0 = G->deg[s0];
                 if (d0 == 0) continue;
@@ -562,6 +563,7 @@ static uint64_t decr_walk(orc_graph *G, orc_graph *H, const uint32_t *src, const
     free(path); free(pathw); free(nop); free(keys);
     return moves;
 }
+#undef DECR_UID
 
 uint64_t orc_decremental_batch(orc_graph *G, orc_graph *H, const uint32_t *src,
                                const uint32_t *dst, uint32_t n, uint64_t first_uid,
@@ -573,7 +575,24 @@ uint64_t orc_decremental_batch(orc_graph *G, orc_graph *H, const uint32_t *src,
     rec_t rc = {0};
     rc.cap_out = rec_cap; rc.out_a = rec_src; rc.out_b = rec_dst; rc.out_kind = rec_kind;
     uint64_t moves = decr_walk(G, H, src, dst, filt, nf, first_uid, 0, p, threads, status, cond, &rc,
-                               NULL);
+                               NULL, NULL);
+    if (n_rec) *n_rec = rc.n;
+    free(filt);
+    return moves;
+}
+
+/* orc_decremental_batch with each deletion's update id read from uids[e] */
+uint64_t orc_decremental_batch_ids(orc_graph *G, orc_graph *H, const uint32_t *src,
+                                   const uint32_t *dst, const uint64_t *uids, uint32_t n,
+                                   const orc_params *p, int threads, int32_t *status,
+                                   float *cond, uint32_t *rec_src, uint32_t *rec_dst,
+                                   uint8_t *rec_kind, uint64_t rec_cap, uint64_t *n_rec) {
+    uint32_t *filt = (uint32_t *)malloc((size_t)(n ? n : 1) * sizeof(uint32_t));
+    uint32_t nf = decr_delete(G, H, src, dst, n, status, cond, filt);
+    rec_t rc = {0};
+    rc.cap_out = rec_cap; rc.out_a = rec_src; rc.out_b = rec_dst; rc.out_kind = rec_kind;
+    uint64_t moves = decr_walk(G, H, src, dst, filt, nf, 0, 0, p, threads, status, cond, &rc,
+                               NULL, uids);
     if (n_rec) *n_rec = rc.n;
     free(filt);
     return moves;
@@ -667,7 +686,7 @@ uint64_t orc_stream_file(orc_graph *G, orc_graph *H, uint32_t op, const uint32_t
         for (uint32_t c0 = 0; c0 < nl; c0 += chunk) {
             uint32_t c1 = nl - c0 < chunk ? nl : c0 + chunk;
             moves += decr_walk(G, H, src, dst, list + c0, c1 - c0, first_uid, 1, p, threads,
-                               status, cond, &rc, NULL);
+                               status, cond, &rc, NULL, NULL);
         }
         if (n_rec) *n_rec = rc.n;
     }
@@ -702,7 +721,7 @@ void orc_decremental_commit_keys(orc_graph *G, orc_graph *H, const uint32_t *src
                                  uint8_t *rec_kind, uint64_t rec_cap, uint64_t *n_rec) {
     rec_t rc = {0};
     rc.cap_out = rec_cap; rc.out_a = rec_src; rc.out_b = rec_dst; rc.out_kind = rec_kind;
-    decr_walk(G, H, src, dst, walk_list, nf, first_uid, 0, p, 1, status, cond, &rc, keys);
+    decr_walk(G, H, src, dst, walk_list, nf, first_uid, 0, p, 1, status, cond, &rc, keys, NULL);
     if (n_rec) *n_rec = rc.n;
 }
 

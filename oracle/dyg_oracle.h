@@ -126,6 +126,13 @@ uint64_t orc_stream_file(orc_graph *G, orc_graph *H, uint32_t op, const uint32_t
 void orc_walk_keys(const orc_graph *g, const uint32_t *src, const uint32_t *dst, const float *w,
                    uint64_t first_uid, uint32_t lo, uint32_t hi, int incr, const orc_params *p,
                    int threads, uint64_t *keys, uint64_t *moves);
+/* orc_decremental_batch with each deletion's update id read from uids[e]
+ * (a union of graphs served together, as the server does). */
+uint64_t orc_decremental_batch_ids(orc_graph *G, orc_graph *H, const uint32_t *src,
+                                   const uint32_t *dst, const uint64_t *uids, uint32_t n,
+                                   const orc_params *p, int threads, int32_t *status,
+                                   float *cond, uint32_t *rec_src, uint32_t *rec_dst,
+                                   uint8_t *rec_kind, uint64_t rec_cap, uint64_t *n_rec);
 /* orc_walk_keys with each edge's update id read from uids[e] (the batched
  * many-graph mode: a union of graphs at vertex offsets, every edge carrying
  * its position in its own graph's stream), incremental walks on g. */

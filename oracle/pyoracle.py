@@ -64,6 +64,8 @@ def lib() -> C.CDLL:
             "orc_walk_keys": ([vp, vp, vp, vp, u64, u32, u32, C.c_int, P, C.c_int, vp, vp], None),
             "orc_incremental_commit_keys": ([vp, vp, vp, vp, vp, u32, vp, vp, vp, vp], None),
             "orc_walk_keys_ids": ([vp, vp, vp, vp, vp, u32, P, C.c_int, vp, vp], None),
+            "orc_decremental_batch_ids": ([vp, vp, vp, vp, vp, u32, P, C.c_int, vp, vp, vp, vp, vp, u64,
+                                           C.POINTER(u64)], u64),
             "orc_decremental_delete": ([vp, vp, vp, vp, u32, vp, vp, vp], u32),
             "orc_decremental_walk_list_keys": ([vp, vp, vp, vp, u32, u32, u64, P, C.c_int, vp], None),
             "orc_decremental_commit_keys": ([vp, vp, vp, vp, vp, u32, u64, P, vp, vp, vp, vp, vp, vp,
@@ -188,6 +190,25 @@ def decremental(G: OGraph, H: OGraph, src, dst, params, batch_size=0, threads=No
                                           _p(st), _p(cd), _p(rx), _p(ry), _p(rk), cap, C.byref(nr))
     k = nr.value
     return st, cd, rx[:k].copy(), ry[:k].copy(), rk[:k].copy(), int(mv)
+
+
+def decremental_ids(G: OGraph, H: OGraph, src, dst, uids, params, threads=None):
+    """One decremental batch whose deletion e uses update id uids[e].
+    Returns (status, cond, rec_src, rec_dst, rec_kind)."""
+    src = np.ascontiguousarray(src, np.uint32)
+    dst = np.ascontiguousarray(dst, np.uint32)
+    uids = np.ascontiguousarray(uids, np.uint64)
+    n = len(src)
+    cap = n * (params.max_steps + 4 * params.heuristic_walkers) + 16
+    st, cd = np.empty(n, np.int32), np.empty(n, np.float32)
+    rx, ry, rk = np.empty(cap, np.uint32), np.empty(cap, np.uint32), np.empty(cap, np.uint8)
+    nr = C.c_uint64()
+    P = Params.from_walk_params(params)
+    lib().orc_decremental_batch_ids(G.h, H.h, _p(src), _p(dst), _p(uids), n, C.byref(P),
+                                    threads or max_threads(), _p(st), _p(cd), _p(rx), _p(ry), _p(rk),
+                                    cap, C.byref(nr))
+    k = nr.value
+    return st, cd, rx[:k].copy(), ry[:k].copy(), rk[:k].copy()
 
 
 def stream_file(G: OGraph, H: OGraph, op, src, dst, w, params, first_uid=0, chunk=0,

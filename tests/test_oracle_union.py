@@ -1,11 +1,14 @@
-"""The batched many-graph mode's premise, checked on the oracle (no GPU):
+"""The batched and serving modes' premise, checked on the oracle (no GPU):
 graphs packed into one union graph at vertex offsets and updated round by
 round, batch r of every graph in one batch whose edges carry their position
 in their own graph's stream as update id, give every graph exactly the
 found_at, conductance and accepted flags, and the final sparsifier rows, of
 its own reference-style loop (ceil(n/10)-edge batches, first update id = the
-batch's first position).  The CUDA path is held to the same property by
-tests/test_multi.py and tests/test_serve.py."""
+batch's first position).  The same for the server's steps: the oldest
+request of every graph per step, the step's insertions as one batch and its
+deletions as another, each update with its graph's own update id.  The CUDA
+path is held to the same property by tests/test_multi.py and
+tests/test_serve.py."""
 import os
 import sys
 
@@ -83,3 +86,79 @@ def test_update_ids_matter():
     fb, cb, _ = pyoracle.incremental_ids(Hv, rd.src, rd.dst, rd.w,
                                          np.arange(len(rd.src), dtype=np.uint64), p, threads=4)
     assert not (np.array_equal(fa, fb) and np.array_equal(cd.view(np.uint32), cb.view(np.uint32)))
+
+
+def test_served_steps_equal_each_graph_alone():
+    from dygrass_b200.serve import DELETE, INSERT, poisson_requests
+    cases = small_cases()
+    p = dyg.WalkParams.make(threshold=50.0, walkers=64, max_steps=48)
+    offsets = np.zeros(len(cases) + 1, np.int64)
+    offsets[1:] = np.cumsum([c.n for c in cases])
+    reqs = poisson_requests(cases, rate=1e6, count=40, seed=9, size_hi=60)
+    Hu, Gu = union_graph(cases, offsets, "h"), union_graph(cases, offsets, "g")
+    queues = {g: [r for r in reqs if r.graph == g] for g in range(len(cases))}
+    uid_next = [0] * len(cases)
+    got = {}
+    while any(queues.values()):
+        heads = [queues[g].pop(0) for g in range(len(cases)) if queues[g]]
+        for op in (INSERT, DELETE):
+            sel = [r for r in heads if r.op == op and len(r.src)]
+            if not sel:
+                continue
+            src = np.concatenate([r.src + offsets[r.graph] for r in sel]).astype(np.uint32)
+            dst = np.concatenate([r.dst + offsets[r.graph] for r in sel]).astype(np.uint32)
+            uid = np.concatenate([np.arange(len(r.src), dtype=np.uint64) + np.uint64(uid_next[r.graph])
+                                  for r in sel])
+            if op == INSERT:
+                w = np.concatenate([r.w for r in sel]).astype(np.float32)
+                out = pyoracle.incremental_ids(Hu, src, dst, w, uid, p, G=Gu, threads=4)
+            else:
+                st, cd, rx, ry, rk = pyoracle.decremental_ids(Gu, Hu, src, dst, uid, p, threads=4)
+                owner = np.searchsorted(offsets, rx, side="right") - 1
+                out = (st, cd)
+            k = 0
+            for r in sel:
+                m = len(r.src)
+                res = tuple(a[k:k + m] for a in out)
+                if op == DELETE:
+                    o = owner == r.graph
+                    res += (list(zip((rx[o] - offsets[r.graph]).tolist(),
+                                     (ry[o] - offsets[r.graph]).tolist(), rk[o].tolist())),)
+                got[id(r)] = res
+                k += m
+        for r in heads:
+            uid_next[r.graph] += len(r.src)
+    alone = [(pyoracle.OGraph(c.n, c.h_src, c.h_dst, c.h_w), pyoracle.OGraph(c.n, c.g_src, c.g_dst, c.g_w))
+             for c in cases]
+    uid_alone = [0] * len(cases)
+    n_rec = 0
+    for r in reqs:
+        Hg, Gg = alone[r.graph]
+        u = uid_alone[r.graph]
+        uid_alone[r.graph] += len(r.src)
+        if not len(r.src):
+            continue
+        if r.op == INSERT:
+            fa, cd, ac, _ = pyoracle.incremental(Hg, r.src, r.dst, r.w, p, G=Gg, threads=4, first_uid=u,
+                                                 single_batch=True)
+            gfa, gcd, gac = got[id(r)]
+            assert np.array_equal(gfa, fa) and np.array_equal(gac, ac)
+            assert np.array_equal(gcd.view(np.uint32), cd.view(np.uint32))
+        else:
+            st, cd, rx, ry, rk, _ = pyoracle.decremental(Gg, Hg, r.src, r.dst, p, threads=4, first_uid=u,
+                                                         single_batch=True)
+            gst, gcd, grec = got[id(r)]
+            assert np.array_equal(gst, st)
+            assert np.array_equal(gcd.view(np.uint32), cd.view(np.uint32))
+            assert grec == list(zip(rx.tolist(), ry.tolist(), rk.tolist()))
+            n_rec += len(grec)
+    assert n_rec > 0                                  # deletions recovered edges
+    for which, u in (("H", Hu), ("G", Gu)):
+        rp, col, w = u.export()
+        for g in range(len(cases)):
+            lo, hi = int(offsets[g]), int(offsets[g + 1])
+            a, b = int(rp[lo]), int(rp[hi])
+            rp1, col1, w1 = alone[g][0 if which == "H" else 1].export()
+            assert np.array_equal(rp[lo:hi + 1] - rp[lo], rp1), (which, g)
+            assert np.array_equal(col[a:b] - lo, col1), (which, g)
+            assert np.array_equal(w[a:b].view(np.uint32), w1.view(np.uint32)), (which, g)
