@@ -1,4 +1,4 @@
-"""A batch sharded over two processes (gloo, world size 2, CPU): the driver
+"""A batch sharded over processes (gloo, world size 2 and 3, CPU): the driver
 of dygrass_b200.shard with the oracle as its compute gives every rank the
 whole-batch result, insertions and deletions, over several batches."""
 import json
@@ -76,11 +76,13 @@ def _rank_main(rank, world, port, out_dir):
         json.dump({"ok": bool(ok), "why": why}, f)
 
 
-def test_sharded_batches_match_whole_batches(tmp_path):
+@pytest.mark.parametrize("world", [2, 3])
+def test_sharded_batches_match_whole_batches(tmp_path, world):
+    """world 3 splits the batches and walk lists into uneven rank ranges."""
     import torch.multiprocessing as mp
     port = _free_port()
-    mp.start_processes(_rank_main, args=(2, port, str(tmp_path)), nprocs=2, join=True,
+    mp.start_processes(_rank_main, args=(world, port, str(tmp_path)), nprocs=world, join=True,
                        start_method="spawn")
-    for r in range(2):
+    for r in range(world):
         res = json.load(open(tmp_path / f"rank{r}.json"))
         assert res["ok"], res["why"]
