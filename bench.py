@@ -56,6 +56,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -182,14 +183,14 @@ class ClockSampler:
     def __init__(self, device_index: int):
         self.dev = device_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device_index}.csv")
+        fd, self.path = tempfile.mkstemp(prefix=f"dyg_clocks{device_index}_", suffix=".csv")
+        os.close(fd)
 
     def start(self):
         """Starts nvidia-smi and returns once its first sample is written, so
         that the samples after it fall inside the timed region."""
         self.n0 = 0
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
@@ -232,6 +233,10 @@ class ClockSampler:
             for nm, v in zip(names, parts[5:9]):
                 if v.lower() == "active":
                     reasons.add(nm)
+        try:
+            os.unlink(self.path)
+        except OSError:
+            pass
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
                 "reasons": sorted(reasons), "samples": len(sm) if inside else 0,
                 "when": "during the timed region" if inside else "just before the timed region"}

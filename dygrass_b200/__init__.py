@@ -134,6 +134,7 @@ def lib() -> C.CDLL:
         "dyg_decremental_stream": ([vp, vp, vp, vp, u32, u32, C.POINTER(WalkParams), vp, vp, vp, vp, vp, u64,
                                     C.POINTER(u64), vp], C.c_int),
         "dyg_stream_default_chunk": ([u32], u32),
+        "dyg_recovered_read": ([vp, u64, u64, vp, vp, vp], C.c_int),
         "dyg_stream_file": ([vp, vp, u32, vp, vp, vp, u32, u64, u32, C.POINTER(WalkParams), vp, vp, vp,
                              vp, vp, u64, C.POINTER(u64), vp], C.c_int),
         "dyg_synth_rmat": ([u32, u32, C.c_double, C.c_double, C.c_double, C.c_float, C.c_float, u64,
@@ -377,17 +378,32 @@ class DecrementalResult:
     rec_kind: np.ndarray    # u8: REC_PATH / REC_FALLBACK
 
 
+def recovered_read(G: Graph, count: int, first: int = 0):
+    """Recovered edges [first, first + count) of the last decremental call on
+    G (dyg_recovered_read): (rec_src, rec_dst, rec_kind) as numpy arrays."""
+    rx = np.empty(max(count, 1), np.uint32)
+    ry = np.empty(max(count, 1), np.uint32)
+    rk = np.empty(max(count, 1), np.uint8)
+    _check(lib().dyg_recovered_read(G.handle, int(first), int(count), _ptr(rx), _ptr(ry), _ptr(rk)),
+           "dyg_recovered_read")
+    return rx[:count], ry[:count], rk[:count]
+
+
 def _decremental(fn, G, H, src, dst, params, arg, stream, rec_cap):
+    """With rec_cap None the call records no edges into caller buffers; the
+    total comes back in n_rec and exactly that many are read afterwards."""
     src, dst = _as(src, np.uint32), _as(dst, np.uint32)
     n = len(src)
-    if rec_cap is None:
-        rec_cap = n * (params.max_steps + 4 * params.heuristic_walkers) + 16
     st = np.empty(n, np.int32)
     cd = np.empty(n, np.float32)
+    nrec = C.c_uint64()
+    if rec_cap is None:
+        _check(fn(G.handle, H.handle, _ptr(src), _ptr(dst), n, int(arg), C.byref(params), _ptr(st),
+                  _ptr(cd), None, None, None, 0, C.byref(nrec), stream), fn.__name__)
+        return DecrementalResult(st, cd, *recovered_read(G, nrec.value))
     rx = np.empty(max(rec_cap, 1), np.uint32)
     ry = np.empty(max(rec_cap, 1), np.uint32)
     rk = np.empty(max(rec_cap, 1), np.uint8)
-    nrec = C.c_uint64()
     _check(fn(G.handle, H.handle, _ptr(src), _ptr(dst), n, int(arg), C.byref(params), _ptr(st),
               _ptr(cd), _ptr(rx), _ptr(ry), _ptr(rk), rec_cap, C.byref(nrec), stream),
            fn.__name__)
@@ -561,10 +577,16 @@ def stream_file(G: Graph, H: Graph, op: int, src, dst, w, params: WalkParams,
     src, dst = _as(src, np.uint32), _as(dst, np.uint32)
     w = None if w is None else _as(w, np.float32)
     n = len(src)
-    if rec_cap is None:
-        rec_cap = 0 if op == STREAM_INSERT else n * (params.max_steps + 4 * params.heuristic_walkers) + 16
     st = np.empty(n, np.int32)
     cd = np.empty(n, np.float32)
+    if rec_cap is None:
+        nrec = C.c_uint64()
+        _check(lib().dyg_stream_file(G.handle, H.handle, int(op), _ptr(src), _ptr(dst), _ptr(w), n,
+                                     int(first_update_id), int(chunk), C.byref(params), _ptr(st),
+                                     _ptr(cd), None, None, None, 0, C.byref(nrec), stream),
+               "dyg_stream_file")
+        recs = recovered_read(G, nrec.value) if op != STREAM_INSERT else recovered_read(G, 0)
+        return DecrementalResult(st, cd, *recs)
     rx = np.empty(max(rec_cap, 1), np.uint32)
     ry = np.empty(max(rec_cap, 1), np.uint32)
     rk = np.empty(max(rec_cap, 1), np.uint8)
@@ -595,4 +617,4 @@ def stream_file_into(G: Graph, H: Graph, op: int, src, dst, w, params: WalkParam
 __all__ = ["Graph", "WalkParams", "GraphOpts", "DygError", "incremental_batch",
            "incremental_stream", "decremental_batch", "decremental_stream", "lib", "version",
            "reference_batch_size", "IncrementalResult", "DecrementalResult", "stream_file",
-           "stream_file_into", "stream_default_chunk", "kappa", "graph_edges"]
+           "stream_file_into", "stream_default_chunk", "kappa", "graph_edges", "recovered_read"]

@@ -29,6 +29,29 @@ dyg_status cuda_fail(cudaError_t e, const char *what, const char *file, int line
     return DYG_ECUDA;
 }
 
+PtrPlace ptr_place(const void *p, int device) {
+    if (!p) return kOnHost;
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return kOnHost;
+    }
+    if (at.type == cudaMemoryTypeManaged) return kOnDevice;
+    if (at.type == cudaMemoryTypeDevice) return at.device == device ? kOnDevice : kOnOtherDevice;
+    return kOnHost;
+}
+
+dyg_status check_same_device(int device, const void *const *ptrs, const char *const *names,
+                             int count) {
+    for (int i = 0; i < count; ++i)
+        if (ptrs[i] && ptr_place(ptrs[i], device) == kOnOtherDevice) {
+            set_error(std::string(names[i]) + " is device memory of another GPU than the graph's (device " +
+                      std::to_string(device) + ")");
+            return DYG_EINVAL;
+        }
+    return DYG_OK;
+}
+
 namespace {
 
 struct DeviceGuard {
@@ -135,6 +158,10 @@ dyg_status check_device_errors(dyg_graph *G, cudaStream_t st) {
                             cudaMemcpyHostToDevice));
         if (err & kErrVertex) {
             set_error("a batch endpoint is not a vertex of the graph");
+            return DYG_EINVAL;
+        }
+        if (err & kErrWeight) {
+            set_error("a batch weight is not finite and > 0");
             return DYG_EINVAL;
         }
         set_error("internal consistency check failed (device error bits " + std::to_string(err) + ")");
@@ -545,6 +572,11 @@ static dyg_status incremental_common(dyg_graph *H, dyg_graph *G, const uint32_t 
     if (n == 0) return DYG_OK;
     DeviceGuard dg(H->device);
     cudaStream_t st = (cudaStream_t)stream;
+    {
+        const void *ps[] = {src, dst, w, uids, found_at, conductance, accepted};
+        const char *nm[] = {"src", "dst", "w", "update_ids", "found_at", "conductance", "accepted"};
+        DYG_TRY(check_same_device(H->device, ps, nm, 7));
+    }
     DYG_TRY(check_host_ids(src, n, H->g.n, "src"));
     DYG_TRY(check_host_ids(dst, n, H->g.n, "dst"));
     DYG_TRY(check_host_weights(w, n));
@@ -573,9 +605,11 @@ static dyg_status incremental_common(dyg_graph *H, dyg_graph *G, const uint32_t 
         o_acc = ptr<uint8_t>(ws.s_o3);
     }
     const uint32_t B = batch_size ? batch_size : dyg_reference_batch_size(n);
+    // inputs read in place from device memory were not checked on the host
+    const bool dev_in = d_src == src || d_dst == dst || d_w == w;
     DYG_TRY(incremental_run(H, G, d_src, d_dst, d_w, n, B, uid_base,
                             (const unsigned long long *)d_uid, *p, o_found, o_cond, o_acc,
-                            st));
+                            st, dev_in));
     if (H->ws.host_scalars[S_ERR]) DYG_TRY(check_device_errors(H, st));
     bool host_out = false;
     if (found_at && o_found != found_at) DYG_TRY(copy_out(found_at, (const int32_t *)o_found, n, st, &host_out));
@@ -624,6 +658,12 @@ static dyg_status decremental_common(dyg_graph *G, dyg_graph *H, const uint32_t 
     if (n == 0) return DYG_OK;
     DeviceGuard dg(G->device);
     cudaStream_t st = (cudaStream_t)stream;
+    {
+        const void *ps[] = {src, dst, uids, status, conductance, rec_src, rec_dst, rec_kind};
+        const char *nm[] = {"src", "dst", "update_ids", "status", "conductance",
+                            "rec_src", "rec_dst", "rec_kind"};
+        DYG_TRY(check_same_device(G->device, ps, nm, 8));
+    }
     DYG_TRY(check_host_ids(src, n, G->g.n, "src"));
     DYG_TRY(check_host_ids(dst, n, G->g.n, "dst"));
     Workspace &ws = G->ws;
@@ -644,8 +684,11 @@ static dyg_status decremental_common(dyg_graph *G, dyg_graph *H, const uint32_t 
     }
     const uint32_t B = batch_size ? batch_size : dyg_reference_batch_size(n);
     uint64_t total = 0;
+    const bool dev_in = d_src == src || d_dst == dst;
+    G->last_rec = 0;
     DYG_TRY(decremental_run(G, H, d_src, d_dst, n, B, uid_base, (const unsigned long long *)d_uid,
-                            *p, o_st, o_cd, &total, st));
+                            *p, o_st, o_cd, &total, st, dev_in));
+    G->last_rec = total;
     if (G->ws.host_scalars[S_ERR]) DYG_TRY(check_device_errors(G, st));
     bool host_out = false;
     if (status && o_st != status) DYG_TRY(copy_out(status, (const int32_t *)o_st, n, st, &host_out));
@@ -708,6 +751,35 @@ dyg_status dyg_decremental_batch_ids(dyg_graph *G, dyg_graph *H, const uint32_t 
                               rec_src, rec_dst, rec_kind, rec_cap, n_rec, stream);
 }
 
+dyg_status dyg_recovered_read(const dyg_graph *g, uint64_t first, uint64_t count,
+                              uint32_t *rec_src, uint32_t *rec_dst, uint8_t *rec_kind) {
+    set_error("");
+    if (!g) {
+        set_error("NULL graph");
+        return DYG_EINVAL;
+    }
+    if (first > g->last_rec || count > g->last_rec - first) {
+        set_error("records [" + std::to_string(first) + ", " + std::to_string(first + count) +
+                  ") are not all among the last call's " + std::to_string(g->last_rec));
+        return DYG_ERANGE;
+    }
+    if (count == 0) return DYG_OK;
+    DeviceGuard dg(g->device);
+    const Workspace &ws = g->ws;
+    const void *ps[] = {rec_src, rec_dst, rec_kind};
+    const char *nm[] = {"rec_src", "rec_dst", "rec_kind"};
+    DYG_TRY(check_same_device(g->device, ps, nm, 3));
+    if (rec_src)
+        DYG_CUDA(cudaMemcpy(rec_src, ptr<uint32_t>(ws.rx2) + first, sizeof(uint32_t) * count,
+                            cudaMemcpyDefault));
+    if (rec_dst)
+        DYG_CUDA(cudaMemcpy(rec_dst, ptr<uint32_t>(ws.ry2) + first, sizeof(uint32_t) * count,
+                            cudaMemcpyDefault));
+    if (rec_kind)
+        DYG_CUDA(cudaMemcpy(rec_kind, ptr<uint8_t>(ws.rk2) + first, count, cudaMemcpyDefault));
+    return DYG_OK;
+}
+
 uint32_t dyg_stream_default_chunk(uint32_t n_vertices) {
     return stream_default_chunk(n_vertices);
 }
@@ -737,6 +809,12 @@ dyg_status dyg_stream_file(dyg_graph *G, dyg_graph *H, uint32_t op, const uint32
     if (n == 0) return DYG_OK;
     DeviceGuard dg(G->device);
     cudaStream_t st = (cudaStream_t)stream;
+    {
+        const void *ps[] = {src, dst, w, status, conductance, rec_src, rec_dst, rec_kind};
+        const char *nm[] = {"src", "dst", "w", "status", "conductance", "rec_src", "rec_dst",
+                            "rec_kind"};
+        DYG_TRY(check_same_device(G->device, ps, nm, 8));
+    }
     DYG_TRY(check_host_ids(src, n, G->g.n, "src"));
     DYG_TRY(check_host_ids(dst, n, G->g.n, "dst"));
     if (ins) DYG_TRY(check_host_weights(w, n));
@@ -757,8 +835,11 @@ dyg_status dyg_stream_file(dyg_graph *G, dyg_graph *H, uint32_t op, const uint32
         o_cd = ptr<float>(ws.s_o2);
     }
     uint64_t total = 0;
+    const bool dev_in = d_src == src || d_dst == dst || (ins && d_w == w);
+    if (!ins) G->last_rec = 0;
     DYG_TRY(stream_file_run(G, H, op, d_src, d_dst, d_w, n, first_update_id, chunk, *p, o_st, o_cd,
-                            &total, st));
+                            &total, st, dev_in));
+    if (!ins) G->last_rec = total;
     if (G->ws.host_scalars[S_ERR]) DYG_TRY(check_device_errors(G, st));
     bool host_out = false;
     if (status && o_st != status) DYG_TRY(copy_out(status, (const int32_t *)o_st, n, st, &host_out));

@@ -36,6 +36,7 @@ constexpr uint32_t kDomainHeur = 2u;   // 2-step fallback walks
 constexpr uint32_t kErrVertex = 1u;    // vertex id >= n in a batch
 constexpr uint32_t kErrPath = 2u;      // winner re-walk disagreed with its key
 constexpr uint32_t kErrArena = 4u;     // arena overflow in a commit
+constexpr uint32_t kErrWeight = 8u;    // weight not finite and > 0 in a batch
 
 struct DevGraph {
     uint2 *desc;
@@ -215,6 +216,7 @@ enum Count : int {
 // Halt codes: (batch + 1) << 8 | kind << 4 | phase.
 constexpr unsigned long long kHaltArena = 1;    // an arena reservation did not fit
 constexpr unsigned long long kHaltRecords = 2;  // the recovered-edge buffers are full
+constexpr unsigned long long kHaltInvalid = 3;  // a device-resident batch failed its input check
 __host__ __device__ __forceinline__ unsigned long long halt_code(uint32_t batch, uint32_t kind,
                                                                  uint32_t phase) {
     return ((unsigned long long)(batch + 1) << 8) | (kind << 4) | phase;
@@ -236,6 +238,9 @@ struct dyg_graph {
     double headroom = 0.5;
     dyg::Workspace ws;
     uint64_t moves_total = 0, walks_total = 0;
+    // Recovered edges recorded by the last decremental call on this handle
+    // (as G); they stay in ws.rx2 / ry2 / rk2 until the next such call.
+    uint64_t last_rec = 0;
     // The graph has (or may have) a row longer than kBigRow: row operations
     // then send such rows to the block-cooperative kernels.  Without it every
     // row takes the one-thread path (same results, no extra launches).
@@ -260,6 +265,16 @@ dyg_status cuda_fail(cudaError_t e, const char *what, const char *file, int line
     } while (0)
 
 dyg_status ensure(Buf &b, size_t bytes);
+// Where a caller's pointer lives as seen from `device`: host memory (pageable
+// or pinned), device memory this device's kernels may read (its own, or
+// managed), or device memory of another GPU, which a kernel on `device`
+// must not be given.
+enum PtrPlace : int { kOnHost = 0, kOnDevice = 1, kOnOtherDevice = 2 };
+PtrPlace ptr_place(const void *p, int device);
+// DYG_EINVAL (with the argument's name in the message) if any non-null
+// pointer of `ptrs` is device memory of another GPU than `device`.
+dyg_status check_same_device(int device, const void *const *ptrs, const char *const *names,
+                             int count);
 template <typename T>
 inline T *ptr(const Buf &b) { return static_cast<T *>(b.p); }
 
@@ -301,15 +316,28 @@ dyg_status device_errors(dyg_graph *G, cudaStream_t st);
 dyg_status check_walk_params(const dyg_walk_params *p);
 
 // --- pipeline.cu
+// Checks a device-resident batch before anything else of the call runs: an
+// endpoint >= nv (kErrVertex) or a weight that is not finite and > 0
+// (kErrWeight, when w is given) sets the error bits and the halt code
+// kHaltInvalid, so every later kernel of the call returns at once and the
+// graphs stay exactly as they were.
+dyg_status validate_enqueue(unsigned long long *halt, unsigned long long *err,
+                            const uint32_t *src, const uint32_t *dst, const float *w, uint32_t n,
+                            uint32_t nv, cudaStream_t st);
+// After a run halted with kHaltInvalid: clears the halt and the error bits of
+// D (the handle whose scalars held them) and returns DYG_EINVAL with the
+// failed check as the message.
+dyg_status rejected_inputs(dyg_graph *D, cudaStream_t st);
 // uids (device, may be null): per-edge update ids instead of uid_base + e.
 dyg_status incremental_run(dyg_graph *H, dyg_graph *G, const uint32_t *src, const uint32_t *dst,
                            const float *w, uint32_t n, uint32_t B, uint64_t uid_base,
                            const unsigned long long *uids, const dyg_walk_params &p, int32_t *found, float *cond, uint8_t *acc,
-                           cudaStream_t st);
+                           cudaStream_t st, bool check_inputs = false);
 dyg_status decremental_run(dyg_graph *G, dyg_graph *H, const uint32_t *src, const uint32_t *dst,
                            uint32_t n, uint32_t B, uint64_t uid_base,
                            const unsigned long long *uids, const dyg_walk_params &p,
-                           int32_t *status, float *cond, uint64_t *n_rec, cudaStream_t st);
+                           int32_t *status, float *cond, uint64_t *n_rec, cudaStream_t st,
+                           bool check_inputs = false);
 
 dyg_status decr_delete_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src,
                                const uint32_t *dst, uint32_t n, uint64_t uid0,
@@ -336,7 +364,7 @@ uint32_t stream_default_chunk(uint32_t n_vertices);
 dyg_status stream_file_run(dyg_graph *G, dyg_graph *H, uint32_t op, const uint32_t *src,
                            const uint32_t *dst, const float *w, uint32_t n, uint64_t uid0,
                            uint32_t chunk, const dyg_walk_params &p, int32_t *status, float *cond,
-                           uint64_t *n_rec, cudaStream_t st);
+                           uint64_t *n_rec, cudaStream_t st, bool check_inputs = false);
 
 // --- graph.cu
 dyg_status upload_graph(dyg_graph *G, uint32_t n, const uint64_t *row_ptr, const uint32_t *col,

@@ -17,8 +17,13 @@
 // counters it uses; calls whose work overlaps on the GPU (different streams,
 // or different host threads) race on it and must be serialized by the
 // caller.  The first call on a device looks up the array's device address
-// with cudaGetSymbolAddress (set-up); make that first call before any stream
+// with cudaGetSymbolAddress (set-up), and so does the first call after the
+// device's context was replaced (cudaDeviceReset destroys the array with the
+// context; the address is cached together with the context's unique id and
+// looked up again when the id changes).  Make those calls before any stream
 // capture.
+#include <cuda.h>
+
 #include <mutex>
 
 #include "dyg_internal.cuh"
@@ -37,17 +42,47 @@ namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mu;
 unsigned long long *g_scratch_addr[kMaxDevices] = {nullptr};
+unsigned long long g_scratch_ctx[kMaxDevices] = {0};
+
+// Unique id of the context current on this thread (cuCtxGetId, reached through
+// the runtime's driver entry points, so no libcuda link is needed); 0 when the
+// driver does not provide it.
+unsigned long long current_context_id() {
+    typedef CUresult (*GetCurrent)(CUcontext *);
+    typedef CUresult (*GetId)(CUcontext, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(f);
+        cudaGetLastError();
+    });
+    if (!get_current || !get_id) return 0ull;
+    CUcontext c = nullptr;
+    unsigned long long id = 0ull;
+    if (get_current(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0ull;
+    return id;
+}
 
 // Device address of g_noalloc_scratch on `dev` (which must be current).  In
 // host code the symbol's name is only a host-side stand-in, so the address is
-// looked up once per device.
+// looked up once per device and context.
 dyg_status scratch_on(int dev, unsigned long long **out) {
     if (dev < 0 || dev >= kMaxDevices) {
         set_error("device ordinal out of range for the no-allocation path");
         return DYG_EINVAL;
     }
     std::lock_guard<std::mutex> lk(g_setup_mu);
-    if (!g_scratch_addr[dev]) {
+    const unsigned long long ctx = current_context_id();
+    if (!g_scratch_addr[dev] || (ctx && ctx != g_scratch_ctx[dev])) {
         void *p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p) {
@@ -57,19 +92,10 @@ dyg_status scratch_on(int dev, unsigned long long **out) {
             return DYG_ECUDA;
         }
         g_scratch_addr[dev] = static_cast<unsigned long long *>(p);
+        g_scratch_ctx[dev] = ctx;
     }
     *out = g_scratch_addr[dev];
     return DYG_OK;
-}
-
-bool is_device_ptr(const void *p) {
-    if (!p) return false;
-    cudaPointerAttributes at;
-    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
 }
 
 // found_at = winner's step or -1; -2 marks an edge whose endpoint is not a
@@ -131,11 +157,18 @@ extern "C" dyg_status dyg_incremental_walk_noalloc(const dyg_graph *H, const uin
     }
     dyg_status rc = DYG_OK;
     const void *ptrs[] = {src, dst, w, found_at, conductance, accepted};
-    for (const void *q : ptrs)
-        if (q && !is_device_ptr(q)) {
+    for (const void *q : ptrs) {
+        if (!q || rc != DYG_OK) continue;
+        const PtrPlace at = ptr_place(q, H->device);
+        if (at == kOnOtherDevice) {
+            set_error("dyg_incremental_walk_noalloc: a pointer is device memory of another GPU "
+                      "than the graph's");
+            rc = DYG_EINVAL;
+        } else if (at != kOnDevice) {
             set_error("dyg_incremental_walk_noalloc takes device pointers only");
             rc = DYG_EINVAL;
         }
+    }
     unsigned long long *scratch = nullptr;
     if (rc == DYG_OK) rc = scratch_on(H->device, &scratch);
     cudaStream_t st = (cudaStream_t)stream;

@@ -39,6 +39,24 @@ __device__ __forceinline__ uint32_t dcount(const uint32_t *dev, uint32_t host) {
 #define GSTRIDE(i, m) \
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < (m); i += gridDim.x * blockDim.x)
 
+// ------------------------------------------------------- input check
+
+__global__ void k_validate(unsigned long long *halt, const uint32_t *src, const uint32_t *dst,
+                           const float *w, uint32_t n, uint32_t nv, unsigned long long *err) {
+    GSTRIDE(e, n) {
+        unsigned long long bits = 0ull;
+        if (src[e] >= nv || dst[e] >= nv) bits |= kErrVertex;
+        if (w) {
+            const float x = w[e];
+            if (!(x > 0.0f) || !isfinite(x)) bits |= kErrWeight;
+        }
+        if (bits) {
+            atomicOr(err, bits);
+            atomicCAS(halt, 0ull, halt_code(0, (uint32_t)kHaltInvalid, 0));
+        }
+    }
+}
+
 // --------------------------------------------------------- incremental
 
 __global__ void k_incr_decode(const unsigned long long *halt, const unsigned long long *keys,
@@ -418,6 +436,34 @@ dyg_status recover_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *cx, const
 
 }  // namespace
 
+dyg_status validate_enqueue(unsigned long long *halt, unsigned long long *err,
+                            const uint32_t *src, const uint32_t *dst, const float *w, uint32_t n,
+                            uint32_t nv, cudaStream_t st) {
+    if (n == 0) return DYG_OK;
+    k_validate<<<grid_for(n), 256, 0, st>>>(halt, src, dst, w, n, nv, err);
+    count_launch();
+    DYG_CUDA(cudaGetLastError());
+    return DYG_OK;
+}
+
+// A call whose device-resident inputs failed k_validate: clear the halt and
+// the error bits, and report which check failed.  Nothing was changed.
+dyg_status rejected_inputs(dyg_graph *D, cudaStream_t st) {
+    const unsigned long long err = D->ws.host_scalars[S_ERR];
+    DYG_CUDA(cudaMemsetAsync(ptr<unsigned long long>(D->ws.scalars) + S_ERR, 0,
+                             sizeof(unsigned long long), st));
+    DYG_CUDA(cudaMemsetAsync(ptr<unsigned long long>(D->ws.scalars) + S_HALT, 0,
+                             sizeof(unsigned long long), st));
+    DYG_CUDA(cudaStreamSynchronize(st));
+    D->ws.host_scalars[S_ERR] = 0ull;
+    D->ws.host_scalars[S_HALT] = 0ull;
+    if (err & kErrVertex)
+        set_error("a batch endpoint is not a vertex of the graph (the call changed nothing)");
+    else
+        set_error("a batch weight is not finite and > 0 (the call changed nothing)");
+    return DYG_EINVAL;
+}
+
 dyg_status grow_keep(Buf &b, size_t bytes, size_t used, cudaStream_t st) {
     if (b.bytes >= bytes) return DYG_OK;
     Buf nb;
@@ -662,9 +708,11 @@ dyg_status grow_for_halt(dyg_graph *A, dyg_graph *B, cudaStream_t st) {
 dyg_status incremental_run(dyg_graph *H, dyg_graph *G, const uint32_t *src, const uint32_t *dst,
                            const float *w, uint32_t n, uint32_t B, uint64_t uid_base,
                            const unsigned long long *uids, const dyg_walk_params &p, int32_t *found, float *cond, uint8_t *acc,
-                           cudaStream_t st) {
-    unsigned long long *halt = ptr<unsigned long long>(H->ws.scalars) + S_HALT;
+                           cudaStream_t st, bool check_inputs) {
+    unsigned long long *sc = ptr<unsigned long long>(H->ws.scalars);
+    unsigned long long *halt = sc + S_HALT;
     DYG_TRY(clear_halt(H, st));
+    if (check_inputs) DYG_TRY(validate_enqueue(halt, sc + S_ERR, src, dst, w, n, H->g.n, st));
     uint32_t b_start = 0;
     for (int round = 0; round < 64; ++round) {
         for (uint32_t b = b_start; (uint64_t)b * B < n; ++b) {
@@ -678,6 +726,7 @@ dyg_status incremental_run(dyg_graph *H, dyg_graph *G, const uint32_t *src, cons
         const unsigned long long h = H->ws.host_scalars[S_HALT];
         if (!h) return DYG_OK;
         const HaltInfo hi = decode_halt(h);
+        if (hi.kind == kHaltInvalid) return rejected_inputs(H, st);
         DYG_TRY(grow_for_halt(H, G, st));
         DYG_TRY(clear_halt(H, st));
         b_start = hi.batch;   // nothing of the halted batch changed: redo it whole
@@ -689,7 +738,8 @@ dyg_status incremental_run(dyg_graph *H, dyg_graph *G, const uint32_t *src, cons
 dyg_status decremental_run(dyg_graph *G, dyg_graph *H, const uint32_t *src, const uint32_t *dst,
                            uint32_t n, uint32_t B, uint64_t uid_base,
                            const unsigned long long *uids, const dyg_walk_params &p,
-                           int32_t *status, float *cond, uint64_t *n_rec, cudaStream_t st) {
+                           int32_t *status, float *cond, uint64_t *n_rec, cudaStream_t st,
+                           bool check_inputs) {
     Workspace &ws = G->ws;
     unsigned long long *sc = ptr<unsigned long long>(ws.scalars);
     unsigned long long *halt = sc + S_HALT;
@@ -704,6 +754,7 @@ dyg_status decremental_run(dyg_graph *G, dyg_graph *H, const uint32_t *src, cons
     unsigned long long init[2] = {0ull, cap};   // S_RECCNT, S_RECCAP
     DYG_CUDA(cudaMemcpyAsync(sc + S_RECCNT, init, sizeof(init), cudaMemcpyHostToDevice, st));
     DYG_TRY(clear_halt(G, st));
+    if (check_inputs) DYG_TRY(validate_enqueue(halt, sc + S_ERR, src, dst, nullptr, n, G->g.n, st));
     uint32_t b_start = 0, ph_start = 0;
     for (int round = 0; round < 64; ++round) {
         for (uint32_t b = b_start; (uint64_t)b * B < n; ++b) {
@@ -719,6 +770,7 @@ dyg_status decremental_run(dyg_graph *G, dyg_graph *H, const uint32_t *src, cons
             return DYG_OK;
         }
         const HaltInfo hi = decode_halt(h);
+        if (hi.kind == kHaltInvalid) return rejected_inputs(G, st);
         if (hi.kind == kHaltRecords) {
             const uint64_t used = ws.host_scalars[S_RECCNT];
             const uint64_t ncap = cap * 2;

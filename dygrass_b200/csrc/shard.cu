@@ -83,6 +83,11 @@ dyg_status dyg_walk_keys(dyg_graph *X, const uint32_t *src, const uint32_t *dst,
         set_error("dyg_walk_keys: keys must be a device array");
         return DYG_EINVAL;
     }
+    {
+        const void *ps[] = {src, dst, w, update_ids};
+        const char *nm[] = {"src", "dst", "w", "update_ids"};
+        DYG_TRY(check_same_device(X->device, ps, nm, 4));
+    }
     cudaStream_t st = (cudaStream_t)stream;
     Workspace &ws = X->ws;
     const uint32_t *d_src, *d_dst;
@@ -93,13 +98,20 @@ dyg_status dyg_walk_keys(dyg_graph *X, const uint32_t *src, const uint32_t *dst,
     if (incremental) DYG_TRY(stage(ws.s_w, w, n, st, &d_w));
     DYG_TRY(stage(ws.s_uid, update_ids, n, st, &d_ids));
     unsigned long long *k = (unsigned long long *)keys + lo;
+    unsigned long long *sc = ptr<unsigned long long>(ws.scalars);
+    DYG_TRY(clear_halt_of(X, st));
+    // the range is checked on the device before it walks (host arrays too:
+    // they are staged whole, and this call reads only [lo, hi))
+    DYG_TRY(validate_enqueue(sc + S_HALT, sc + S_ERR, d_src + lo, d_dst + lo,
+                             incremental ? d_w + lo : nullptr, hi - lo, X->g.n, st));
     DYG_CUDA(cudaMemsetAsync(k, 0, sizeof(unsigned long long) * (hi - lo), st));
-    WalkJob job{nullptr, d_src + lo, d_dst + lo, incremental ? d_w + lo : nullptr,
+    WalkJob job{sc + S_HALT, d_src + lo, d_dst + lo, incremental ? d_w + lo : nullptr,
                 d_ids ? (const unsigned long long *)d_ids + lo : nullptr,
                 (unsigned long long)(first_update_id + lo), nullptr, hi - lo,
                 incremental ? kDomainIncr : kDomainDecr};
     DYG_TRY(launch_walk(X, job, *p, incremental != 0, k, st));
-    DYG_CUDA(cudaStreamSynchronize(st));
+    DYG_TRY(read_scalars(X, st));
+    if (ws.host_scalars[S_HALT]) return rejected_inputs(X, st);
     return DYG_OK;
 }
 
@@ -125,6 +137,11 @@ dyg_status dyg_incremental_commit_keys(dyg_graph *H, dyg_graph *G, const uint32_
         set_error("dyg_incremental_commit_keys: keys and outputs must be device arrays");
         return DYG_EINVAL;
     }
+    {
+        const void *ps[] = {src, dst, w, keys, found_at, conductance, accepted};
+        const char *nm[] = {"src", "dst", "w", "keys", "found_at", "conductance", "accepted"};
+        DYG_TRY(check_same_device(H->device, ps, nm, 7));
+    }
     cudaStream_t st = (cudaStream_t)stream;
     Workspace &ws = H->ws;
     const uint32_t *d_src, *d_dst;
@@ -135,10 +152,15 @@ dyg_status dyg_incremental_commit_keys(dyg_graph *H, dyg_graph *G, const uint32_
     unsigned long long *halt = ptr<unsigned long long>(ws.scalars) + S_HALT;
     for (int round = 0; round < 64; ++round) {
         DYG_TRY(clear_halt_of(H, st));
+        if (round == 0)
+            DYG_TRY(validate_enqueue(halt, ptr<unsigned long long>(ws.scalars) + S_ERR, d_src, d_dst,
+                                     d_w, n, H->g.n, st));
         DYG_TRY(incr_commit_enqueue(H, G, d_src, d_dst, d_w, n, (const unsigned long long *)keys,
                                     halt, 0, found_at, conductance, accepted, st));
         DYG_TRY(read_scalars2(H, G, st));
-        if (!H->ws.host_scalars[S_HALT]) return DYG_OK;
+        const unsigned long long h = H->ws.host_scalars[S_HALT];
+        if (!h) return DYG_OK;
+        if (((h >> 4) & 0xF) == kHaltInvalid) return rejected_inputs(H, st);
         DYG_TRY(grow_arena(H, H->g.arena_cap * 2, st));
         if (G) DYG_TRY(grow_arena(G, G->g.arena_cap * 2, st));
     }
@@ -166,6 +188,11 @@ dyg_status dyg_decremental_delete(dyg_graph *G, dyg_graph *H, const uint32_t *sr
         set_error("dyg_decremental_delete: status and conductance must be device arrays");
         return DYG_EINVAL;
     }
+    {
+        const void *ps[] = {src, dst, update_ids, status, conductance};
+        const char *nm[] = {"src", "dst", "update_ids", "status", "conductance"};
+        DYG_TRY(check_same_device(G->device, ps, nm, 5));
+    }
     cudaStream_t st = (cudaStream_t)stream;
     Workspace &ws = G->ws;
     const uint32_t *d_src, *d_dst;
@@ -175,10 +202,13 @@ dyg_status dyg_decremental_delete(dyg_graph *G, dyg_graph *H, const uint32_t *sr
     DYG_TRY(stage(ws.s_uid, update_ids, n, st, &d_ids));
     unsigned long long *halt = ptr<unsigned long long>(ws.scalars) + S_HALT;
     DYG_TRY(clear_halt_of(G, st));
+    DYG_TRY(validate_enqueue(halt, ptr<unsigned long long>(ws.scalars) + S_ERR, d_src, d_dst,
+                             nullptr, n, G->g.n, st));
     DYG_TRY(decr_delete_enqueue(G, H, d_src, d_dst, n, first_update_id,
                                 (const unsigned long long *)d_ids, false, halt, status,
                                 conductance, st));
     DYG_TRY(read_scalars2(G, H, st));
+    if (ws.host_scalars[S_HALT]) return rejected_inputs(G, st);
     if (ws.host_scalars[S_ERR]) {
         set_error("a deletion endpoint is not a vertex of the graph");
         return DYG_EINVAL;
@@ -202,6 +232,11 @@ dyg_status dyg_decremental_walk_keys(dyg_graph *G, uint32_t lo, uint32_t hi,
     if (!dev_ptr(keys) || ws.f_src.bytes < sizeof(uint32_t) * (size_t)hi) {
         set_error("dyg_decremental_walk_keys: device keys and a range inside the walk list needed");
         return DYG_EINVAL;
+    }
+    {
+        const void *ps[] = {keys};
+        const char *nm[] = {"keys"};
+        DYG_TRY(check_same_device(G->device, ps, nm, 1));
     }
     cudaStream_t st = (cudaStream_t)stream;
     unsigned long long *k = (unsigned long long *)keys + lo;
@@ -231,6 +266,11 @@ dyg_status dyg_decremental_commit_keys(dyg_graph *G, dyg_graph *H, const dyg_wal
         set_error("dyg_decremental_commit_keys: keys, status and conductance must be device arrays");
         return DYG_EINVAL;
     }
+    {
+        const void *ps[] = {keys, status, conductance, rec_src, rec_dst, rec_kind};
+        const char *nm[] = {"keys", "status", "conductance", "rec_src", "rec_dst", "rec_kind"};
+        DYG_TRY(check_same_device(G->device, ps, nm, 6));
+    }
     cudaStream_t st = (cudaStream_t)stream;
     Workspace &ws = G->ws;
     unsigned long long *sc = ptr<unsigned long long>(ws.scalars);
@@ -247,6 +287,7 @@ dyg_status dyg_decremental_commit_keys(dyg_graph *G, dyg_graph *H, const dyg_wal
     uint32_t phase = 0;
     uint64_t total = 0;
     int round = 0;
+    G->last_rec = 0;
     for (; round < 64; ++round) {
         DYG_TRY(clear_halt_of(G, st));
         DYG_TRY(decr_walk_enqueue(G, H, 0, n_walk, nullptr, *p, halt, 0, phase, status,
@@ -276,6 +317,7 @@ dyg_status dyg_decremental_commit_keys(dyg_graph *G, dyg_graph *H, const dyg_wal
         set_error("decremental commit: too many buffer regrowths");
         return DYG_ENOMEM;
     }
+    G->last_rec = total;
     const uint64_t nout = total < rec_cap ? total : rec_cap;
     const bool any_host = (rec_src && !dev_ptr(rec_src)) || (rec_dst && !dev_ptr(rec_dst)) ||
                           (rec_kind && !dev_ptr(rec_kind));

@@ -401,7 +401,7 @@ dyg_status clear_halt(dyg_graph *D, cudaStream_t st) {
 dyg_status insert_file_run(dyg_graph *G, dyg_graph *H, const uint32_t *src, const uint32_t *dst,
                            const float *w, uint32_t n, uint64_t uid0, uint32_t chunk,
                            const dyg_walk_params &p, int32_t *status, float *cond,
-                           cudaStream_t st) {
+                           cudaStream_t st, bool check_inputs) {
     Workspace &wg = G->ws, &wh = H->ws;
     const uint32_t nc_max = n < chunk ? n : chunk;
     // every buffer at its final size before anything is enqueued: a resumed
@@ -432,6 +432,9 @@ dyg_status insert_file_run(dyg_graph *G, dyg_graph *H, const uint32_t *src, cons
     DYG_TRY(ensure(wh.hw, sizeof(float) * (size_t)nc_max * 2));
     unsigned long long *halt = ptr<unsigned long long>(wg.scalars) + S_HALT;
     DYG_TRY(clear_halt(G, st));
+    if (check_inputs)
+        DYG_TRY(validate_enqueue(halt, ptr<unsigned long long>(wg.scalars) + S_ERR, src, dst, w, n,
+                                 G->g.n, st));
     DYG_TRY(insert_prep_enqueue(G, H, src, dst, w, n, uid0, halt, status, cond, st));
     const uint32_t nchunks = (uint32_t)(((uint64_t)n + chunk - 1) / chunk);
     uint32_t start = 0;   // 0 = G append, c + 1 = chunk c
@@ -446,6 +449,7 @@ dyg_status insert_file_run(dyg_graph *G, dyg_graph *H, const uint32_t *src, cons
         const unsigned long long h = wg.host_scalars[S_HALT];
         if (!h) return DYG_OK;
         const HaltInfo hi = decode_halt(h);
+        if (hi.kind == kHaltInvalid) return rejected_inputs(G, st);
         dyg_graph *grow = hi.batch == 0 ? G : H;
         DYG_TRY(grow_arena(grow, grow->g.arena_cap * 2, st));
         DYG_TRY(clear_halt(G, st));
@@ -457,7 +461,8 @@ dyg_status insert_file_run(dyg_graph *G, dyg_graph *H, const uint32_t *src, cons
 
 dyg_status delete_file_run(dyg_graph *G, dyg_graph *H, const uint32_t *src, const uint32_t *dst,
                            uint32_t n, uint64_t uid0, uint32_t chunk, const dyg_walk_params &p,
-                           int32_t *status, float *cond, uint64_t *n_rec, cudaStream_t st) {
+                           int32_t *status, float *cond, uint64_t *n_rec, cudaStream_t st,
+                           bool check_inputs) {
     Workspace &ws = G->ws;
     unsigned long long *sc = ptr<unsigned long long>(ws.scalars);
     unsigned long long *halt = sc + S_HALT;
@@ -471,6 +476,8 @@ dyg_status delete_file_run(dyg_graph *G, dyg_graph *H, const uint32_t *src, cons
     unsigned long long init[2] = {0ull, cap};   // S_RECCNT, S_RECCAP
     DYG_CUDA(cudaMemcpyAsync(sc + S_RECCNT, init, sizeof(init), cudaMemcpyHostToDevice, st));
     DYG_TRY(clear_halt(G, st));
+    if (check_inputs)
+        DYG_TRY(validate_enqueue(halt, sc + S_ERR, src, dst, nullptr, n, G->g.n, st));
     DYG_TRY(decr_delete_enqueue(G, H, src, dst, n, uid0, nullptr, true, halt, status, cond, st));
     const uint32_t nchunks = (uint32_t)(((uint64_t)n + chunk - 1) / chunk);
     uint32_t c_start = 0, ph_start = 0;
@@ -488,6 +495,7 @@ dyg_status delete_file_run(dyg_graph *G, dyg_graph *H, const uint32_t *src, cons
             return DYG_OK;
         }
         const HaltInfo hi = decode_halt(h);
+        if (hi.kind == kHaltInvalid) return rejected_inputs(G, st);
         if (hi.kind == kHaltRecords) {
             const uint64_t used = ws.host_scalars[S_RECCNT];
             const uint64_t ncap = cap * 2;
@@ -518,12 +526,14 @@ uint32_t stream_default_chunk(uint32_t n_vertices) {
 dyg_status stream_file_run(dyg_graph *G, dyg_graph *H, uint32_t op, const uint32_t *src,
                            const uint32_t *dst, const float *w, uint32_t n, uint64_t uid0,
                            uint32_t chunk, const dyg_walk_params &p, int32_t *status, float *cond,
-                           uint64_t *n_rec, cudaStream_t st) {
+                           uint64_t *n_rec, cudaStream_t st, bool check_inputs) {
     *n_rec = 0;
     if (chunk == 0) chunk = stream_default_chunk(G->g.n);
     if (op == DYG_STREAM_INSERT)
-        return insert_file_run(G, H, src, dst, w, n, uid0, chunk, p, status, cond, st);
-    return delete_file_run(G, H, src, dst, n, uid0, chunk, p, status, cond, n_rec, st);
+        return insert_file_run(G, H, src, dst, w, n, uid0, chunk, p, status, cond, st,
+                               check_inputs);
+    return delete_file_run(G, H, src, dst, n, uid0, chunk, p, status, cond, n_rec, st,
+                           check_inputs);
 }
 
 }  // namespace dyg

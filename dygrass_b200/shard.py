@@ -19,7 +19,7 @@ import ctypes as C
 
 import numpy as np
 
-from . import WalkParams, _check, _ptr, lib
+from . import WalkParams, _check, _ptr, lib, recovered_read
 
 
 def split(n: int, rank: int, world: int):
@@ -85,12 +85,20 @@ class GpuBackend:
         _check(self.L.dyg_decremental_walk_keys(G.handle, lo, hi, C.byref(p), _ptr(keys),
                                                 self.stream), "dyg_decremental_walk_keys")
 
-    def decr_commit(self, G, H, p, keys, n_walk, state, rec_cap):
+    def decr_commit(self, G, H, p, keys, n_walk, state, rec_cap=None):
+        """rec_cap None: no record buffers are passed; the total comes back
+        from the commit and exactly that many records are read afterwards."""
         st, cd = state
+        nr = C.c_uint64()
+        if rec_cap is None:
+            _check(self.L.dyg_decremental_commit_keys(G.handle, H.handle, C.byref(p), _ptr(keys),
+                                                      n_walk, _ptr(st), _ptr(cd), None, None, None,
+                                                      0, C.byref(nr), self.stream),
+                   "dyg_decremental_commit_keys")
+            return (st, cd) + tuple(recovered_read(G, nr.value))
         rx = np.empty(max(rec_cap, 1), np.uint32)
         ry = np.empty(max(rec_cap, 1), np.uint32)
         rk = np.empty(max(rec_cap, 1), np.uint8)
-        nr = C.c_uint64()
         _check(self.L.dyg_decremental_commit_keys(G.handle, H.handle, C.byref(p), _ptr(keys), n_walk,
                                                   _ptr(st), _ptr(cd), _ptr(rx), _ptr(ry), _ptr(rk),
                                                   rec_cap, C.byref(nr), self.stream),
@@ -120,8 +128,6 @@ def decremental_sharded(backend, G, H, src, dst, first_uid, p, rank, world, comb
     lo, hi = split(n_walk, rank, world)
     backend.decr_walk_keys(G, lo, hi, p, keys)
     keys = combine(keys)
-    if rec_cap is None:
-        rec_cap = len(src) * (p.max_steps + 4 * p.heuristic_walkers) + 16
     return backend.decr_commit(G, H, p, keys, n_walk, state, rec_cap)
 
 

@@ -41,7 +41,11 @@
  *
  * Conventions: the caller owns every host buffer; the library owns device
  * graph state.  Array arguments may be host or device pointers (detected per
- * call); with host outputs the call returns after the results are on the
+ * call); device pointers must be memory of the graph's own GPU (or managed
+ * memory), else DYG_EINVAL.  Inputs are checked before anything changes:
+ * an endpoint >= |V| or a weight that is not finite and > 0, in host or
+ * device memory, makes the call return DYG_EINVAL with G and H unchanged.
+ * With host outputs the call returns after the results are on the
  * host.  A handle is not thread-safe; distinct handles are.  Calls are
  * ordered on the given CUDA stream (NULL = legacy default stream).
  * No torch types cross this boundary.
@@ -196,6 +200,18 @@ dyg_status dyg_decremental_stream(dyg_graph *G, dyg_graph *H, const uint32_t *sr
                                   uint32_t *rec_src, uint32_t *rec_dst, uint8_t *rec_kind,
                                   uint64_t rec_cap, uint64_t *n_rec, dyg_stream_t stream);
 
+/* Recovered edges [first, first + count) of the last decremental call on G
+ * (dyg_decremental_batch / _stream / _batch_ids, dyg_stream_file with
+ * DYG_STREAM_DELETE, dyg_decremental_commit_keys); they stay readable until
+ * the next such call on G.  Lets a caller pass rec_cap = 0 (no record
+ * buffers), learn the total from *n_rec, and then read exactly that many
+ * instead of sizing buffers for the worst case up front.  Host or device
+ * outputs; blocking.  DYG_ERANGE if the range is not inside the last call's
+ * records.  The reference writes these edges to added_edges.mtx
+ * (random_walk_decremental/gpu_graph.cuh:633-646). */
+dyg_status dyg_recovered_read(const dyg_graph *G, uint64_t first, uint64_t count,
+                              uint32_t *rec_src, uint32_t *rec_dst, uint8_t *rec_kind);
+
 /* dyg_incremental_batch / dyg_decremental_batch with an explicit update id
  * per edge (update_ids[e] in place of first_update_id + e; host or device
  * array).  With a union of independent graphs (each graph's vertices at its
@@ -287,13 +303,16 @@ dyg_status dyg_stream_file(dyg_graph *G, dyg_graph *H, uint32_t op, const uint32
  * callers that cannot call cudaMalloc: a serving loop that reserves its device
  * memory at start-up and allows no allocation afterwards, or a plugin inside a
  * host framework that owns all device allocations.  Accepted edges are NOT
- * appended to H.  All array arguments must be device pointers; found_at is -2
+ * appended to H.  All array arguments must be device pointers on H's device
+ * (memory of another GPU is rejected with DYG_EINVAL); found_at is -2
  * for an edge whose endpoint is not a vertex of H.  Scratch lives in a static
  * device array of DYG_NOALLOC_MAX_EDGES 64-bit keys (512 KiB) plus counters,
  * held by every device that loads the library until exit; batches larger than
  * DYG_NOALLOC_MAX_EDGES are rejected with DYG_EINVAL.  Calls share that array:
  * calls that overlap on the GPU race and must be serialized by the caller.
- * The first call on a device looks up the array's address (set-up); make it
+ * The first call on a device looks up the array's address (set-up), and so
+ * does the first call after the device's context is replaced (for example by
+ * cudaDeviceReset, which frees the array with the context); make those calls
  * before any stream capture.  Stream-ordered; returns before the results are
  * ready. */
 #define DYG_NOALLOC_MAX_EDGES 65536u

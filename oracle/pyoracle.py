@@ -288,9 +288,11 @@ class ShardBackend:
         lib().orc_decremental_walk_list_keys(G.h, _p(src), _p(dst), _p(wl), lo, hi, first_uid,
                                              C.byref(P), self.th, _p(self._u64(keys)))
 
-    def decr_commit(self, G, H, p, keys, n_walk, state, rec_cap):
+    def decr_commit(self, G, H, p, keys, n_walk, state, rec_cap=None):
         src, dst, wl, first_uid = self._last
         st, cd = state
+        if rec_cap is None:   # the bound of a batch: a path plus fallback edges per deletion
+            rec_cap = len(src) * (p.max_steps + 4 * p.heuristic_walkers) + 16
         P = Params.from_walk_params(p)
         rx, ry, rk = (np.empty(max(rec_cap, 1), np.uint32), np.empty(max(rec_cap, 1), np.uint32),
                       np.empty(max(rec_cap, 1), np.uint8))

@@ -20,7 +20,20 @@ import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF_SRC = "/root/reference/dynamic_update"
+
+
+def _reference_root() -> str:
+    """$REF, else the default of oracle/Makefile's REF."""
+    if os.environ.get("REF"):
+        return os.environ["REF"]
+    with open(os.path.join(ROOT, "oracle", "Makefile")) as f:
+        for line in f:
+            if line.startswith("REF ?="):
+                return line.split("?=", 1)[1].strip()
+    raise RuntimeError("set REF to the reference's source tree")
+
+
+REF_SRC = os.path.join(_reference_root(), "dynamic_update")
 DETECT = os.path.join(ROOT, "oracle", "_ref", "ref_detect")
 
 FIELDS = ["skip_lines", "has_header", "has_dimensions", "weighted", "laplacian", "triangular",
