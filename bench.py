@@ -90,6 +90,8 @@ def parse():
                          "strong scaling; default N > 1 runs independent replicas")
     ap.add_argument("--no-plain", action="store_true",
                     help="rgg_many: skip timing the plain per-graph loop")
+    ap.add_argument("--no-exhaustive-leg", action="store_true",
+                    help="skip the extra timed pass with every walker run to its end")
     ap.add_argument("--exhaustive", action="store_true",
                     help="run every walker to its natural end (no pruning)")
     ap.add_argument("--profile-only", action="store_true",
@@ -431,6 +433,45 @@ def run_ours(args, rank, world, local_rank):
                "h2d_bytes_per_step": int(nin * 12 + ndel * 8),
                "d2h_bytes_per_step": int(nin * 9 + ndel * 8 + nrec_h * 9)}
 
+    # ---- the same step with every walker run to its natural end (as the
+    # reference's and the CPU port's walkers run): separates the pruning
+    # saving from the hardware's
+    exh = None
+    if not args.exhaustive and not args.shard and not args.no_exhaustive_leg:
+        pe = type(W.params).from_buffer_copy(W.params)
+        pde = type(W.dparams).from_buffer_copy(W.dparams)
+        pe.flags |= dyg.FLAG_EXHAUSTIVE
+        pde.flags |= dyg.FLAG_EXHAUSTIVE
+        barrier()
+        torch.cuda.synchronize()
+        xm0 = (H.counters()[0], G.counters()[0])
+        xt = []
+        for _ in range(max(1, args.steps)):
+            reset()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            dyg.incremental_stream(H, d_is, d_id, d_iw, pe, G=G, stream=sp, out=o_inc)
+            if ndel:
+                dyg.decremental_stream_into(G, H, d_ds, d_dd, pde, o_st, o_cd, o_rx, o_ry, o_rk,
+                                            rec_cap, stream=sp)
+            e1.record(stream)
+            e1.synchronize()
+            xt.append(e0.elapsed_time(e1))
+        xm1 = (H.counters()[0], G.counters()[0])
+        barrier()
+        xms = float(np.mean(xt))
+        if world > 1:
+            import torch.distributed as dist
+            tt = torch.tensor([xms], dtype=torch.float64, device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            xms = float(tt.item())
+        assert int(o_inc.accepted.sum().item()) == accepted   # pruning changes no result
+        n_x = max(1, args.steps)
+        exh = {"value": world * (nin + ndel) / (xms / 1e3), "unit": "edge_updates/s",
+               "ms_per_step": xms, "incr_walker_moves": (xm1[0] - xm0[0]) / n_x,
+               "decr_walker_moves": (xm1[1] - xm0[1]) / n_x}
+
     walk_ms = prof["incr_walk_ms"] + prof["decr_walk_ms"]
     walk_launches = prof["incr_walk_launches"] + prof["decr_walk_launches"]
     moves_total = (incr_moves + decr_moves) * args.steps
@@ -439,6 +480,7 @@ def run_ours(args, rank, world, local_rank):
         "recovered": nrec, "incr_moves": incr_moves, "decr_moves": decr_moves,
         "walk_ms_per_step": walk_ms / args.steps, "walk_launches": walk_launches,
         "prof": prof, "launches_per_step": launches / args.steps, "clocks": clk, "e2e": e2e,
+        "exhaustive": exh,
         "walk_bytes_per_launch": moves_total * BYTES_PER_MOVE / max(walk_launches, 1),
         "walk_ms_per_launch": walk_ms / max(walk_launches, 1),
         # dominant kernel: the walk kernel with the larger measured time
@@ -907,89 +949,142 @@ def cpu_baseline_serve(W, threads=None, max_requests=300):
 
 
 def cpu_baseline_many(W, threads=None):
-    """The oracle's per-graph update loop on every 16th graph (a spread of
-    sizes), per-insertion cost extrapolated to all graphs' insertions."""
+    """The oracle's per-graph update loop over every graph of the workload,
+    measured end to end (graph loading not timed)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
     th = threads or pyoracle.max_threads()
-    sample = W.cases[::16] or W.cases[:1]
+    gs = [(pyoracle.OGraph(c.n, c.h_src, c.h_dst, c.h_w), pyoracle.OGraph(c.n, c.g_src, c.g_dst, c.g_w))
+          for c in W.cases]
     t0 = time.perf_counter()
-    for c in sample:
-        Ho = pyoracle.OGraph(c.n, c.h_src, c.h_dst, c.h_w)
-        Go = pyoracle.OGraph(c.n, c.g_src, c.g_dst, c.g_w)
+    for c, (Ho, Go) in zip(W.cases, gs):
         pyoracle.incremental(Ho, c.ins_src, c.ins_dst, c.ins_w, W.params, G=Go, threads=th)
     dt = time.perf_counter() - t0
-    ns = sum(len(c.ins_src) for c in sample)
-    return {"value": ns / dt, "unit": "edge_updates/s", "cores": th, "kind": "port", "seconds": dt,
-            "sample": f"oracle (C/OpenMP, {th} threads): the update loops of {len(sample)} of the "
-                      f"{len(W.cases)} graphs (every 16th), {ns} insertions; per-insertion cost "
-                      f"extrapolated to all {W.n_updates}"}
+    return {"value": W.n_updates / dt, "unit": "edge_updates/s", "cores": th, "kind": "port",
+            "seconds": dt,
+            "sample": f"oracle (C/OpenMP, {th} threads): the whole workload, every graph's update "
+                      f"loop ({len(W.cases)} graphs, {W.n_updates} insertions), measured; walkers "
+                      f"run to their natural end as the reference's do"}
 
 
-def cpu_baseline_mixed(W, threads=None):
-    """The oracle on a bounded sample of the mixed stream: the first insertion
-    file and the first deletion file (applied in stream order), per-update
-    costs extrapolated to the stream's insert/delete mix."""
+def _one_core(pyoracle, th, runs):
+    """Times each (label, fn(threads)) of `runs` at 1 thread and at `th`
+    threads; fn gets fresh identical state each time.  Returns the rates."""
+    out = {}
+    tot = [0, 0.0, 0.0]
+    for label, n_upd, fn in runs:
+        t1 = fn(1)
+        tn = fn(th)
+        out[label] = {"updates": n_upd, "seconds_1_core": t1, f"seconds_{th}_cores": tn,
+                      "value_1_core": n_upd / t1, f"value_{th}_cores": n_upd / tn}
+        tot[0] += n_upd
+        tot[1] += t1
+        tot[2] += tn
+    # the samples together: updates over the summed measured times
+    out["samples_together"] = {"updates": tot[0], "value_1_core": tot[0] / tot[1],
+                               f"value_{th}_cores": tot[0] / tot[2]}
+    return out
+
+
+def cpu_baseline_mixed(W, threads=None, one_core=True):
+    """The oracle on the whole mixed stream, file by file in stream order,
+    measured end to end.  With one_core: the first insertion file and the
+    first deletion file, each from identical cloned state, at 1 thread and at
+    all threads (measured rates of that sample)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
     th = threads or pyoracle.max_threads()
     Ho = pyoracle.OGraph(W.n, W.h_src, W.h_dst, W.h_w)
     Go = pyoracle.OGraph(W.n, W.g_src, W.g_dst, W.g_w)
-    t_op, n_op = [0.0, 0.0], [0, 0]
-    uid = 0
+    snaps = {}
+    uid, dt = 0, 0.0
     for op, s_, d_, w_ in W.files:
-        if n_op[0] and n_op[1]:
-            break
+        if one_core and op not in snaps:
+            snaps[op] = (Go.clone(), Ho.clone(), uid, s_, d_, w_)
         p = W.dparams if op else W.iparams
         t0 = time.perf_counter()
         pyoracle.stream_file(Go, Ho, op, s_, d_, w_, p, first_uid=uid, threads=th)
-        dt = time.perf_counter() - t0
+        dt += time.perf_counter() - t0
         uid += len(s_)
-        if not n_op[op]:
-            t_op[op] += dt
-            n_op[op] += len(s_)
     nins = sum(len(f[1]) for f in W.files if f[0] == 0)
-    ndel = W.n_updates - nins
-    est = t_op[0] / max(n_op[0], 1) * nins + t_op[1] / max(n_op[1], 1) * ndel
-    return {"value": W.n_updates / est, "unit": "edge_updates/s", "cores": th, "kind": "port",
-            "seconds": sum(t_op),
-            "sample": f"oracle (C/OpenMP, {th} threads): the stream files up to the first deletion "
-                      f"file, timing the first insertion file ({n_op[0]} updates) and the first "
-                      f"deletion file ({n_op[1]} updates); per-update costs extrapolated to the "
-                      f"stream's mix ({nins} insertions, {ndel} deletions)"}
+    out = {"value": W.n_updates / dt, "unit": "edge_updates/s", "cores": th, "kind": "port",
+           "seconds": dt,
+           "sample": f"oracle (C/OpenMP, {th} threads): the whole stream ({len(W.files)} files, "
+                     f"{nins} insertions, {W.n_updates - nins} deletions) in order, measured; "
+                     f"walkers run to their natural end as the reference's do"}
+    if one_core:
+        runs = []
+        for op, (g0, h0, u0, s_, d_, w_) in sorted(snaps.items()):
+            p = W.dparams if op else W.iparams
+
+            def fn(t, g0=g0, h0=h0, u0=u0, s_=s_, d_=d_, w_=w_, op=op, p=p):
+                g, h = g0.clone(), h0.clone()
+                t0 = time.perf_counter()
+                pyoracle.stream_file(g, h, op, s_, d_, w_, p, first_uid=u0, threads=t)
+                return time.perf_counter() - t0
+            runs.append(("first_delete_file" if op else "first_insert_file", len(s_), fn))
+        out["one_core"] = _one_core(pyoracle, th, runs)
+    return out
 
 
-def cpu_baseline(W, threads=None, max_incr=None):
-    """The oracle (CPU port of the reference update loop) on a bounded sample:
-    the full insertion stream (or its first max_incr edges), then the first
-    deletion batch; per-edge costs are extrapolated to the workload's mix."""
+def cpu_baseline(W, threads=None, one_core=True):
+    """The oracle (the reference's update loop restated in C; OpenMP over the
+    (edge, walker) pairs of a batch) on the whole workload, measured end to
+    end: the insertion stream in the reference's ceil(N/10) batches, every
+    insertion also entering G, then the deletion stream in ceil(N/10)
+    batches.  Walkers run to their natural end, as the reference's do.
+    With one_core: two samples, each timed at 1 thread and at all threads
+    from identical cloned state -- the first insertion batch on the initial
+    graphs, and the first tenth of the first deletion batch (as one batch) on
+    the graphs the insertions left."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
     th = threads or pyoracle.max_threads()
     nin, ndel = len(W.ins_src), len(W.del_src)
-    ni = nin if max_incr is None else min(nin, max_incr)
     Ho = pyoracle.OGraph(W.n, W.h_src, W.h_dst, W.h_w)
-    Go = pyoracle.OGraph(W.n, W.g_src, W.g_dst, W.g_w) if ndel else None
+    Go = pyoracle.OGraph(W.n, W.g_src, W.g_dst, W.g_w)
+    h_init, g_init = (Ho.clone(), Go.clone()) if one_core else (None, None)
     from dygrass_b200 import reference_batch_size
     B = reference_batch_size(nin)
     t0 = time.perf_counter()
-    pyoracle.incremental(Ho, W.ins_src[:ni], W.ins_dst[:ni], W.ins_w[:ni], W.params,
-                         batch_size=B, G=Go, threads=th)
+    pyoracle.incremental(Ho, W.ins_src, W.ins_dst, W.ins_w, W.params, batch_size=B, G=Go, threads=th)
     t_in = time.perf_counter() - t0
-    t_de, nd = 0.0, 0
+    h_mid, g_mid = (Ho.clone(), Go.clone()) if (one_core and ndel) else (None, None)
+    t_de = 0.0
     if ndel:
         Bd = reference_batch_size(ndel)
-        nd = Bd
         t0 = time.perf_counter()
-        pyoracle.decremental(Go, Ho, W.del_src[:nd], W.del_dst[:nd], W.dparams, batch_size=Bd,
-                             threads=th)
+        pyoracle.decremental(Go, Ho, W.del_src, W.del_dst, W.dparams, batch_size=Bd, threads=th)
         t_de = time.perf_counter() - t0
-    est = t_in / ni * nin + (t_de / nd * ndel if nd else 0.0)
-    return {"value": (nin + ndel) / est, "unit": "edge_updates/s", "cores": th,
-            "kind": "port", "seconds": t_in + t_de,
-            "sample": f"oracle (C/OpenMP, {th} threads): {ni} insertions in batches of {B}"
-                      + (f" + first deletion batch ({nd} deletions) on the updated graphs" if nd else "")
-                      + "; per-edge costs extrapolated to the full stream"}
+    out = {"value": (nin + ndel) / (t_in + t_de), "unit": "edge_updates/s", "cores": th,
+           "kind": "port", "seconds": t_in + t_de,
+           "seconds_insertions": t_in, "seconds_deletions": t_de,
+           "sample": f"oracle (C/OpenMP, {th} threads): the whole workload, {nin} insertions in "
+                     f"batches of {B}" + (f" then {ndel} deletions in batches of "
+                                          f"{reference_batch_size(ndel)}" if ndel else "")
+                     + ", measured; walkers run to their natural end as the reference's do"}
+    if one_core:
+        runs = []
+
+        def f_ins(t):
+            h, g = h_init.clone(), g_init.clone()
+            t0 = time.perf_counter()
+            pyoracle.incremental(h, W.ins_src[:B], W.ins_dst[:B], W.ins_w[:B], W.params, G=g,
+                                 threads=t, first_uid=0, single_batch=True)
+            return time.perf_counter() - t0
+        runs.append(("first_insertion_batch", B, f_ins))
+        if ndel:
+            nd = max(1, reference_batch_size(ndel) // 10)
+
+            def f_del(t):
+                g, h = g_mid.clone(), h_mid.clone()
+                t0 = time.perf_counter()
+                pyoracle.decremental(g, h, W.del_src[:nd], W.del_dst[:nd], W.dparams, threads=t,
+                                     first_uid=0, single_batch=True)
+                return time.perf_counter() - t0
+            runs.append(("first_deletions_as_one_batch", nd, f_del))
+        out["one_core"] = _one_core(pyoracle, th, runs)
+    return out
 
 
 # ---------------------------------------------------------------- main
@@ -1008,14 +1103,16 @@ def main():
                 "serve": cpu_baseline_serve}.get(args.workload, cpu_baseline)
         vals = []
         for i in range(args.warmup + args.steps):
-            r = base(W)
+            r = base(W, one_core=False) if base is not cpu_baseline_many and \
+                base is not cpu_baseline_serve else base(W)
             if i >= args.warmup:
                 vals.append(r)
+        # a step's time is the measured time of its sample (the whole workload,
+        # except for serve)
         v = float(np.mean([r["value"] for r in vals]))
         out = {"metric": "edge updates/sec (incr+decr)", "value": v, "unit": "edge_updates/s",
                "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-               "ms_per_step": (W.n_updates if args.workload in ("rmat", "rgg_many", "serve")
-                               else len(W.ins_src) + len(W.del_src)) / v * 1e3,
+               "ms_per_step": float(np.mean([r["seconds"] for r in vals])) * 1e3,
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                "data": "synthetic (seeded)", "config": workload_config(W, args),
                "cpu_baseline": {k: vals[-1][k] for k in ("value", "unit", "cores", "kind", "sample")},
@@ -1089,7 +1186,9 @@ def main():
                       "incr_walker_moves": res["incr_moves"], "decr_walker_moves": res["decr_moves"],
                       "walk_kernel_ms_per_step": res["walk_ms_per_step"],
                       "walk_launches_per_step": res["walk_launches"] / args.steps,
-                      "steps_ms": res["steps_ms"]},
+                      "launches_per_step": res["launches_per_step"],
+                      "steps_ms": res["steps_ms"],
+                      **({"exhaustive": res["exhaustive"]} if res.get("exhaustive") else {})},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": traffic,
                      "peak_source": f"{peak_note} hbm_gbs (MEASURED_PEAKS.json)",

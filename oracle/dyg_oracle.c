@@ -164,6 +164,27 @@ void orc_graph_free(orc_graph *g) {
     free(g);
 }
 
+orc_graph *orc_graph_clone(const orc_graph *g) {
+    orc_graph *c = (orc_graph *)calloc(1, sizeof(orc_graph));
+    const uint32_t n = g->n;
+    c->n = n;
+    c->deg = (uint32_t *)calloc(n ? n : 1, sizeof(uint32_t));
+    c->cap = (uint32_t *)calloc(n ? n : 1, sizeof(uint32_t));
+    c->col = (uint32_t **)calloc(n ? n : 1, sizeof(uint32_t *));
+    c->w = (float **)calloc(n ? n : 1, sizeof(float *));
+    for (uint32_t x = 0; x < n; ++x) {
+        c->deg[x] = g->deg[x];
+        c->cap[x] = g->cap[x];
+        if (g->cap[x]) {
+            c->col[x] = (uint32_t *)malloc(sizeof(uint32_t) * g->cap[x]);
+            c->w[x] = (float *)malloc(sizeof(float) * g->cap[x]);
+            memcpy(c->col[x], g->col[x], sizeof(uint32_t) * g->deg[x]);
+            memcpy(c->w[x], g->w[x], sizeof(float) * g->deg[x]);
+        }
+    }
+    return c;
+}
+
 uint32_t orc_graph_num_vertices(const orc_graph *g) { return g->n; }
 
 uint64_t orc_graph_num_slots(const orc_graph *g) {

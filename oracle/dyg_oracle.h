@@ -46,6 +46,8 @@ uint32_t orc_draw(uint64_t seed, uint64_t uid, uint32_t domain, uint32_t walker,
 orc_graph *orc_graph_from_edges(uint32_t n, uint64_t m, const uint32_t *src,
                                 const uint32_t *dst, const float *w);
 void orc_graph_free(orc_graph *g);
+/* A deep copy (rows in the same order). */
+orc_graph *orc_graph_clone(const orc_graph *g);
 uint32_t orc_graph_num_vertices(const orc_graph *g);
 uint64_t orc_graph_num_slots(const orc_graph *g);
 /* row_ptr[n+1], col[slots], w[slots]; any of the outputs may be NULL. */

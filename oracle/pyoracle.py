@@ -48,6 +48,7 @@ def lib() -> C.CDLL:
             "orc_draw": ([u64, u64, u32, u32, u32], u32),
             "orc_graph_from_edges": ([u32, u64, vp, vp, vp], vp),
             "orc_graph_free": ([vp], None),
+            "orc_graph_clone": ([vp], vp),
             "orc_graph_num_vertices": ([vp], u32),
             "orc_graph_num_slots": ([vp], u64),
             "orc_graph_export": ([vp, vp, vp, vp], u64),
@@ -107,6 +108,15 @@ class OGraph:
         dst = np.ascontiguousarray(dst, np.uint32)
         w = np.ascontiguousarray(w, np.float32)
         self.h = lib().orc_graph_from_edges(int(n), len(src), _p(src), _p(dst), _p(w))
+
+    @classmethod
+    def _wrap(cls, h):
+        g = cls.__new__(cls)
+        g.h = h
+        return g
+
+    def clone(self) -> "OGraph":
+        return OGraph._wrap(lib().orc_graph_clone(self.h))
 
     def __del__(self):
         if getattr(self, "h", None):
