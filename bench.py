@@ -73,7 +73,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["mesh", "grid", "rmat", "rgg_many", "serve"],
+    ap.add_argument("--refgpu-repeats", type=int, default=10)
+    ap.add_argument("--workload", choices=["mesh", "grid", "rmat", "rgg_many", "serve", "refgpu"],
                     default="mesh")
     ap.add_argument("--serve-requests", type=int, default=2000)
     ap.add_argument("--rgg-graphs", type=int, default=256)
@@ -1087,6 +1088,177 @@ def cpu_baseline(W, threads=None, one_core=True):
     return out
 
 
+# ------------------------------------------------- the reference's GPU updater
+
+_TIME_RE = None
+
+
+def _time_taken(stdout):
+    """The "Time taken: N milliseconds" line both updaters print."""
+    import re
+    global _TIME_RE
+    _TIME_RE = _TIME_RE or re.compile(r"Time taken: (\d+) milliseconds")
+    m = _TIME_RE.search(stdout)
+    return int(m.group(1)) if m else None
+
+
+def _write_mtx(path, s, d, w=None, base=1):
+    with open(path, "w") as f:
+        for i in range(len(s)):
+            f.write(f"{int(s[i]) + base} {int(d[i]) + base}"
+                    + ("" if w is None else f" {float(w[i]):.9g}") + "\n")
+
+
+def run_refgpu(args):
+    """The reference's own CUDA updaters (unmodified sources built for sm_100a
+    into oracle/_ref) against this library on identical input files, on one
+    B200.  Cases are those the reference runs correctly: the 100x100 grid
+    with 1,000 insertions, a 30^3 mesh with 6,000 insertions (inside the room
+    its grown rows have), and 1,000 sparsifier deletions on a 20^3 mesh (every
+    deletion in H, which its batch indexing needs).  Each binary prints its
+    own "Time taken" (ms resolution, the span of
+    random_walk_incremental/main.cu:297-344 and
+    random_walk_decremental/main.cu:388-449); each runs `repeats` times and
+    the median counts.  This library is timed three ways on the same inputs
+    with max_steps 100 (the reference's compile-time value): the drop-in
+    executables (same print, same span), the library call with host arrays
+    (copies included; CUDA events), and the library call on device-resident
+    arrays, each with pruned and with exhaustive walkers."""
+    import shutil
+    import torch
+    import dygrass_b200 as dyg
+    import dygrass_b200.workloads as wl
+    ref_dir = os.path.join(ROOT, "oracle", "_ref")
+    our_dir = os.path.join(ROOT, "dygrass_b200", "bin")
+    need = [os.path.join(ref_dir, b) for b in ("incremental_update", "decremental_update")]
+    if not all(os.path.exists(x) for x in need):
+        print(json.dumps({"workload": "refgpu", "unavailable": "the reference's updaters are not "
+                          "built in oracle/_ref (make -C oracle ref-gpu where its sources are)"}))
+        return 0
+    torch.cuda.set_device(0)
+    R = max(1, args.refgpu_repeats)
+    tmp = tempfile.mkdtemp(prefix="dyg_refgpu_")
+    cases = []
+
+    def run_cli(exe, argv, cwd):
+        cp = subprocess.run([exe] + argv, cwd=cwd, capture_output=True, text=True, timeout=600)
+        return _time_taken(cp.stdout), cp
+
+    def lib_times(fn, reps):
+        ts = []
+        for _ in range(reps):
+            setup = fn(None)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            fn(setup)
+            e1.record()
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return ts
+
+    try:
+        for name, kind, thr in (("grid 100x100, 1,000 insertions, threshold 10, 512 walkers", "incr", 10.0),
+                                ("mesh 30^3, 6,000 insertions, threshold 100, 512 walkers", "incr", 100.0),
+                                ("mesh 20^3 + 2,000 insertions, 1,000 sparsifier deletions, 512 walkers",
+                                 "decr", 100.0)):
+            case = {"case": name}
+            if kind == "incr":
+                W = wl.grid_2d(100, 100, inserts=1000) if "grid" in name else wl.mesh_3d(30, inserts=6000)
+                n_upd = len(W.ins_src)
+                files = lambda ds: (_write_mtx(os.path.join(ds, "adj_sparse.mtx"), W.h_src, W.h_dst,
+                                               W.h_w, base=0),
+                                    _write_mtx(os.path.join(ds, "ext.mtx"), W.ins_src, W.ins_dst,
+                                               W.ins_w, base=1))
+                argv = lambda g: [g, repr(thr), "512"]
+                exe_ref, exe_our = need[0], os.path.join(our_dir, "incremental_update")
+                p = dyg.WalkParams.make(threshold=thr, walkers=512, max_steps=100)
+                H0 = dyg.Graph.from_edges(W.n, W.h_src, W.h_dst, W.h_w)
+                H = H0.clone()
+                dev = [torch.from_numpy(np.ascontiguousarray(a).view(np.int32 if a.dtype == np.uint32
+                                                                      else a.dtype)).cuda()
+                       for a in (W.ins_src, W.ins_dst, W.ins_w)]
+
+                def lib_call(pp, arrays):
+                    def fn(setup):
+                        if setup is None:
+                            H.copy_from(H0)
+                            return True
+                        dyg.incremental_stream(H, *arrays, pp)
+                    return fn
+                host = (W.ins_src, W.ins_dst, W.ins_w)
+            else:
+                W = wl.mesh_3d(20, inserts=2000)
+                gs = np.concatenate([W.g_src, W.ins_src, [W.n]]).astype(np.uint32)
+                gd = np.concatenate([W.g_dst, W.ins_dst, [W.n + 1]]).astype(np.uint32)
+                gw = np.concatenate([W.g_w, W.ins_w, [1.0]]).astype(np.float32)
+                hs = np.concatenate([W.h_src, [W.n]]).astype(np.uint32)
+                hd = np.concatenate([W.h_dst, [W.n + 1]]).astype(np.uint32)
+                hw = np.concatenate([W.h_w, [1.0]]).astype(np.float32)
+                pick = np.random.default_rng(8).choice(len(W.h_src), 1000, replace=False)
+                ds_, dd_ = W.h_src[pick].astype(np.uint32), W.h_dst[pick].astype(np.uint32)
+                n_upd = len(ds_)
+                files = lambda ds: (_write_mtx(os.path.join(ds, "updated_dense.mtx"), gs, gd, gw),
+                                    _write_mtx(os.path.join(ds, "updated_adj_sparse.mtx"), hs, hd, hw),
+                                    _write_mtx(os.path.join(ds, "del.mtx"), ds_, dd_))
+                argv = lambda g: [g]
+                exe_ref, exe_our = need[1], os.path.join(our_dir, "decremental_update")
+                p = dyg.WalkParams.make(walkers=512, max_steps=100)
+                nv = W.n + 2
+                G0, H0 = dyg.Graph.from_edges(nv, gs, gd, gw), dyg.Graph.from_edges(nv, hs, hd, hw)
+                G, H = G0.clone(), H0.clone()
+                dev = [torch.from_numpy(a.view(np.int32)).cuda() for a in (ds_, dd_)]
+
+                def lib_call(pp, arrays):
+                    def fn(setup):
+                        if setup is None:
+                            G.copy_from(G0)
+                            H.copy_from(H0)
+                            return True
+                        dyg.decremental_stream(G, H, *arrays, pp)
+                    return fn
+                host = (ds_, dd_)
+            case["updates"] = n_upd
+            for who, exe in (("reference", exe_ref), ("ours_cli", exe_our)):
+                ms = []
+                for r in range(R):
+                    root = os.path.join(tmp, f"{who}{r}")
+                    ds = os.path.join(root, "dataset", "g")
+                    os.makedirs(ds)
+                    os.makedirs(os.path.join(root, "run"))
+                    files(ds)
+                    t, cp = run_cli(exe, argv("g"), os.path.join(root, "run"))
+                    if t is None:
+                        raise RuntimeError(f"{who} printed no time: {cp.stdout[-300:]} {cp.stderr[-300:]}")
+                    ms.append(t)
+                    shutil.rmtree(root, ignore_errors=True)
+                case[f"{who}_ms"] = {"median": float(np.median(ms)), "runs": ms,
+                                     "resolution": "1 ms (the binary's own print)"}
+            pe = type(p).from_buffer_copy(p)
+            pe.flags |= dyg.FLAG_EXHAUSTIVE
+            for label, pp, arrays in (("ours_lib_device", p, dev), ("ours_lib_device_exhaustive", pe, dev),
+                                      ("ours_lib_host", p, host), ("ours_lib_host_exhaustive", pe, host)):
+                lib_times(lib_call(pp, arrays), 2)   # warm-up
+                ts = lib_times(lib_call(pp, arrays), R)
+                case[f"{label}_ms"] = {"median": float(np.median(ts)), "runs": ts,
+                                       "resolution": "CUDA events"}
+            ref_ms = case["reference_ms"]["median"]
+            for label in ("ours_cli", "ours_lib_device", "ours_lib_device_exhaustive", "ours_lib_host",
+                          "ours_lib_host_exhaustive"):
+                m = case[f"{label}_ms"]["median"]
+                case[f"{label}_updates_per_s"] = n_upd / (m / 1e3) if m > 0 else None
+                case[f"speedup_{label}_vs_reference"] = ref_ms / m if m > 0 else None
+            case["reference_updates_per_s"] = n_upd / (ref_ms / 1e3) if ref_ms > 0 else None
+            cases.append(case)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    print(json.dumps({"metric": "edge updates/sec, the reference's CUDA updater vs this library",
+                      "workload": "refgpu", "unit": "edge_updates/s", "n_gpus": 1, "repeats": R,
+                      "data": "synthetic (seeded generators, dygrass_b200/workloads.py), written as "
+                              "the reference's .mtx files", "cases": cases}))
+    return 0
+
+
 # ---------------------------------------------------------------- main
 
 def main():
@@ -1095,6 +1267,8 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
 
+    if args.workload == "refgpu":   # one line holding both updaters' times
+        return run_refgpu(args) if rank == 0 else 0
     if args.impl == "reference":
         if rank != 0:
             return 0

@@ -101,14 +101,71 @@ struct Walker {
 
 enum : int { kContinue = 0, kFail = 1, kFound = 2 };
 
+// Draw for the walker's current step: word (step-1)&3 of the Philox block
+// (step-1)>>2, computed once per block of four draws.
+__device__ __forceinline__ uint32_t draw_next(Walker &s, uint2 key) {
+    const uint32_t di = s.step - 1u, b = di >> 2;
+    if (b != s.rblk) {
+        s.rbuf = philox4x32_10(make_uint4(b, s.walker, s.c2, s.c3), key);
+        s.rblk = b;
+    }
+    return pick4(s.rbuf, di & 3u);
+}
+
+// The move's common end: R += 1/w; distortion test (incremental only, from
+// step 2 on), then the target test; the walk ends when the step counter
+// reaches max_steps (main.cu:116, 139-157).
+template <bool INCR>
+__device__ __forceinline__ int finish_move(Walker &s, uint2 sl, uint32_t at, bool first,
+                                           uint32_t max_steps, float thr, bool *moved,
+                                           uint2 *taken, uint32_t *taken_at) {
+    *moved = true;
+    *taken = sl;
+    *taken_at = at;
+    // the slot holds the correctly rounded 1/w: one add per move, as R += 1/w
+    s.R = __fadd_rn(s.R, __uint_as_float(sl.y));
+    if (INCR && !first && __fmul_rn(s.R, s.we) >= thr) return kFail;
+    if (sl.x == s.tgt) return kFound;
+    s.prev = s.cur;
+    s.cur = sl.x;
+    s.step += 1u;
+    if (s.step >= max_steps) return kFail;
+    return kContinue;
+}
+
+// Weight-proportional choice in row [lo, lo + deg) by one thread: the first
+// slot, in row order, among those whose column is not `ex` (when has_ex),
+// whose inclusive prefix of fixed-point weights wq(w) exceeds
+// floor(r * total / 2^32).  ~0u when total is 0.
+__device__ __forceinline__ uint32_t lane_pick_weighted(const uint2 *__restrict__ slots,
+                                                       const float *__restrict__ wts, uint32_t lo,
+                                                       uint32_t deg, uint32_t ex, bool has_ex,
+                                                       uint32_t r) {
+    unsigned long long total = 0ull;
+    for (uint32_t j = 0; j < deg; ++j) {
+        if (has_ex && __ldg(&slots[lo + j].x) == ex) continue;
+        total += wq(__ldg(wts + lo + j));
+    }
+    if (total == 0ull) return ~0u;
+    const unsigned long long target = mul_hi32(r, total);
+    unsigned long long acc = 0ull;
+    uint32_t last = deg;
+    for (uint32_t j = 0; j < deg; ++j) {
+        if (has_ex && __ldg(&slots[lo + j].x) == ex) continue;
+        acc += wq(__ldg(wts + lo + j));
+        last = j;
+        if (acc > target) break;
+    }
+    return lo + last;
+}
+
 // One move of one walker, mirroring the reference loop body:
 //   step 1:  any neighbour, r % deg                    (main.cu:99-106)
 //   step >1: dead end if deg == 1; r % (deg - 1) and the last slot when the
 //            draw lands on the previous vertex          (main.cu:118-137)
-//   R += 1/w; distortion test (incremental only, from step 2 on), then the
-//   target test; walk ends when the step counter reaches max_steps
-//                                                       (main.cu:116, 139-157)
-// *moved is set when a neighbour was drawn; *taken receives its slot.
+// then finish_move.  *moved is set when a neighbour was drawn; *taken
+// receives its slot.  WEIGHTED rows are scanned by this thread alone (the
+// walk kernel searches long rows with the whole warp instead).
 template <bool INCR, bool WEIGHTED>
 __device__ __forceinline__ int step_once(Walker &s, const uint2 *__restrict__ desc,
                                          const uint2 *__restrict__ slots,
@@ -120,12 +177,7 @@ __device__ __forceinline__ int step_once(Walker &s, const uint2 *__restrict__ de
     const uint32_t deg = d.y;
     const bool first = (s.step == 1u);
     if (first ? (deg == 0u) : (deg <= 1u)) return kFail;
-    const uint32_t di = s.step - 1u, b = di >> 2;
-    if (b != s.rblk) {
-        s.rbuf = philox4x32_10(make_uint4(b, s.walker, s.c2, s.c3), key);
-        s.rblk = b;
-    }
-    const uint32_t r = pick4(s.rbuf, di & 3u);
+    const uint32_t r = draw_next(s, key);
     uint2 sl;
     uint32_t at;
     if (!WEIGHTED) {
@@ -144,36 +196,190 @@ __device__ __forceinline__ int step_once(Walker &s, const uint2 *__restrict__ de
             }
         }
     } else {
-        unsigned long long total = 0ull;
-        for (uint32_t j = 0; j < deg; ++j) {
-            if (!first && __ldg(&slots[d.x + j].x) == s.prev) continue;
-            total += wq(__ldg(wts + d.x + j));
-        }
-        if (total == 0ull) return kFail;
-        const unsigned long long target = mul_hi32(r, total);
-        unsigned long long acc = 0ull;
-        uint32_t last = deg;
-        for (uint32_t j = 0; j < deg; ++j) {
-            if (!first && __ldg(&slots[d.x + j].x) == s.prev) continue;
-            acc += wq(__ldg(wts + d.x + j));
-            last = j;
-            if (acc > target) break;
-        }
-        at = d.x + last;
+        at = lane_pick_weighted(slots, wts, d.x, deg, s.prev, !first, r);
+        if (at == ~0u) return kFail;
         sl = __ldg(slots + at);
     }
-    *moved = true;
-    *taken = sl;
-    *taken_at = at;
-    // the slot holds the correctly rounded 1/w: one add per move, as R += 1/w
-    s.R = __fadd_rn(s.R, __uint_as_float(sl.y));
-    if (INCR && !first && __fmul_rn(s.R, s.we) >= thr) return kFail;
-    if (sl.x == s.tgt) return kFound;
-    s.prev = s.cur;
-    s.cur = sl.x;
-    s.step += 1u;
-    if (s.step >= max_steps) return kFail;
-    return kContinue;
+    return finish_move<INCR>(s, sl, at, first, max_steps, thr, moved, taken, taken_at);
+}
+
+// ------------------------------------------------ weighted, warp-cooperative
+// Rows longer than kCoopRow slots are searched by the whole warp, one lane's
+// row at a time: each lane takes four consecutive slots per pass over 128
+// slots (two 128-bit slot loads and one 128-bit weight load for a quad inside
+// the row; the quad grid starts at the row start rounded down to four slots,
+// so every vector load is 16-byte aligned), a warp reduction gives the sum of
+// each 128-slot tile, and the sums of up to kSegs segments of tiles are kept
+// in shared memory.  The second pass finds the segment holding the target
+// from those sums and scans only its tiles with a warp prefix scan.  The
+// choice is the per-thread scan's: prefix sums of the fixed-point weights are
+// exact integers, so the order of additions does not matter; only when a sum
+// wraps past 2^64 (weights near 2^32) are prefixes not monotone, and then the
+// second pass scans the whole row from its start, as the per-thread scan does.
+constexpr uint32_t kCoopRow = 32;
+constexpr uint32_t kSegs = 64;
+
+__device__ __forceinline__ unsigned long long wq_ex(uint32_t col, float w, uint32_t ex,
+                                                    bool has_ex) {
+    return (has_ex && col == ex) ? 0ull : wq(w);
+}
+
+// Fixed-point weights of slots [j, j + 4) inside row [lo, hi) (0 outside it
+// or for the excluded column).
+__device__ __forceinline__ void quad_weights(const uint2 *__restrict__ slots,
+                                             const float *__restrict__ wts, uint32_t j,
+                                             uint32_t lo, uint32_t hi, uint32_t ex, bool has_ex,
+                                             unsigned long long q[4]) {
+    if (j >= lo && j + 4u <= hi) {
+        const uint4 s01 = __ldg(reinterpret_cast<const uint4 *>(slots + j));
+        const uint4 s23 = __ldg(reinterpret_cast<const uint4 *>(slots + j + 2u));
+        const float4 w4 = __ldg(reinterpret_cast<const float4 *>(wts + j));
+        q[0] = wq_ex(s01.x, w4.x, ex, has_ex);
+        q[1] = wq_ex(s01.z, w4.y, ex, has_ex);
+        q[2] = wq_ex(s23.x, w4.z, ex, has_ex);
+        q[3] = wq_ex(s23.z, w4.w, ex, has_ex);
+    } else {
+#pragma unroll
+        for (uint32_t u = 0; u < 4u; ++u) {
+            const uint32_t k = j + u;
+            q[u] = (k >= lo && k < hi) ? wq_ex(__ldg(&slots[k].x), __ldg(wts + k), ex, has_ex) : 0ull;
+        }
+    }
+}
+
+// Sum over the warp with a wrap flag (any addition past 2^64).
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v, bool *wrap) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long t = __shfl_xor_sync(kFull, v, o);
+        const unsigned long long x = v + t;
+        *wrap |= x < v;
+        v = x;
+    }
+    return v;
+}
+
+__device__ __forceinline__ unsigned long long warp_incl_scan_u64(unsigned long long v,
+                                                                 uint32_t lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long t = __shfl_up_sync(kFull, v, o);
+        if (lane >= (uint32_t)o) v += t;
+    }
+    return v;
+}
+
+// Every lane of the warp calls this with the same row; returns the chosen
+// slot (absolute index) on every lane, or ~0u when the total weight is 0.
+__device__ __forceinline__ uint32_t warp_pick_weighted(const uint2 *__restrict__ slots,
+                                                    const float *__restrict__ wts, uint32_t lo,
+                                                    uint32_t deg, uint32_t ex, bool has_ex,
+                                                    uint32_t r, unsigned long long *seg,
+                                                    uint32_t lane) {
+    const uint32_t hi = lo + deg;
+    const uint32_t abase = lo & ~3u;
+    const uint32_t ntile = (hi - abase + 127u) >> 7;
+    uint32_t G = (ntile + kSegs - 1u) / kSegs;   // tiles per segment
+    unsigned long long total = 0ull, segsum = 0ull;
+    bool wrap = false;
+    for (uint32_t t = 0; t < ntile; ++t) {
+        unsigned long long q[4];
+        quad_weights(slots, wts, abase + (t << 7) + 4u * lane, lo, hi, ex, has_ex, q);
+        unsigned long long v = q[0] + q[1];
+        wrap |= v < q[0];
+        unsigned long long v2 = q[2] + q[3];
+        wrap |= v2 < q[2];
+        const unsigned long long v3 = v + v2;
+        wrap |= v3 < v;
+        v = warp_sum_u64(v3, &wrap);
+        const unsigned long long nt = total + v;
+        wrap |= nt < total;
+        total = nt;
+        segsum += v;
+        if (t % G == G - 1u || t == ntile - 1u) {
+            if (lane == 0u) seg[t / G] = segsum;
+            segsum = 0ull;
+        }
+    }
+    wrap = __any_sync(kFull, wrap);
+    __syncwarp();
+    if (total == 0ull) return ~0u;
+    const unsigned long long target = mul_hi32(r, total);
+    uint32_t t0 = 0u, t1 = ntile;
+    unsigned long long base = 0ull;
+    if (!wrap) {
+        // the segment holding the target: lane l holds segments 2l and 2l+1
+        const uint32_t nseg = (ntile + G - 1u) / G;
+        const unsigned long long a = 2u * lane < nseg ? seg[2u * lane] : 0ull;
+        const unsigned long long b = 2u * lane + 1u < nseg ? seg[2u * lane + 1u] : 0ull;
+        const unsigned long long incl = warp_incl_scan_u64(a + b, lane);
+        const unsigned long long excl = incl - (a + b);
+        const uint32_t L = __ffs(__ballot_sync(kFull, incl > target)) - 1u;
+        const bool in_a = excl + a > target;
+        const uint32_t sidx = __shfl_sync(kFull, 2u * lane + (in_a ? 0u : 1u), L);
+        base = __shfl_sync(kFull, in_a ? excl : excl + a, L);
+        t0 = sidx * G;
+        t1 = min(ntile, t0 + G);
+    }
+    __syncwarp();   // every lane read seg before a later row overwrites it
+    for (uint32_t t = t0; t < t1; ++t) {
+        const uint32_t j = abase + (t << 7) + 4u * lane;
+        unsigned long long q[4];
+        quad_weights(slots, wts, j, lo, hi, ex, has_ex, q);
+        const unsigned long long v = q[0] + q[1] + q[2] + q[3];
+        const unsigned long long incl = warp_incl_scan_u64(v, lane);
+        // wrapped prefixes when `wrap`: then every tile is scanned in order
+        // and the first slot whose prefix exceeds the target is the
+        // per-thread scan's choice
+        unsigned long long acc = base + incl - v;
+        uint32_t hit = ~0u;
+#pragma unroll
+        for (uint32_t u = 0; u < 4u; ++u) {
+            acc += q[u];
+            if (hit == ~0u && j + u >= lo && j + u < hi && acc > target) hit = j + u;
+        }
+        const unsigned m = __ballot_sync(kFull, hit != ~0u);
+        if (m) return __shfl_sync(kFull, hit, __ffs(m) - 1u);
+        base += __shfl_sync(kFull, incl, 31);
+    }
+    return ~0u;
+}
+
+// One move of every active lane's walker, with rows longer than kCoopRow
+// searched by the whole warp (all 32 lanes call this).  Returns the move's
+// result for active lanes.
+template <bool INCR>
+__device__ __forceinline__ int step_weighted_warp(Walker &s, bool active, const DevGraph &g,
+                                                  uint32_t max_steps, float thr, uint2 key,
+                                                  unsigned long long *seg, uint32_t lane,
+                                                  bool *moved, uint2 *taken, uint32_t *taken_at) {
+    *moved = false;
+    uint2 d = make_uint2(0u, 0u);
+    bool first = false, pick = false;
+    uint32_t r = 0u;
+    if (active) {
+        d = __ldg(g.desc + s.cur);
+        first = (s.step == 1u);
+        if (!(first ? (d.y == 0u) : (d.y <= 1u))) {
+            r = draw_next(s, key);
+            pick = true;
+        }
+    }
+    uint32_t at = ~0u;
+    if (pick && d.y <= kCoopRow) at = lane_pick_weighted(g.slots, g.wts, d.x, d.y, s.prev, !first, r);
+    unsigned coop = __ballot_sync(kFull, pick && d.y > kCoopRow);
+    while (coop) {
+        const uint32_t L = __ffs(coop) - 1u;
+        coop &= coop - 1u;
+        const uint32_t lo = __shfl_sync(kFull, d.x, L), dg = __shfl_sync(kFull, d.y, L);
+        const uint32_t ex = __shfl_sync(kFull, s.prev, L), rr = __shfl_sync(kFull, r, L);
+        const bool hx = __shfl_sync(kFull, first ? 0u : 1u, L) != 0u;
+        const uint32_t j = warp_pick_weighted(g.slots, g.wts, lo, dg, ex, hx, rr, seg, lane);
+        if (lane == L) at = j;
+    }
+    if (!pick || at == ~0u) return kFail;
+    const uint2 sl = __ldg(g.slots + at);
+    return finish_move<INCR>(s, sl, at, first, max_steps, thr, moved, taken, taken_at);
 }
 
 // RN(1/R) < c for positive finite R, c, decided by one product where it can
@@ -190,6 +396,8 @@ __device__ __forceinline__ bool below_best(float R, float c) {
 
 template <bool INCR, bool WEIGHTED>
 __global__ void __launch_bounds__(kWalkThreads) k_walk(WalkArgs a) {
+    // per-warp segment sums of the cooperative weighted search
+    __shared__ unsigned long long s_seg[WEIGHTED ? (kWalkThreads / 32) * kSegs : 1];
     if (a.job.halt && *a.job.halt) return;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
@@ -277,12 +485,19 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(WalkArgs a) {
         }
         if (!__any_sync(kFull, active)) break;
         uint32_t fc = 0u;  // conductance bits of a walker that found its target now
+        int r = kContinue;
+        bool moved = false;
+        uint2 taken;
+        uint32_t taken_at;
+        if constexpr (WEIGHTED) {
+            r = step_weighted_warp<INCR>(s, active, a.g, a.max_steps, a.threshold, a.key,
+                                         s_seg + (threadIdx.x >> 5) * kSegs, lane, &moved, &taken,
+                                         &taken_at);
+        } else if (active) {
+            r = step_once<INCR, false>(s, a.g.desc, a.g.slots, a.g.wts, a.max_steps, a.threshold,
+                                       a.key, &moved, &taken, &taken_at);
+        }
         if (active) {
-            bool moved;
-            uint2 taken;
-            uint32_t taken_at;
-            const int r = step_once<INCR, WEIGHTED>(s, a.g.desc, a.g.slots, a.g.wts, a.max_steps,
-                                                   a.threshold, a.key, &moved, &taken, &taken_at);
             moves += moved ? 1u : 0u;
             if (r != kContinue) {
                 if (r == kFound) {

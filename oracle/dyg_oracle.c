@@ -265,8 +265,12 @@ static int32_t walk_one(const orc_graph *g, uint32_t s, uint32_t t, float we, in
     if (deg == 0) { *R_out = 0.0f; return -1; }
     /* first step: any neighbour (main.cu:99-106) */
     uint32_t r = rng_get(rng, 0);
-    if (p->transition == 1) idx = pick_weighted(g->col[cur], g->w[cur], deg, 0, 0, r);
-    else idx = r % deg;
+    if (p->transition == 1) {
+        idx = pick_weighted(g->col[cur], g->w[cur], deg, 0, 0, r);
+        if (idx == deg) { *R_out = 0.0f; return -1; }   /* no weight in the row: no move */
+    } else {
+        idx = r % deg;
+    }
     nxt = g->col[cur][idx];
     w = g->w[cur][idx];
     R = R + 1.0f / w;

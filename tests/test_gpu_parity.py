@@ -315,3 +315,51 @@ def test_compaction_and_snapshots(dyg, oracle):
     H.copy_from(H0)
     r2 = dyg.incremental_stream(H, W.ins_src[:half], W.ins_dst[:half], W.ins_w[:half], W.params)
     assert np.array_equal(r1.accepted, r2.accepted)
+
+
+def hub_graph(n_leaves, seed, huge=0):
+    """A hub joined to every leaf, plus a ring through the leaves; weights
+    U[0.5, 2] except the hub edges to the first 50 leaves (100; the first
+    `huge` of them 5e9, whose fixed-point weights saturate, so row sums wrap
+    past 2^64).  H = the star + every 10th ring edge.  Insertions: 20 pairs
+    of heavy leaves (walkers reach them through the hub) and 20 random
+    pairs."""
+    rng = np.random.default_rng(seed)
+    leaves = np.arange(1, n_leaves + 1, dtype=np.uint32)
+    ring = np.roll(leaves, -1)
+    gs = np.concatenate([np.zeros(n_leaves, np.uint32), leaves])
+    gd = np.concatenate([leaves, ring])
+    gw = rng.uniform(0.5, 2.0, len(gs)).astype(np.float32)
+    gw[:50] = 100.0
+    gw[:huge] = 5e9
+    h = np.concatenate([np.arange(n_leaves), n_leaves + np.arange(0, n_leaves, 10)])
+    ins = np.concatenate([rng.choice(leaves[:50], size=(20, 2)), rng.choice(leaves, size=(20, 2))])
+    ins = ins[ins[:, 0] != ins[:, 1]]
+    iw = rng.uniform(0.5, 2.0, len(ins)).astype(np.float32)
+    return (n_leaves + 1, gs, gd, gw, gs[h], gd[h], gw[h], ins[:, 0].copy(), ins[:, 1].copy(), iw)
+
+
+@pytest.mark.parametrize("leaves,huge", [(200, 0), (9000, 0), (9000, 3)])
+def test_weighted_long_rows(dyg, oracle, leaves, huge):
+    """Weighted walks through a hub row: 200 slots (one warp pass), 9,000
+    slots (71 tiles of 128, segments of two tiles), and 9,000 slots whose
+    sums wrap past 2^64 (the whole row is scanned in order); insertions with
+    G, then deletions of hub edges in H (walks on G through the hub)."""
+    n, gs, gd, gw, hs, hd, hw, es, ed, ew = hub_graph(leaves, 11 + huge, huge)
+    p = dyg.WalkParams.make(threshold=10.0, walkers=32, max_steps=20, transition=1)
+    H, Ho, r, _ = run_incr_both(dyg, oracle, n, hs, hd, hw, es, ed, ew, p, with_g=(gs, gd, gw))
+    assert 0 < r.accepted.sum() < len(r.accepted)
+    G = dyg.Graph.from_edges(n, np.concatenate([gs, es]), np.concatenate([gd, ed]),
+                             np.concatenate([gw, ew]))
+    Go = oracle.OGraph(n, np.concatenate([gs, es]), np.concatenate([gd, ed]), np.concatenate([gw, ew]))
+    rng = np.random.default_rng(5)
+    k = rng.choice(leaves, 24, replace=False)
+    ds, dd = np.zeros(24, np.uint32), (k + 1).astype(np.uint32)
+    pd = dyg.WalkParams.make(walkers=32, max_steps=20, transition=1)
+    d = dyg.decremental_stream(G, H, ds, dd, pd)
+    st, cd, rx, ry, rk, _ = oracle.decremental(Go, Ho, ds, dd, pd)
+    assert np.array_equal(d.status, st)
+    assert np.array_equal(d.conductance.view(np.uint32), cd.view(np.uint32))
+    assert np.array_equal(d.rec_src, rx) and np.array_equal(d.rec_dst, ry)
+    same_graph(G, Go)
+    same_graph(H, Ho)
