@@ -31,23 +31,27 @@ union graph and a step is the 10 rounds that carry batch r of every graph
 (dygrass_b200/multi.py), after an autotune of the walk launch shape.  The
 plain per-graph loop on the same updates is timed beside it.
 
-Workload "serve": the serving configuration -- 64 resident graphs mixed from
-the mesh, R-MAT and random-geometric generators, update requests of log-
-uniform size in [1, 4096], 60% insertions / 40% deletions.  value = the
-continuous-batching server's throughput (the native scheduler of
-include/dyg_serve.h, driven by dygrass_b200/serve.py) replaying a fixed
-request set that is all pending at once (saturation), timed with CUDA events
-from a restored snapshot; then p50/p99 latency at Poisson arrival rates
-swept around that capacity, for the server and for the plain sequential path
-(every request alone on its graph's own handles), and the same steps
-scheduled from Python for comparison.
+Workload "serve": the serving configuration -- 64 graphs mixed from the
+mesh, R-MAT and random-geometric generators (--serve-mix large: about 10 GB
+of footprint), update requests of log-uniform size in [1, 4096], 60%
+insertions / 40% deletions.  value = the continuous-batching pool server's
+throughput (the native scheduler of include/dyg_serve.h, driven by
+dygrass_b200/serve.py) replaying a fixed request set that is all pending at
+once (saturation), timed with CUDA events with every graph resident; then
+p50/p99 latency at Poisson arrival rates swept around that capacity, for the
+server and for the plain sequential path (every request alone on its graph's
+own handles), and the same replay with a budget of half the footprint, where
+graphs are admitted and evicted while requests run.
 
 N > 1 (torchrun): every rank runs an independent replica of the workload
 (weak scaling, no data-path collective); times are the max over ranks.
 
 --impl reference: the reference has no CPU implementation of this path, so
 the reference arm times the CPU port of its update loop (oracle/, all host
-threads) on a bounded sample of the same workload.
+threads) on the whole workload per step (serve: the first 300 requests).
+
+Workload "refgpu": the reference's own CUDA updaters (built unmodified for
+sm_100a in oracle/_ref) against this library on identical input files.
 """
 from __future__ import annotations
 
@@ -77,6 +81,9 @@ def parse():
     ap.add_argument("--workload", choices=["mesh", "grid", "rmat", "rgg_many", "serve", "refgpu"],
                     default="mesh")
     ap.add_argument("--serve-requests", type=int, default=2000)
+    ap.add_argument("--serve-mix", choices=["small", "large"], default="large",
+                    help="serving graphs: large = meshes 60^3..100^3, R-MAT scales 17..20, "
+                         "random geometric graphs (about 10 GB); small = the quick mix")
     ap.add_argument("--rgg-graphs", type=int, default=256)
     ap.add_argument("--rgg-n-hi", type=int, default=200_000)
     ap.add_argument("--tune-walkers", action="store_true",
@@ -91,6 +98,8 @@ def parse():
                          "strong scaling; default N > 1 runs independent replicas")
     ap.add_argument("--no-plain", action="store_true",
                     help="rgg_many: skip timing the plain per-graph loop")
+    ap.add_argument("--transition", choices=["uniform", "weighted"], default="uniform",
+                    help="walk transition: uniform (the reference's) or the opt-in weighted mode")
     ap.add_argument("--no-exhaustive-leg", action="store_true",
                     help="skip the extra timed pass with every walker run to its end")
     ap.add_argument("--exhaustive", action="store_true",
@@ -105,7 +114,7 @@ def make_workload(args, rank):
     seed = wl.MASTER_SEED + 1000 * rank
     if args.workload == "serve":
         from dygrass_b200.serve import footprint_bytes, poisson_requests
-        cases, ip, dp = wl.serving_mix(seed=seed)
+        cases, ip, dp = wl.serving_mix(seed=seed, large=args.serve_mix == "large")
 
         class Serve:
             pass
@@ -137,13 +146,28 @@ def make_workload(args, rank):
         import dygrass_b200 as dyg
         W.params.flags |= dyg.FLAG_EXHAUSTIVE
         W.dparams.flags |= dyg.FLAG_EXHAUSTIVE
+    if args.transition == "weighted":
+        import dygrass_b200 as dyg
+        W.params.transition = dyg.TRANSITION_WEIGHTED
+        W.dparams.transition = dyg.TRANSITION_WEIGHTED
     return W
 
 
 def workload_config(W, args):
+    cfg = _workload_config(W, args)
+    if args.transition == "weighted":
+        cfg["workload"] += ", weighted transition (opt-in, not the reference's rule)"
+        cfg["transition"] = "weighted"
+    return cfg
+
+
+def _workload_config(W, args):
     if args.workload == "serve":
         ins = sum(len(r.src) for r in W.requests if r.op == 0)
-        return {"workload": f"serve {len(W.cases)} resident graphs (meshes, R-MAT, random geometric), "
+        mix = ("meshes 60^3..100^3, R-MAT scales 17..20, random geometric n <= 2e5"
+               if args.serve_mix == "large" else "meshes 12^3..48^3, R-MAT scales 10..16, "
+                                                 "random geometric n <= 2e5")
+        return {"workload": f"serve {len(W.cases)} graphs ({mix}) in a native pool server, "
                             f"{len(W.requests)} requests of log-uniform size [1, 4096], 60% insert / "
                             f"40% delete, threshold 100, 512 walkers, max_steps 100",
                 "graphs": len(W.cases), "vertices": W.n,
@@ -807,22 +831,37 @@ def _arrive(reqs, rate):
 
 
 def run_serve(args, rank, world, local_rank):
+    """The serving workload through the native pool server.  Steady state:
+    before every replay (untimed) the server is reset to the registered graphs
+    and every graph is prefetched, then the requests are replayed at
+    saturation (all pending at once) or at Poisson rates, device-timed, each
+    request getting the result it gets alone.  Oversubscribed: the same replay
+    with a budget of half the mix's footprint, starting with no graph
+    resident, so graphs are admitted and evicted while requests run.  The
+    plain path is every graph on its own handles, requests one at a time."""
     import torch
     import dygrass_b200 as dyg
-    from dygrass_b200.serve import PlainServer, Server, latency_stats
+    from dygrass_b200.serve import PlainServer, PoolServer, footprint_bytes, latency_stats
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     W = make_workload(args, rank)
-    S = Server(W.cases, W.params, W.dparams, device=local_rank)
-    S.snapshot()
+    fp_total = sum(footprint_bytes(c.n, len(c.g_src), len(c.h_src)) for c in W.cases)
+    S = PoolServer(W.cases, W.params, W.dparams, hbm_budget=int(fp_total * 1.5), device=local_rank)
     stream = torch.cuda.current_stream(dev)
     sync = torch.cuda.synchronize
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     n_upd = W.n_updates
+    n_ins = sum(len(r.src) for r in W.requests if r.op == 0)
 
-    def replay(server, rate):
+    def warm(server):
         server.restore()
+        if isinstance(server, PoolServer):
+            for g in range(len(W.cases)):
+                assert server.prefetch(g)
+
+    def replay(server, rate, reset=warm):
+        reset(server)
         flush.fill_(rank + 1)
         sync()
         return server.serve(_arrive(W.requests, rate), sync=sync)
@@ -835,30 +874,35 @@ def run_serve(args, rank, world, local_rank):
     sync()
     clocks = ClockSampler(local_rank)
     clocks.start()
-    m0 = S.H.counters()[0] + S.G.counters()[0]
     launches0 = dyg.kernel_launches()
     dyg.profile_reset()
-    dyg.profile_enable(True)
-    times, steps = [], 0
+    times, steps, moves = [], 0, [0, 0]
+    nrec = 0
     for _ in range(args.steps):
-        S.restore()
+        warm(S)
         flush.fill_(rank + 1)
         sync()
+        m0 = S.counters()
         reqs = _arrive(W.requests, None)
+        dyg.profile_enable(True)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        S.serve(reqs)
+        done = S.serve(reqs)
         e1.record(stream)
         e1.synchronize()
+        dyg.profile_enable(False)
         times.append(e0.elapsed_time(e1))
-        steps = S.steps
-    dyg.profile_enable(False)
+        m1 = S.counters()
+        moves[0] += m1[0] - m0[0]
+        moves[1] += m1[1] - m0[1]
+        steps = S.stats()["steps"]
+        nrec = sum(len(r.rec_src) for r in done if r.op == 1 and r.rec_src is not None)
     prof = dyg.profile_read()
     launches = dyg.kernel_launches() - launches0
-    moves = (S.H.counters()[0] + S.G.counters()[0] - m0) / args.steps
     clk = clocks.stop()
     ms = float(np.mean(times))
+    incr_moves, decr_moves = moves[0] / args.steps, moves[1] / args.steps
     capacity = len(W.requests) / (ms / 1e3)      # requests per second at saturation
 
     # latency at swept arrival rates, server and plain path
@@ -875,25 +919,31 @@ def run_serve(args, rank, world, local_rank):
     plain_sat = latency_stats(replay(P, None))
     P.close()
     S.close()
-    # the same steps scheduled from Python (per-step library calls), for comparison
-    Sp = Server(W.cases, W.params, W.dparams, device=local_rank, native=False)
-    Sp.snapshot()
-    py_ms = []
+    # oversubscribed: half the footprint, no graph resident at the start
+    S2 = PoolServer(W.cases, W.params, W.dparams, hbm_budget=int(fp_total * 0.5), device=local_rank)
+    over = []
     for _ in range(2):
-        Sp.restore()
+        S2.restore()
         flush.fill_(rank + 1)
         sync()
+        reqs = _arrive(W.requests, None)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        Sp.serve(_arrive(W.requests, None))
+        done2 = S2.serve(reqs)
         e1.record(stream)
         e1.synchronize()
-        py_ms.append(e0.elapsed_time(e1))
-    Sp.close()
+        st2 = S2.stats()
+        row = {"ms_per_replay": e0.elapsed_time(e1), "admissions": st2["admissions"],
+               "evictions": st2["evictions"], "steps": st2["steps"]}
+        row.update({k: v for k, v in latency_stats(done2).items() if k != "throughput_updates_per_s"})
+        row["updates_per_s"] = n_upd / (row["ms_per_replay"] / 1e3)
+        over.append(row)
+    S2.close()
+    plain_ups = plain_sat["throughput_updates_per_s"]
     res = {
         "ms_per_step": ms, "steps_ms": times, "nin": n_upd, "ndel": 0, "accepted": None,
-        "recovered": 0, "incr_moves": moves, "decr_moves": 0.0,
+        "recovered": nrec, "incr_moves": incr_moves, "decr_moves": decr_moves,
         "walk_ms_per_step": (prof["incr_walk_ms"] + prof["decr_walk_ms"]) / args.steps,
         "walk_launches": prof["incr_walk_launches"] + prof["decr_walk_launches"], "prof": prof,
         "launches_per_step": launches / args.steps, "clocks": clk,
@@ -904,14 +954,16 @@ def run_serve(args, rank, world, local_rank):
                                               for r in W.requests)),
                 "note": "the server takes host arrays: its device-timed run is end to end"},
         "dom_kernel": dom_name(prof),
-        "dom_bytes_per_launch": BYTES_PER_MOVE * moves * args.steps / max(
-            prof["decr_walk_launches"] + prof["incr_walk_launches"], 1),
-        "dom_ms_per_launch": (prof["incr_walk_ms"] + prof["decr_walk_ms"]) / max(
-            prof["decr_walk_launches"] + prof["incr_walk_launches"], 1),
+        "dom_bytes_per_launch": dom_bytes(prof, incr_moves, decr_moves, args.steps),
+        "dom_ms_per_launch": dom_ms(prof),
         "serving": {"server_steps_per_replay": steps, "capacity_req_per_s": capacity,
+                    "insertions_per_replay": n_ins, "deletions_per_replay": n_upd - n_ins,
+                    "footprint_bytes": fp_total, "budget_bytes": int(fp_total * 1.5),
                     "sweep": sweep, "plain_saturated": plain_sat,
-                    "python_scheduler_ms_per_replay": float(np.mean(py_ms)),
-                    "scheduler": "native (include/dyg_serve.h): loop thread, pinned staging"},
+                    "speedup_vs_plain": (n_upd / (ms / 1e3)) / plain_ups if plain_ups else None,
+                    "oversubscribed": {"budget_bytes": int(fp_total * 0.5), "replays": over},
+                    "scheduler": "native pool server (include/dyg_serve.h): loop thread, pinned "
+                                 "staging, admission by footprint, eviction to host memory"},
         "W": W,
     }
     return res

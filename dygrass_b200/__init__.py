@@ -95,6 +95,20 @@ class ServerDone(C.Structure):
                 ("t_done_ns", C.c_uint64)]
 
 
+class ServerStats(C.Structure):
+    """Mirror of dyg_server_stats (include/dyg_serve.h)."""
+    _fields_ = [("graphs", C.c_uint32), ("resident", C.c_uint32), ("waiting", C.c_uint32),
+                ("pending", C.c_uint32), ("resident_bytes", C.c_uint64), ("budget_bytes", C.c_uint64),
+                ("admissions", C.c_uint64), ("evictions", C.c_uint64), ("steps", C.c_uint64)]
+
+
+class ServerGraphInfo(C.Structure):
+    """Mirror of dyg_server_graph_info (include/dyg_serve.h)."""
+    _fields_ = [("n_vertices", C.c_uint32), ("resident", C.c_uint32), ("vertex_offset", C.c_uint32),
+                ("pad", C.c_uint32), ("footprint_bytes", C.c_uint64), ("updates", C.c_uint64),
+                ("admissions", C.c_uint64), ("evictions", C.c_uint64), ("pending", C.c_uint64)]
+
+
 class GraphOpts(C.Structure):
     _fields_ = [("slack_per_row", C.c_uint32), ("reserved", C.c_uint32),
                 ("arena_headroom", C.c_double), ("device", C.c_int32), ("pad", C.c_int32)]
@@ -192,6 +206,14 @@ def lib() -> C.CDLL:
         "dyg_server_steps": ([vp], u64),
         "dyg_server_now_ns": ([vp], u64),
         "dyg_server_last_error": ([vp], C.c_char_p),
+        "dyg_server_create_pool": ([u32, u64, C.POINTER(WalkParams), C.POINTER(WalkParams), C.c_int, u32,
+                                    vp, C.POINTER(vp)], C.c_int),
+        "dyg_server_add_graph": ([vp, u32, u64, vp, vp, vp, u64, vp, vp, vp, C.POINTER(u32)], C.c_int),
+        "dyg_server_prefetch": ([vp, u32, C.POINTER(u32)], C.c_int),
+        "dyg_server_stats_read": ([vp, C.POINTER(ServerStats)], C.c_int),
+        "dyg_server_graph_info_read": ([vp, u32, C.POINTER(ServerGraphInfo)], C.c_int),
+        "dyg_server_graph_export": ([vp, u32, u32, vp, vp, vp, u64], C.c_int),
+        "dyg_server_counters": ([vp, C.POINTER(u64), C.POINTER(u64)], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

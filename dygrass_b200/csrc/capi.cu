@@ -214,6 +214,51 @@ void free_graph(dyg_graph *G) {
 
 dyg_status check_walk_params(const dyg_walk_params *p) { return check_params(p); }
 
+dyg_status create_empty_graph(uint32_t n, uint64_t arena_slots, int device, uint32_t slack,
+                              double headroom, dyg_graph **out) {
+    *out = nullptr;
+    if (arena_slots < 1024) arena_slots = 1024;
+    if (arena_slots >= 0xFFFFFFFFull) {
+        set_error("arena would exceed 32-bit slot offsets");
+        return DYG_EINVAL;
+    }
+    DeviceGuard dg(device);
+    dyg_graph *G = new dyg_graph();
+    G->device = device;
+    G->slack = slack;
+    G->headroom = headroom;
+    G->g.n = n;
+    G->g.arena_cap = arena_slots;
+    dyg_status rc = graph_alloc_scalars(G);
+    if (rc == DYG_OK &&
+        (cudaMalloc(&G->g.desc, sizeof(uint2) * (size_t)(n ? n : 1)) != cudaSuccess ||
+         cudaMalloc(&G->g.cap, sizeof(uint32_t) * (size_t)(n ? n : 1)) != cudaSuccess ||
+         cudaMalloc(&G->g.slots, sizeof(uint2) * (size_t)arena_slots) != cudaSuccess ||
+         cudaMalloc(&G->g.wts, sizeof(float) * (size_t)arena_slots) != cudaSuccess)) {
+        cudaGetLastError();
+        set_error("cudaMalloc of a pool graph failed");
+        rc = DYG_ENOMEM;
+    }
+    if (rc == DYG_OK && (cudaMemset(G->g.desc, 0, sizeof(uint2) * (size_t)(n ? n : 1)) != cudaSuccess ||
+                         cudaMemset(G->g.cap, 0, sizeof(uint32_t) * (size_t)(n ? n : 1)) != cudaSuccess))
+        rc = cuda_fail(cudaGetLastError(), "cudaMemset", __FILE__, __LINE__);
+    if (rc != DYG_OK) {
+        free_graph(G);
+        return rc;
+    }
+    *out = G;
+    return DYG_OK;
+}
+
+void destroy_graph(dyg_graph *G) {
+    if (!G) return;
+    {
+        DeviceGuard dg(G->device);
+        cudaDeviceSynchronize();
+    }
+    free_graph(G);
+}
+
 dyg_status device_errors(dyg_graph *G, cudaStream_t st) {
     return G->ws.host_scalars[S_ERR] ? check_device_errors(G, st) : DYG_OK;
 }

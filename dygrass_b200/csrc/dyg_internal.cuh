@@ -22,6 +22,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/dyg.h"
 
@@ -381,5 +382,19 @@ dyg_status exclusive_scan_u32(Workspace &ws, const uint32_t *in, uint32_t *out, 
 dyg_status compact_graph(dyg_graph *G, cudaStream_t st);
 dyg_status grow_arena(dyg_graph *G, uint64_t min_cap, cudaStream_t st);
 dyg_status read_scalars(dyg_graph *G, cudaStream_t st);
+// Rows of local graph [v0, v0 + n) of a pool graph: load places them at the
+// arena top (compacting, then growing, when they do not fit) with columns
+// shifted by v0 and sets the range's descriptors; save copies them back
+// (columns local again, row order kept); clear empties the range (its old
+// slots become a hole that compaction reclaims).  load and save synchronize.
+dyg_status load_range(dyg_graph *G, uint32_t v0, uint32_t n, const uint64_t *row_ptr,
+                      const uint32_t *col, const float *w, cudaStream_t st);
+dyg_status save_range(dyg_graph *G, uint32_t v0, uint32_t n, std::vector<uint64_t> &row_ptr,
+                      std::vector<uint32_t> &col, std::vector<float> &w, cudaStream_t st);
+dyg_status clear_range(dyg_graph *G, uint32_t v0, uint32_t n, cudaStream_t st);
+// A graph of n vertices with no slots and an arena of arena_slots (a pool).
+dyg_status create_empty_graph(uint32_t n, uint64_t arena_slots, int device, uint32_t slack,
+                              double headroom, dyg_graph **out);
+void destroy_graph(dyg_graph *G);
 
 }  // namespace dyg

@@ -4,7 +4,10 @@
 // bump arena: offsets differ from run to run but contents never do.
 #include <cub/cub.cuh>
 
+#include <algorithm>
 #include <atomic>
+#include <cstring>
+#include <vector>
 
 #include "dyg_internal.cuh"
 
@@ -195,9 +198,13 @@ dyg_status exclusive_scan_u32(Workspace &ws, const uint32_t *in, uint32_t *out, 
 
 // -------------------------------------------------------------- compaction
 
+// Rows keep slack; a vertex with neither slots nor capacity (an unoccupied
+// vertex of a pool graph) keeps none.
 __global__ void k_new_caps(DevGraph g, uint32_t slack, uint32_t *caps) {
     const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v < g.n) caps[v] = g.desc[v].y + slack;
+    if (v >= g.n) return;
+    const uint32_t deg = g.desc[v].y;
+    caps[v] = (deg == 0u && g.cap[v] == 0u) ? 0u : deg + slack;
 }
 
 __global__ void k_move_rows(DevGraph g, uint2 *ns, float *nw, const uint32_t *off,
@@ -253,6 +260,121 @@ dyg_status compact_graph(dyg_graph *G, cudaStream_t st) {
     G->g.slots = ns;
     G->g.wts = nw;
     G->g.arena_cap = cap;
+    return DYG_OK;
+}
+
+// ----------------------------------------------------------- vertex ranges
+// A graph that holds many graphs at vertex offsets (the serving pool) loads,
+// saves and clears one graph's rows at a time.
+
+// One warp per vertex: row v0 + i goes to [out_off[i], out_off[i] + deg) of
+// col / w, with columns made local (minus v0).
+__global__ void k_gather_rows(DevGraph g, uint32_t v0, uint32_t n, const unsigned long long *out_off,
+                              uint32_t *col, float *w) {
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n;
+         i += (gridDim.x * blockDim.x) >> 5) {
+        const uint2 d = g.desc[v0 + i];
+        const unsigned long long o = out_off[i];
+        for (uint32_t j = lane; j < d.y; j += 32u) {
+            col[o + j] = g.slots[d.x + j].x - v0;
+            w[o + j] = g.wts[d.x + j];
+        }
+    }
+}
+
+dyg_status load_range(dyg_graph *G, uint32_t v0, uint32_t n, const uint64_t *row_ptr,
+                      const uint32_t *col, const float *w, cudaStream_t st) {
+    if (n == 0) return DYG_OK;
+    if ((uint64_t)v0 + n > G->g.n) {
+        set_error("vertex range outside the graph");
+        return DYG_EINVAL;
+    }
+    uint64_t need = 0;
+    for (uint32_t v = 0; v < n; ++v) need += row_ptr[v + 1] - row_ptr[v] + G->slack;
+    DYG_TRY(read_scalars(G, st));
+    uint64_t top = G->ws.host_scalars[S_TOP];
+    if (top + need > G->g.arena_cap) {
+        // holes left by evicted graphs and moved rows go first
+        DYG_TRY(compact_graph(G, st));
+        DYG_TRY(read_scalars(G, st));
+        top = G->ws.host_scalars[S_TOP];
+        if (top + need > G->g.arena_cap) DYG_TRY(grow_arena(G, top + need, st));
+    }
+    if (top + need >= 0xFFFFFFFFull) {
+        set_error("arena would exceed 32-bit slot offsets");
+        return DYG_ENOMEM;
+    }
+    std::vector<uint2> h_desc(n), h_slots(need ? need : 1);
+    std::vector<uint32_t> h_cap(n);
+    std::vector<float> h_w(need ? need : 1, 0.0f);
+    uint64_t o = top;
+    for (uint32_t v = 0; v < n; ++v) {
+        const uint64_t deg = row_ptr[v + 1] - row_ptr[v];
+        if (deg > kBigRow) G->long_rows = true;
+        h_desc[v] = make_uint2((uint32_t)o, (uint32_t)deg);
+        h_cap[v] = (uint32_t)(deg + G->slack);
+        for (uint64_t j = 0; j < deg; ++j) {
+            const float x = w[row_ptr[v] + j];
+            const float rw = 1.0f / x;   // IEEE division: equals __frcp_rn(x)
+            uint32_t rb;
+            memcpy(&rb, &rw, 4);
+            h_slots[o - top + j] = make_uint2(col[row_ptr[v] + j] + v0, rb);
+            h_w[o - top + j] = x;
+        }
+        o += deg + G->slack;
+    }
+    DYG_CUDA(cudaMemcpyAsync(G->g.slots + top, h_slots.data(), sizeof(uint2) * need,
+                             cudaMemcpyHostToDevice, st));
+    DYG_CUDA(cudaMemcpyAsync(G->g.wts + top, h_w.data(), sizeof(float) * need, cudaMemcpyHostToDevice, st));
+    DYG_CUDA(cudaMemcpyAsync(G->g.desc + v0, h_desc.data(), sizeof(uint2) * n, cudaMemcpyHostToDevice, st));
+    DYG_CUDA(cudaMemcpyAsync(G->g.cap + v0, h_cap.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, st));
+    const unsigned long long ntop = top + need;
+    DYG_CUDA(cudaMemcpyAsync(G->g.top, &ntop, sizeof(ntop), cudaMemcpyHostToDevice, st));
+    DYG_CUDA(cudaStreamSynchronize(st));
+    G->ws.host_scalars[S_TOP] = ntop;
+    return DYG_OK;
+}
+
+dyg_status save_range(dyg_graph *G, uint32_t v0, uint32_t n, std::vector<uint64_t> &row_ptr,
+                      std::vector<uint32_t> &col, std::vector<float> &w, cudaStream_t st) {
+    row_ptr.assign((size_t)n + 1, 0);
+    col.clear();
+    w.clear();
+    if (n == 0) return DYG_OK;
+    std::vector<uint2> h_desc(n);
+    DYG_CUDA(cudaMemcpyAsync(h_desc.data(), G->g.desc + v0, sizeof(uint2) * n, cudaMemcpyDeviceToHost, st));
+    DYG_CUDA(cudaStreamSynchronize(st));
+    std::vector<unsigned long long> off(n);
+    for (uint32_t v = 0; v < n; ++v) {
+        off[v] = row_ptr[v];
+        row_ptr[v + 1] = row_ptr[v] + h_desc[v].y;
+    }
+    const uint64_t m = row_ptr[n];
+    col.resize(m);
+    w.resize(m);
+    if (m == 0) return DYG_OK;
+    Workspace &ws = G->ws;
+    DYG_TRY(ensure(ws.f_uid, sizeof(unsigned long long) * n));
+    DYG_TRY(ensure(ws.cand_x, sizeof(uint32_t) * m));
+    DYG_TRY(ensure(ws.cand_w, sizeof(float) * m));
+    DYG_CUDA(cudaMemcpyAsync(ws.f_uid.p, off.data(), sizeof(unsigned long long) * n,
+                             cudaMemcpyHostToDevice, st));
+    const int gr = (int)std::min<uint64_t>(((uint64_t)n * 32 + 255) / 256, (uint64_t)num_sms() * 16);
+    k_gather_rows<<<gr, 256, 0, st>>>(G->g, v0, n, ptr<unsigned long long>(ws.f_uid),
+                                      ptr<uint32_t>(ws.cand_x), ptr<float>(ws.cand_w));
+    count_launch();
+    DYG_CUDA(cudaGetLastError());
+    DYG_CUDA(cudaMemcpyAsync(col.data(), ws.cand_x.p, sizeof(uint32_t) * m, cudaMemcpyDeviceToHost, st));
+    DYG_CUDA(cudaMemcpyAsync(w.data(), ws.cand_w.p, sizeof(float) * m, cudaMemcpyDeviceToHost, st));
+    DYG_CUDA(cudaStreamSynchronize(st));
+    return DYG_OK;
+}
+
+dyg_status clear_range(dyg_graph *G, uint32_t v0, uint32_t n, cudaStream_t st) {
+    if (n == 0) return DYG_OK;
+    DYG_CUDA(cudaMemsetAsync(G->g.desc + v0, 0, sizeof(uint2) * n, st));
+    DYG_CUDA(cudaMemsetAsync(G->g.cap + v0, 0, sizeof(uint32_t) * n, st));
     return DYG_OK;
 }
 

@@ -4,20 +4,34 @@
 // (random_walk_incremental/main.cu:314-340, random_walk_decremental/
 // main.cu:395-444); it has no request loop.  Here many graphs stay resident
 // in one union graph and requests for them are scheduled in steps.  A step
-// takes the oldest pending request of every graph that has one, gathers the
-// insertion requests into one batch and the deletion requests into another
-// (global vertex ids = local id + the graph's offset; per-edge update ids =
-// the graph's own update counter), stages both through page-locked memory,
-// runs the incremental pipeline and then the decremental pipeline on the
-// device (one host synchronize each, for the halt/resume protocol), and
-// splits the results back per request: per-edge arrays by position,
-// recovered edges by the graph whose vertex range holds them (each step runs
-// at most one deletion request per graph, and a recovered edge joins two
-// vertices of the graph it was recovered in).
+// takes the oldest pending request of every resident graph that has one,
+// gathers the insertion requests into one batch and the deletion requests
+// into another (global vertex ids = local id + the graph's offset; per-edge
+// update ids = the graph's own update counter), stages both through
+// page-locked memory, runs the incremental pipeline and then the decremental
+// pipeline on the device (one host synchronize each, for the halt/resume
+// protocol), and splits the results back per request: per-edge arrays by
+// position, recovered edges by the graph whose vertex range holds them (each
+// step runs at most one deletion request per graph, and a recovered edge
+// joins two vertices of the graph it was recovered in).
 //
 // Graphs are disjoint in the union, every walk stays inside its own graph, and
 // a graph's update ids do not depend on the other graphs, so each request's
 // result equals the one it gets alone on its graph's own handles.
+//
+// Two ways to hold the graphs:
+//   static (dyg_server_create): the caller builds the union; every graph is
+//     resident for the server's life.
+//   pool (dyg_server_create_pool): the server owns the union graphs and an
+//     HBM budget for the graphs' estimated footprints.  Registered graphs live
+//     in host memory until a request for them is scheduled; then, at the start
+//     of a step, waiting graphs (oldest pending request first) are admitted
+//     into a free vertex range while their footprint fits the budget, and to
+//     make room the server evicts resident graphs -- idle ones least recently
+//     used first, then busy ones whose oldest pending request is younger than
+//     the waiting graph's -- by copying their rows back to host memory.  A
+//     graph's rows keep their order through eviction and admission, so its
+//     results do not depend on where or how often it was resident.
 #include <math.h>
 #include <string.h>
 
@@ -85,12 +99,39 @@ struct DevSet {
     }
 };
 
+// Rows of one graph in host memory (local ids, row order as on the device).
+struct HostRows {
+    std::vector<uint64_t> rp;
+    std::vector<uint32_t> col;
+    std::vector<float> w;
+    void clear() {
+        std::vector<uint64_t>().swap(rp);
+        std::vector<uint32_t>().swap(col);
+        std::vector<float>().swap(w);
+    }
+};
+
+// A graph of a pool server.  `resident`, `v0` and the counters change only in
+// the thread that runs steps (or in a call that needs an idle server), under
+// the server's lock; host rows are touched only by those threads.
+struct PoolGraph {
+    uint32_t n = 0;
+    bool resident = false;
+    uint32_t v0 = 0;              // first vertex in the union while resident
+    uint64_t footprint = 0;       // estimated device bytes (admission size)
+    uint64_t last_step = 0;       // last step that ran one of its requests
+    uint64_t admissions = 0, evictions = 0;
+    HostRows g, h;                // while not resident
+    HostRows g0, h0;              // the registered rows (reset), if kept
+};
+
 }  // namespace
 }  // namespace dyg
 
 struct dyg_server {
     dyg_graph *G = nullptr, *H = nullptr;
-    std::vector<uint32_t> off;            // n_graphs + 1 vertex offsets
+    bool pool = false;
+    std::vector<uint32_t> off;            // static: n_graphs + 1 vertex offsets
     dyg_walk_params ip{}, dp{};
     cudaStream_t st = nullptr;
     std::chrono::steady_clock::time_point t0;
@@ -98,6 +139,7 @@ struct dyg_server {
     std::mutex mu;                        // guards everything below up to `loop`
     std::condition_variable cv_work, cv_idle;
     std::vector<std::deque<dyg::Request *>> queues;
+    std::vector<uint64_t> uid_next;
     std::unordered_map<uint64_t, dyg::Request *> by_tag;   // submitted, not fetched
     std::deque<dyg_server_done> done;
     uint32_t pending = 0;
@@ -106,9 +148,14 @@ struct dyg_server {
     std::string err;
     std::thread loop;
 
+    // pool mode (graph states: see PoolGraph)
+    std::deque<dyg::PoolGraph> pg;        // stable addresses while it grows
+    uint64_t budget = 0, resident_bytes = 0, admissions = 0, evictions = 0;
+    uint32_t vcap = 0;
+    bool keep_initial = false;
+    std::vector<std::pair<uint32_t, uint32_t>> free_ranges;   // [a, b), ascending
+
     // owned by the thread that runs the step
-    std::vector<uint64_t> uid_next;
-    std::vector<dyg::Request *> owner;
     dyg::Pinned<uint32_t> h_src, h_dst, h_rx, h_ry;
     dyg::Pinned<float> h_w, h_cond;
     dyg::Pinned<unsigned long long> h_uid;
@@ -118,6 +165,10 @@ struct dyg_server {
 };
 
 namespace {
+
+using dyg::HostRows;
+using dyg::PoolGraph;
+using dyg::Request;
 
 uint64_t now_ns(const dyg_server *s) {
     return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
@@ -133,7 +184,189 @@ dyg_status fail(dyg_server *s, dyg_status code, const std::string &msg) {
     return code;
 }
 
-using dyg::Request;
+uint32_t graph_count(const dyg_server *s) { return (uint32_t)s->queues.size(); }
+
+// First vertex and vertex count of graph g in the union (pool: while resident).
+uint32_t graph_base(const dyg_server *s, uint32_t g) { return s->pool ? s->pg[g].v0 : s->off[g]; }
+uint32_t graph_size(const dyg_server *s, uint32_t g) {
+    return s->pool ? s->pg[g].n : s->off[g + 1] - s->off[g];
+}
+
+// Estimated device bytes of a graph: per slot 12 B (slot + weight) with the
+// arena's headroom and per-row slack, per vertex 12 B (descriptor + capacity),
+// for G and H each.
+uint64_t footprint_of(uint32_t n, uint64_t g_slots, uint64_t h_slots, uint32_t slack,
+                      double headroom) {
+    const double gs = ((double)g_slots + (double)slack * n) * (1.0 + headroom);
+    const double hs = ((double)h_slots + (double)slack * n) * (1.0 + headroom);
+    return (uint64_t)(12.0 * (gs + hs)) + 24ull * n;
+}
+
+// ------------------------------------------------------ vertex ranges (pool)
+
+bool range_find(const dyg_server *s, uint32_t n, uint32_t *v0) {
+    for (const auto &r : s->free_ranges)
+        if (r.second - r.first >= n) {
+            *v0 = r.first;
+            return true;
+        }
+    return false;
+}
+
+void range_take(dyg_server *s, uint32_t v0, uint32_t n) {
+    for (size_t i = 0; i < s->free_ranges.size(); ++i) {
+        auto &r = s->free_ranges[i];
+        if (r.first == v0) {
+            r.first += n;
+            if (r.first == r.second) s->free_ranges.erase(s->free_ranges.begin() + (long)i);
+            return;
+        }
+    }
+}
+
+void range_free(dyg_server *s, uint32_t v0, uint32_t n) {
+    if (n == 0) return;
+    auto &fr = s->free_ranges;
+    auto it = std::lower_bound(fr.begin(), fr.end(), std::make_pair(v0, v0));
+    it = fr.insert(it, std::make_pair(v0, v0 + n));
+    // merge with the following and the preceding range
+    if (it + 1 != fr.end() && it->second == (it + 1)->first) {
+        it->second = (it + 1)->second;
+        fr.erase(it + 1);
+    }
+    if (it != fr.begin() && (it - 1)->second == it->first) {
+        (it - 1)->second = it->second;
+        fr.erase(it);
+    }
+}
+
+// Copies a resident graph's rows to host memory and frees its range.
+dyg_status evict(dyg_server *s, uint32_t g) {
+    PoolGraph &p = s->pg[g];
+    DYG_TRY(dyg::save_range(s->G, p.v0, p.n, p.g.rp, p.g.col, p.g.w, s->st));
+    DYG_TRY(dyg::save_range(s->H, p.v0, p.n, p.h.rp, p.h.col, p.h.w, s->st));
+    DYG_TRY(dyg::clear_range(s->G, p.v0, p.n, s->st));
+    DYG_TRY(dyg::clear_range(s->H, p.v0, p.n, s->st));
+    DYG_CUDA(cudaStreamSynchronize(s->st));
+    std::lock_guard<std::mutex> lk(s->mu);
+    range_free(s, p.v0, p.n);
+    p.resident = false;
+    s->resident_bytes -= p.footprint;
+    p.footprint = footprint_of(p.n, p.g.col.size(), p.h.col.size(), s->G->slack, s->G->headroom);
+    ++p.evictions;
+    ++s->evictions;
+    return DYG_OK;
+}
+
+// Loads a graph's host rows into [v0, v0 + n) of both union graphs.
+dyg_status admit(dyg_server *s, uint32_t g, uint32_t v0) {
+    PoolGraph &p = s->pg[g];
+    dyg_status rc = dyg::load_range(s->G, v0, p.n, p.g.rp.data(), p.g.col.data(), p.g.w.data(), s->st);
+    if (rc == DYG_OK) {
+        rc = dyg::load_range(s->H, v0, p.n, p.h.rp.data(), p.h.col.data(), p.h.w.data(), s->st);
+        if (rc != DYG_OK) {
+            dyg::clear_range(s->G, v0, p.n, s->st);
+            cudaStreamSynchronize(s->st);
+        }
+    }
+    if (rc != DYG_OK) return rc;
+    p.g.clear();
+    p.h.clear();
+    std::lock_guard<std::mutex> lk(s->mu);
+    range_take(s, v0, p.n);
+    p.v0 = v0;
+    p.resident = true;
+    s->resident_bytes += p.footprint;
+    ++p.admissions;
+    ++s->admissions;
+    return DYG_OK;
+}
+
+// Makes room for graph g (evicting in the victim order) and admits it; *ok
+// is false when it does not fit yet.  `t_wait` is the arrival of its oldest
+// pending request (busy graphs with an older one are not evicted for it);
+// `keep` marks graphs that must stay (admitted in this step).
+dyg_status make_room_and_admit(dyg_server *s, uint32_t g, uint64_t t_wait,
+                               const std::vector<char> &keep, bool *ok) {
+    *ok = false;
+    PoolGraph &p = s->pg[g];
+    struct Victim {
+        uint32_t g;
+        bool busy;
+        uint64_t head_t, last;
+    };
+    std::vector<Victim> vs;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (uint32_t k = 0; k < graph_count(s); ++k) {
+            if (!s->pg[k].resident || keep[k]) continue;
+            const bool busy = !s->queues[k].empty();
+            const uint64_t ht = busy ? s->queues[k].front()->rec.t_submit_ns : ~0ull;
+            if (busy && ht <= t_wait) continue;
+            vs.push_back(Victim{k, busy, ht, s->pg[k].last_step});
+        }
+    }
+    // idle graphs least recently used first, then busy graphs with the
+    // youngest oldest request first
+    std::sort(vs.begin(), vs.end(), [](const Victim &a, const Victim &b) {
+        if (a.busy != b.busy) return !a.busy;
+        if (!a.busy) return a.last < b.last;
+        return a.head_t > b.head_t;
+    });
+    // would evicting every candidate make room?  Otherwise evict nothing.
+    uint64_t freeable = 0;
+    for (const Victim &v : vs) freeable += s->pg[v.g].footprint;
+    if (s->resident_bytes - std::min(s->resident_bytes, freeable) + p.footprint > s->budget) return DYG_OK;
+    size_t k = 0;
+    uint32_t v0 = 0;
+    while (!(s->resident_bytes + p.footprint <= s->budget && range_find(s, p.n, &v0))) {
+        if (k == vs.size()) return DYG_OK;
+        DYG_TRY(evict(s, vs[k++].g));
+    }
+    DYG_TRY(admit(s, g, v0));
+    *ok = true;
+    return DYG_OK;
+}
+
+// Pool admission at the start of a step.  Graphs whose admission fails for
+// lack of memory, or whose footprint outgrew the budget, go to `failed` with
+// the status their pending requests complete with.
+dyg_status admit_waiting(dyg_server *s, std::vector<std::pair<uint32_t, dyg_status>> *failed) {
+    struct Wait {
+        uint64_t t;
+        uint32_t g;
+    };
+    std::vector<Wait> waiting;
+    std::vector<char> keep;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        keep.assign(graph_count(s), 0);
+        for (uint32_t g = 0; g < graph_count(s); ++g)
+            if (!s->pg[g].resident && !s->queues[g].empty())
+                waiting.push_back(Wait{s->queues[g].front()->rec.t_submit_ns, g});
+    }
+    std::sort(waiting.begin(), waiting.end(), [](const Wait &a, const Wait &b) {
+        return a.t != b.t ? a.t < b.t : a.g < b.g;
+    });
+    for (const Wait &w : waiting) {
+        if (s->pg[w.g].footprint > s->budget) {
+            dyg::set_error("graph " + std::to_string(w.g) + " outgrew the HBM budget");
+            failed->push_back({w.g, DYG_ENOMEM});
+            continue;
+        }
+        bool ok = false;
+        const dyg_status rc = make_room_and_admit(s, w.g, w.t, keep, &ok);
+        if (rc == DYG_ENOMEM) {
+            failed->push_back({w.g, rc});
+            continue;
+        }
+        DYG_TRY(rc);
+        if (ok) keep[w.g] = 1;
+    }
+    return DYG_OK;
+}
+
+// ------------------------------------------------------------------- steps
 
 // Stages the step's batches, runs both pipelines and splits the results.
 dyg_status stage_and_run(dyg_server *s, const std::vector<Request *> &heads, uint64_t ni,
@@ -145,7 +378,6 @@ dyg_status stage_and_run(dyg_server *s, const std::vector<Request *> &heads, uin
         set_error("a step holds more than 2^32 - 1 updates of one kind");
         return DYG_EINVAL;
     }
-    DevSet ds(s->H->device);
     cudaStream_t st = s->st;
     DYG_TRY(s->h_src.ensure(nt));
     DYG_TRY(s->h_dst.ensure(nt));
@@ -156,7 +388,7 @@ dyg_status stage_and_run(dyg_server *s, const std::vector<Request *> &heads, uin
     for (Request *r : heads) {
         const uint32_t n = r->rec.n;
         if (!n) continue;
-        const uint32_t o = s->off[r->rec.graph];
+        const uint32_t o = graph_base(s, r->rec.graph);
         const bool ins = r->rec.op == DYG_STREAM_INSERT;
         uint64_t &k = ins ? ki : kd;
         for (uint32_t i = 0; i < n; ++i) {
@@ -211,7 +443,12 @@ dyg_status stage_and_run(dyg_server *s, const std::vector<Request *> &heads, uin
         DYG_CUDA(cudaMemcpyAsync(s->h_rk.p, ws.rk2.p, nrec, cudaMemcpyDeviceToHost, st));
     }
     DYG_CUDA(cudaStreamSynchronize(st));
-    std::fill(s->owner.begin(), s->owner.end(), nullptr);
+    // vertex ranges of the step's deletion requests, ascending
+    struct Owner {
+        uint32_t lo, hi;
+        Request *r;
+    };
+    std::vector<Owner> owners;
     ki = 0;
     kd = ni;
     for (Request *r : heads) {
@@ -221,76 +458,116 @@ dyg_status stage_and_run(dyg_server *s, const std::vector<Request *> &heads, uin
         uint64_t &k = ins ? ki : kd;
         r->out_i.assign(s->h_out.p + k, s->h_out.p + k + n);
         r->out_c.assign(s->h_cond.p + k, s->h_cond.p + k + n);
-        if (ins) r->out_a.assign(s->h_acc.p + k, s->h_acc.p + k + n);
-        else s->owner[r->rec.graph] = r;
+        if (ins) {
+            r->out_a.assign(s->h_acc.p + k, s->h_acc.p + k + n);
+        } else {
+            const uint32_t b = graph_base(s, r->rec.graph);
+            owners.push_back(Owner{b, b + graph_size(s, r->rec.graph), r});
+        }
         k += n;
     }
+    std::sort(owners.begin(), owners.end(), [](const Owner &a, const Owner &b) { return a.lo < b.lo; });
     for (uint64_t j = 0; j < nrec; ++j) {
         const uint32_t x = s->h_rx.p[j], y = s->h_ry.p[j];
-        const size_t g = (size_t)(std::upper_bound(s->off.begin(), s->off.end(), x) - s->off.begin()) - 1;
-        Request *r = g < s->owner.size() ? s->owner[g] : nullptr;
-        if (!r || y < s->off[g] || y >= s->off[g + 1]) {
+        auto it = std::upper_bound(owners.begin(), owners.end(), x,
+                                   [](uint32_t v, const Owner &o) { return v < o.lo; });
+        if (it == owners.begin() || x >= (it - 1)->hi || y < (it - 1)->lo || y >= (it - 1)->hi) {
             set_error("a recovered edge lies outside the graphs deleting in this step");
             return DYG_ESTATE;
         }
-        r->rx.push_back(x - s->off[g]);
-        r->ry.push_back(y - s->off[g]);
-        r->rk.push_back(s->h_rk.p[j]);
+        const Owner &o = *(it - 1);
+        o.r->rx.push_back(x - o.lo);
+        o.r->ry.push_back(y - o.lo);
+        o.r->rk.push_back(s->h_rk.p[j]);
     }
     for (Request *r : heads) r->rec.n_rec = r->rx.size();
     return DYG_OK;
 }
 
+void complete(dyg_server *s, Request *r, dyg_status rc, uint64_t t_start, uint64_t t_done,
+              uint64_t step) {
+    r->rec.status = (int32_t)rc;
+    r->rec.step = step;
+    if (!r->rec.t_start_ns) r->rec.t_start_ns = t_start;
+    r->rec.t_done_ns = t_done;
+    r->finished = true;
+    s->done.push_back(r->rec);
+}
+
 dyg_status run_step(dyg_server *s, uint32_t *n_done) {
-    std::vector<Request *> heads;
+    if (n_done) *n_done = 0;
     {
         std::lock_guard<std::mutex> lk(s->mu);
         if (s->stepping) {
-            dyg::set_error("another step is running");
+            dyg::set_error("another step (or an exclusive call) is running");
             return DYG_ESTATE;
         }
-        for (auto &q : s->queues)
-            if (!q.empty()) {
-                heads.push_back(q.front());
+        if (s->pending == 0) return DYG_OK;
+        s->stepping = true;
+    }
+    dyg::DevSet ds(s->H->device);
+    const uint64_t t_start = now_ns(s);
+    std::vector<std::pair<uint32_t, dyg_status>> failed;
+    dyg_status arc = DYG_OK;
+    std::string amsg;
+    if (s->pool) {
+        try {
+            arc = admit_waiting(s, &failed);
+        } catch (const std::bad_alloc &) {
+            dyg::set_error("host allocation failed while admitting graphs");
+            arc = DYG_ENOMEM;
+        }
+        if (arc != DYG_OK || !failed.empty()) amsg = dyg_last_error_string();
+    }
+    std::vector<Request *> heads, dead;
+    uint64_t ni = 0, nd = 0;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (uint32_t g = 0; g < graph_count(s); ++g) {
+            auto &q = s->queues[g];
+            if (q.empty() || (s->pool && !s->pg[g].resident)) continue;
+            Request *r = q.front();
+            q.pop_front();
+            r->rec.first_update_id = s->uid_next[g];
+            s->uid_next[g] += r->rec.n;
+            r->rec.t_start_ns = t_start;
+            if (s->pool) s->pg[g].last_step = s->steps;
+            heads.push_back(r);
+            if (r->rec.op == DYG_STREAM_INSERT) ni += r->rec.n;
+            else nd += r->rec.n;
+        }
+        for (const auto &f : failed) {
+            auto &q = s->queues[f.first];
+            while (!q.empty()) {
+                q.front()->rec.status = (int32_t)f.second;
+                dead.push_back(q.front());
                 q.pop_front();
             }
-        s->pending -= (uint32_t)heads.size();
-        if (!heads.empty()) s->stepping = true;
+        }
+        s->pending -= (uint32_t)(heads.size() + dead.size());
     }
-    if (n_done) *n_done = (uint32_t)heads.size();
-    if (heads.empty()) return DYG_OK;
-    const uint64_t t_start = now_ns(s);
-    uint64_t ni = 0, nd = 0;
-    for (Request *r : heads) {
-        r->rec.first_update_id = s->uid_next[r->rec.graph];
-        s->uid_next[r->rec.graph] += r->rec.n;
-        r->rec.t_start_ns = t_start;
-        if (r->rec.op == DYG_STREAM_INSERT) ni += r->rec.n;
-        else nd += r->rec.n;
+    if (n_done) *n_done = (uint32_t)(heads.size() + dead.size());
+    dyg_status rc = arc;
+    if (rc == DYG_OK) {
+        try {
+            rc = stage_and_run(s, heads, ni, nd);
+        } catch (const std::bad_alloc &) {
+            dyg::set_error("host allocation failed in a server step");
+            rc = DYG_ENOMEM;
+        }
     }
-    dyg_status rc;
-    try {
-        rc = stage_and_run(s, heads, ni, nd);
-    } catch (const std::bad_alloc &) {
-        dyg::set_error("host allocation failed in a server step");
-        rc = DYG_ENOMEM;
-    }
-    const std::string msg = rc == DYG_OK ? std::string() : std::string(dyg_last_error_string());
+    const std::string msg = rc == DYG_OK ? amsg : std::string(dyg_last_error_string());
     const uint64_t t_done = now_ns(s);
     {
         std::lock_guard<std::mutex> lk(s->mu);
-        for (Request *r : heads) {
-            r->rec.status = (int32_t)rc;
-            r->rec.step = s->steps;
-            r->rec.t_done_ns = t_done;
-            r->finished = true;
-            s->done.push_back(r->rec);
-        }
+        for (Request *r : heads) complete(s, r, rc, t_start, t_done, s->steps);
+        for (Request *r : dead) complete(s, r, (dyg_status)r->rec.status, t_start, t_done, s->steps);
         ++s->steps;
         s->stepping = false;
-        if (rc != DYG_OK) s->err = msg;
+        if (!msg.empty()) s->err = msg;
     }
     s->cv_idle.notify_all();
+    s->cv_work.notify_all();
     return rc;
 }
 
@@ -298,7 +575,7 @@ void loop_main(dyg_server *s) {
     dyg::DevSet ds(s->H->device);
     std::unique_lock<std::mutex> lk(s->mu);
     while (!s->stop) {
-        if (s->pending == 0) {
+        if (s->pending == 0 || s->stepping) {   // stepping: an exclusive call holds the graphs
             s->cv_work.wait(lk);
             continue;
         }
@@ -308,14 +585,14 @@ void loop_main(dyg_server *s) {
     }
 }
 
-// The checks of one request (no lock held); "" when it is valid.
+// The checks of one request (the lock held); "" when it is valid.
 std::string check_request(const dyg_server *s, uint32_t graph, uint32_t op, const uint32_t *src,
                           const uint32_t *dst, const float *w, uint64_t n) {
-    if (graph >= s->queues.size()) return "graph index out of range";
+    if (graph >= graph_count(s)) return "graph index out of range";
     if (op != DYG_STREAM_INSERT && op != DYG_STREAM_DELETE) return "unknown op";
     if (n > 0xFFFFFFFFull) return "a request holds more than 2^32 - 1 updates";
     if (n && (!src || !dst || (op == DYG_STREAM_INSERT && !w))) return "NULL array";
-    const uint32_t nv = s->off[graph + 1] - s->off[graph];
+    const uint32_t nv = graph_size(s, graph);
     for (uint64_t i = 0; i < n; ++i) {
         if (src[i] >= nv || dst[i] >= nv)
             return "update " + std::to_string(i) + " names a vertex outside graph " +
@@ -343,6 +620,66 @@ Request *make_request(const dyg_server *s, uint64_t tag, uint32_t graph, uint32_
     return r;
 }
 
+// Rows of an edge list in the order dyg_graph_create_from_edges gives them:
+// for each edge (s, d), row s gets d, then row d gets s.
+void rows_from_edges(uint32_t n, uint64_t m, const uint32_t *src, const uint32_t *dst,
+                     const float *w, HostRows *out) {
+    out->rp.assign((size_t)n + 1, 0);
+    for (uint64_t i = 0; i < m; ++i) {
+        out->rp[src[i] + 1]++;
+        out->rp[dst[i] + 1]++;
+    }
+    for (uint32_t v = 0; v < n; ++v) out->rp[v + 1] += out->rp[v];
+    out->col.resize(out->rp[n]);
+    out->w.resize(out->rp[n]);
+    std::vector<uint64_t> fill(out->rp.begin(), out->rp.end() - 1);
+    for (uint64_t i = 0; i < m; ++i) {
+        const uint64_t a = fill[src[i]]++;
+        out->col[a] = dst[i];
+        out->w[a] = w[i];
+        const uint64_t b = fill[dst[i]]++;
+        out->col[b] = src[i];
+        out->w[b] = w[i];
+    }
+}
+
+// Exclusive access to the graphs for a call that needs an idle server:
+// holds `stepping` so that no step starts meanwhile.
+struct Exclusive {
+    dyg_server *s;
+    bool ok = false;
+    explicit Exclusive(dyg_server *sv) : s(sv) {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->stepping || s->pending) return;
+        s->stepping = true;
+        ok = true;
+    }
+    ~Exclusive() {
+        if (!ok) return;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->stepping = false;
+        }
+        s->cv_work.notify_all();
+        s->cv_idle.notify_all();
+    }
+};
+
+dyg_status server_alloc(dyg_graph *G, dyg_graph *H, const dyg_walk_params *ip,
+                        const dyg_walk_params *dp, dyg_stream_t stream, dyg_server **out) {
+    DYG_TRY(dyg::check_walk_params(ip));
+    DYG_TRY(dyg::check_walk_params(dp));
+    dyg_server *s = new dyg_server;
+    s->G = G;
+    s->H = H;
+    s->ip = *ip;
+    s->dp = *dp;
+    s->st = (cudaStream_t)stream;
+    s->t0 = std::chrono::steady_clock::now();
+    *out = s;
+    return DYG_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -364,20 +701,107 @@ dyg_status dyg_server_create(dyg_graph *G, dyg_graph *H, uint32_t n_graphs,
             return fail(nullptr, DYG_EINVAL, "vertex offsets must ascend");
     if (vertex_offsets[n_graphs] > G->g.n)
         return fail(nullptr, DYG_EINVAL, "vertex offsets exceed the vertex count");
-    DYG_TRY(dyg::check_walk_params(insert_params));
-    DYG_TRY(dyg::check_walk_params(delete_params));
-    dyg_server *s = new dyg_server;
-    s->G = G;
-    s->H = H;
+    dyg_server *s = nullptr;
+    DYG_TRY(server_alloc(G, H, insert_params, delete_params, stream, &s));
     s->off.assign(vertex_offsets, vertex_offsets + n_graphs + 1);
-    s->ip = *insert_params;
-    s->dp = *delete_params;
-    s->st = (cudaStream_t)stream;
-    s->t0 = std::chrono::steady_clock::now();
     s->queues.resize(n_graphs);
     s->uid_next.assign(n_graphs, 0);
-    s->owner.assign(n_graphs, nullptr);
     *out = s;
+    return DYG_OK;
+}
+
+dyg_status dyg_server_create_pool(uint32_t vertex_capacity, uint64_t hbm_budget_bytes,
+                                  const dyg_walk_params *insert_params,
+                                  const dyg_walk_params *delete_params, int device,
+                                  uint32_t keep_initial, dyg_stream_t stream, dyg_server **out) {
+    dyg::set_error("");
+    if (!out) return fail(nullptr, DYG_EINVAL, "NULL out");
+    *out = nullptr;
+    if (vertex_capacity == 0 || hbm_budget_bytes == 0)
+        return fail(nullptr, DYG_EINVAL, "vertex capacity and budget must be positive");
+    DYG_TRY(dyg::check_walk_params(insert_params));
+    DYG_TRY(dyg::check_walk_params(delete_params));
+    int dev = device;
+    if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(nullptr, DYG_ECUDA, "cudaGetDevice failed");
+    }
+    // arenas start small against the budget and grow on demand
+    const uint64_t arena = std::max<uint64_t>(1 << 20, std::min<uint64_t>(hbm_budget_bytes / 12 / 16,
+                                                                         0xF0000000ull));
+    dyg_graph *G = nullptr, *H = nullptr;
+    dyg_status rc = dyg::create_empty_graph(vertex_capacity, arena, dev, 2, 0.5, &G);
+    if (rc == DYG_OK) rc = dyg::create_empty_graph(vertex_capacity, arena / 2, dev, 2, 0.5, &H);
+    dyg_server *s = nullptr;
+    if (rc == DYG_OK) rc = server_alloc(G, H, insert_params, delete_params, stream, &s);
+    if (rc != DYG_OK) {
+        dyg::destroy_graph(G);
+        dyg::destroy_graph(H);
+        return rc;
+    }
+    s->pool = true;
+    s->budget = hbm_budget_bytes;
+    s->vcap = vertex_capacity;
+    s->keep_initial = keep_initial != 0;
+    s->free_ranges.push_back({0u, vertex_capacity});
+    *out = s;
+    return DYG_OK;
+}
+
+dyg_status dyg_server_add_graph(dyg_server *s, uint32_t n_vertices, uint64_t g_edges,
+                                const uint32_t *g_src, const uint32_t *g_dst, const float *g_w,
+                                uint64_t h_edges, const uint32_t *h_src, const uint32_t *h_dst,
+                                const float *h_w, uint32_t *graph) {
+    if (!s) return fail(nullptr, DYG_EINVAL, "NULL server");
+    if (!s->pool) return fail(s, DYG_EINVAL, "graphs are added to pool servers only");
+    if (!graph || n_vertices == 0 || (g_edges && (!g_src || !g_dst || !g_w)) ||
+        (h_edges && (!h_src || !h_dst || !h_w)))
+        return fail(s, DYG_EINVAL, "NULL argument or an empty graph");
+    if (n_vertices > s->vcap) return fail(s, DYG_EINVAL, "graph has more vertices than the pool");
+    for (uint64_t i = 0; i < g_edges; ++i)
+        if (g_src[i] >= n_vertices || g_dst[i] >= n_vertices || !(g_w[i] > 0.0f && isfinite(g_w[i])))
+            return fail(s, DYG_EINVAL, "G edge " + std::to_string(i) + " has a bad vertex or weight");
+    for (uint64_t i = 0; i < h_edges; ++i)
+        if (h_src[i] >= n_vertices || h_dst[i] >= n_vertices || !(h_w[i] > 0.0f && isfinite(h_w[i])))
+            return fail(s, DYG_EINVAL, "H edge " + std::to_string(i) + " has a bad vertex or weight");
+    const uint64_t fp = footprint_of(n_vertices, 2 * g_edges, 2 * h_edges, s->G->slack, s->G->headroom);
+    if (fp > s->budget) return fail(s, DYG_ENOMEM, "the graph's footprint exceeds the HBM budget");
+    PoolGraph p;
+    try {
+        rows_from_edges(n_vertices, g_edges, g_src, g_dst, g_w, &p.g);
+        rows_from_edges(n_vertices, h_edges, h_src, h_dst, h_w, &p.h);
+        if (s->keep_initial) {
+            p.g0 = p.g;
+            p.h0 = p.h;
+        }
+    } catch (const std::bad_alloc &) {
+        return fail(s, DYG_ENOMEM, "host allocation failed while copying a graph");
+    }
+    p.n = n_vertices;
+    p.footprint = fp;
+    std::lock_guard<std::mutex> lk(s->mu);
+    *graph = (uint32_t)s->queues.size();
+    s->pg.push_back(std::move(p));
+    s->queues.emplace_back();
+    s->uid_next.push_back(0);
+    return DYG_OK;
+}
+
+dyg_status dyg_server_prefetch(dyg_server *s, uint32_t graph, uint32_t *resident) {
+    if (resident) *resident = 0;
+    if (!s) return fail(nullptr, DYG_EINVAL, "NULL server");
+    if (!s->pool) return fail(s, DYG_EINVAL, "prefetch is for pool servers");
+    Exclusive ex(s);
+    if (!ex.ok) return fail(s, DYG_ESTATE, "prefetch needs an idle server");
+    if (graph >= graph_count(s)) return fail(s, DYG_EINVAL, "graph index out of range");
+    dyg::DevSet ds(s->H->device);
+    if (!s->pg[graph].resident) {
+        std::vector<char> keep(graph_count(s), 0);
+        bool ok = false;
+        // nothing is pending: only idle graphs are evicted
+        DYG_TRY(make_room_and_admit(s, graph, 0, keep, &ok));
+    }
+    if (resident) *resident = s->pg[graph].resident ? 1u : 0u;
     return DYG_OK;
 }
 
@@ -399,7 +823,7 @@ dyg_status dyg_server_stop(dyg_server *s) {
 dyg_status dyg_server_destroy(dyg_server *s) {
     if (!s) return DYG_OK;
     dyg_server_stop(s);
-    for (auto &kv : s->by_tag) delete kv.second;
+    for (auto &kv : s->by_tag) delete kv.second;   // every request, queued or done
     {
         dyg::DevSet ds(s->H->device);
         for (dyg::Buf *b : {&s->d_src, &s->d_dst, &s->d_w, &s->d_uid, &s->d_out, &s->d_cond, &s->d_acc})
@@ -414,6 +838,10 @@ dyg_status dyg_server_destroy(dyg_server *s) {
         s->h_out.release();
         s->h_acc.release();
         s->h_rk.release();
+    }
+    if (s->pool) {
+        dyg::destroy_graph(s->G);
+        dyg::destroy_graph(s->H);
     }
     delete s;
     return DYG_OK;
@@ -440,7 +868,12 @@ dyg_status dyg_server_submit_many(dyg_server *s, uint32_t n_req, const uint64_t 
             }
             const uint32_t *sj = src ? src + a : nullptr, *dj = dst ? dst + a : nullptr;
             const float *wj = (w && ops[j] == DYG_STREAM_INSERT) ? w + a : nullptr;
-            const std::string e = check_request(s, graphs[j], ops[j], sj, dj, wj, b - a);
+            std::string e;
+            {
+                // graphs only ever get added, and a graph's size never changes
+                std::lock_guard<std::mutex> lk(s->mu);
+                e = check_request(s, graphs[j], ops[j], sj, dj, wj, b - a);
+            }
             if (!e.empty()) {
                 drop();
                 return fail(s, DYG_EINVAL, "request " + std::to_string(j) + ": " + e);
@@ -593,17 +1026,129 @@ dyg_status dyg_server_fetch(dyg_server *s, uint64_t tag, int32_t *found_or_statu
 
 dyg_status dyg_server_reset(dyg_server *s) {
     if (!s) return fail(nullptr, DYG_EINVAL, "NULL server");
-    std::lock_guard<std::mutex> lk(s->mu);
-    if (s->pending || s->stepping) {
-        s->err = "reset needs an idle server";
-        dyg::set_error(s->err);
-        return DYG_ESTATE;
+    Exclusive ex(s);
+    if (!ex.ok) return fail(s, DYG_ESTATE, "reset needs an idle server");
+    if (s->pool) {
+        if (!s->keep_initial)
+            return fail(s, DYG_EINVAL, "a pool server resets only when it keeps the registered graphs");
+        dyg::DevSet ds(s->H->device);
+        for (uint32_t g = 0; g < graph_count(s); ++g) {
+            PoolGraph &p = s->pg[g];
+            if (p.resident) {
+                DYG_TRY(dyg::clear_range(s->G, p.v0, p.n, s->st));
+                DYG_TRY(dyg::clear_range(s->H, p.v0, p.n, s->st));
+            }
+            try {
+                p.g = p.g0;
+                p.h = p.h0;
+            } catch (const std::bad_alloc &) {
+                return fail(s, DYG_ENOMEM, "host allocation failed while restoring graphs");
+            }
+        }
+        DYG_CUDA(cudaStreamSynchronize(s->st));
+        // reclaim every slot: the union graphs are empty again
+        DYG_TRY(dyg::compact_graph(s->G, s->st));
+        DYG_TRY(dyg::compact_graph(s->H, s->st));
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (uint32_t g = 0; g < graph_count(s); ++g) {
+            PoolGraph &p = s->pg[g];
+            p.resident = false;
+            p.footprint = footprint_of(p.n, p.g.col.size(), p.h.col.size(), s->G->slack,
+                                       s->G->headroom);
+            p.last_step = 0;
+        }
+        s->free_ranges.assign(1, {0u, s->vcap});
+        s->resident_bytes = 0;
     }
+    std::lock_guard<std::mutex> lk(s->mu);
     for (auto &kv : s->by_tag) delete kv.second;
     s->by_tag.clear();
     s->done.clear();
     std::fill(s->uid_next.begin(), s->uid_next.end(), 0ull);
     s->steps = 0;
+    return DYG_OK;
+}
+
+dyg_status dyg_server_stats_read(dyg_server *s, dyg_server_stats *out) {
+    if (!s || !out) return fail(s, DYG_EINVAL, "NULL argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    dyg_server_stats r{};
+    r.graphs = graph_count(s);
+    for (uint32_t g = 0; g < r.graphs; ++g) {
+        const bool res = !s->pool || s->pg[g].resident;
+        r.resident += res ? 1u : 0u;
+        r.waiting += (!res && !s->queues[g].empty()) ? 1u : 0u;
+    }
+    r.resident_bytes = s->pool ? s->resident_bytes : 0;
+    r.budget_bytes = s->pool ? s->budget : 0;
+    r.admissions = s->admissions;
+    r.evictions = s->evictions;
+    r.steps = s->steps;
+    r.pending = s->pending;
+    *out = r;
+    return DYG_OK;
+}
+
+dyg_status dyg_server_graph_info_read(dyg_server *s, uint32_t graph, dyg_server_graph_info *out) {
+    if (!s || !out) return fail(s, DYG_EINVAL, "NULL argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (graph >= graph_count(s)) {
+        s->err = "graph index out of range";
+        dyg::set_error(s->err);
+        return DYG_EINVAL;
+    }
+    dyg_server_graph_info r{};
+    r.n_vertices = graph_size(s, graph);
+    r.resident = (!s->pool || s->pg[graph].resident) ? 1u : 0u;
+    r.vertex_offset = r.resident ? graph_base(s, graph) : 0u;
+    r.footprint_bytes = s->pool ? s->pg[graph].footprint : 0;
+    r.updates = s->uid_next[graph];
+    r.admissions = s->pool ? s->pg[graph].admissions : 0;
+    r.evictions = s->pool ? s->pg[graph].evictions : 0;
+    r.pending = s->queues[graph].size();
+    *out = r;
+    return DYG_OK;
+}
+
+dyg_status dyg_server_graph_export(dyg_server *s, uint32_t graph, uint32_t which,
+                                   uint64_t *row_ptr, uint32_t *col, float *w, uint64_t slot_cap) {
+    if (!s || !row_ptr) return fail(s, DYG_EINVAL, "NULL argument");
+    if (which > 1) return fail(s, DYG_EINVAL, "which: 0 = G, 1 = H");
+    Exclusive ex(s);
+    if (!ex.ok) return fail(s, DYG_ESTATE, "export needs an idle server");
+    if (graph >= graph_count(s)) return fail(s, DYG_EINVAL, "graph index out of range");
+    HostRows tmp;
+    const HostRows *rows = &tmp;
+    if (!s->pool || s->pg[graph].resident) {
+        dyg::DevSet ds(s->H->device);
+        try {
+            DYG_TRY(dyg::save_range(which ? s->H : s->G, graph_base(s, graph), graph_size(s, graph),
+                                    tmp.rp, tmp.col, tmp.w, s->st));
+        } catch (const std::bad_alloc &) {
+            return fail(s, DYG_ENOMEM, "host allocation failed while exporting");
+        }
+    } else {
+        rows = which ? &s->pg[graph].h : &s->pg[graph].g;
+    }
+    const uint32_t n = graph_size(s, graph);
+    std::copy(rows->rp.begin(), rows->rp.begin() + n + 1, row_ptr);
+    const uint64_t m = rows->rp[n];
+    const uint64_t k = std::min(m, slot_cap);
+    if (col) std::copy(rows->col.begin(), rows->col.begin() + (long)k, col);
+    if (w) std::copy(rows->w.begin(), rows->w.begin() + (long)k, w);
+    if (m > slot_cap && (col || w)) return fail(s, DYG_ERANGE, "slot_cap smaller than the graph's slots");
+    return DYG_OK;
+}
+
+dyg_status dyg_server_counters(dyg_server *s, uint64_t *incr_moves, uint64_t *decr_moves) {
+    if (!s) return fail(nullptr, DYG_EINVAL, "NULL server");
+    Exclusive ex(s);
+    if (!ex.ok) return fail(s, DYG_ESTATE, "counters need an idle server");
+    dyg::DevSet ds(s->H->device);
+    DYG_TRY(dyg::read_scalars(s->H, s->st));
+    DYG_TRY(dyg::read_scalars(s->G, s->st));
+    if (incr_moves) *incr_moves = s->H->ws.host_scalars[dyg::S_MOVES];
+    if (decr_moves) *decr_moves = s->G->ws.host_scalars[dyg::S_MOVES];
     return DYG_OK;
 }
 

@@ -18,10 +18,11 @@ per request, and this module submits, polls and fetches.  Server(native=False)
 runs the same steps from Python over dyg_incremental_batch_ids /
 dyg_decremental_batch_ids (kept to measure the scheduler against).
 
-Admission: graphs are admitted in the given order while their estimated
-device footprint (dense graph and sparsifier arenas and descriptors, plus
-the per-request workspace) fits the HBM budget; requests for other graphs
-are refused.
+Admission (Server): graphs are admitted in the given order while their
+estimated device footprint (dense graph and sparsifier arenas and
+descriptors) fits the HBM budget; requests for other graphs are refused.
+PoolServer admits graphs as their requests are scheduled and evicts
+resident ones to host memory to make room, within the same budget.
 """
 from __future__ import annotations
 
@@ -32,8 +33,8 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from . import (DygError, Graph, ServerDone, WalkParams, _check, _ptr, decremental_batch_ids,
-               incremental_batch_ids, lib)
+from . import (DygError, Graph, ServerDone, ServerGraphInfo, ServerStats, WalkParams, _check, _ptr,
+               decremental_batch_ids, incremental_batch_ids, lib)
 
 INSERT, DELETE = 0, 1
 
@@ -361,6 +362,95 @@ class Server:
             self._srv = None
         for x in (self.H, self.G) + tuple(getattr(self, "_snap", ())):
             x.close()
+
+
+class PoolServer(Server):
+    """The native server in pool mode (dyg_server_create_pool): it owns its
+    union graphs and admits the registered graphs by footprint within
+    `hbm_budget` bytes as their requests are scheduled, evicting resident
+    graphs to host memory to make room (idle ones least recently used first).
+    Results equal each graph's requests run alone on its own handles."""
+
+    def __init__(self, cases, iparams: WalkParams, dparams: WalkParams, hbm_budget: float,
+                 vertex_capacity: int | None = None, device: int = -1, keep_initial: bool = True):
+        self.iparams, self.dparams = iparams, dparams
+        self.native = True
+        self.admitted = list(range(len(cases)))     # every graph is registered
+        self.slot = {g: g for g in self.admitted}
+        self.H = self.G = None
+        self._srv = None
+        L = lib()
+        vcap = int(vertex_capacity or sum(c.n for c in cases))
+        h = C.c_void_p()
+        _check(L.dyg_server_create_pool(vcap, int(hbm_budget), C.byref(iparams), C.byref(dparams),
+                                        int(device), 1 if keep_initial else 0, None, C.byref(h)),
+               "dyg_server_create_pool")
+        self._srv = h
+        a = lambda x, t: np.ascontiguousarray(x, t)
+        for c in cases:
+            gid = C.c_uint32()
+            gs, gd, gw = a(c.g_src, np.uint32), a(c.g_dst, np.uint32), a(c.g_w, np.float32)
+            hs, hd, hw = a(c.h_src, np.uint32), a(c.h_dst, np.uint32), a(c.h_w, np.float32)
+            _check(L.dyg_server_add_graph(h, int(c.n), len(gs), _ptr(gs), _ptr(gd), _ptr(gw), len(hs),
+                                          _ptr(hs), _ptr(hd), _ptr(hw), C.byref(gid)),
+                   "dyg_server_add_graph")
+        self._tags = {}
+        self._next_tag = 0
+        self._poll = (ServerDone * 1024)()
+        self._t0_ns = 0
+        self.t0 = time.perf_counter()
+
+    @property
+    def footprint(self) -> int:
+        return self.stats()["resident_bytes"]
+
+    def snapshot(self):
+        """The registered graphs are kept by the server (keep_initial)."""
+
+    def restore(self, stream: int | None = None):
+        """Every graph back to its registered rows, none resident."""
+        _check(lib().dyg_server_reset(self._srv), "dyg_server_reset")
+        self._tags.clear()
+
+    def prefetch(self, graph: int) -> bool:
+        r = C.c_uint32()
+        _check(lib().dyg_server_prefetch(self._srv, int(graph), C.byref(r)), "dyg_server_prefetch")
+        return bool(r.value)
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib().dyg_server_stats_read(self._srv, C.byref(st)), "dyg_server_stats_read")
+        return {k: getattr(st, k) for k, _ in st._fields_}
+
+    def counters(self) -> tuple[int, int]:
+        """Walker moves so far: (insertion walks on H, deletion walks on G)."""
+        a, b = C.c_uint64(), C.c_uint64()
+        _check(lib().dyg_server_counters(self._srv, C.byref(a), C.byref(b)), "dyg_server_counters")
+        return a.value, b.value
+
+    def graph_info(self, graph: int) -> dict:
+        gi = ServerGraphInfo()
+        _check(lib().dyg_server_graph_info_read(self._srv, int(graph), C.byref(gi)),
+               "dyg_server_graph_info_read")
+        return {k: getattr(gi, k) for k, _ in gi._fields_ if k != "pad"}
+
+    def export(self, graph: int, which: str):
+        """(row_ptr, col, w) of a graph's G or H, local ids."""
+        n = self.graph_info(graph)["n_vertices"]
+        rp = np.zeros(n + 1, np.uint64)
+        k = 0 if which == "G" else 1
+        _check(lib().dyg_server_graph_export(self._srv, int(graph), k, _ptr(rp), None, None, 0),
+               "dyg_server_graph_export")
+        m = int(rp[n])
+        col, w = np.empty(max(m, 1), np.uint32), np.empty(max(m, 1), np.float32)
+        _check(lib().dyg_server_graph_export(self._srv, int(graph), k, _ptr(rp), _ptr(col), _ptr(w), m),
+               "dyg_server_graph_export")
+        return rp, col[:m], w[:m]
+
+    def close(self):
+        if self._srv is not None:
+            lib().dyg_server_destroy(self._srv)
+            self._srv = None
 
 
 class PlainServer:

@@ -59,8 +59,80 @@ dyg_status dyg_server_create(dyg_graph *G, dyg_graph *H, uint32_t n_graphs,
                              const dyg_walk_params *delete_params, dyg_stream_t stream,
                              dyg_server **out);
 
+/* Pool mode: the server owns its union graphs (vertex_capacity vertices) and
+ * admits registered graphs by footprint.  hbm_budget_bytes bounds the sum of
+ * the resident graphs' estimated footprints (per slot 12 B with the arena's
+ * 50 % headroom and 2 slack slots per row, plus 24 B per vertex, for G and H).
+ * A registered graph stays in host memory until a request for it is
+ * scheduled; at the start of each step, graphs with pending requests that are
+ * not resident are admitted, oldest pending request first, into a free vertex
+ * range while their footprint fits the budget; to make room, resident graphs
+ * are evicted (their rows copied back to host memory, row order kept): idle
+ * ones least recently used first, then busy ones whose oldest pending request
+ * is younger than the waiting graph's.  Every request still gets the result it
+ * gets alone on its graph's own handles.  device < 0: the current device.
+ * keep_initial: keep a host copy of each graph as registered, so that
+ * dyg_server_reset can restore it.  The reference keeps one graph per process
+ * and has no counterpart. */
+dyg_status dyg_server_create_pool(uint32_t vertex_capacity, uint64_t hbm_budget_bytes,
+                                  const dyg_walk_params *insert_params,
+                                  const dyg_walk_params *delete_params, int device,
+                                  uint32_t keep_initial, dyg_stream_t stream, dyg_server **out);
+
+/* Registers a graph with a pool server: its dense graph G and sparsifier H as
+ * edge lists with local ids (rows are built as dyg_graph_create_from_edges
+ * builds them), copied to host memory; *graph gets its index.  Not resident
+ * until a request for it is scheduled (or dyg_server_prefetch).  DYG_ENOMEM
+ * if its footprint alone exceeds the budget; DYG_EINVAL for bad ids or
+ * weights, or more vertices than the pool holds. */
+dyg_status dyg_server_add_graph(dyg_server *s, uint32_t n_vertices, uint64_t g_edges,
+                                const uint32_t *g_src, const uint32_t *g_dst, const float *g_w,
+                                uint64_t h_edges, const uint32_t *h_src, const uint32_t *h_dst,
+                                const float *h_w, uint32_t *graph);
+
+/* Admits a pool graph now if it fits (evicting idle graphs least recently
+ * used first); *resident (may be NULL) tells whether it is resident.  Needs an
+ * idle server (DYG_ESTATE otherwise). */
+dyg_status dyg_server_prefetch(dyg_server *s, uint32_t graph, uint32_t *resident);
+
+typedef struct dyg_server_stats {
+    uint32_t graphs;           /* given (static) or registered (pool)           */
+    uint32_t resident;         /* graphs on the device                          */
+    uint32_t waiting;          /* graphs with pending requests, not resident    */
+    uint32_t pending;          /* requests queued and not yet run               */
+    uint64_t resident_bytes;   /* estimated footprint of the resident graphs    */
+    uint64_t budget_bytes;     /* 0 for a static server                         */
+    uint64_t admissions, evictions;
+    uint64_t steps;
+} dyg_server_stats;
+dyg_status dyg_server_stats_read(dyg_server *s, dyg_server_stats *out);
+
+typedef struct dyg_server_graph_info {
+    uint32_t n_vertices;
+    uint32_t resident;
+    uint32_t vertex_offset;    /* first vertex in the union while resident      */
+    uint32_t pad;
+    uint64_t footprint_bytes;  /* pool: estimate used for admission             */
+    uint64_t updates;          /* updates run so far (its next update id)       */
+    uint64_t admissions, evictions;
+    uint64_t pending;          /* its queued requests                           */
+} dyg_server_graph_info;
+dyg_status dyg_server_graph_info_read(dyg_server *s, uint32_t graph, dyg_server_graph_info *out);
+
+/* The current rows of a graph's G (which = 0) or H (which = 1) with local
+ * ids: row_ptr[n_vertices + 1], col / w up to slot_cap slots (DYG_ERANGE if
+ * there are more; row_ptr is complete then).  From the device while resident,
+ * else from the host copy.  Needs an idle server (DYG_ESTATE otherwise). */
+dyg_status dyg_server_graph_export(dyg_server *s, uint32_t graph, uint32_t which,
+                                   uint64_t *row_ptr, uint32_t *col, float *w, uint64_t slot_cap);
+
+/* Walker moves so far on the sparsifier (insertion walks) and on the dense
+ * graph (deletion walks) of the server's union graphs.  Needs an idle server. */
+dyg_status dyg_server_counters(dyg_server *s, uint64_t *incr_moves, uint64_t *decr_moves);
+
 /* Stops the loop thread (after its current step) and frees the server; the
- * graphs stay the caller's and must outlive the server (destroy it first). */
+ * graphs of a static server stay the caller's and must outlive the server
+ * (destroy it first); a pool server frees its own. */
 dyg_status dyg_server_destroy(dyg_server *s);
 
 /* Queues a request: op DYG_STREAM_INSERT (w required, finite and > 0) or
@@ -81,8 +153,10 @@ dyg_status dyg_server_submit_many(dyg_server *s, uint32_t n_req, const uint64_t 
                                   const uint64_t *offsets, const uint32_t *src,
                                   const uint32_t *dst, const float *w);
 
-/* Runs one scheduler step in the calling thread; *n_done (may be NULL) gets
- * the number of requests it completed (0 when nothing is pending).
+/* Runs one scheduler step in the calling thread (pool: admissions first);
+ * *n_done (may be NULL) gets the number of requests it completed (0 when
+ * nothing is pending; requests of a graph that cannot be admitted, because
+ * it outgrew the budget, complete with DYG_ENOMEM).
  * DYG_EINVAL while the loop thread runs.  A failed step completes its
  * requests with its status and returns it. */
 dyg_status dyg_server_step(dyg_server *s, uint32_t *n_done);
@@ -114,8 +188,9 @@ dyg_status dyg_server_fetch(dyg_server *s, uint64_t tag, int32_t *found_or_statu
                             uint32_t *rec_dst, uint8_t *rec_kind, uint64_t rec_cap);
 
 /* Back to update id 0 for every graph, with no results or completion records
- * kept (for a caller that restores the graphs to an earlier state).
- * DYG_ESTATE unless idle. */
+ * kept (for a caller that restores the graphs to an earlier state; a pool
+ * server created with keep_initial restores every graph to its registered
+ * rows itself, none resident).  DYG_ESTATE unless idle. */
 dyg_status dyg_server_reset(dyg_server *s);
 
 /* Steps run so far (since creation or reset). */

@@ -182,3 +182,121 @@ def test_native_server_errors(dyg):
         assert L.dyg_server_fetch(h, t, None, None, None, None, None, None, 0) == 0
     assert L.dyg_server_reset(h) == 0 and L.dyg_server_steps(h) == 0
     S.close()
+
+
+def check_pool_against_plain(S, P, reqs, alone, n_graphs):
+    for a, b in zip(reqs, alone):
+        same_request(a, b)
+    for k in range(n_graphs):
+        for which, mine in (("H", P.H[k]), ("G", P.G[k])):
+            want = mine.export()
+            got = S.export(k, which)
+            assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+            assert np.array_equal(got[2].view(np.uint32), want[2].view(np.uint32))
+
+
+@pytest.mark.parametrize("frac", [1.0, 0.4])
+def test_pool_admission_matches_alone(dyg, frac):
+    """Pool mode: graphs enter the device as their requests are scheduled.
+    With a budget for all graphs each is admitted once; with 40 % of it
+    graphs are evicted to host memory and admitted again as requests arrive
+    (the loop thread, requests arriving meanwhile).  Every request still gets
+    its result alone, and every graph ends with the rows of its own handles."""
+    from dygrass_b200.serve import PlainServer, PoolServer, footprint_bytes, poisson_requests
+    cases = mixed_cases()
+    fps = [footprint_bytes(c.n, len(c.g_src), len(c.h_src)) for c in cases]
+    budget = int(max(frac * sum(fps), max(fps)) * 1.3)
+    p = dyg.WalkParams.make(threshold=100.0, walkers=64)
+    reqs = poisson_requests(cases, rate=3000.0, count=90, seed=6, size_hi=150)
+    alone = [dataclasses.replace(r) for r in reqs]
+    S = PoolServer(cases, p, p, hbm_budget=budget)
+    st0 = S.stats()
+    assert st0["graphs"] == len(cases) and st0["resident"] == 0
+    done = S.serve(reqs)
+    assert len(done) == len(reqs)
+    st = S.stats()
+    assert st["resident_bytes"] <= budget and st["pending"] == 0
+    if frac < 1.0:
+        assert st["evictions"] > 0 and st["admissions"] > len(cases)
+    else:
+        assert st["evictions"] == 0
+    P = PlainServer(cases, p, p)
+    P.serve(alone)
+    check_pool_against_plain(S, P, reqs, alone, len(cases))
+    infos = [S.graph_info(k) for k in range(len(cases))]
+    assert [i["updates"] for i in infos] == [P.uid_next[k] for k in range(len(cases))]
+    # the same replay after a reset: every graph back to its registered rows
+    again = [dataclasses.replace(r, found_at=None, status=None, rec_src=None) for r in reqs]
+    S.restore()
+    assert S.stats()["resident"] == 0
+    S.serve(again)
+    for a, b in zip(again, alone):
+        same_request(a, b)
+    S.close()
+    P.close()
+
+
+def test_pool_stepwise_eviction_and_prefetch(dyg):
+    """Stepping by hand with room for one graph at a time: each step admits
+    the graph of the oldest pending request after evicting the resident one,
+    a prefetch evicts idle graphs only, and exports read evicted graphs from
+    their host copies."""
+    import ctypes as C
+    from dygrass_b200.serve import PlainServer, PoolServer, Request, footprint_bytes
+    cases = [W.grid_2d(20, 20, inserts=60, seed=s) for s in (31, 32, 33)]
+    fps = [footprint_bytes(c.n, len(c.g_src), len(c.h_src)) for c in cases]
+    budget = int(max(fps) * 1.5)          # never two of these at once
+    assert budget < 2 * min(fps)
+    p = dyg.WalkParams.make(walkers=32)
+    S = PoolServer(cases, p, p, hbm_budget=budget)
+    P = PlainServer(cases, p, p)
+    L, h = dyg.lib(), S._srv
+    assert S.prefetch(0) and S.graph_info(0)["resident"] == 1
+    assert S.prefetch(1) and S.graph_info(0)["resident"] == 0      # idle graph 0 evicted
+    reqs = []
+    for g in (2, 0, 1, 2):
+        c = cases[g]
+        k = len(reqs)
+        reqs.append(Request(g, 0, c.ins_src[k * 5:k * 5 + 5], c.ins_dst[k * 5:k * 5 + 5],
+                            c.ins_w[k * 5:k * 5 + 5]))
+    alone = [dataclasses.replace(r) for r in reqs]
+    S.submit_many(reqs)
+    order = []
+    k = C.c_uint32()
+    while L.dyg_server_pending(h):
+        assert L.dyg_server_step(h, C.byref(k)) == 0 and k.value == 1
+        order.append([i for i in range(3) if S.graph_info(i)["resident"]])
+    assert order == [[2], [0], [1], [2]]   # oldest request first, one graph resident
+    done = S._collect()
+    assert len(done) == 4
+    for r in alone:
+        P.run_one(r)
+    check_pool_against_plain(S, P, reqs, alone, 3)
+    S.close()
+    P.close()
+
+
+def test_pool_errors(dyg):
+    import ctypes as C
+    from dygrass_b200.serve import footprint_bytes
+    c = mixed_cases()[0]
+    p = dyg.WalkParams.make(walkers=32)
+    L = dyg.lib()
+    h = C.c_void_p()
+    fp = footprint_bytes(c.n, len(c.g_src), len(c.h_src))
+    assert L.dyg_server_create_pool(0, 1 << 20, C.byref(p), C.byref(p), -1, 0, None, C.byref(h)) == \
+        dyg.DYG_EINVAL
+    assert L.dyg_server_create_pool(c.n, fp // 2, C.byref(p), C.byref(p), -1, 0, None, C.byref(h)) == 0
+    g = C.c_uint32()
+    a = lambda x, t: np.ascontiguousarray(x, t)
+    gs, gd, gw = a(c.g_src, np.uint32), a(c.g_dst, np.uint32), a(c.g_w, np.float32)
+    hs, hd, hw = a(c.h_src, np.uint32), a(c.h_dst, np.uint32), a(c.h_w, np.float32)
+    args = lambda n: (h, n, len(gs), dyg._ptr(gs), dyg._ptr(gd), dyg._ptr(gw), len(hs), dyg._ptr(hs),
+                      dyg._ptr(hd), dyg._ptr(hw), C.byref(g))
+    assert L.dyg_server_add_graph(*args(c.n)) == dyg.DYG_ENOMEM          # over the budget
+    assert b"budget" in L.dyg_server_last_error(h)
+    assert L.dyg_server_add_graph(*args(c.n - 1)) == dyg.DYG_EINVAL      # an id >= n
+    assert L.dyg_server_reset(h) == dyg.DYG_EINVAL                       # registered rows not kept
+    st = dyg.ServerStats()
+    assert L.dyg_server_stats_read(h, C.byref(st)) == 0 and st.graphs == 0 and st.budget_bytes == fp // 2
+    assert L.dyg_server_destroy(h) == 0
