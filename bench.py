@@ -93,6 +93,8 @@ def parse():
     ap.add_argument("--mesh-k", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--split", choices=["auto", "replicas", "shard", "partition"], default="auto",
+                    help="how N > 1 ranks share the work (see resolve_split)")
     ap.add_argument("--shard", action="store_true",
                     help="mesh: one graph, every batch split over the ranks (keys all-reduced), "
                          "strong scaling; default N > 1 runs independent replicas")
@@ -109,30 +111,70 @@ def parse():
     return ap.parse_args()
 
 
-def make_workload(args, rank):
+def resolve_split(args, world):
+    """How N > 1 ranks share the work: "shard" (one graph, each batch's
+    walks split over the ranks, winner keys all-reduced), "partition"
+    (independent graphs divided by footprint) or "replicas" (each rank its
+    own copy of the workload).  auto: shard for the mesh and grid, partition
+    for the many-graph and serving workloads, replicas for the mixed stream
+    (stream files have no split entry points)."""
+    if world == 1:
+        return "replicas"
+    if args.shard:
+        return "shard"
+    if args.split != "auto":
+        return args.split
+    return {"mesh": "shard", "grid": "shard", "rgg_many": "partition",
+            "serve": "partition"}.get(args.workload, "replicas")
+
+
+def _my_graphs(args, cases, rank, world):
+    """This rank's graphs when the graphs are partitioned, else all."""
+    if args.split_mode != "partition":
+        return list(range(len(cases)))
+    from dygrass_b200.serve import footprint_bytes
+    from dygrass_b200.shard import partition_by_footprint
+    fps = [footprint_bytes(c.n, len(c.g_src), len(c.h_src)) for c in cases]
+    return partition_by_footprint(fps, world)[rank]
+
+
+def make_workload(args, rank, world=1):
     import dygrass_b200.workloads as wl
-    seed = wl.MASTER_SEED + 1000 * rank
+    # replicas draw their own inputs; a sharded or partitioned job is one workload
+    seed = wl.MASTER_SEED + (1000 * rank if args.split_mode == "replicas" else 0)
     if args.workload == "serve":
-        from dygrass_b200.serve import footprint_bytes, poisson_requests
+        from dygrass_b200.serve import Request, footprint_bytes, poisson_requests
         cases, ip, dp = wl.serving_mix(seed=seed, large=args.serve_mix == "large")
+        reqs = poisson_requests(cases, 1.0, args.serve_requests, seed + 5)
+        job = sum(len(r.src) for r in reqs)
+        mine = _my_graphs(args, cases, rank, world)
+        if len(mine) != len(cases):
+            slot = {g: k for k, g in enumerate(mine)}
+            cases = [cases[g] for g in mine]
+            reqs = [Request(slot[r.graph], r.op, r.src, r.dst, r.w, arrival=r.arrival)
+                    for r in reqs if r.graph in slot]
 
         class Serve:
             pass
         W = Serve()
         W.cases, W.params, W.dparams = cases, ip, dp
-        W.requests = poisson_requests(cases, 1.0, args.serve_requests, seed + 5)
+        W.requests = reqs
         W.n_updates = sum(len(r.src) for r in W.requests)
+        W.job_updates = job
         W.n = sum(c.n for c in cases)
         W.footprint = sum(footprint_bytes(c.n, len(c.g_src), len(c.h_src)) for c in cases)
         return W
     if args.workload == "rgg_many":
         cases, p = wl.rgg_many(k=args.rgg_graphs, n_hi=args.rgg_n_hi, seed=seed)
+        job = sum(len(c.ins_src) for c in cases)
+        cases = [cases[g] for g in _my_graphs(args, cases, rank, world)]
 
         class Many:
             pass
         W = Many()
         W.cases, W.params, W.dparams = cases, p, p
         W.n_updates = sum(len(c.ins_src) for c in cases)
+        W.job_updates = job
         W.n = sum(c.n for c in cases)
         return W
     if args.workload == "rmat":
@@ -302,7 +344,7 @@ def run_ours(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    W = make_workload(args, rank)
+    W = make_workload(args, rank, world)
     nin, ndel = len(W.ins_src), len(W.del_src)
 
     H0 = dyg.Graph.from_edges(W.n, W.h_src, W.h_dst, W.h_w, device=local_rank)
@@ -526,7 +568,7 @@ def run_mixed(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    W = make_workload(args, rank)
+    W = make_workload(args, rank, world)
     H0 = dyg.Graph.from_edges(W.n, W.h_src, W.h_dst, W.h_w, device=local_rank)
     G0 = dyg.Graph.from_edges(W.n, W.g_src, W.g_dst, W.g_w, device=local_rank)
     H, G = H0.clone(), G0.clone()
@@ -668,7 +710,7 @@ def run_many(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    W = make_workload(args, rank)
+    W = make_workload(args, rank, world)
     p = W.params
     best, trials = autotune(W.cases, params=p, chunks=(32, 64), blocks=(0, 4),
                             walkers=(128, 256) if args.tune_walkers else (), repeats=2,
@@ -798,7 +840,13 @@ def run_many(args, rank, world, local_rank):
             e1.synchronize()
             et.append(e0.elapsed_time(e1))
         ems = float(np.mean(et))
-        e2e = {"value": world * plan.n_edges / (ems / 1e3), "unit": "edge_updates/s",
+        if world > 1:
+            import torch.distributed as dist
+            tt = torch.tensor([ems], dtype=torch.float64, device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ems = float(tt.item())
+        units_e2e = W.job_updates if args.split_mode == "partition" else world * plan.n_edges
+        e2e = {"value": units_e2e / (ems / 1e3), "unit": "edge_updates/s",
                "ms_per_step": ems, "h2d_bytes_per_step": int(plan.n_edges * 20),
                "d2h_bytes_per_step": int(plan.n_edges * 9)}
 
@@ -845,7 +893,7 @@ def run_serve(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    W = make_workload(args, rank)
+    W = make_workload(args, rank, world)
     fp_total = sum(footprint_bytes(c.n, len(c.g_src), len(c.h_src)) for c in W.cases)
     S = PoolServer(W.cases, W.params, W.dparams, hbm_budget=int(fp_total * 1.5), device=local_rank)
     stream = torch.cuda.current_stream(dev)
@@ -902,6 +950,11 @@ def run_serve(args, rank, world, local_rank):
     launches = dyg.kernel_launches() - launches0
     clk = clocks.stop()
     ms = float(np.mean(times))
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
     incr_moves, decr_moves = moves[0] / args.steps, moves[1] / args.steps
     capacity = len(W.requests) / (ms / 1e3)      # requests per second at saturation
 
@@ -947,7 +1000,8 @@ def run_serve(args, rank, world, local_rank):
         "walk_ms_per_step": (prof["incr_walk_ms"] + prof["decr_walk_ms"]) / args.steps,
         "walk_launches": prof["incr_walk_launches"] + prof["decr_walk_launches"], "prof": prof,
         "launches_per_step": launches / args.steps, "clocks": clk,
-        "e2e": {"value": n_upd / (ms / 1e3), "unit": "edge_updates/s", "ms_per_step": ms,
+        "e2e": {"value": (W.job_updates if args.split_mode == "partition" else world * n_upd)
+                         / (ms / 1e3), "unit": "edge_updates/s", "ms_per_step": ms,
                 "h2d_bytes_per_step": int(sum(len(r.src) * (20 if r.op == 0 else 16)
                                               for r in W.requests)),
                 "d2h_bytes_per_step": int(sum(len(r.src) * (9 if r.op == 0 else 8)
@@ -1318,6 +1372,9 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    args.split_mode = resolve_split(args, world) if args.impl != "reference" else "replicas"
+    if args.split_mode == "shard":
+        args.shard = True
 
     if args.workload == "refgpu":   # one line holding both updaters' times
         return run_refgpu(args) if rank == 0 else 0
@@ -1392,7 +1449,13 @@ def main():
                               "(profiles/roofline_traffic.json)"
     nin, ndel = res["nin"], res["ndel"]
     ms = res["ms_per_step"]
-    value = (1 if args.shard else world) * (nin + ndel) / (ms / 1e3)
+    if args.split_mode == "shard":
+        units = nin + ndel                  # one workload, split over the ranks
+    elif args.split_mode == "partition":
+        units = W.job_updates               # the graphs divided over the ranks
+    else:
+        units = world * (nin + ndel)        # one replica per rank
+    value = units / (ms / 1e3)
     moves = res["incr_moves"] + res["decr_moves"]
     cpu = None
     if not args.no_cpu_baseline and world == 1:
@@ -1403,10 +1466,12 @@ def main():
         "value": value, "unit": "edge_updates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators, dygrass_b200/workloads.py)",
-        **({"scaling": "strong"} if args.shard else {}),
+        **({"scaling": "strong"} if args.split_mode in ("shard", "partition") else {}),
         "config": dict(workload_config(W, args), l2="flushed between steps (256 MB write)",
-                       parallelism=(f"one graph, batches sharded x{world} (winner keys all-reduced)"
-                                    if args.shard else f"replicas x{world}")),
+                       parallelism={"shard": f"one graph, batches sharded x{world} (winner keys "
+                                                      f"all-reduced)",
+                                    "partition": f"graphs partitioned by footprint x{world}",
+                                    "replicas": f"replicas x{world}"}[args.split_mode]),
         "walker_steps_per_s": world * moves / (ms / 1e3),
         "breakdown": {"insertions_added": res["accepted"], "edges_recovered": res["recovered"],
                       "incr_walker_moves": res["incr_moves"], "decr_walker_moves": res["decr_moves"],

@@ -27,6 +27,19 @@ def split(n: int, rank: int, world: int):
     return n * rank // world, n * (rank + 1) // world
 
 
+def partition_by_footprint(sizes, world: int) -> list:
+    """Independent graphs over `world` ranks by device footprint: largest
+    first, each to the rank holding the least so far (ties to the lower
+    rank).  Returns one ascending index list per rank."""
+    parts = [[] for _ in range(world)]
+    load = [0] * world
+    for i in sorted(range(len(sizes)), key=lambda i: (-sizes[i], i)):
+        r = min(range(world), key=lambda k: (load[k], k))
+        parts[r].append(i)
+        load[r] += sizes[i]
+    return [sorted(p) for p in parts]
+
+
 class GpuBackend:
     """Replicas on one GPU per process; keys and outputs are torch tensors."""
 

@@ -153,3 +153,37 @@ def test_server_needs_an_admitted_graph():
     cases = fake_cases(k=2)
     with pytest.raises(ValueError, match="HBM budget"):
         Server(cases, None, None, hbm_budget=10.0)
+
+
+def test_partition_by_footprint():
+    """Graphs over ranks by footprint: every graph once, largest first onto
+    the least loaded rank, loads within the largest graph of each other."""
+    from dygrass_b200.shard import partition_by_footprint
+    rng = np.random.default_rng(3)
+    sizes = [int(x) for x in np.exp(rng.uniform(np.log(1e3), np.log(2e5), 256))]
+    for world in (1, 2, 3, 8):
+        parts = partition_by_footprint(sizes, world)
+        assert len(parts) == world
+        assert sorted(i for p in parts for i in p) == list(range(len(sizes)))
+        loads = [sum(sizes[i] for i in p) for p in parts]
+        assert max(loads) - min(loads) <= max(sizes)
+    assert partition_by_footprint([5, 1, 4, 2], 2) == [[0, 1], [2, 3]]
+
+
+def test_bench_split_modes():
+    """bench.py's N > 1 defaults: the mesh shards one graph's batches, the
+    many-graph and serving workloads partition their graphs, the mixed
+    stream runs replicas; N = 1 is a single replica."""
+    import argparse
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    ns = lambda **kw: argparse.Namespace(**{"shard": False, "split": "auto", **kw})
+    assert bench.resolve_split(ns(workload="mesh"), 1) == "replicas"
+    assert bench.resolve_split(ns(workload="mesh"), 4) == "shard"
+    assert bench.resolve_split(ns(workload="rgg_many"), 4) == "partition"
+    assert bench.resolve_split(ns(workload="serve"), 2) == "partition"
+    assert bench.resolve_split(ns(workload="rmat"), 8) == "replicas"
+    assert bench.resolve_split(ns(workload="mesh", split="replicas"), 8) == "replicas"
+    assert bench.resolve_split(ns(workload="rmat", shard=True), 2) == "shard"
