@@ -211,6 +211,7 @@ enum Count : int {
     C_RANGE = 6,      // walk-list entries of the current range
     C_WALKLIST = 7,   // stream file: new insertions to walk
     C_GHALF = 8,      // stream file: half-edges of the new insertions (G append)
+    C_CANDS_ALL = 9,  // recovery candidates: path, then fallback
     C_NCOUNTS = 12
 };
 
@@ -302,12 +303,13 @@ dyg_status launch_walk_scalars(const DevGraph &g, const WalkJob &job, const dyg_
 dyg_status launch_winner_paths(dyg_graph *G, const WalkJob &job, const dyg_walk_params &p,
                                const unsigned long long *keys, uint32_t n_max, uint32_t path_stride,
                                uint32_t *path_v, float *path_w, int32_t *path_len, cudaStream_t st);
+// Writes its candidates at cx/cy/cw + *base_dev.
 dyg_status launch_fallback_walks(dyg_graph *G, const unsigned long long *halt,
                                  const uint32_t *f_src, const uint32_t *f_dst,
                                  const unsigned long long *f_uid, const uint32_t *nop,
                                  const uint32_t *n_nop_dev, uint32_t n_nop_max,
-                                 const dyg_walk_params &p, uint32_t *cx, uint32_t *cy, float *cw,
-                                 cudaStream_t st);
+                                 const dyg_walk_params &p, const uint32_t *base_dev, uint32_t *cx,
+                                 uint32_t *cy, float *cw, cudaStream_t st);
 
 // --- capi.cu
 // After a run: DYG_OK, or the error the kernels flagged in G's scalars (last

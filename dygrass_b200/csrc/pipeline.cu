@@ -14,9 +14,10 @@
 //   together.  Resumes at the batch start (nothing of the batch changed).
 // Decremental batch (random_walk_decremental/main.cu:413-444), phases:
 //   0: delete from G and H in input order, compact the edges found in both,
-//      walk G, replay winners, path candidates in (edge, step) order;
-//   1: dedup the path edges, drop those in H, append the rest in order;
-//   2: 2-step fallback walks for the edges without a path, same dedup/append.
+//      walk G, replay winners, path candidates in (edge, step) order, then
+//      the 2-step fallback walks' candidates for the edges without a path;
+//   1: dedup all candidates (first occurrence), drop those in H, append the
+//      rest in order (path edges, then fallback edges).
 #include "dyg_internal.cuh"
 
 namespace dyg {
@@ -196,6 +197,7 @@ __global__ void k_path_cands(const unsigned long long *halt, const uint32_t *pv,
         counts[C_CANDS] = coff[f] + clen[f];
         counts[C_NOPATH] = nopos[f] + noflag[f];
         counts[C_CANDS2] = (nopos[f] + noflag[f]) * 4u * hw;
+        counts[C_CANDS_ALL] = counts[C_CANDS] + counts[C_CANDS2];
     }
     if (noflag[f]) nop[nopos[f]] = f;
     const uint32_t L = clen[f];
@@ -343,10 +345,12 @@ __global__ void k_rec_check(unsigned long long *halt, const uint32_t *keep, cons
 __global__ void k_emit_kept(const unsigned long long *halt, const uint32_t *cx, const uint32_t *cy,
                             const float *cw, const uint32_t *M_dev, uint32_t M_host,
                             const uint32_t *keep, const uint32_t *kpos, uint8_t kind,
+                            const uint32_t *split, uint8_t kind_after,
                             const unsigned long long *sc, uint32_t *hx, uint32_t *hy, float *hw,
                             uint32_t *rx, uint32_t *ry, uint8_t *rk, uint32_t *counts) {
     if (HALTED(halt)) return;
     const uint32_t M = dcount(M_dev, M_host);
+    const uint32_t sp = split ? *split : M;   // candidates from sp on get kind_after
     const unsigned long long base = sc[S_RECCNT];
     GSTRIDE(i, M) {
         if (i == M - 1) counts[C_KEPT] = 2u * (kpos[i] + keep[i]);
@@ -362,7 +366,7 @@ __global__ void k_emit_kept(const unsigned long long *halt, const uint32_t *cx, 
         hw[2 * q + 1] = w;
         rx[base + q] = x;
         ry[base + q] = y;
-        rk[base + q] = kind;
+        rk[base + q] = i < sp ? kind : kind_after;
     }
 }
 
@@ -372,9 +376,12 @@ __global__ void k_rec_advance(const unsigned long long *halt, const uint32_t *co
     sc[S_RECCNT] += counts[C_KEPT] / 2u;
 }
 
-// Dedup + membership + ordered append of one candidate list (phase 1 or 2).
+// Dedup + membership + ordered append of one candidate list; candidates
+// before *split (device, may be null) are recorded with `kind`, the rest with
+// `kind_after`.
 dyg_status recover_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *cx, const uint32_t *cy,
                            const float *cw, const uint32_t *M_dev, uint32_t M_host, uint8_t kind,
+                           const uint32_t *split, uint8_t kind_after,
                            unsigned long long *halt, uint32_t batch, uint32_t phase,
                            cudaStream_t st) {
     if (M_host == 0) return DYG_OK;
@@ -418,7 +425,8 @@ dyg_status recover_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *cx, const
     k_rec_check<<<1, 1, 0, st>>>(halt, keep, kpos, M_dev, M_host, sc,
                                  halt_code(batch, (uint32_t)kHaltRecords, phase));
     count_launch();
-    k_emit_kept<<<gr, 256, 0, st>>>(halt, cx, cy, cw, M_dev, M_host, keep, kpos, kind, sc,
+    k_emit_kept<<<gr, 256, 0, st>>>(halt, cx, cy, cw, M_dev, M_host, keep, kpos, kind, split,
+                                    kind_after, sc,
                                     ptr<uint32_t>(ws.hx), ptr<uint32_t>(ws.hy), ptr<float>(ws.hw),
                                     ptr<uint32_t>(ws.rx2), ptr<uint32_t>(ws.ry2),
                                     ptr<uint8_t>(ws.rk2), counts);
@@ -601,9 +609,11 @@ dyg_status decr_walk_enqueue(dyg_graph *G, dyg_graph *H, uint32_t f0, uint32_t n
     DYG_TRY(ensure(ws.path_len, sizeof(int32_t) * n));
     DYG_TRY(ensure(ws.nop, sizeof(uint32_t) * (size_t)n * 4));
     DYG_TRY(ensure(ws.nopos, sizeof(uint32_t) * (size_t)n));
-    DYG_TRY(ensure(ws.cand_x, sizeof(uint32_t) * (size_t)n * stride));
-    DYG_TRY(ensure(ws.cand_y, sizeof(uint32_t) * (size_t)n * stride));
-    DYG_TRY(ensure(ws.cand_w, sizeof(float) * (size_t)n * stride));
+    // path candidates at [0, C_CANDS), then the fallback candidates
+    const size_t n_path = (size_t)n * (stride - 1u), n_fb = (size_t)n * 4u * hwk;
+    DYG_TRY(ensure(ws.cand_x, sizeof(uint32_t) * (n_path + n_fb)));
+    DYG_TRY(ensure(ws.cand_y, sizeof(uint32_t) * (n_path + n_fb)));
+    DYG_TRY(ensure(ws.cand_w, sizeof(float) * (n_path + n_fb)));
     uint32_t *counts = ptr<uint32_t>(ws.counts);
     uint32_t *clen = ptr<uint32_t>(ws.nop) + n, *coff = clen + n, *noflag = coff + n;
     uint32_t *nopos = ptr<uint32_t>(ws.nopos);
@@ -643,25 +653,28 @@ dyg_status decr_walk_enqueue(dyg_graph *G, dyg_graph *H, uint32_t f0, uint32_t n
                                                       ptr<uint32_t>(ws.nop), counts, hwk);
         count_launch();
         DYG_CUDA(cudaGetLastError());
+        if (hwk > 0) {
+            // 2-step fallback walks for the edges without a path
+            // (main.cu:400-408, 428-436); their candidates follow the path
+            // candidates.  They read G only, which recovery does not change.
+            DYG_TRY(launch_fallback_walks(G, halt, fsrc, fdst, fuid, ptr<uint32_t>(ws.nop),
+                                          counts + C_NOPATH, n, p, counts + C_CANDS,
+                                          ptr<uint32_t>(ws.cand_x), ptr<uint32_t>(ws.cand_y),
+                                          ptr<float>(ws.cand_w), st));
+        }
     }
     if (phase0 <= 1) {
-        // path recovery (gpu_graph.cuh:514-552)
+        // Path recovery (gpu_graph.cuh:514-552) and the fallback edges
+        // (gpu_graph.cuh:577-615) in one pass over [path candidates, fallback
+        // candidates].  It keeps what the two passes in turn keep: a fallback
+        // edge equal to an earlier candidate is a repeat (dropped, as the
+        // second pass drops it for being in H once the first appended it or
+        // found it there), every other one is tested against H as before, and
+        // appends and records follow candidate order.
         DYG_TRY(recover_enqueue(G, H, ptr<uint32_t>(ws.cand_x), ptr<uint32_t>(ws.cand_y),
-                                ptr<float>(ws.cand_w), counts + C_CANDS, n * (stride - 1u),
-                                DYG_REC_PATH, halt, batch, 1, st));
-    }
-    if (hwk > 0) {
-        // fallback walks for the edges without a path (main.cu:400-408, 428-436)
-        const uint32_t hm = n * 4u * hwk;
-        DYG_TRY(ensure(ws.cand_x, sizeof(uint32_t) * (size_t)hm));
-        DYG_TRY(ensure(ws.cand_y, sizeof(uint32_t) * (size_t)hm));
-        DYG_TRY(ensure(ws.cand_w, sizeof(float) * (size_t)hm));
-        DYG_TRY(launch_fallback_walks(G, halt, fsrc, fdst, fuid, ptr<uint32_t>(ws.nop),
-                                      counts + C_NOPATH, n, p, ptr<uint32_t>(ws.cand_x),
-                                      ptr<uint32_t>(ws.cand_y), ptr<float>(ws.cand_w), st));
-        DYG_TRY(recover_enqueue(G, H, ptr<uint32_t>(ws.cand_x), ptr<uint32_t>(ws.cand_y),
-                                ptr<float>(ws.cand_w), counts + C_CANDS2, hm, DYG_REC_FALLBACK,
-                                halt, batch, 2, st));
+                                ptr<float>(ws.cand_w), counts + C_CANDS_ALL,
+                                (uint32_t)(n_path + n_fb), DYG_REC_PATH, counts + C_CANDS,
+                                DYG_REC_FALLBACK, halt, batch, 1, st));
     }
     return DYG_OK;
 }

@@ -28,8 +28,9 @@
 //     of a step, waiting graphs (oldest pending request first) are admitted
 //     into a free vertex range while their footprint fits the budget, and to
 //     make room the server evicts resident graphs -- idle ones least recently
-//     used first, then busy ones whose oldest pending request is younger than
-//     the waiting graph's -- by copying their rows back to host memory.  A
+//     used first; busy ones, whose oldest pending request is younger than the
+//     waiting graph's, only once the waiting graph has waited kPatienceSteps
+//     steps -- by copying their rows back to host memory.  A
 //     graph's rows keep their order through eviction and admission, so its
 //     results do not depend on where or how often it was resident.
 #include <math.h>
@@ -56,6 +57,7 @@ namespace {
 struct Request {
     std::vector<uint32_t> src, dst;   // local ids
     std::vector<float> w;
+    uint64_t submit_step = 0;         // the server's step count when it was queued
     bool finished = false;
     dyg_server_done rec{};
     std::vector<int32_t> out_i;       // found_at (insertion) or status (deletion)
@@ -282,11 +284,18 @@ dyg_status admit(dyg_server *s, uint32_t g, uint32_t v0) {
     return DYG_OK;
 }
 
+// Steps a graph's oldest request waits before busy graphs (ones with requests
+// pending) may be evicted for it.  Until then only idle graphs make room, so an
+// oversubscribed server rotates graphs as their queues drain instead of
+// trading them in and out on every step.
+constexpr uint64_t kPatienceSteps = 32;
+
 // Makes room for graph g (evicting in the victim order) and admits it; *ok
 // is false when it does not fit yet.  `t_wait` is the arrival of its oldest
-// pending request (busy graphs with an older one are not evicted for it);
-// `keep` marks graphs that must stay (admitted in this step).
-dyg_status make_room_and_admit(dyg_server *s, uint32_t g, uint64_t t_wait,
+// pending request (busy graphs with an older one are never evicted for it,
+// busy graphs at all only when allow_busy); `keep` marks graphs that must stay
+// (admitted in this step).
+dyg_status make_room_and_admit(dyg_server *s, uint32_t g, uint64_t t_wait, bool allow_busy,
                                const std::vector<char> &keep, bool *ok) {
     *ok = false;
     PoolGraph &p = s->pg[g];
@@ -302,7 +311,7 @@ dyg_status make_room_and_admit(dyg_server *s, uint32_t g, uint64_t t_wait,
             if (!s->pg[k].resident || keep[k]) continue;
             const bool busy = !s->queues[k].empty();
             const uint64_t ht = busy ? s->queues[k].front()->rec.t_submit_ns : ~0ull;
-            if (busy && ht <= t_wait) continue;
+            if (busy && (!allow_busy || ht <= t_wait)) continue;
             vs.push_back(Victim{k, busy, ht, s->pg[k].last_step});
         }
     }
@@ -335,6 +344,7 @@ dyg_status admit_waiting(dyg_server *s, std::vector<std::pair<uint32_t, dyg_stat
     struct Wait {
         uint64_t t;
         uint32_t g;
+        bool patient;   // waited long enough to evict busy graphs
     };
     std::vector<Wait> waiting;
     std::vector<char> keep;
@@ -342,8 +352,11 @@ dyg_status admit_waiting(dyg_server *s, std::vector<std::pair<uint32_t, dyg_stat
         std::lock_guard<std::mutex> lk(s->mu);
         keep.assign(graph_count(s), 0);
         for (uint32_t g = 0; g < graph_count(s); ++g)
-            if (!s->pg[g].resident && !s->queues[g].empty())
-                waiting.push_back(Wait{s->queues[g].front()->rec.t_submit_ns, g});
+            if (!s->pg[g].resident && !s->queues[g].empty()) {
+                const Request *h = s->queues[g].front();
+                waiting.push_back(Wait{h->rec.t_submit_ns, g,
+                                       s->steps >= h->submit_step + kPatienceSteps});
+            }
     }
     std::sort(waiting.begin(), waiting.end(), [](const Wait &a, const Wait &b) {
         return a.t != b.t ? a.t < b.t : a.g < b.g;
@@ -355,7 +368,7 @@ dyg_status admit_waiting(dyg_server *s, std::vector<std::pair<uint32_t, dyg_stat
             continue;
         }
         bool ok = false;
-        const dyg_status rc = make_room_and_admit(s, w.g, w.t, keep, &ok);
+        const dyg_status rc = make_room_and_admit(s, w.g, w.t, w.patient, keep, &ok);
         if (rc == DYG_ENOMEM) {
             failed->push_back({w.g, rc});
             continue;
@@ -799,7 +812,7 @@ dyg_status dyg_server_prefetch(dyg_server *s, uint32_t graph, uint32_t *resident
         std::vector<char> keep(graph_count(s), 0);
         bool ok = false;
         // nothing is pending: only idle graphs are evicted
-        DYG_TRY(make_room_and_admit(s, graph, 0, keep, &ok));
+        DYG_TRY(make_room_and_admit(s, graph, 0, false, keep, &ok));
     }
     if (resident) *resident = s->pg[graph].resident ? 1u : 0u;
     return DYG_OK;
@@ -913,6 +926,7 @@ dyg_status dyg_server_submit_many(dyg_server *s, uint32_t n_req, const uint64_t 
             return DYG_ENOMEM;
         }
         for (uint32_t j = 0; j < n_req; ++j) {
+            made[j]->submit_step = s->steps;
             s->by_tag[tags[j]] = made[j];
             s->queues[graphs[j]].push_back(made[j]);
         }

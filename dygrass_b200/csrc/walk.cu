@@ -394,8 +394,8 @@ __device__ __forceinline__ bool below_best(float R, float c) {
     return __frcp_rn(R) < c;
 }
 
-template <bool INCR, bool WEIGHTED>
-__global__ void __launch_bounds__(kWalkThreads) k_walk(WalkArgs a) {
+template <bool INCR, bool WEIGHTED, int MOVES>
+__global__ void __launch_bounds__(kWalkThreads, WEIGHTED ? 3 : 6) k_walk(WalkArgs a) {
     // per-warp segment sums of the cooperative weighted search
     __shared__ unsigned long long s_seg[WEIGHTED ? (kWalkThreads / 32) * kSegs : 1];
     if (a.job.halt && *a.job.halt) return;
@@ -436,7 +436,11 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(WalkArgs a) {
     while (true) {
         uint32_t free_mask = __ballot_sync(kFull, !active);
         if (free_mask == kFull) T = 0u;
-        const bool refill = (T & 3u) == 0u;
+        // walkers start when their steps stay aligned to the 4-draw Philox
+        // blocks: every fourth iteration with one move per iteration, every
+        // second with two, every iteration with four
+        constexpr uint32_t kAlign = MOVES >= 4 ? 0u : (MOVES == 2 ? 1u : 3u);
+        const bool refill = (T & kAlign) == 0u;
         while (free_mask != 0u && !exhausted && refill) {
             if (c_next >= c_end) {
                 unsigned long long c = 0ull;
@@ -485,30 +489,33 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(WalkArgs a) {
         }
         if (!__any_sync(kFull, active)) break;
         uint32_t fc = 0u;  // conductance bits of a walker that found its target now
-        int r = kContinue;
-        bool moved = false;
-        uint2 taken;
-        uint32_t taken_at;
-        if constexpr (WEIGHTED) {
-            r = step_weighted_warp<INCR>(s, active, a.g, a.max_steps, a.threshold, a.key,
-                                         s_seg + (threadIdx.x >> 5) * kSegs, lane, &moved, &taken,
-                                         &taken_at);
-        } else if (active) {
-            r = step_once<INCR, false>(s, a.g.desc, a.g.slots, a.g.wts, a.max_steps, a.threshold,
-                                       a.key, &moved, &taken, &taken_at);
-        }
-        if (active) {
-            moves += moved ? 1u : 0u;
-            if (r != kContinue) {
-                if (r == kFound) {
-                    const float cond = __frcp_rn(s.R);
-                    fc = __float_as_uint(cond);
-                    // published at once, so walkers of this edge in other warps
-                    // can stop early
-                    atomicMax(a.keys + my_e, pack_key(cond, s.walker, s.step));
+#pragma unroll
+        for (int mv = 0; mv < (WEIGHTED ? 1 : MOVES); ++mv) {
+            int r = kContinue;
+            bool moved = false;
+            uint2 taken;
+            uint32_t taken_at;
+            if constexpr (WEIGHTED) {
+                r = step_weighted_warp<INCR>(s, active, a.g, a.max_steps, a.threshold, a.key,
+                                             s_seg + (threadIdx.x >> 5) * kSegs, lane, &moved,
+                                             &taken, &taken_at);
+            } else if (active) {
+                r = step_once<INCR, false>(s, a.g.desc, a.g.slots, a.g.wts, a.max_steps,
+                                           a.threshold, a.key, &moved, &taken, &taken_at);
+            }
+            if (active) {
+                moves += moved ? 1u : 0u;
+                if (r != kContinue) {
+                    if (r == kFound) {
+                        const float cond = __frcp_rn(s.R);
+                        fc = __float_as_uint(cond);
+                        // published at once, so walkers of this edge in other
+                        // warps can stop early
+                        atomicMax(a.keys + my_e, pack_key(cond, s.walker, s.step));
+                    }
+                    active = false;
+                    ++walks;
                 }
-                active = false;
-                ++walks;
             }
         }
         if (a.prune) {
@@ -520,7 +527,9 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk(WalkArgs a) {
                 pe_best = max(pe_best, __reduce_max_sync(kFull, (fc && my_e == pe) ? fc : 0u));
             }
             if (active) {
-                if ((s.step & 3u) == 0u)
+                // the edge's best is read again every fourth move
+                constexpr uint32_t kEvery = MOVES >= 4 ? 1u : (MOVES == 2 ? 2u : 4u);
+                if (T % kEvery == kEvery - 1u)
                     gbest = max(gbest, (uint32_t)(*(volatile unsigned long long *)(a.keys + my_e) >> 32));
                 const uint32_t known = max(gbest, (my_e == ce) ? ce_best
                                                   : (my_e == pe ? pe_best : 0u));
@@ -591,6 +600,67 @@ __global__ void k_winner_paths(DevGraph g, WalkJob job, uint32_t max_steps, uint
     if (found != key_found(k)) atomicOr(scalars + S_ERR, (unsigned long long)kErrPath);
 }
 
+// Weighted winner replays, one warp per path: the walker lives in lane 0 and
+// rows longer than kCoopRow are searched by the whole warp, as in the walk
+// kernel (a replay through a hub row would otherwise scan it one slot at a
+// time).
+constexpr int kReplayThreads = 128;
+__global__ void __launch_bounds__(kReplayThreads)
+k_winner_paths_weighted(DevGraph g, WalkJob job, uint32_t max_steps, uint2 key,
+                        const unsigned long long *keys, uint32_t stride, uint32_t *pv, float *pw,
+                        int32_t *plen, unsigned long long *scalars) {
+    __shared__ unsigned long long s_seg[(kReplayThreads / 32) * kSegs];
+    if (job.halt && *job.halt) return;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t f = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t n = job.n_dev ? *job.n_dev : job.n_host;
+    if (f >= n) return;   // whole warps leave together
+    const unsigned long long k = keys[f];
+    if (!k) {
+        if (lane == 0u) plen[f] = -1;
+        return;
+    }
+    Walker s;
+    s.walker = key_walker(k);
+    s.cur = job.src[f];
+    s.tgt = job.dst[f];
+    s.we = 0.f;
+    const unsigned long long uid = job.uid ? job.uid[f] : job.uid0 + f;
+    s.c2 = (uint32_t)uid;
+    s.c3 = ctr3_of(uid, job.domain);
+    s.rblk = 0xFFFFFFFFu;
+    s.rbuf = make_uint4(0u, 0u, 0u, 0u);
+    s.step = 1u;
+    s.R = 0.f;
+    s.prev = 0u;
+    uint32_t *row_v = pv + (size_t)f * stride;
+    float *row_w = pw + (size_t)f * stride;
+    if (lane == 0u) {
+        row_v[0] = s.cur;
+        row_w[0] = 0.f;
+    }
+    unsigned long long *seg = s_seg + (threadIdx.x >> 5) * kSegs;
+    int r;
+    do {
+        const uint32_t at = s.step;
+        bool moved;
+        uint2 taken;
+        uint32_t taken_at;
+        r = step_weighted_warp<false>(s, lane == 0u, g, max_steps, 0.f, key, seg, lane, &moved,
+                                      &taken, &taken_at);
+        r = __shfl_sync(kFull, r, 0);
+        if (lane == 0u && moved && at < stride) {
+            row_v[at] = taken.x;
+            row_w[at] = g.wts[taken_at];
+        }
+    } while (r == kContinue);
+    if (lane == 0u) {
+        const int32_t found = (r == kFound) ? (int32_t)s.step : -1;
+        plen[f] = found;
+        if (found != key_found(k)) atomicOr(scalars + S_ERR, (unsigned long long)kErrPath);
+    }
+}
+
 // 2-step fallback walks from both endpoints of each edge that found no path
 // (random_walk_decremental/main.cu:243-290, with the second step reading the
 // row of the vertex the walker stands on).  Candidate pair 2i, 2i+1 of item
@@ -598,11 +668,15 @@ __global__ void k_winner_paths(DevGraph g, WalkJob job, uint32_t max_steps, uint
 __global__ void k_fallback(DevGraph g, const unsigned long long *halt, const uint32_t *f_src,
                            const uint32_t *f_dst, const unsigned long long *f_uid,
                            const uint32_t *nop, const uint32_t *n_nop_dev, uint32_t hw, uint2 key,
-                           uint32_t *cx, uint32_t *cy, float *cw) {
+                           const uint32_t *base_dev, uint32_t *cx, uint32_t *cy, float *cw) {
     if (halt && *halt) return;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t per = 2u * hw;
     if (i >= *n_nop_dev * per) return;
+    const uint32_t b = *base_dev;
+    cx += b;
+    cy += b;
+    cw += b;
     const uint32_t q = i / per, rem = i - q * per, side = rem / hw, j = rem - side * hw;
     const uint32_t f = nop[q];
     const uint32_t s0 = side ? f_dst[f] : f_src[f];
@@ -664,6 +738,48 @@ static int persistent_blocks(K kernel) {
     return b * num_sms();
 }
 
+// Moves per warp iteration of the uniform walk: 2 by default (the warp's
+// refill, prune and loop bookkeeping then runs once per two moves: walk
+// 11.08 -> 9.98 ms per step on the 100^3 mesh); DYG_WALK_MOVES = 1, 2 or 4
+// overrides it for tuning runs.  Results do not depend on it.
+static int walk_moves() {
+    static int m = 0;
+    if (!m) {
+        const char *v = getenv("DYG_WALK_MOVES");
+        const int x = v ? atoi(v) : 2;
+        m = (x == 1 || x == 4) ? x : 2;
+    }
+    return m;
+}
+
+template <bool INCR, bool WTD>
+static void launch_walk_kernel(const WalkArgs &a, cudaStream_t st) {
+    if constexpr (!WTD) {
+        if (walk_moves() == 2) {
+            const int grid = persistent_blocks(k_walk<INCR, WTD, 2>);
+            k_walk<INCR, WTD, 2><<<grid, kWalkThreads, 0, st>>>(a);
+            return;
+        }
+        if (walk_moves() == 4) {
+            const int grid = persistent_blocks(k_walk<INCR, WTD, 4>);
+            k_walk<INCR, WTD, 4><<<grid, kWalkThreads, 0, st>>>(a);
+            return;
+        }
+    }
+    const int grid = persistent_blocks(k_walk<INCR, WTD, 1>);
+    k_walk<INCR, WTD, 1><<<grid, kWalkThreads, 0, st>>>(a);
+}
+
+static void launch_walk_any(const WalkArgs &a, bool incremental, bool wtd, cudaStream_t st) {
+    if (incremental) {
+        if (wtd) launch_walk_kernel<true, true>(a, st);
+        else launch_walk_kernel<true, false>(a, st);
+    } else {
+        if (wtd) launch_walk_kernel<false, true>(a, st);
+        else launch_walk_kernel<false, false>(a, st);
+    }
+}
+
 dyg_status launch_walk(dyg_graph *G, const WalkJob &job, const dyg_walk_params &p, bool incremental,
                        unsigned long long *keys, cudaStream_t st) {
     WalkArgs a;
@@ -678,30 +794,9 @@ dyg_status launch_walk(dyg_graph *G, const WalkJob &job, const dyg_walk_params &
     a.keys = keys;
     a.scalars = ptr<unsigned long long>(G->ws.scalars);
     DYG_CUDA(cudaMemsetAsync(a.scalars + S_WORK, 0, sizeof(unsigned long long), st));
-    const bool wtd = p.transition == DYG_TRANSITION_WEIGHTED;
-    int grid;
     ProfScope prof(incremental ? 0 : 1, st);
-    if (incremental) {
-        if (wtd) {
-            grid = persistent_blocks(k_walk<true, true>);
-            k_walk<true, true><<<grid, kWalkThreads, 0, st>>>(a);
-            count_launch();
-        } else {
-            grid = persistent_blocks(k_walk<true, false>);
-            k_walk<true, false><<<grid, kWalkThreads, 0, st>>>(a);
-            count_launch();
-        }
-    } else {
-        if (wtd) {
-            grid = persistent_blocks(k_walk<false, true>);
-            k_walk<false, true><<<grid, kWalkThreads, 0, st>>>(a);
-            count_launch();
-        } else {
-            grid = persistent_blocks(k_walk<false, false>);
-            k_walk<false, false><<<grid, kWalkThreads, 0, st>>>(a);
-            count_launch();
-        }
-    }
+    launch_walk_any(a, incremental, p.transition == DYG_TRANSITION_WEIGHTED, st);
+    count_launch();
     DYG_CUDA(cudaGetLastError());
     return DYG_OK;
 }
@@ -723,25 +818,7 @@ dyg_status launch_walk_scalars(const DevGraph &g, const WalkJob &job, const dyg_
     a.key = make_uint2((uint32_t)p.seed, (uint32_t)(p.seed >> 32));
     a.keys = keys;
     a.scalars = scalars;
-    const bool wtd = p.transition == DYG_TRANSITION_WEIGHTED;
-    int grid;
-    if (incremental) {
-        if (wtd) {
-            grid = persistent_blocks(k_walk<true, true>);
-            k_walk<true, true><<<grid, kWalkThreads, 0, st>>>(a);
-        } else {
-            grid = persistent_blocks(k_walk<true, false>);
-            k_walk<true, false><<<grid, kWalkThreads, 0, st>>>(a);
-        }
-    } else {
-        if (wtd) {
-            grid = persistent_blocks(k_walk<false, true>);
-            k_walk<false, true><<<grid, kWalkThreads, 0, st>>>(a);
-        } else {
-            grid = persistent_blocks(k_walk<false, false>);
-            k_walk<false, false><<<grid, kWalkThreads, 0, st>>>(a);
-        }
-    }
+    launch_walk_any(a, incremental, p.transition == DYG_TRANSITION_WEIGHTED, st);
     count_launch();
     DYG_CUDA(cudaGetLastError());
     return DYG_OK;
@@ -757,8 +834,9 @@ dyg_status launch_winner_paths(dyg_graph *G, const WalkJob &job, const dyg_walk_
     unsigned long long *sc = ptr<unsigned long long>(G->ws.scalars);
     ProfScope prof(2, st);
     if (p.transition == DYG_TRANSITION_WEIGHTED)
-        k_winner_paths<true><<<grid, threads, 0, st>>>(G->g, job, p.max_steps, key, keys, stride,
-                                                       path_v, path_w, path_len, sc);
+        k_winner_paths_weighted<<<(unsigned)(((uint64_t)n_max * 32 + kReplayThreads - 1) / kReplayThreads),
+                                  kReplayThreads, 0, st>>>(G->g, job, p.max_steps, key, keys, stride,
+                                                           path_v, path_w, path_len, sc);
     else
         k_winner_paths<false><<<grid, threads, 0, st>>>(G->g, job, p.max_steps, key, keys, stride,
                                                         path_v, path_w, path_len, sc);
@@ -771,15 +849,16 @@ dyg_status launch_fallback_walks(dyg_graph *G, const unsigned long long *halt,
                                  const uint32_t *f_src, const uint32_t *f_dst,
                                  const unsigned long long *f_uid, const uint32_t *nop,
                                  const uint32_t *n_nop_dev, uint32_t n_nop_max,
-                                 const dyg_walk_params &p, uint32_t *cx, uint32_t *cy, float *cw,
-                                 cudaStream_t st) {
+                                 const dyg_walk_params &p, const uint32_t *base_dev, uint32_t *cx,
+                                 uint32_t *cy, float *cw, cudaStream_t st) {
     const uint64_t items = (uint64_t)n_nop_max * 2u * p.heuristic_walkers;
     if (items == 0) return DYG_OK;
     const uint2 key = make_uint2((uint32_t)p.seed, (uint32_t)(p.seed >> 32));
     const int threads = 128;
     ProfScope prof(2, st);
     k_fallback<<<(unsigned)((items + threads - 1) / threads), threads, 0, st>>>(
-        G->g, halt, f_src, f_dst, f_uid, nop, n_nop_dev, p.heuristic_walkers, key, cx, cy, cw);
+        G->g, halt, f_src, f_dst, f_uid, nop, n_nop_dev, p.heuristic_walkers, key, base_dev, cx, cy,
+        cw);
     count_launch();
     DYG_CUDA(cudaGetLastError());
     return DYG_OK;

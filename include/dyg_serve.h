@@ -68,8 +68,10 @@ dyg_status dyg_server_create(dyg_graph *G, dyg_graph *H, uint32_t n_graphs,
  * not resident are admitted, oldest pending request first, into a free vertex
  * range while their footprint fits the budget; to make room, resident graphs
  * are evicted (their rows copied back to host memory, row order kept): idle
- * ones least recently used first, then busy ones whose oldest pending request
- * is younger than the waiting graph's.  Every request still gets the result it
+ * ones least recently used first; busy ones (requests pending), whose oldest
+ * pending request is younger than the waiting graph's, only after the waiting
+ * graph's oldest request has waited 32 steps, so that an oversubscribed
+ * server rotates graphs as their queues drain.  Every request still gets the result it
  * gets alone on its graph's own handles.  device < 0: the current device.
  * keep_initial: keep a host copy of each graph as registered, so that
  * dyg_server_reset can restore it.  The reference keeps one graph per process

@@ -237,10 +237,11 @@ def test_pool_admission_matches_alone(dyg, frac):
 
 
 def test_pool_stepwise_eviction_and_prefetch(dyg):
-    """Stepping by hand with room for one graph at a time: each step admits
-    the graph of the oldest pending request after evicting the resident one,
-    a prefetch evicts idle graphs only, and exports read evicted graphs from
-    their host copies."""
+    """Stepping by hand with room for one graph at a time: a waiting graph
+    evicts idle graphs only (a busy one only after it has waited 32 steps), so
+    the resident graph runs its queue dry before the oldest waiting graph
+    comes in; a prefetch evicts idle graphs only, and exports read evicted
+    graphs from their host copies."""
     import ctypes as C
     from dygrass_b200.serve import PlainServer, PoolServer, Request, footprint_bytes
     cases = [W.grid_2d(20, 20, inserts=60, seed=s) for s in (31, 32, 33)]
@@ -266,7 +267,9 @@ def test_pool_stepwise_eviction_and_prefetch(dyg):
     while L.dyg_server_pending(h):
         assert L.dyg_server_step(h, C.byref(k)) == 0 and k.value == 1
         order.append([i for i in range(3) if S.graph_info(i)["resident"]])
-    assert order == [[2], [0], [1], [2]]   # oldest request first, one graph resident
+    # graph 1 (resident, busy) first; then the oldest waiting graph (2) twice,
+    # since it stays while its queue lasts; then graph 0
+    assert order == [[1], [2], [2], [0]]
     done = S._collect()
     assert len(done) == 4
     for r in alone:
