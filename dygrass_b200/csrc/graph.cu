@@ -283,6 +283,31 @@ __global__ void k_gather_rows(DevGraph g, uint32_t v0, uint32_t n, const unsigne
     }
 }
 
+// One warp per vertex: row i of the staged CSR goes to the arena at
+// top + rp[i] + slack * i, columns shifted by v0, with the correctly rounded
+// 1/w beside each column.
+__global__ void k_place_rows(DevGraph g, uint32_t v0, uint32_t n, unsigned long long top,
+                             uint32_t slack, const unsigned long long *rp, const uint32_t *col,
+                             const float *w, unsigned long long *long_flag) {
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n;
+         i += (gridDim.x * blockDim.x) >> 5) {
+        const unsigned long long a = rp[i];
+        const uint32_t deg = (uint32_t)(rp[i + 1] - a);
+        const unsigned long long off = top + a + (unsigned long long)slack * i;
+        for (uint32_t j = lane; j < deg; j += 32u) {
+            const float x = w[a + j];
+            g.slots[off + j] = make_uint2(col[a + j] + v0, __float_as_uint(__frcp_rn(x)));
+            g.wts[off + j] = x;
+        }
+        if (lane == 0u) {
+            g.desc[v0 + i] = make_uint2((uint32_t)off, deg);
+            g.cap[v0 + i] = deg + slack;
+            if (deg > kBigRow) *long_flag = 1ull;
+        }
+    }
+}
+
 dyg_status load_range(dyg_graph *G, uint32_t v0, uint32_t n, const uint64_t *row_ptr,
                       const uint32_t *col, const float *w, cudaStream_t st) {
     if (n == 0) return DYG_OK;
@@ -290,8 +315,8 @@ dyg_status load_range(dyg_graph *G, uint32_t v0, uint32_t n, const uint64_t *row
         set_error("vertex range outside the graph");
         return DYG_EINVAL;
     }
-    uint64_t need = 0;
-    for (uint32_t v = 0; v < n; ++v) need += row_ptr[v + 1] - row_ptr[v] + G->slack;
+    const uint64_t m = row_ptr[n];
+    const uint64_t need = m + (uint64_t)G->slack * n;
     DYG_TRY(read_scalars(G, st));
     uint64_t top = G->ws.host_scalars[S_TOP];
     if (top + need > G->g.arena_cap) {
@@ -305,34 +330,25 @@ dyg_status load_range(dyg_graph *G, uint32_t v0, uint32_t n, const uint64_t *row
         set_error("arena would exceed 32-bit slot offsets");
         return DYG_ENOMEM;
     }
-    std::vector<uint2> h_desc(n), h_slots(need ? need : 1);
-    std::vector<uint32_t> h_cap(n);
-    std::vector<float> h_w(need ? need : 1, 0.0f);
-    uint64_t o = top;
-    for (uint32_t v = 0; v < n; ++v) {
-        const uint64_t deg = row_ptr[v + 1] - row_ptr[v];
-        if (deg > kBigRow) G->long_rows = true;
-        h_desc[v] = make_uint2((uint32_t)o, (uint32_t)deg);
-        h_cap[v] = (uint32_t)(deg + G->slack);
-        for (uint64_t j = 0; j < deg; ++j) {
-            const float x = w[row_ptr[v] + j];
-            const float rw = 1.0f / x;   // IEEE division: equals __frcp_rn(x)
-            uint32_t rb;
-            memcpy(&rb, &rw, 4);
-            h_slots[o - top + j] = make_uint2(col[row_ptr[v] + j] + v0, rb);
-            h_w[o - top + j] = x;
-        }
-        o += deg + G->slack;
-    }
-    DYG_CUDA(cudaMemcpyAsync(G->g.slots + top, h_slots.data(), sizeof(uint2) * need,
+    Workspace &ws = G->ws;
+    DYG_TRY(ensure(ws.f_uid, sizeof(unsigned long long) * ((size_t)n + 1)));
+    DYG_TRY(ensure(ws.cand_x, sizeof(uint32_t) * (m ? m : 1)));
+    DYG_TRY(ensure(ws.cand_w, sizeof(float) * (m ? m : 1)));
+    DYG_CUDA(cudaMemcpyAsync(ws.f_uid.p, row_ptr, sizeof(uint64_t) * ((size_t)n + 1),
                              cudaMemcpyHostToDevice, st));
-    DYG_CUDA(cudaMemcpyAsync(G->g.wts + top, h_w.data(), sizeof(float) * need, cudaMemcpyHostToDevice, st));
-    DYG_CUDA(cudaMemcpyAsync(G->g.desc + v0, h_desc.data(), sizeof(uint2) * n, cudaMemcpyHostToDevice, st));
-    DYG_CUDA(cudaMemcpyAsync(G->g.cap + v0, h_cap.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, st));
+    if (m) {
+        DYG_CUDA(cudaMemcpyAsync(ws.cand_x.p, col, sizeof(uint32_t) * m, cudaMemcpyHostToDevice, st));
+        DYG_CUDA(cudaMemcpyAsync(ws.cand_w.p, w, sizeof(float) * m, cudaMemcpyHostToDevice, st));
+    }
+    unsigned long long *sc = ptr<unsigned long long>(ws.scalars);
+    const int gr = (int)std::min<uint64_t>(((uint64_t)n * 32 + 255) / 256, (uint64_t)num_sms() * 16);
+    k_place_rows<<<gr, 256, 0, st>>>(G->g, v0, n, top, G->slack, ptr<unsigned long long>(ws.f_uid),
+                                     ptr<uint32_t>(ws.cand_x), ptr<float>(ws.cand_w), sc + S_LONG);
+    count_launch();
+    DYG_CUDA(cudaGetLastError());
     const unsigned long long ntop = top + need;
     DYG_CUDA(cudaMemcpyAsync(G->g.top, &ntop, sizeof(ntop), cudaMemcpyHostToDevice, st));
-    DYG_CUDA(cudaStreamSynchronize(st));
-    G->ws.host_scalars[S_TOP] = ntop;
+    DYG_TRY(read_scalars(G, st));   // synchronizes; picks up a long row
     return DYG_OK;
 }
 

@@ -29,9 +29,9 @@ __device__ __forceinline__ uint32_t dcount(const uint32_t *dev, uint32_t host) {
     return dev ? min(*dev, host) : host;
 }
 
-__global__ void k_rank(DevGraph g, const uint32_t *hx, const uint32_t *m_dev, uint32_t m_host,
-                       uint32_t *rank, uint32_t *rowcnt, const unsigned long long *halt,
-                       unsigned long long *ran) {
+__device__ __forceinline__ void dev_rank(DevGraph g, const uint32_t *hx, const uint32_t *m_dev,
+                                         uint32_t m_host, uint32_t *rank, uint32_t *rowcnt,
+                                         const unsigned long long *halt, unsigned long long *ran) {
     if (*halt) return;
     if (blockIdx.x == 0 && threadIdx.x == 0 && ran) *ran = 1ull;
     const uint32_t m = dcount(m_dev, m_host);
@@ -43,10 +43,11 @@ __global__ void k_rank(DevGraph g, const uint32_t *hx, const uint32_t *m_dev, ui
 
 // ------------------------------------------------------------------ append
 
-__global__ void k_app_need(DevGraph g, const uint32_t *hx, const uint32_t *m_dev, uint32_t m_host,
-                           const uint32_t *rank, const uint32_t *rowcnt, uint32_t slack,
-                           uint32_t *lneed, unsigned long long *need_total,
-                           const unsigned long long *halt) {
+__device__ __forceinline__ void dev_app_need(DevGraph g, const uint32_t *hx, const uint32_t *m_dev,
+                                             uint32_t m_host, const uint32_t *rank,
+                                             const uint32_t *rowcnt, uint32_t slack, uint32_t *lneed,
+                                             unsigned long long *need_total,
+                                             const unsigned long long *halt) {
     if (*halt) return;
     const uint32_t m = dcount(m_dev, m_host);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
@@ -88,10 +89,11 @@ __global__ void k_reserve(unsigned long long *top1, uint64_t cap1, const unsigne
 // slots is copied by its leader's lane, a longer one by the whole warp (rows
 // longer than kBigRow, with big_ok, by k_app_move_big instead).  Every lane of a warp runs the same
 // iterations.
-__global__ void k_app_move(DevGraph g, const uint32_t *hx, const uint32_t *m_dev, uint32_t m_host,
-                           const uint32_t *rank, const uint32_t *lneed, unsigned long long *cursor,
-                           uint4 *big, unsigned long long *nbig, bool big_ok,
-                           const unsigned long long *halt) {
+__device__ __forceinline__ void dev_app_move(DevGraph g, const uint32_t *hx, const uint32_t *m_dev,
+                                             uint32_t m_host, const uint32_t *rank,
+                                             const uint32_t *lneed, unsigned long long *cursor,
+                                             uint4 *big, unsigned long long *nbig, bool big_ok,
+                                             const unsigned long long *halt) {
     if (*halt) return;
     const uint32_t m = dcount(m_dev, m_host);
     const uint32_t lane = threadIdx.x & 31u;
@@ -205,9 +207,10 @@ __global__ void k_app_move_big(DevGraph g, const uint32_t *hx, const uint32_t *l
     }
 }
 
-__global__ void k_app_write(DevGraph g, const uint32_t *hx, const uint32_t *hy, const float *hw,
-                            const uint32_t *m_dev, uint32_t m_host, const uint32_t *rank,
-                            const unsigned long long *halt) {
+__device__ __forceinline__ void dev_app_write(DevGraph g, const uint32_t *hx, const uint32_t *hy,
+                                              const float *hw, const uint32_t *m_dev,
+                                              uint32_t m_host, const uint32_t *rank,
+                                              const unsigned long long *halt) {
     if (*halt) return;
     const uint32_t m = dcount(m_dev, m_host);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
@@ -228,10 +231,11 @@ constexpr uint32_t kTailLane = 8;     // ... and from this length on (shorter: b
 // this operation's ranks were taken).  A tail of kTailLane+1..kTailWarp
 // entries is ordered by the whole warp (each entry placed at its rank among
 // the tail's list indices, which are distinct); other tails by the leader.
-__global__ void k_app_finish(DevGraph g, const uint32_t *hx, const uint32_t *m_dev,
-                             uint32_t m_host, const uint32_t *rank, uint32_t *rowcnt,
-                             const unsigned long long *halt, const unsigned long long *ran,
-                             unsigned long long *long_flag) {
+__device__ __forceinline__ void dev_app_finish(DevGraph g, const uint32_t *hx, const uint32_t *m_dev,
+                                               uint32_t m_host, const uint32_t *rank,
+                                               uint32_t *rowcnt, const unsigned long long *halt,
+                                               const unsigned long long *ran,
+                                               unsigned long long *long_flag) {
     const bool halted = *halt != 0ull;
     if (halted && !*ran) return;
     const uint32_t m = dcount(m_dev, m_host);
@@ -332,6 +336,58 @@ __global__ void k_app_finish(DevGraph g, const uint32_t *hx, const uint32_t *m_d
             if (d.y + cnt > kBigRow && d.y <= kBigRow) *long_flag = 1ull;
         }
     }
+}
+
+__global__ void k_rank(DevGraph g, const uint32_t *hx, const uint32_t *m_dev, uint32_t m_host,
+                       uint32_t *rank, uint32_t *rowcnt, const unsigned long long *halt,
+                       unsigned long long *ran) {
+    dev_rank(g, hx, m_dev, m_host, rank, rowcnt, halt, ran);
+}
+
+// One append list and its graph.  The append kernels take two and pick one
+// by blockIdx.y, so the appends to H and to G of one batch share each launch.
+struct AppSide {
+    DevGraph g;
+    const uint32_t *hx, *hy;
+    const float *hw;
+    const uint32_t *m_dev;
+    uint32_t m_host;
+    uint32_t slack;
+    uint32_t *rank, *rowcnt, *lneed;
+    unsigned long long *sc;   // the graph's scalars
+    uint4 *big;
+    bool big_ok;
+};
+struct AppSides {
+    AppSide s[2];
+};
+
+__global__ void k_app_rank(AppSides A, const unsigned long long *halt) {
+    const AppSide &a = A.s[blockIdx.y];
+    dev_rank(a.g, a.hx, a.m_dev, a.m_host, a.rank, a.rowcnt, halt, a.sc + S_OPRAN);
+}
+
+__global__ void k_app_need(AppSides A, const unsigned long long *halt) {
+    const AppSide &a = A.s[blockIdx.y];
+    dev_app_need(a.g, a.hx, a.m_dev, a.m_host, a.rank, a.rowcnt, a.slack, a.lneed, a.sc + S_NEED,
+                 halt);
+}
+
+__global__ void k_app_move(AppSides A, const unsigned long long *halt) {
+    const AppSide &a = A.s[blockIdx.y];
+    dev_app_move(a.g, a.hx, a.m_dev, a.m_host, a.rank, a.lneed, a.sc + S_CURSOR, a.big,
+                 a.sc + S_NBIG, a.big_ok, halt);
+}
+
+__global__ void k_app_write(AppSides A, const unsigned long long *halt) {
+    const AppSide &a = A.s[blockIdx.y];
+    dev_app_write(a.g, a.hx, a.hy, a.hw, a.m_dev, a.m_host, a.rank, halt);
+}
+
+__global__ void k_app_finish(AppSides A, const unsigned long long *halt) {
+    const AppSide &a = A.s[blockIdx.y];
+    dev_app_finish(a.g, a.hx, a.m_dev, a.m_host, a.rank, a.rowcnt, halt, a.sc + S_OPRAN,
+                   a.sc + S_LONG);
 }
 
 // ------------------------------------------------------------------ delete
@@ -651,55 +707,47 @@ dyg_status append_enqueue(dyg_graph *GA, const AppendList &A, dyg_graph *GB, con
                           unsigned long long *halt, unsigned long long code, cudaStream_t st) {
     dyg_graph *gs[2] = {GA, B ? GB : nullptr};
     const AppendList *ls[2] = {&A, B};
-    for (int k = 0; k < 2; ++k) {
+    const int ns = gs[1] ? 2 : 1;
+    AppSides S{};
+    uint32_t m_max = 0;
+    for (int k = 0; k < ns; ++k) {
         dyg_graph *G = gs[k];
-        if (!G) continue;
         DYG_TRY(rowops_ensure(G, ls[k]->m_host));
         unsigned long long *sc = ptr<unsigned long long>(G->ws.scalars);
         // need, cursor, ran [, long-row count]
         DYG_CUDA(cudaMemsetAsync(sc + S_NEED, 0, sizeof(unsigned long long) * (G->long_rows ? 4 : 3),
                                  st));
-        if (ls[k]->m_host == 0) continue;
-        const int gr = grid_for(ls[k]->m_host);
-        k_rank<<<gr, 256, 0, st>>>(G->g, ls[k]->hx, ls[k]->m_dev, ls[k]->m_host,
-                                   ptr<uint32_t>(G->ws.rank), ptr<uint32_t>(G->ws.rowcnt), halt,
-                                   sc + S_OPRAN);
-        count_launch();
-        k_app_need<<<gr, 256, 0, st>>>(G->g, ls[k]->hx, ls[k]->m_dev, ls[k]->m_host,
-                                       ptr<uint32_t>(G->ws.rank), ptr<uint32_t>(G->ws.rowcnt),
-                                       G->slack, ptr<uint32_t>(G->ws.lneed), sc + S_NEED, halt);
-        count_launch();
+        S.s[k] = AppSide{G->g, ls[k]->hx, ls[k]->hy, ls[k]->hw, ls[k]->m_dev, ls[k]->m_host,
+                         G->slack, ptr<uint32_t>(G->ws.rank), ptr<uint32_t>(G->ws.rowcnt),
+                         ptr<uint32_t>(G->ws.lneed), sc, ptr<uint4>(G->ws.big), G->long_rows};
+        if (ls[k]->m_host > m_max) m_max = ls[k]->m_host;
     }
+    if (m_max == 0) return DYG_OK;
+    const dim3 grid(grid_for(m_max), ns);
+    k_app_rank<<<grid, 256, 0, st>>>(S, halt);
+    count_launch();
+    k_app_need<<<grid, 256, 0, st>>>(S, halt);
+    count_launch();
     unsigned long long *s1 = ptr<unsigned long long>(GA->ws.scalars);
     unsigned long long *s2 = gs[1] ? ptr<unsigned long long>(gs[1]->ws.scalars) : nullptr;
     k_reserve<<<1, 1, 0, st>>>(GA->g.top, GA->g.arena_cap, s1 + S_NEED, s1 + S_CURSOR,
                                s2 ? gs[1]->g.top : nullptr, s2 ? gs[1]->g.arena_cap : 0,
                                s2 ? s2 + S_NEED : nullptr, s2 ? s2 + S_CURSOR : nullptr, halt, code);
     count_launch();
-    for (int k = 0; k < 2; ++k) {
+    k_app_move<<<grid, 256, 0, st>>>(S, halt);
+    count_launch();
+    for (int k = 0; k < ns; ++k) {
         dyg_graph *G = gs[k];
-        if (!G || ls[k]->m_host == 0) continue;
+        if (!G->long_rows || ls[k]->m_host == 0) continue;
         unsigned long long *sc = ptr<unsigned long long>(G->ws.scalars);
-        const int gr = grid_for(ls[k]->m_host);
-        k_app_move<<<gr, 256, 0, st>>>(G->g, ls[k]->hx, ls[k]->m_dev, ls[k]->m_host,
-                                       ptr<uint32_t>(G->ws.rank), ptr<uint32_t>(G->ws.lneed),
-                                       sc + S_CURSOR, ptr<uint4>(G->ws.big), sc + S_NBIG,
-                                       G->long_rows, halt);
-        count_launch();
-        if (G->long_rows) {
-            k_app_move_big<<<num_sms() * 2, kBigThreads, 0, st>>>(
-                G->g, ls[k]->hx, ptr<uint32_t>(G->ws.lneed), ptr<uint4>(G->ws.big), sc + S_NBIG,
-                halt);
-            count_launch();
-        }
-        k_app_write<<<gr, 256, 0, st>>>(G->g, ls[k]->hx, ls[k]->hy, ls[k]->hw, ls[k]->m_dev,
-                                        ls[k]->m_host, ptr<uint32_t>(G->ws.rank), halt);
-        count_launch();
-        k_app_finish<<<gr, 256, 0, st>>>(G->g, ls[k]->hx, ls[k]->m_dev, ls[k]->m_host,
-                                         ptr<uint32_t>(G->ws.rank), ptr<uint32_t>(G->ws.rowcnt),
-                                         halt, sc + S_OPRAN, sc + S_LONG);
+        k_app_move_big<<<num_sms() * 2, kBigThreads, 0, st>>>(
+            G->g, ls[k]->hx, ptr<uint32_t>(G->ws.lneed), ptr<uint4>(G->ws.big), sc + S_NBIG, halt);
         count_launch();
     }
+    k_app_write<<<grid, 256, 0, st>>>(S, halt);
+    count_launch();
+    k_app_finish<<<grid, 256, 0, st>>>(S, halt);
+    count_launch();
     DYG_CUDA(cudaGetLastError());
     return DYG_OK;
 }

@@ -1059,10 +1059,13 @@ dyg_status dyg_server_reset(dyg_server *s) {
                 return fail(s, DYG_ENOMEM, "host allocation failed while restoring graphs");
             }
         }
+        // no graph holds a row any more: the arenas start over at 0, keeping
+        // the capacity they grew to (a replay after a reset then needs no
+        // growth that the one before it did not need)
+        const unsigned long long zero = 0ull;
+        DYG_CUDA(cudaMemcpyAsync(s->G->g.top, &zero, sizeof(zero), cudaMemcpyHostToDevice, s->st));
+        DYG_CUDA(cudaMemcpyAsync(s->H->g.top, &zero, sizeof(zero), cudaMemcpyHostToDevice, s->st));
         DYG_CUDA(cudaStreamSynchronize(s->st));
-        // reclaim every slot: the union graphs are empty again
-        DYG_TRY(dyg::compact_graph(s->G, s->st));
-        DYG_TRY(dyg::compact_graph(s->H, s->st));
         std::lock_guard<std::mutex> lk(s->mu);
         for (uint32_t g = 0; g < graph_count(s); ++g) {
             PoolGraph &p = s->pg[g];

@@ -738,16 +738,17 @@ static int persistent_blocks(K kernel) {
     return b * num_sms();
 }
 
-// Moves per warp iteration of the uniform walk: 2 by default (the warp's
-// refill, prune and loop bookkeeping then runs once per two moves: walk
-// 11.08 -> 9.98 ms per step on the 100^3 mesh); DYG_WALK_MOVES = 1, 2 or 4
-// overrides it for tuning runs.  Results do not depend on it.
+// Moves per warp iteration of the uniform walk: 4 by default (the warp's
+// refill, prune and loop bookkeeping then runs once per four moves; walk time
+// per step on the 100^3 mesh: 11.08 ms with one move, 9.99 with two, 9.64 with
+// four); DYG_WALK_MOVES = 1, 2 or 4 overrides it for tuning runs.  Results do
+// not depend on it.
 static int walk_moves() {
     static int m = 0;
     if (!m) {
         const char *v = getenv("DYG_WALK_MOVES");
-        const int x = v ? atoi(v) : 2;
-        m = (x == 1 || x == 4) ? x : 2;
+        const int x = v ? atoi(v) : 4;
+        m = (x == 1 || x == 2) ? x : 4;
     }
     return m;
 }
