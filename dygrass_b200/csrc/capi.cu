@@ -149,6 +149,11 @@ dyg_status check_host_weights(const float *w, size_t n) {
     return DYG_OK;
 }
 
+// Host batches up to this size are checked on the host (the message names
+// the entry); larger ones are staged first and checked by k_validate on the
+// device, like device batches, instead of by a serial host loop.
+constexpr uint32_t kHostCheckMax = 65536;
+
 dyg_status check_device_errors(dyg_graph *G, cudaStream_t st) {
     DYG_TRY(read_scalars(G, st));
     const unsigned long long err = G->ws.host_scalars[S_ERR];
@@ -163,6 +168,10 @@ dyg_status check_device_errors(dyg_graph *G, cudaStream_t st) {
         if (err & kErrWeight) {
             set_error("a batch weight is not finite and > 0");
             return DYG_EINVAL;
+        }
+        if (err & kErrScan) {
+            set_error("a prefix scan tile timed out waiting for its predecessor");
+            return DYG_ESTATE;
         }
         set_error("internal consistency check failed (device error bits " + std::to_string(err) + ")");
         return DYG_ESTATE;
@@ -194,7 +203,7 @@ void free_graph(dyg_graph *G) {
     Buf *bufs[] = {&ws.keys, &ws.flags, &ws.pos, &ws.f_src, &ws.f_dst, &ws.f_idx, &ws.f_uid,
                    &ws.f_w, &ws.found, &ws.hx, &ws.hy, &ws.hw, &ws.path_v, &ws.path_w,
                    &ws.path_len, &ws.cand_x, &ws.cand_y, &ws.cand_w, &ws.keep, &ws.htab_k,
-                   &ws.htab_v, &ws.nop, &ws.cub_tmp, &ws.s_src, &ws.s_dst, &ws.s_w, &ws.s_o1,
+                   &ws.htab_v, &ws.nop, &ws.cub_tmp, &ws.scan_status, &ws.s_src, &ws.s_dst, &ws.s_w, &ws.s_o1,
                    &ws.s_o2, &ws.s_o3, &ws.rx2, &ws.ry2, &ws.rk2, &ws.rank, &ws.lneed, &ws.dtmp,
                    &ws.rowcnt, &ws.rowtmp, &ws.tmask, &ws.del_hx, &ws.del_hy, &ws.nopos,
                    &ws.st_key, &ws.st_val, &ws.st_pos, &ws.st_wapp, &ws.big, &ws.s_uid, &ws.scalars,
@@ -622,9 +631,12 @@ static dyg_status incremental_common(dyg_graph *H, dyg_graph *G, const uint32_t 
         const char *nm[] = {"src", "dst", "w", "update_ids", "found_at", "conductance", "accepted"};
         DYG_TRY(check_same_device(H->device, ps, nm, 7));
     }
-    DYG_TRY(check_host_ids(src, n, H->g.n, "src"));
-    DYG_TRY(check_host_ids(dst, n, H->g.n, "dst"));
-    DYG_TRY(check_host_weights(w, n));
+    const bool host_check = n <= kHostCheckMax;
+    if (host_check) {
+        DYG_TRY(check_host_ids(src, n, H->g.n, "src"));
+        DYG_TRY(check_host_ids(dst, n, H->g.n, "dst"));
+        DYG_TRY(check_host_weights(w, n));
+    }
     Workspace &ws = H->ws;
     const uint32_t *d_src, *d_dst;
     const float *d_w;
@@ -651,7 +663,7 @@ static dyg_status incremental_common(dyg_graph *H, dyg_graph *G, const uint32_t 
     }
     const uint32_t B = batch_size ? batch_size : dyg_reference_batch_size(n);
     // inputs read in place from device memory were not checked on the host
-    const bool dev_in = d_src == src || d_dst == dst || d_w == w;
+    const bool dev_in = !host_check || d_src == src || d_dst == dst || d_w == w;
     DYG_TRY(incremental_run(H, G, d_src, d_dst, d_w, n, B, uid_base,
                             (const unsigned long long *)d_uid, *p, o_found, o_cond, o_acc,
                             st, dev_in));
@@ -709,8 +721,11 @@ static dyg_status decremental_common(dyg_graph *G, dyg_graph *H, const uint32_t 
                             "rec_src", "rec_dst", "rec_kind"};
         DYG_TRY(check_same_device(G->device, ps, nm, 8));
     }
-    DYG_TRY(check_host_ids(src, n, G->g.n, "src"));
-    DYG_TRY(check_host_ids(dst, n, G->g.n, "dst"));
+    const bool host_check = n <= kHostCheckMax;
+    if (host_check) {
+        DYG_TRY(check_host_ids(src, n, G->g.n, "src"));
+        DYG_TRY(check_host_ids(dst, n, G->g.n, "dst"));
+    }
     Workspace &ws = G->ws;
     const uint32_t *d_src, *d_dst;
     DYG_TRY(stage_in(ws.s_src, src, n, st, &d_src));
@@ -729,7 +744,7 @@ static dyg_status decremental_common(dyg_graph *G, dyg_graph *H, const uint32_t 
     }
     const uint32_t B = batch_size ? batch_size : dyg_reference_batch_size(n);
     uint64_t total = 0;
-    const bool dev_in = d_src == src || d_dst == dst;
+    const bool dev_in = !host_check || d_src == src || d_dst == dst;
     G->last_rec = 0;
     DYG_TRY(decremental_run(G, H, d_src, d_dst, n, B, uid_base, (const unsigned long long *)d_uid,
                             *p, o_st, o_cd, &total, st, dev_in));
@@ -860,9 +875,12 @@ dyg_status dyg_stream_file(dyg_graph *G, dyg_graph *H, uint32_t op, const uint32
                             "rec_kind"};
         DYG_TRY(check_same_device(G->device, ps, nm, 8));
     }
-    DYG_TRY(check_host_ids(src, n, G->g.n, "src"));
-    DYG_TRY(check_host_ids(dst, n, G->g.n, "dst"));
-    if (ins) DYG_TRY(check_host_weights(w, n));
+    const bool host_check = n <= kHostCheckMax;
+    if (host_check) {
+        DYG_TRY(check_host_ids(src, n, G->g.n, "src"));
+        DYG_TRY(check_host_ids(dst, n, G->g.n, "dst"));
+        if (ins) DYG_TRY(check_host_weights(w, n));
+    }
     Workspace &ws = G->ws;
     const uint32_t *d_src, *d_dst;
     const float *d_w = nullptr;
@@ -880,7 +898,7 @@ dyg_status dyg_stream_file(dyg_graph *G, dyg_graph *H, uint32_t op, const uint32
         o_cd = ptr<float>(ws.s_o2);
     }
     uint64_t total = 0;
-    const bool dev_in = d_src == src || d_dst == dst || (ins && d_w == w);
+    const bool dev_in = !host_check || d_src == src || d_dst == dst || (ins && d_w == w);
     if (!ins) G->last_rec = 0;
     DYG_TRY(stream_file_run(G, H, op, d_src, d_dst, d_w, n, first_update_id, chunk, *p, o_st, o_cd,
                             &total, st, dev_in));

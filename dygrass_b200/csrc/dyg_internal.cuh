@@ -38,6 +38,7 @@ constexpr uint32_t kErrVertex = 1u;    // vertex id >= n in a batch
 constexpr uint32_t kErrPath = 2u;      // winner re-walk disagreed with its key
 constexpr uint32_t kErrArena = 4u;     // arena overflow in a commit
 constexpr uint32_t kErrWeight = 8u;    // weight not finite and > 0 in a batch
+constexpr uint32_t kErrScan = 16u;     // a scan tile gave up waiting for its predecessor
 
 struct DevGraph {
     uint2 *desc;
@@ -164,6 +165,9 @@ struct Workspace {
     Buf htab_k, htab_v;                       // dedup hash table
     Buf nop;                                  // u32 no-path filtered indices
     Buf cub_tmp;
+    Buf scan_status;                          // u64 per tile of the single-pass scan
+    unsigned long long scan_tickets = 0;      // tile tickets handed out so far (S_SCAN)
+    uint32_t scan_epoch = 0;                  // tags this workspace's scan statuses per call
     Buf s_src, s_dst, s_w, s_o1, s_o2, s_o3;  // whole-stream staging
     Buf rx2, ry2;                             // recovered edges of a whole stream
     Buf rk2;
@@ -199,6 +203,7 @@ enum Scalar : int {
     S_RECCNT = 11,    // recovered edges recorded so far in a decremental stream
     S_RECCAP = 12,    // capacity of the record buffers (follows S_RECCNT)
     S_LONG = 13,      // set by an append that made a row longer than kBigRow
+    S_SCAN = 14,      // tile tickets of the single-pass scan (accumulating)
     S_NSCALARS = 16
 };
 enum Count : int {
