@@ -1436,7 +1436,7 @@ def main():
     peak_note = "measured" if hbm else "fallback"
     hbm = hbm or 6650.0
     achieved = res["dom_bytes_per_launch"] / (res["dom_ms_per_launch"] / 1e3) / 1e9
-    traffic, traffic_src = None, None
+    traffic, traffic_src, l2_bytes = None, None, None
     tpath = os.path.join(ROOT, "profiles", "roofline_traffic.json")
     if os.path.exists(tpath):
         for t in json.load(open(tpath)).get("entries", []):
@@ -1445,6 +1445,7 @@ def main():
                     and t.get("exhaustive", False) == args.exhaustive \
                     and all(t[o] == getattr(args, o) for o in opts if o in t):
                 traffic = t.get("dram_bytes_per_launch")
+                l2_bytes = t.get("l2_bytes_per_launch")
                 traffic_src = "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch " \
                               "(profiles/roofline_traffic.json)"
     nin, ndel = res["nin"], res["ndel"]
@@ -1489,6 +1490,11 @@ def main():
                      "ms_per_launch": res["dom_ms_per_launch"],
                      "useful_bytes_per_move": 16,
                      "sector_efficiency": 16 / BYTES_PER_MOVE,
+                     # payload bytes only (8 B descriptor + 8 B slot per move)
+                     "sector_efficient_frac": achieved * 16 / BYTES_PER_MOVE / hbm,
+                     # L2 bytes per launch (ncu lts__t_bytes.sum) over the live launch time
+                     "l2_bytes_per_launch": l2_bytes,
+                     "l2_gbs": (l2_bytes / (res["dom_ms_per_launch"] / 1e3) / 1e9) if l2_bytes else None,
                      "note": "the graphs are largely L2-resident: traffic (ncu DRAM bytes per launch) "
                              "is well below the algorithmic bytes, so frac is an equivalent-bandwidth "
                              "figure; the walk is bound by instruction issue and L1 gathers "

@@ -205,7 +205,7 @@ void free_graph(dyg_graph *G) {
                    &ws.path_len, &ws.cand_x, &ws.cand_y, &ws.cand_w, &ws.keep, &ws.htab_k,
                    &ws.htab_v, &ws.nop, &ws.cub_tmp, &ws.scan_status, &ws.s_src, &ws.s_dst, &ws.s_w, &ws.s_o1,
                    &ws.s_o2, &ws.s_o3, &ws.rx2, &ws.ry2, &ws.rk2, &ws.rank, &ws.lneed, &ws.dtmp,
-                   &ws.rowcnt, &ws.rowtmp, &ws.tmask, &ws.del_hx, &ws.del_hy, &ws.nopos,
+                   &ws.rowcnt, &ws.rowtmp, &ws.tmask, &ws.del_hx, &ws.del_hy,
                    &ws.st_key, &ws.st_val, &ws.st_pos, &ws.st_wapp, &ws.big, &ws.s_uid, &ws.scalars,
                    &ws.counts};
     for (Buf *b : bufs) free_buf(*b);

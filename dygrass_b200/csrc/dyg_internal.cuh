@@ -158,7 +158,7 @@ struct Workspace {
     Buf f_w;                                  // f32 per walk-list entry (insertions)
     Buf found;                                // u8 per half-edge
     Buf hx, hy, hw;                           // half-edge lists (u32/f32)
-    Buf path_v, path_w;                       // winner paths
+    Buf path_v, path_w;                       // winner paths: vertices, edge weights
     Buf path_len;                             // i32 per filtered edge
     Buf cand_x, cand_y, cand_w;               // recovery candidates
     Buf keep;                                 // u32 per candidate
@@ -175,7 +175,6 @@ struct Workspace {
     Buf rowcnt, rowtmp;                       // row operations: per-row counter / run base
     Buf tmask;                                // dedup table size (device)
     Buf del_hx, del_hy;                       // deletion half-edges
-    Buf nopos;                                // no-path positions
     Buf st_key, st_val;                       // stream file: (min, max) keys and indices, sorted
     Buf st_pos;                               // stream file: uint4 slot positions in G and H
     Buf st_wapp;                              // stream file: G weight of each new edge
@@ -217,6 +216,7 @@ enum Count : int {
     C_WALKLIST = 7,   // stream file: new insertions to walk
     C_GHALF = 8,      // stream file: half-edges of the new insertions (G append)
     C_CANDS_ALL = 9,  // recovery candidates: path, then fallback
+    C_HHALF = 10,     // incremental: half-edges of the accepted edges (H append)
     C_NCOUNTS = 12
 };
 
@@ -384,8 +384,9 @@ dyg_status delete_enqueue(dyg_graph *G, const uint32_t *hx, const uint32_t *hy, 
                           cudaStream_t st);
 // Copies both graphs' scalars and counts to the host with one synchronize.
 dyg_status read_scalars2(dyg_graph *A, dyg_graph *B, cudaStream_t st);
+// Exclusive scan of in[0, m) into out; with m_dev, of in[0, min(m, *m_dev)).
 dyg_status exclusive_scan_u32(Workspace &ws, const uint32_t *in, uint32_t *out, uint32_t m,
-                              cudaStream_t st);
+                              cudaStream_t st, const uint32_t *m_dev = nullptr);
 dyg_status compact_graph(dyg_graph *G, cudaStream_t st);
 dyg_status grow_arena(dyg_graph *G, uint64_t min_cap, cudaStream_t st);
 dyg_status read_scalars(dyg_graph *G, cudaStream_t st);

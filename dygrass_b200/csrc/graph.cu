@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "dyg_internal.cuh"
+#include "scan.cuh"
 
 namespace dyg {
 
@@ -184,124 +185,19 @@ dyg_status grow_arena(dyg_graph *G, uint64_t min_cap, cudaStream_t st) {
 }
 
 // ---------------------------------------------------------- exclusive scan
-// Single-pass exclusive scan of u32 (decoupled look-back, Merrill & Garland,
-// "Single-pass Parallel Prefix Scan with Decoupled Look-back", 2016): each
-// block takes the next tile in ticket order, publishes its tile's sum, then
-// walks back over its predecessors' published sums until one holds an
-// inclusive prefix, and publishes its own inclusive prefix.  One launch
-// instead of a library scan's two.  A tile waits only on tiles that took
-// earlier tickets, so they are running or done and publish without waiting;
-// the wait is still bounded, and a tile that gives up sets kErrScan (the call
-// then fails) instead of spinning on.  Status words carry the call's epoch, so
-// no memset is needed between calls: (epoch << 34) | (flag << 32) | value,
-// flag 1 = tile sum, 2 = inclusive prefix.
-constexpr int kScanThreads = 256;
-constexpr int kScanItems = 8;
-constexpr uint32_t kScanTile = kScanThreads * kScanItems;
-constexpr uint32_t kScanSpinLimit = 1u << 21;   // about a second of L2 reads
-
-__device__ __forceinline__ unsigned long long scan_word(uint32_t epoch, uint32_t flag, uint32_t v) {
-    return ((unsigned long long)(epoch & 0x3FFFFFFFu) << 34) | ((unsigned long long)flag << 32) | v;
-}
-
-__global__ void __launch_bounds__(kScanThreads)
-k_scan_u32(const uint32_t *__restrict__ in, uint32_t *__restrict__ out, uint32_t m,
-           unsigned long long *status, unsigned long long *ticket, unsigned long long base,
-           uint32_t epoch, unsigned long long *err) {
-    __shared__ uint32_t s_tile, s_prefix;
-    __shared__ uint32_t s_warp[kScanThreads / 32];
-    if (threadIdx.x == 0) {
-        const unsigned long long t = atomicAdd(ticket, 1ull) - base;
-        s_tile = t < gridDim.x ? (uint32_t)t : ~0u;
-        if (t >= gridDim.x) atomicOr(err, (unsigned long long)kErrScan);   // tickets out of step
-    }
-    __syncthreads();
-    const uint32_t tile = s_tile;
-    if (tile == ~0u) return;
-    const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
-    const uint64_t i0 = (uint64_t)tile * kScanTile + (uint64_t)threadIdx.x * kScanItems;
-    uint32_t v[kScanItems];
-    uint32_t sum = 0;
-#pragma unroll
-    for (int u = 0; u < kScanItems; ++u) {
-        v[u] = (i0 + u < m) ? in[i0 + u] : 0u;
-        sum += v[u];
-    }
-    // block scan of the per-thread sums
-    uint32_t incl = sum;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-        if (lane >= (uint32_t)o) incl += t;
-    }
-    if (lane == 31u) s_warp[wid] = incl;
-    __syncthreads();
-    if (wid == 0) {
-        uint32_t w = lane < kScanThreads / 32 ? s_warp[lane] : 0u;
-#pragma unroll
-        for (int o = 1; o < kScanThreads / 32; o <<= 1) {
-            const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, w, o);
-            if (lane >= (uint32_t)o) w += t;
-        }
-        if (lane < kScanThreads / 32) s_warp[lane] = w;   // inclusive over warps
-    }
-    __syncthreads();
-    const uint32_t before_warp = wid ? s_warp[wid - 1] : 0u;
-    const uint32_t tile_sum = s_warp[kScanThreads / 32 - 1];
-    if (threadIdx.x == 0) {
-        volatile unsigned long long *vs = status;
-        if (tile == 0) {
-            atomicExch(status, scan_word(epoch, 2u, tile_sum));
-            s_prefix = 0u;
-        } else {
-            atomicExch(status + tile, scan_word(epoch, 1u, tile_sum));
-            uint32_t excl = 0;
-            int64_t j = (int64_t)tile - 1;
-            uint32_t spins = 0;
-            while (j >= 0) {
-                const unsigned long long w = vs[j];
-                const uint32_t ep = (uint32_t)(w >> 34), fl = (uint32_t)(w >> 32) & 3u;
-                if (ep != (epoch & 0x3FFFFFFFu) || fl == 0u) {
-                    if (++spins > kScanSpinLimit) {
-                        atomicOr(err, (unsigned long long)kErrScan);
-                        break;
-                    }
-                    continue;
-                }
-                excl += (uint32_t)w;
-                if (fl == 2u) break;
-                --j;
-            }
-            atomicExch(status + tile, scan_word(epoch, 2u, excl + tile_sum));
-            s_prefix = excl;
-        }
-    }
-    __syncthreads();
-    uint32_t run = s_prefix + before_warp + incl - sum;
-#pragma unroll
-    for (int u = 0; u < kScanItems; ++u) {
-        if (i0 + u < m) out[i0 + u] = run;
-        run += v[u];
-    }
-}
+namespace {
+struct CopyScan {
+    const uint32_t *in;
+    uint32_t *out;
+    __device__ uint32_t load(uint32_t i) const { return in[i]; }
+    __device__ void store(uint32_t i, uint32_t excl, uint32_t) const { out[i] = excl; }
+    __device__ void last(uint32_t) const {}
+};
+}  // namespace
 
 dyg_status exclusive_scan_u32(Workspace &ws, const uint32_t *in, uint32_t *out, uint32_t m,
-                              cudaStream_t st) {
-    if (m == 0) return DYG_OK;
-    const uint32_t tiles = (m + kScanTile - 1) / kScanTile;
-    if (ws.scan_status.bytes < sizeof(unsigned long long) * tiles) {
-        DYG_TRY(ensure(ws.scan_status, sizeof(unsigned long long) * tiles));
-        DYG_CUDA(cudaMemsetAsync(ws.scan_status.p, 0, ws.scan_status.bytes, st));
-    }
-    ws.scan_epoch = ws.scan_epoch + 1u == 0x40000000u ? 1u : ws.scan_epoch + 1u;
-    unsigned long long *sc = ptr<unsigned long long>(ws.scalars);
-    k_scan_u32<<<tiles, kScanThreads, 0, st>>>(in, out, m, ptr<unsigned long long>(ws.scan_status),
-                                                sc + S_SCAN, ws.scan_tickets, ws.scan_epoch,
-                                                sc + S_ERR);
-    count_launch();
-    DYG_CUDA(cudaGetLastError());
-    ws.scan_tickets += tiles;   // every launched tile takes one ticket
-    return DYG_OK;
+                              cudaStream_t st, const uint32_t *m_dev) {
+    return scan_op(ws, CopyScan{in, out}, m, m_dev, nullptr, st);
 }
 
 // -------------------------------------------------------------- compaction

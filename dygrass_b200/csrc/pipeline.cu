@@ -19,6 +19,7 @@
 //   1: dedup all candidates (first occurrence), drop those in H, append the
 //      rest in order (path edges, then fallback edges).
 #include "dyg_internal.cuh"
+#include "scan.cuh"
 
 namespace dyg {
 
@@ -60,41 +61,52 @@ __global__ void k_validate(unsigned long long *halt, const uint32_t *src, const 
 
 // --------------------------------------------------------- incremental
 
-__global__ void k_incr_decode(const unsigned long long *halt, const unsigned long long *keys,
-                              uint32_t n, int32_t *found, float *cond, uint8_t *acc,
-                              uint32_t *flags) {
-    if (HALTED(halt)) return;
-    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= n) return;
-    const unsigned long long k = keys[e];
-    if (found) found[e] = key_found(k);
-    if (cond) cond[e] = k ? __uint_as_float((uint32_t)(k >> 32)) : 0.f;
-    if (acc) acc[e] = k ? 0 : 1;
-    flags[e] = k ? 0u : 1u;
-}
-
-// Half-edges in input order (u gets v, then v gets u:
-// random_walk_incremental/gpu_graph.cuh:320-325); with flags only the
-// accepted edges, at their scanned positions; entries not written keep the
-// 0xFFFFFFFF row that append ignores.
-__global__ void k_half_edges(const unsigned long long *halt, const uint32_t *src,
-                             const uint32_t *dst, const float *w, uint32_t n,
-                             const uint32_t *flags, const uint32_t *pos, uint32_t *hx,
-                             uint32_t *hy, float *hw) {
-    if (HALTED(halt)) return;
-    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= n) return;
-    if (flags && !flags[e]) return;
-    const uint32_t q = flags ? pos[e] : e;
-    const uint32_t u = src[e], v = dst[e];
-    const float ww = w[e];
-    hx[2 * q] = u;
-    hy[2 * q] = v;
-    hw[2 * q] = ww;
-    hx[2 * q + 1] = v;
-    hy[2 * q + 1] = u;
-    hw[2 * q + 1] = ww;
-}
+// Incremental commit of one batch in one scan: element e is decoded from its
+// winner key (found step, conductance, accept flag; keys[e] = 0: no walker
+// connected the edge), the accept flags are scanned in input order, and the
+// accepted edge goes to H's half-edge list at its scanned position -- u gets
+// v, then v gets u (random_walk_incremental/gpu_graph.cuh:320-325).  With G,
+// every edge also goes to G's list at its input position.
+struct IncrCommitOp {
+    const unsigned long long *keys;
+    const uint32_t *src, *dst;
+    const float *w;
+    int32_t *found;
+    float *cond;
+    uint8_t *acc;
+    uint32_t *hx, *hy;   // H: accepted edges, compacted
+    float *hw;
+    uint32_t *gx, *gy;   // G: every edge (null: no G)
+    float *gw;
+    uint32_t *half_count;   // 2 * accepted
+    __device__ uint32_t load(uint32_t e) const {
+        const unsigned long long k = keys[e];
+        if (found) found[e] = key_found(k);
+        if (cond) cond[e] = k ? __uint_as_float((uint32_t)(k >> 32)) : 0.f;
+        if (acc) acc[e] = k ? 0 : 1;
+        return k ? 0u : 1u;
+    }
+    __device__ void store(uint32_t e, uint32_t q, uint32_t v) const {
+        const uint32_t u = src[e], x = dst[e];
+        const float ww = w[e];
+        if (gx) {
+            gx[2 * e] = u;
+            gy[2 * e] = x;
+            gw[2 * e] = ww;
+            gx[2 * e + 1] = x;
+            gy[2 * e + 1] = u;
+            gw[2 * e + 1] = ww;
+        }
+        if (!v) return;
+        hx[2 * q] = u;
+        hy[2 * q] = x;
+        hw[2 * q] = ww;
+        hx[2 * q + 1] = x;
+        hy[2 * q + 1] = u;
+        hw[2 * q + 1] = ww;
+    }
+    __device__ void last(uint32_t total) const { *half_count = 2u * total; }
+};
 
 // ---------------------------------------------------------- decremental
 
@@ -122,37 +134,35 @@ __global__ void k_del_half_edges(const unsigned long long *halt, const uint32_t 
     hy[2 * e + 1] = a;
 }
 
-__global__ void k_del_filter(const unsigned long long *halt, const uint8_t *fG, const uint8_t *fH,
-                             uint32_t n, uint32_t *flags, int32_t *status, float *cond) {
-    if (HALTED(halt)) return;
-    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= n) return;
-    const bool inG = fG[2 * e] && fG[2 * e + 1];
-    const bool inH = inG && fH[2 * e] && fH[2 * e + 1];
-    flags[e] = inH ? 1u : 0u;
-    status[e] = !inG ? DYG_DEL_NOT_IN_G : (!inH ? DYG_DEL_NOT_IN_H : DYG_DEL_NO_PATH);
-    cond[e] = 0.f;
-}
-
-// Walk list entry f of deletion e: min -> max, or with osrc/odst the file
-// orientation.
-__global__ void k_del_compact(const unsigned long long *halt, const uint32_t *hx,
-                              const uint32_t *hy, const uint32_t *osrc, const uint32_t *odst,
-                              uint32_t n, const uint32_t *flags, const uint32_t *pos,
-                              unsigned long long uid0, const unsigned long long *uids,
-                              uint32_t *f_src, uint32_t *f_dst, unsigned long long *f_uid,
-                              uint32_t *f_idx, uint32_t *count) {
-    if (HALTED(halt)) return;
-    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= n) return;
-    if (e == n - 1) *count = pos[e] + flags[e];
-    if (!flags[e]) return;
-    const uint32_t f = pos[e];
-    f_src[f] = osrc ? osrc[e] : hx[2 * e];
-    f_dst[f] = odst ? odst[e] : hy[2 * e];
-    f_uid[f] = uids ? uids[e] : uid0 + e;
-    f_idx[f] = e;
-}
+// Deletion e found in G and in H goes to the walk list at its scanned
+// position f: min -> max, or with osrc/odst the file orientation; every
+// deletion gets its status code.
+struct DelFilterOp {
+    const uint8_t *fG, *fH;
+    int32_t *status;
+    float *cond;
+    const uint32_t *hx, *hy, *osrc, *odst;
+    unsigned long long uid0;
+    const unsigned long long *uids;
+    uint32_t *f_src, *f_dst;
+    unsigned long long *f_uid;
+    uint32_t *f_idx, *count;
+    __device__ uint32_t load(uint32_t e) const {
+        const bool inG = fG[2 * e] && fG[2 * e + 1];
+        const bool inH = inG && fH[2 * e] && fH[2 * e + 1];
+        status[e] = !inG ? DYG_DEL_NOT_IN_G : (!inH ? DYG_DEL_NOT_IN_H : DYG_DEL_NO_PATH);
+        cond[e] = 0.f;
+        return inH ? 1u : 0u;
+    }
+    __device__ void store(uint32_t e, uint32_t f, uint32_t v) const {
+        if (!v) return;
+        f_src[f] = osrc ? osrc[e] : hx[2 * e];
+        f_dst[f] = odst ? odst[e] : hy[2 * e];
+        f_uid[f] = uids ? uids[e] : uid0 + e;
+        f_idx[f] = e;
+    }
+    __device__ void last(uint32_t total) const { *count = total; }
+};
 
 __global__ void k_range_count(const unsigned long long *halt, const uint32_t *F_dev, uint32_t f0,
                               uint32_t nf, uint32_t *out) {
@@ -161,53 +171,71 @@ __global__ void k_range_count(const unsigned long long *halt, const uint32_t *F_
     *out = F > f0 ? min(F - f0, nf) : 0u;
 }
 
-// Per filtered edge: status / conductance, path-candidate counts and the
-// no-path flags (zero for f >= F).
-__global__ void k_decr_results(const unsigned long long *halt, const unsigned long long *keys,
-                               const int32_t *plen, const uint32_t *f_idx, const uint32_t *F_dev,
-                               uint32_t n, int32_t *status, float *cond, uint32_t *clen,
-                               uint32_t *noflag) {
-    if (HALTED(halt)) return;
-    const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= n) return;
-    const uint32_t F = F_dev ? *F_dev : n;
-    if (f >= F) {
-        clen[f] = 0;
-        noflag[f] = 0;
-        return;
+// Per walk-list entry f (f < F; zero past it): status and conductance of its
+// deletion, and its path length as the value scanned into the candidate
+// offsets coff; the no-path flags go to noflag for the second scan.
+struct DecrResultsOp {
+    const unsigned long long *keys;
+    const int32_t *plen;
+    const uint32_t *f_idx, *F_dev;
+    int32_t *status;
+    float *cond;
+    uint32_t *clen, *coff, *noflag, *counts;
+    __device__ uint32_t load(uint32_t f) const {
+        const uint32_t F = F_dev ? *F_dev : 0xFFFFFFFFu;
+        if (f >= F) {
+            noflag[f] = 0u;
+            return 0u;
+        }
+        const uint32_t e = f_idx[f];
+        const int32_t L = plen[f];
+        const unsigned long long k = keys[f];
+        status[e] = L > 0 ? L : DYG_DEL_NO_PATH;
+        cond[e] = k ? __uint_as_float((uint32_t)(k >> 32)) : 0.f;
+        noflag[f] = L > 0 ? 0u : 1u;
+        return L > 0 ? (uint32_t)L : 0u;
     }
-    const uint32_t e = f_idx[f];
-    const int32_t L = plen[f];
-    const unsigned long long k = keys[f];
-    status[e] = L > 0 ? L : DYG_DEL_NO_PATH;
-    cond[e] = k ? __uint_as_float((uint32_t)(k >> 32)) : 0.f;
-    clen[f] = L > 0 ? (uint32_t)L : 0u;
-    noflag[f] = L > 0 ? 0u : 1u;
-}
+    __device__ void store(uint32_t f, uint32_t excl, uint32_t v) const {
+        coff[f] = excl;
+        clen[f] = v;
+    }
+    __device__ void last(uint32_t total) const { counts[C_CANDS] = total; }
+};
 
+// The edges without a path, in walk-list order, for the fallback walks.
+struct NoPathOp {
+    const uint32_t *noflag;
+    uint32_t *nop, *counts;
+    uint32_t hw;
+    __device__ uint32_t load(uint32_t f) const { return noflag[f]; }
+    __device__ void store(uint32_t f, uint32_t q, uint32_t v) const {
+        if (v) nop[q] = f;
+    }
+    __device__ void last(uint32_t total) const {
+        counts[C_NOPATH] = total;
+        counts[C_CANDS2] = total * 4u * hw;
+        counts[C_CANDS_ALL] = counts[C_CANDS] + total * 4u * hw;
+    }
+};
+
+// Path edges of walk-list entry f as recovery candidates at coff[f], one warp
+// per path (consecutive lanes copy consecutive path edges).
 __global__ void k_path_cands(const unsigned long long *halt, const uint32_t *pv, const float *pw,
                              uint32_t stride, const uint32_t *clen, const uint32_t *coff,
-                             uint32_t n, const uint32_t *noflag, const uint32_t *nopos,
-                             uint32_t *cx, uint32_t *cy, float *cw, uint32_t *nop,
-                             uint32_t *counts, uint32_t hw) {
+                             uint32_t n, uint32_t *cx, uint32_t *cy, float *cw) {
     if (HALTED(halt)) return;
-    const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= n) return;
-    if (f == n - 1) {
-        counts[C_CANDS] = coff[f] + clen[f];
-        counts[C_NOPATH] = nopos[f] + noflag[f];
-        counts[C_CANDS2] = (nopos[f] + noflag[f]) * 4u * hw;
-        counts[C_CANDS_ALL] = counts[C_CANDS] + counts[C_CANDS2];
-    }
-    if (noflag[f]) nop[nopos[f]] = f;
-    const uint32_t L = clen[f];
-    const uint32_t base = coff[f];
-    const uint32_t *v = pv + (size_t)f * stride;
-    const float *w = pw + (size_t)f * stride;
-    for (uint32_t j = 0; j < L; ++j) {
-        cx[base + j] = v[j];
-        cy[base + j] = v[j + 1];
-        cw[base + j] = w[j + 1];
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t f = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; f < n; f += warps) {
+        const uint32_t L = clen[f];
+        const uint32_t base = coff[f];
+        const uint32_t *v = pv + (size_t)f * stride;
+        const float *w = pw + (size_t)f * stride;
+        for (uint32_t j = lane; j < L; j += 32u) {
+            cx[base + j] = v[j];
+            cy[base + j] = v[j + 1];
+            cw[base + j] = w[j + 1];
+        }
     }
 }
 
@@ -226,20 +254,19 @@ __device__ __forceinline__ uint32_t hslot(unsigned long long k, uint32_t mask) {
     return (uint32_t)k & mask;
 }
 
-__global__ void k_rec_setup(const unsigned long long *halt, const uint32_t *M_dev, uint32_t M_host,
-                            uint32_t *tmask, uint32_t *counts) {
+// Table of T = the smallest power of two >= max(1024, 2M) slots cleared; its
+// mask and the kept count reset by the first thread.
+__global__ void k_hash_clear(const unsigned long long *halt, const uint32_t *M_dev, uint32_t M_host,
+                             unsigned long long *tk, uint32_t *tv, uint32_t *tmask,
+                             uint32_t *counts) {
     if (HALTED(halt)) return;
     const uint32_t M = dcount(M_dev, M_host);
     uint32_t T = 1024u;
     while (T < 2u * M) T <<= 1;
-    *tmask = T - 1u;
-    counts[C_KEPT] = 0u;
-}
-
-__global__ void k_hash_clear(const unsigned long long *halt, unsigned long long *tk, uint32_t *tv,
-                             const uint32_t *tmask) {
-    if (HALTED(halt)) return;
-    const uint32_t T = *tmask + 1u;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *tmask = T - 1u;
+        counts[C_KEPT] = 0u;
+    }
     GSTRIDE(i, T) {
         tk[i] = ~0ull;
         tv[i] = ~0u;
@@ -330,32 +357,26 @@ __global__ void k_keep_big(const unsigned long long *halt, DevGraph h, const uin
     }
 }
 
-// One thread: the kept edges must fit the record buffers, or halt.
-__global__ void k_rec_check(unsigned long long *halt, const uint32_t *keep, const uint32_t *kpos,
-                            const uint32_t *M_dev, uint32_t M_host, const unsigned long long *sc,
-                            unsigned long long code) {
-    if (*halt) return;
-    const uint32_t M = dcount(M_dev, M_host);
-    const unsigned long long K = M ? (unsigned long long)kpos[M - 1] + keep[M - 1] : 0ull;
-    if (sc[S_RECCNT] + K > sc[S_RECCAP]) *halt = code;
-}
-
 // Kept candidates -> half-edges (x gets y, then y gets x), in candidate order,
-// and the recovered-edge records after the ones recorded so far.
-__global__ void k_emit_kept(const unsigned long long *halt, const uint32_t *cx, const uint32_t *cy,
-                            const float *cw, const uint32_t *M_dev, uint32_t M_host,
-                            const uint32_t *keep, const uint32_t *kpos, uint8_t kind,
-                            const uint32_t *split, uint8_t kind_after,
-                            const unsigned long long *sc, uint32_t *hx, uint32_t *hy, float *hw,
-                            uint32_t *rx, uint32_t *ry, uint8_t *rk, uint32_t *counts) {
-    if (HALTED(halt)) return;
-    const uint32_t M = dcount(M_dev, M_host);
-    const uint32_t sp = split ? *split : M;   // candidates from sp on get kind_after
-    const unsigned long long base = sc[S_RECCNT];
-    GSTRIDE(i, M) {
-        if (i == M - 1) counts[C_KEPT] = 2u * (kpos[i] + keep[i]);
-        if (!keep[i]) continue;
-        const uint32_t q = kpos[i];
+// and the recovered-edge records after the ones recorded so far.  The kept
+// edges must fit the record buffers: the records past them are not written
+// and the last candidate halts the batch (it is resumed with larger buffers).
+struct KeepEmitOp {
+    const uint32_t *keep, *cx, *cy;
+    const float *cw;
+    uint8_t kind, kind_after;
+    const uint32_t *split;   // candidates from *split on get kind_after (null: none)
+    const unsigned long long *sc;
+    unsigned long long *halt;
+    unsigned long long code;
+    uint32_t *hx, *hy;
+    float *hw;
+    uint32_t *rx, *ry;
+    uint8_t *rk;
+    uint32_t *counts;
+    __device__ uint32_t load(uint32_t i) const { return keep[i]; }
+    __device__ void store(uint32_t i, uint32_t q, uint32_t v) const {
+        if (!v) return;
         const uint32_t x = cx[i], y = cy[i];
         const float w = cw[i];
         hx[2 * q] = x;
@@ -364,11 +385,18 @@ __global__ void k_emit_kept(const unsigned long long *halt, const uint32_t *cx, 
         hx[2 * q + 1] = y;
         hy[2 * q + 1] = x;
         hw[2 * q + 1] = w;
-        rx[base + q] = x;
-        ry[base + q] = y;
-        rk[base + q] = i < sp ? kind : kind_after;
+        const unsigned long long r = sc[S_RECCNT] + q;
+        if (r < sc[S_RECCAP]) {
+            rx[r] = x;
+            ry[r] = y;
+            rk[r] = (split && i >= *split) ? kind_after : kind;
+        }
     }
-}
+    __device__ void last(uint32_t total) const {
+        counts[C_KEPT] = 2u * total;
+        if (sc[S_RECCNT] + total > sc[S_RECCAP]) atomicCAS(halt, 0ull, code);
+    }
+};
 
 __global__ void k_rec_advance(const unsigned long long *halt, const uint32_t *counts,
                               unsigned long long *sc) {
@@ -391,20 +419,19 @@ dyg_status recover_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *cx, const
     DYG_TRY(ensure(ws.htab_k, sizeof(unsigned long long) * T));
     DYG_TRY(ensure(ws.htab_v, sizeof(uint32_t) * T));
     DYG_TRY(ensure(ws.tmask, sizeof(uint32_t)));
-    DYG_TRY(ensure(ws.keep, sizeof(uint32_t) * (size_t)M_host * 2));
+    DYG_TRY(ensure(ws.keep, sizeof(uint32_t) * (size_t)M_host));
     DYG_TRY(ensure(ws.big, sizeof(uint4) * (size_t)M_host));
     DYG_TRY(ensure(ws.hx, sizeof(uint32_t) * (size_t)M_host * 2));
     DYG_TRY(ensure(ws.hy, sizeof(uint32_t) * (size_t)M_host * 2));
     DYG_TRY(ensure(ws.hw, sizeof(float) * (size_t)M_host * 2));
-    uint32_t *keep = ptr<uint32_t>(ws.keep), *kpos = keep + M_host;
+    uint32_t *keep = ptr<uint32_t>(ws.keep);
     uint32_t *counts = ptr<uint32_t>(ws.counts);
     unsigned long long *sc = ptr<unsigned long long>(ws.scalars);
     const int gr = grid_for(M_host);
-    k_rec_setup<<<1, 1, 0, st>>>(halt, M_dev, M_host, ptr<uint32_t>(ws.tmask), counts);
-    count_launch();
-    k_hash_clear<<<grid_for((uint64_t)T), 256, 0, st>>>(halt, ptr<unsigned long long>(ws.htab_k),
+    k_hash_clear<<<grid_for((uint64_t)T), 256, 0, st>>>(halt, M_dev, M_host,
+                                                        ptr<unsigned long long>(ws.htab_k),
                                                         ptr<uint32_t>(ws.htab_v),
-                                                        ptr<uint32_t>(ws.tmask));
+                                                        ptr<uint32_t>(ws.tmask), counts);
     count_launch();
     k_hash_insert<<<gr, 256, 0, st>>>(halt, cx, cy, M_dev, M_host, ptr<unsigned long long>(ws.htab_k),
                                       ptr<uint32_t>(ws.htab_v), ptr<uint32_t>(ws.tmask));
@@ -421,16 +448,11 @@ dyg_status recover_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *cx, const
                                                           sc + S_NBIG, keep);
         count_launch();
     }
-    DYG_TRY(exclusive_scan_u32(ws, keep, kpos, M_host, st));
-    k_rec_check<<<1, 1, 0, st>>>(halt, keep, kpos, M_dev, M_host, sc,
-                                 halt_code(batch, (uint32_t)kHaltRecords, phase));
-    count_launch();
-    k_emit_kept<<<gr, 256, 0, st>>>(halt, cx, cy, cw, M_dev, M_host, keep, kpos, kind, split,
-                                    kind_after, sc,
-                                    ptr<uint32_t>(ws.hx), ptr<uint32_t>(ws.hy), ptr<float>(ws.hw),
-                                    ptr<uint32_t>(ws.rx2), ptr<uint32_t>(ws.ry2),
-                                    ptr<uint8_t>(ws.rk2), counts);
-    count_launch();
+    const KeepEmitOp op{keep, cx, cy, cw, kind, kind_after, split, sc, halt,
+                        halt_code(batch, (uint32_t)kHaltRecords, phase),
+                        ptr<uint32_t>(ws.hx), ptr<uint32_t>(ws.hy), ptr<float>(ws.hw),
+                        ptr<uint32_t>(ws.rx2), ptr<uint32_t>(ws.ry2), ptr<uint8_t>(ws.rk2), counts};
+    DYG_TRY(scan_op(ws, op, M_host, M_dev, halt, st));
     DYG_CUDA(cudaGetLastError());
     AppendList L{ptr<uint32_t>(ws.hx), ptr<uint32_t>(ws.hy), ptr<float>(ws.hw), counts + C_KEPT,
                  2u * M_host};
@@ -498,35 +520,26 @@ dyg_status incr_commit_enqueue(dyg_graph *H, dyg_graph *G, const uint32_t *src,
                                uint32_t batch, int32_t *found, float *cond, uint8_t *acc,
                                cudaStream_t st) {
     Workspace &ws = H->ws;
-    DYG_TRY(ensure(ws.flags, sizeof(uint32_t) * n));
-    DYG_TRY(ensure(ws.pos, sizeof(uint32_t) * n));
     DYG_TRY(ensure(ws.hx, sizeof(uint32_t) * (size_t)n * 2));
     DYG_TRY(ensure(ws.hy, sizeof(uint32_t) * (size_t)n * 2));
     DYG_TRY(ensure(ws.hw, sizeof(float) * (size_t)n * 2));
-    DYG_CUDA(cudaMemsetAsync(ws.hx.p, 0xFF, sizeof(uint32_t) * (size_t)n * 2, st));
-    k_incr_decode<<<blocks(n, 256), 256, 0, st>>>(halt, keys, n, found, cond, acc,
-                                                   ptr<uint32_t>(ws.flags));
-    count_launch();
-    DYG_TRY(exclusive_scan_u32(ws, ptr<uint32_t>(ws.flags), ptr<uint32_t>(ws.pos), n, st));
-    k_half_edges<<<blocks(n, 256), 256, 0, st>>>(halt, src, dst, w, n, ptr<uint32_t>(ws.flags),
-                                                  ptr<uint32_t>(ws.pos), ptr<uint32_t>(ws.hx),
-                                                  ptr<uint32_t>(ws.hy), ptr<float>(ws.hw));
-    count_launch();
-    AppendList LH{ptr<uint32_t>(ws.hx), ptr<uint32_t>(ws.hy), ptr<float>(ws.hw), nullptr, 2u * n};
+    uint32_t *counts = ptr<uint32_t>(ws.counts);
+    IncrCommitOp op{keys, src, dst, w, found, cond, acc, ptr<uint32_t>(ws.hx), ptr<uint32_t>(ws.hy),
+                    ptr<float>(ws.hw), nullptr, nullptr, nullptr, counts + C_HHALF};
+    AppendList LH{ptr<uint32_t>(ws.hx), ptr<uint32_t>(ws.hy), ptr<float>(ws.hw), counts + C_HHALF,
+                  2u * n};
     AppendList LG{};
     if (G) {
         Workspace &wg = G->ws;
         DYG_TRY(ensure(wg.hx, sizeof(uint32_t) * (size_t)n * 2));
         DYG_TRY(ensure(wg.hy, sizeof(uint32_t) * (size_t)n * 2));
         DYG_TRY(ensure(wg.hw, sizeof(float) * (size_t)n * 2));
-        k_half_edges<<<blocks(n, 256), 256, 0, st>>>(halt, src, dst, w, n, nullptr, nullptr,
-                                                      ptr<uint32_t>(wg.hx), ptr<uint32_t>(wg.hy),
-                                                      ptr<float>(wg.hw));
-        count_launch();
-        LG = AppendList{ptr<uint32_t>(wg.hx), ptr<uint32_t>(wg.hy), ptr<float>(wg.hw), nullptr,
-                        2u * n};
+        op.gx = ptr<uint32_t>(wg.hx);
+        op.gy = ptr<uint32_t>(wg.hy);
+        op.gw = ptr<float>(wg.hw);
+        LG = AppendList{op.gx, op.gy, op.gw, nullptr, 2u * n};
     }
-    DYG_CUDA(cudaGetLastError());
+    DYG_TRY(scan_op(ws, op, n, nullptr, halt, st));
     return append_enqueue(H, LH, G, G ? &LG : nullptr, halt,
                           halt_code(batch, (uint32_t)kHaltArena, 0), st);
 }
@@ -561,8 +574,6 @@ dyg_status decr_delete_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src,
     DYG_TRY(ensure(ws.del_hx, sizeof(uint32_t) * (size_t)m));
     DYG_TRY(ensure(ws.del_hy, sizeof(uint32_t) * (size_t)m));
     DYG_TRY(ensure(ws.found, (size_t)m * 2));
-    DYG_TRY(ensure(ws.flags, sizeof(uint32_t) * n));
-    DYG_TRY(ensure(ws.pos, sizeof(uint32_t) * n));
     DYG_TRY(ensure(ws.f_src, sizeof(uint32_t) * n));
     DYG_TRY(ensure(ws.f_dst, sizeof(uint32_t) * n));
     DYG_TRY(ensure(ws.f_idx, sizeof(uint32_t) * n));
@@ -576,16 +587,12 @@ dyg_status decr_delete_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src,
     count_launch();
     DYG_TRY(delete_enqueue(G, hx, hy, m, nullptr, fG, halt, st));
     DYG_TRY(delete_enqueue(H, hx, hy, m, fG, fH, halt, st));
-    k_del_filter<<<blocks(n, 256), 256, 0, st>>>(halt, fG, fH, n, ptr<uint32_t>(ws.flags), status,
-                                                  cond);
-    count_launch();
-    DYG_TRY(exclusive_scan_u32(ws, ptr<uint32_t>(ws.flags), ptr<uint32_t>(ws.pos), n, st));
-    k_del_compact<<<blocks(n, 256), 256, 0, st>>>(
-        halt, hx, hy, file_orient ? src : nullptr, file_orient ? dst : nullptr, n,
-        ptr<uint32_t>(ws.flags), ptr<uint32_t>(ws.pos), uid0, uids,
-        ptr<uint32_t>(ws.f_src), ptr<uint32_t>(ws.f_dst), ptr<unsigned long long>(ws.f_uid),
-        ptr<uint32_t>(ws.f_idx), counts + C_FILTERED);
-    count_launch();
+    const DelFilterOp op{fG, fH, status, cond, hx, hy, file_orient ? src : nullptr,
+                         file_orient ? dst : nullptr, (unsigned long long)uid0, uids,
+                         ptr<uint32_t>(ws.f_src), ptr<uint32_t>(ws.f_dst),
+                         ptr<unsigned long long>(ws.f_uid), ptr<uint32_t>(ws.f_idx),
+                         counts + C_FILTERED};
+    DYG_TRY(scan_op(ws, op, n, nullptr, halt, st));
     DYG_CUDA(cudaGetLastError());
     return DYG_OK;
 }
@@ -608,7 +615,6 @@ dyg_status decr_walk_enqueue(dyg_graph *G, dyg_graph *H, uint32_t f0, uint32_t n
     DYG_TRY(ensure(ws.path_w, sizeof(float) * (size_t)n * stride));
     DYG_TRY(ensure(ws.path_len, sizeof(int32_t) * n));
     DYG_TRY(ensure(ws.nop, sizeof(uint32_t) * (size_t)n * 4));
-    DYG_TRY(ensure(ws.nopos, sizeof(uint32_t) * (size_t)n));
     // path candidates at [0, C_CANDS), then the fallback candidates
     const size_t n_path = (size_t)n * (stride - 1u), n_fb = (size_t)n * 4u * hwk;
     DYG_TRY(ensure(ws.cand_x, sizeof(uint32_t) * (n_path + n_fb)));
@@ -616,7 +622,6 @@ dyg_status decr_walk_enqueue(dyg_graph *G, dyg_graph *H, uint32_t f0, uint32_t n
     DYG_TRY(ensure(ws.cand_w, sizeof(float) * (n_path + n_fb)));
     uint32_t *counts = ptr<uint32_t>(ws.counts);
     uint32_t *clen = ptr<uint32_t>(ws.nop) + n, *coff = clen + n, *noflag = coff + n;
-    uint32_t *nopos = ptr<uint32_t>(ws.nopos);
     const uint32_t *fsrc = ptr<uint32_t>(ws.f_src) + f0, *fdst = ptr<uint32_t>(ws.f_dst) + f0;
     const unsigned long long *fuid = ptr<unsigned long long>(ws.f_uid) + f0;
     const uint32_t *fidx = ptr<uint32_t>(ws.f_idx) + f0;
@@ -640,17 +645,14 @@ dyg_status decr_walk_enqueue(dyg_graph *G, dyg_graph *H, uint32_t f0, uint32_t n
         }
         DYG_TRY(launch_winner_paths(G, job, p, keys, n, stride, ptr<uint32_t>(ws.path_v),
                                     ptr<float>(ws.path_w), ptr<int32_t>(ws.path_len), st));
-        k_decr_results<<<blocks(n, 256), 256, 0, st>>>(halt, keys, ptr<int32_t>(ws.path_len),
-                                                        fidx, cnt_dev, n, status, cond, clen,
-                                                        noflag);
-        count_launch();
-        DYG_TRY(exclusive_scan_u32(ws, clen, coff, n, st));
-        DYG_TRY(exclusive_scan_u32(ws, noflag, nopos, n, st));
-        k_path_cands<<<blocks(n, 256), 256, 0, st>>>(halt, ptr<uint32_t>(ws.path_v),
-                                                      ptr<float>(ws.path_w), stride, clen, coff, n,
-                                                      noflag, nopos, ptr<uint32_t>(ws.cand_x),
-                                                      ptr<uint32_t>(ws.cand_y), ptr<float>(ws.cand_w),
-                                                      ptr<uint32_t>(ws.nop), counts, hwk);
+        const DecrResultsOp rop{keys, ptr<int32_t>(ws.path_len), fidx, cnt_dev, status, cond,
+                                clen, coff, noflag, counts};
+        DYG_TRY(scan_op(ws, rop, n, nullptr, halt, st));
+        const NoPathOp nop_op{noflag, ptr<uint32_t>(ws.nop), counts, hwk};
+        DYG_TRY(scan_op(ws, nop_op, n, nullptr, halt, st));
+        k_path_cands<<<grid_for((uint64_t)n * 32u), 256, 0, st>>>(
+            halt, ptr<uint32_t>(ws.path_v), ptr<float>(ws.path_w), stride, clen, coff, n,
+            ptr<uint32_t>(ws.cand_x), ptr<uint32_t>(ws.cand_y), ptr<float>(ws.cand_w));
         count_launch();
         DYG_CUDA(cudaGetLastError());
         if (hwk > 0) {

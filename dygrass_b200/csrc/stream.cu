@@ -24,6 +24,7 @@
 #include <cub/cub.cuh>
 
 #include "dyg_internal.cuh"
+#include "scan.cuh"
 
 namespace dyg {
 
@@ -212,37 +213,40 @@ __global__ void k_st_merge(const unsigned long long *halt, DevGraph G, DevGraph 
 }
 
 // New edges in file order: the walk list (file orientation, stream weight)
-// and G's half-edges (src gets dst, dst gets src; merged weight).
-__global__ void k_st_compact(const unsigned long long *halt, const uint32_t *src,
-                             const uint32_t *dst, const float *w, uint32_t n,
-                             const uint32_t *nflag, const uint32_t *npos, const float *wapp,
-                             unsigned long long uid0, uint32_t *f_src, uint32_t *f_dst,
-                             float *f_w, unsigned long long *f_uid, uint32_t *f_idx, uint32_t *hx,
-                             uint32_t *hy, float *hw, uint32_t *counts) {
-    if (HALTED(halt)) return;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    if (i == n - 1) {
-        const uint32_t tot = npos[i] + nflag[i];
-        counts[C_WALKLIST] = tot;
-        counts[C_GHALF] = 2u * tot;
+// and G's half-edges (src gets dst, dst gets src; merged weight), at the
+// scanned positions of the new-edge flags.
+struct StCompactOp {
+    const uint32_t *nflag, *src, *dst;
+    const float *w, *wapp;
+    unsigned long long uid0;
+    uint32_t *f_src, *f_dst;
+    float *f_w;
+    unsigned long long *f_uid;
+    uint32_t *f_idx, *hx, *hy;
+    float *hw;
+    uint32_t *counts;
+    __device__ uint32_t load(uint32_t i) const { return nflag[i]; }
+    __device__ void store(uint32_t i, uint32_t q, uint32_t v) const {
+        if (!v) return;
+        const uint32_t u = src[i], x = dst[i];
+        f_src[q] = u;
+        f_dst[q] = x;
+        f_w[q] = w[i];
+        f_uid[q] = uid0 + i;
+        f_idx[q] = i;
+        const float wa = wapp[i];
+        hx[2 * q] = u;
+        hy[2 * q] = x;
+        hw[2 * q] = wa;
+        hx[2 * q + 1] = x;
+        hy[2 * q + 1] = u;
+        hw[2 * q + 1] = wa;
     }
-    if (!nflag[i]) return;
-    const uint32_t q = npos[i];
-    const uint32_t u = src[i], v = dst[i];
-    f_src[q] = u;
-    f_dst[q] = v;
-    f_w[q] = w[i];
-    f_uid[q] = uid0 + i;
-    f_idx[q] = i;
-    const float wa = wapp[i];
-    hx[2 * q] = u;
-    hy[2 * q] = v;
-    hw[2 * q] = wa;
-    hx[2 * q + 1] = v;
-    hy[2 * q + 1] = u;
-    hw[2 * q + 1] = wa;
-}
+    __device__ void last(uint32_t total) const {
+        counts[C_WALKLIST] = total;
+        counts[C_GHALF] = 2u * total;
+    }
+};
 
 __global__ void k_st_range(const unsigned long long *halt, const uint32_t *F_dev, uint32_t f0,
                            uint32_t nf, uint32_t *out) {
@@ -251,44 +255,39 @@ __global__ void k_st_range(const unsigned long long *halt, const uint32_t *F_dev
     *out = F > f0 ? min(F - f0, nf) : 0u;
 }
 
-// Chunk results: found_at / conductance by file index, accept flags by
-// chunk position (zero past the chunk's device count).
-__global__ void k_st_decode(const unsigned long long *halt, const unsigned long long *keys,
-                            const uint32_t *f_idx, const uint32_t *cnt, uint32_t nc,
-                            int32_t *status, float *cond, uint32_t *flags) {
-    if (HALTED(halt)) return;
-    const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= nc) return;
-    if (f >= *cnt) {
-        flags[f] = 0u;
-        return;
+// Chunk results: found_at / conductance by file index, and the accepted
+// edges (no walker connected them) to H's half-edge list in chunk order;
+// entries past the chunk's device count are not accepted.
+struct StAcceptOp {
+    const unsigned long long *keys;
+    const uint32_t *f_idx, *cnt, *f_src, *f_dst;
+    const float *f_w;
+    int32_t *status;
+    float *cond;
+    uint32_t *hx, *hy;
+    float *hw;
+    uint32_t *counts;
+    __device__ uint32_t load(uint32_t f) const {
+        if (f >= *cnt) return 0u;
+        const unsigned long long k = keys[f];
+        const uint32_t i = f_idx[f];
+        status[i] = key_found(k);
+        cond[i] = k ? __uint_as_float((uint32_t)(k >> 32)) : 0.f;
+        return k ? 0u : 1u;
     }
-    const unsigned long long k = keys[f];
-    const uint32_t i = f_idx[f];
-    status[i] = key_found(k);
-    cond[i] = k ? __uint_as_float((uint32_t)(k >> 32)) : 0.f;
-    flags[f] = k ? 0u : 1u;
-}
-
-__global__ void k_st_accept(const unsigned long long *halt, const uint32_t *f_src,
-                            const uint32_t *f_dst, const float *f_w, uint32_t nc,
-                            const uint32_t *flags, const uint32_t *pos, uint32_t *hx, uint32_t *hy,
-                            float *hw, uint32_t *counts) {
-    if (HALTED(halt)) return;
-    const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= nc) return;
-    if (f == nc - 1) counts[C_ACCEPTED] = 2u * (pos[f] + flags[f]);
-    if (!flags[f]) return;
-    const uint32_t q = pos[f];
-    const uint32_t u = f_src[f], v = f_dst[f];
-    const float ww = f_w[f];
-    hx[2 * q] = u;
-    hy[2 * q] = v;
-    hw[2 * q] = ww;
-    hx[2 * q + 1] = v;
-    hy[2 * q + 1] = u;
-    hw[2 * q + 1] = ww;
-}
+    __device__ void store(uint32_t f, uint32_t q, uint32_t v) const {
+        if (!v) return;
+        const uint32_t u = f_src[f], x = f_dst[f];
+        const float ww = f_w[f];
+        hx[2 * q] = u;
+        hy[2 * q] = x;
+        hw[2 * q] = ww;
+        hx[2 * q + 1] = x;
+        hy[2 * q + 1] = u;
+        hw[2 * q + 1] = ww;
+    }
+    __device__ void last(uint32_t total) const { counts[C_ACCEPTED] = 2u * total; }
+};
 
 uint32_t key_bits(uint32_t nv) {
     uint32_t b = 1;
@@ -305,7 +304,7 @@ dyg_status insert_prep_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src,
     const uint32_t nb = key_bits(G->g.n);
     unsigned long long *key = ptr<unsigned long long>(ws.st_key), *skey = key + n;
     uint32_t *val = ptr<uint32_t>(ws.st_val), *sval = val + n;
-    uint32_t *nflag = ptr<uint32_t>(ws.flags), *npos = ptr<uint32_t>(ws.pos);
+    uint32_t *nflag = ptr<uint32_t>(ws.flags);
     uint32_t *counts = ptr<uint32_t>(ws.counts);
     unsigned long long *sc = ptr<unsigned long long>(ws.scalars);
     const bool big_ok = G->long_rows || H->long_rows;
@@ -332,13 +331,11 @@ dyg_status insert_prep_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src,
                                                 ptr<uint4>(ws.st_pos), w, nflag,
                                                 ptr<float>(ws.st_wapp), status, cond);
     count_launch();
-    DYG_TRY(exclusive_scan_u32(ws, nflag, npos, n, st));
-    k_st_compact<<<blocks(n, 256), 256, 0, st>>>(
-        halt, src, dst, w, n, nflag, npos, ptr<float>(ws.st_wapp), (unsigned long long)uid0,
-        ptr<uint32_t>(ws.f_src), ptr<uint32_t>(ws.f_dst), ptr<float>(ws.f_w),
-        ptr<unsigned long long>(ws.f_uid), ptr<uint32_t>(ws.f_idx), ptr<uint32_t>(ws.hx),
-        ptr<uint32_t>(ws.hy), ptr<float>(ws.hw), counts);
-    count_launch();
+    const StCompactOp op{nflag, src, dst, w, ptr<float>(ws.st_wapp), (unsigned long long)uid0,
+                         ptr<uint32_t>(ws.f_src), ptr<uint32_t>(ws.f_dst), ptr<float>(ws.f_w),
+                         ptr<unsigned long long>(ws.f_uid), ptr<uint32_t>(ws.f_idx),
+                         ptr<uint32_t>(ws.hx), ptr<uint32_t>(ws.hy), ptr<float>(ws.hw), counts};
+    DYG_TRY(scan_op(ws, op, n, nullptr, halt, st));
     DYG_CUDA(cudaGetLastError());
     return DYG_OK;
 }
@@ -369,14 +366,9 @@ dyg_status insert_chunk_enqueue(dyg_graph *G, dyg_graph *H, uint32_t c, uint32_t
     WalkJob job{halt, fsrc, fdst, fw, ptr<unsigned long long>(wg.f_uid) + f0, 0ull, cnt, nc,
                 kDomainIncr};
     DYG_TRY(launch_walk(H, job, p, true, keys, st));
-    k_st_decode<<<blocks(nc, 256), 256, 0, st>>>(halt, keys, ptr<uint32_t>(wg.f_idx) + f0, cnt,
-                                                  nc, status, cond, ptr<uint32_t>(wh.flags));
-    count_launch();
-    DYG_TRY(exclusive_scan_u32(wh, ptr<uint32_t>(wh.flags), ptr<uint32_t>(wh.pos), nc, st));
-    k_st_accept<<<blocks(nc, 256), 256, 0, st>>>(halt, fsrc, fdst, fw, nc, ptr<uint32_t>(wh.flags),
-                                                  ptr<uint32_t>(wh.pos), ptr<uint32_t>(wh.hx),
-                                                  ptr<uint32_t>(wh.hy), ptr<float>(wh.hw), hcounts);
-    count_launch();
+    const StAcceptOp op{keys, ptr<uint32_t>(wg.f_idx) + f0, cnt, fsrc, fdst, fw, status, cond,
+                        ptr<uint32_t>(wh.hx), ptr<uint32_t>(wh.hy), ptr<float>(wh.hw), hcounts};
+    DYG_TRY(scan_op(wh, op, nc, nullptr, halt, st));
     DYG_CUDA(cudaGetLastError());
     AppendList L{ptr<uint32_t>(wh.hx), ptr<uint32_t>(wh.hy), ptr<float>(wh.hw),
                  hcounts + C_ACCEPTED, 2u * nc};
@@ -425,8 +417,6 @@ dyg_status insert_file_run(dyg_graph *G, dyg_graph *H, const uint32_t *src, cons
     DYG_TRY(ensure(wg.hy, sizeof(uint32_t) * (size_t)n * 2));
     DYG_TRY(ensure(wg.hw, sizeof(float) * (size_t)n * 2));
     DYG_TRY(ensure(wh.keys, sizeof(unsigned long long) * (size_t)nc_max));
-    DYG_TRY(ensure(wh.flags, sizeof(uint32_t) * (size_t)nc_max));
-    DYG_TRY(ensure(wh.pos, sizeof(uint32_t) * (size_t)nc_max));
     DYG_TRY(ensure(wh.hx, sizeof(uint32_t) * (size_t)nc_max * 2));
     DYG_TRY(ensure(wh.hy, sizeof(uint32_t) * (size_t)nc_max * 2));
     DYG_TRY(ensure(wh.hw, sizeof(float) * (size_t)nc_max * 2));

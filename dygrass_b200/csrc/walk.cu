@@ -159,6 +159,46 @@ __device__ __forceinline__ uint32_t lane_pick_weighted(const uint2 *__restrict__
     return lo + last;
 }
 
+// r % d without a division (Lemire, Kaser & Kurz, "Faster Remainder by Direct
+// Computation", 2019): with M = ceil(2^64 / d), r % d is the high 64 bits of
+// (M * r mod 2^64) * d, exact for every 32-bit r and d.  The walk kernel keeps
+// M for d <= kModTable in shared memory; longer rows divide.
+constexpr uint32_t kModTable = 255;
+
+__device__ __forceinline__ uint32_t mod_direct(uint32_t r, unsigned long long M, uint32_t d) {
+    const unsigned long long low = M * r;
+    const uint32_t lo = (uint32_t)low, hi = (uint32_t)(low >> 32);
+    return (uint32_t)(((unsigned long long)hi * d + __umulhi(lo, d)) >> 32);
+}
+
+__device__ __forceinline__ uint32_t draw_mod(uint32_t r, uint32_t d, const unsigned long long *mods) {
+    return (mods && d <= kModTable) ? mod_direct(r, mods[d], d) : r % d;
+}
+
+// The uniform move from row d (deg = d.y, past the dead-end test) with draw r.
+template <bool INCR>
+__device__ __forceinline__ int move_uniform(Walker &s, uint2 d, uint32_t r,
+                                            const uint2 *__restrict__ slots, uint32_t max_steps,
+                                            float thr, bool *moved, uint2 *taken,
+                                            uint32_t *taken_at, const unsigned long long *mods) {
+    const bool first = (s.step == 1u);
+    const uint32_t deg = d.y;
+    uint32_t at = d.x + draw_mod(r, first ? deg : deg - 1u, mods);
+    uint2 sl = __ldg(slots + at);
+    if (!first) {
+        // the row's last slot is loaded beside the drawn one, not after it:
+        // some lane of a warp lands on its previous vertex in almost every
+        // step, and a dependent reload would hold the whole warp
+        const uint32_t at_last = d.x + deg - 1u;
+        const uint2 sl_last = __ldg(slots + at_last);
+        if (sl.x == s.prev) {
+            at = at_last;
+            sl = sl_last;
+        }
+    }
+    return finish_move<INCR>(s, sl, at, first, max_steps, thr, moved, taken, taken_at);
+}
+
 // One move of one walker, mirroring the reference loop body:
 //   step 1:  any neighbour, r % deg                    (main.cu:99-106)
 //   step >1: dead end if deg == 1; r % (deg - 1) and the last slot when the
@@ -171,35 +211,18 @@ __device__ __forceinline__ int step_once(Walker &s, const uint2 *__restrict__ de
                                          const uint2 *__restrict__ slots,
                                          const float *__restrict__ wts, uint32_t max_steps,
                                          float thr, uint2 key, bool *moved, uint2 *taken,
-                                         uint32_t *taken_at) {
+                                         uint32_t *taken_at,
+                                         const unsigned long long *mods = nullptr) {
     *moved = false;
     const uint2 d = __ldg(desc + s.cur);
     const uint32_t deg = d.y;
     const bool first = (s.step == 1u);
     if (first ? (deg == 0u) : (deg <= 1u)) return kFail;
     const uint32_t r = draw_next(s, key);
-    uint2 sl;
-    uint32_t at;
-    if (!WEIGHTED) {
-        const uint32_t idx = first ? (r % deg) : (r % (deg - 1u));
-        at = d.x + idx;
-        sl = __ldg(slots + at);
-        if (!first) {
-            // the row's last slot is loaded beside the drawn one, not after
-            // it: some lane of a warp lands on its previous vertex in almost
-            // every step, and a dependent reload would hold the whole warp
-            const uint32_t at_last = d.x + deg - 1u;
-            const uint2 sl_last = __ldg(slots + at_last);
-            if (sl.x == s.prev) {
-                at = at_last;
-                sl = sl_last;
-            }
-        }
-    } else {
-        at = lane_pick_weighted(slots, wts, d.x, deg, s.prev, !first, r);
-        if (at == ~0u) return kFail;
-        sl = __ldg(slots + at);
-    }
+    if (!WEIGHTED) return move_uniform<INCR>(s, d, r, slots, max_steps, thr, moved, taken, taken_at, mods);
+    const uint32_t at = lane_pick_weighted(slots, wts, d.x, deg, s.prev, !first, r);
+    if (at == ~0u) return kFail;
+    const uint2 sl = __ldg(slots + at);
     return finish_move<INCR>(s, sl, at, first, max_steps, thr, moved, taken, taken_at);
 }
 
@@ -394,11 +417,20 @@ __device__ __forceinline__ bool below_best(float R, float c) {
     return __frcp_rn(R) < c;
 }
 
+// Resident blocks per SM the register budget is sized for: 6 (40 registers)
+// for the uniform walks, 3 for the weighted ones (shared-memory segment sums).
 template <bool INCR, bool WEIGHTED, int MOVES>
 __global__ void __launch_bounds__(kWalkThreads, WEIGHTED ? 3 : 6) k_walk(WalkArgs a) {
     // per-warp segment sums of the cooperative weighted search
     __shared__ unsigned long long s_seg[WEIGHTED ? (kWalkThreads / 32) * kSegs : 1];
+    // M = ceil(2^64 / d) of the division-free remainder, d <= kModTable
+    __shared__ unsigned long long s_mod[(WEIGHTED || MOVES != 4) ? 1 : kModTable + 1];
     if (a.job.halt && *a.job.halt) return;
+    if constexpr (!WEIGHTED && MOVES == 4) {
+        for (uint32_t d = threadIdx.x; d <= kModTable; d += blockDim.x)
+            s_mod[d] = d ? ~0ull / d + 1ull : 0ull;
+        __syncthreads();
+    }
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
     const uint32_t n = a.job.n_dev ? *a.job.n_dev : a.job.n_host;
@@ -425,13 +457,12 @@ __global__ void __launch_bounds__(kWalkThreads, WEIGHTED ? 3 : 6) k_walk(WalkArg
     s.we = 0.f;
     uint32_t moves = 0u, walks = 0u;
 
-    // Walkers start only on warp iterations T = 0 mod 4.  Every walker moves
-    // once per iteration, so all of a warp's walkers then stand at steps
-    // 1 mod 4 together and draw their next Philox block in the same
-    // iteration: the block (a quarter of the kernel's instructions when
-    // computed) is run once per four iterations by the whole warp instead of
-    // in almost every iteration for a few lanes, and refills are batched.
-    // A lane waits at most three iterations; an empty warp refills at once.
+    // Walkers start only on warp iterations that keep every walker of the
+    // warp aligned to its 4-draw Philox blocks (each walker moves MOVES times
+    // per iteration): then all of them draw their next block at the same
+    // move, so the block (a quarter of the kernel's instructions when
+    // computed) runs for the whole warp at once instead of for a few lanes at
+    // a time, and refills are batched.  An empty warp refills at once.
     uint32_t T = 0u;
     while (true) {
         uint32_t free_mask = __ballot_sync(kFull, !active);
@@ -489,6 +520,11 @@ __global__ void __launch_bounds__(kWalkThreads, WEIGHTED ? 3 : 6) k_walk(WalkArg
         }
         if (!__any_sync(kFull, active)) break;
         uint32_t fc = 0u;  // conductance bits of a walker that found its target now
+        // With four moves per iteration every walker enters an iteration at a
+        // step = 1 (mod 4) (walkers start at the top of an iteration and move
+        // four times in each one they stay in), so its Philox block for the
+        // iteration is drawn once, up front, and word mv serves move mv.
+        uint4 blk = make_uint4(0u, 0u, 0u, 0u);
 #pragma unroll
         for (int mv = 0; mv < (WEIGHTED ? 1 : MOVES); ++mv) {
             int r = kContinue;
@@ -499,7 +535,18 @@ __global__ void __launch_bounds__(kWalkThreads, WEIGHTED ? 3 : 6) k_walk(WalkArg
                 r = step_weighted_warp<INCR>(s, active, a.g, a.max_steps, a.threshold, a.key,
                                              s_seg + (threadIdx.x >> 5) * kSegs, lane, &moved,
                                              &taken, &taken_at);
+            } else if (MOVES == 4 && active) {
+                const uint2 d = __ldg(a.g.desc + s.cur);
+                if (mv == 0)
+                    blk = philox4x32_10(make_uint4((s.step - 1u) >> 2, s.walker, s.c2, s.c3), a.key);
+                const uint32_t rd = mv == 0 ? blk.x : (mv == 1 ? blk.y : (mv == 2 ? blk.z : blk.w));
+                r = (s.step == 1u ? d.y == 0u : d.y <= 1u)
+                        ? kFail
+                        : move_uniform<INCR>(s, d, rd, a.g.slots, a.max_steps, a.threshold, &moved,
+                                             &taken, &taken_at, s_mod);
             } else if (active) {
+                // (the one- and two-move tuning variants divide: their
+                // register budget has no room for the table's M)
                 r = step_once<INCR, false>(s, a.g.desc, a.g.slots, a.g.wts, a.max_steps,
                                            a.threshold, a.key, &moved, &taken, &taken_at);
             }
@@ -725,12 +772,14 @@ static uint32_t chunk_for(uint32_t walkers) {
     return c;
 }
 
-template <typename K>
-static int persistent_blocks(K kernel) {
+// Resident blocks per SM, cached per kernel instance (the instances share one
+// function type but not their launch bounds).
+template <bool INCR, bool WTD, int MOVES>
+static int persistent_blocks() {
     static int per_sm = 0;
     if (!per_sm) {
         int nb = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, kWalkThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_walk<INCR, WTD, MOVES>, kWalkThreads, 0);
         per_sm = nb < 1 ? 1 : nb;
     }
     const uint32_t t = g_tune_bpsm.load();
@@ -757,17 +806,17 @@ template <bool INCR, bool WTD>
 static void launch_walk_kernel(const WalkArgs &a, cudaStream_t st) {
     if constexpr (!WTD) {
         if (walk_moves() == 2) {
-            const int grid = persistent_blocks(k_walk<INCR, WTD, 2>);
+            const int grid = persistent_blocks<INCR, WTD, 2>();
             k_walk<INCR, WTD, 2><<<grid, kWalkThreads, 0, st>>>(a);
             return;
         }
         if (walk_moves() == 4) {
-            const int grid = persistent_blocks(k_walk<INCR, WTD, 4>);
+            const int grid = persistent_blocks<INCR, WTD, 4>();
             k_walk<INCR, WTD, 4><<<grid, kWalkThreads, 0, st>>>(a);
             return;
         }
     }
-    const int grid = persistent_blocks(k_walk<INCR, WTD, 1>);
+    const int grid = persistent_blocks<INCR, WTD, 1>();
     k_walk<INCR, WTD, 1><<<grid, kWalkThreads, 0, st>>>(a);
 }
 
@@ -783,7 +832,7 @@ static void launch_walk_any(const WalkArgs &a, bool incremental, bool wtd, cudaS
 
 dyg_status launch_walk(dyg_graph *G, const WalkJob &job, const dyg_walk_params &p, bool incremental,
                        unsigned long long *keys, cudaStream_t st) {
-    WalkArgs a;
+    WalkArgs a{};
     a.g = G->g;
     a.job = job;
     a.walkers = p.walkers;
@@ -808,7 +857,7 @@ dyg_status launch_walk(dyg_graph *G, const WalkJob &job, const dyg_walk_params &
 dyg_status launch_walk_scalars(const DevGraph &g, const WalkJob &job, const dyg_walk_params &p,
                                bool incremental, unsigned long long *keys,
                                unsigned long long *scalars, cudaStream_t st) {
-    WalkArgs a;
+    WalkArgs a{};
     a.g = g;
     a.job = job;
     a.walkers = p.walkers;
