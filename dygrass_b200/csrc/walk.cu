@@ -159,31 +159,15 @@ __device__ __forceinline__ uint32_t lane_pick_weighted(const uint2 *__restrict__
     return lo + last;
 }
 
-// r % d without a division (Lemire, Kaser & Kurz, "Faster Remainder by Direct
-// Computation", 2019): with M = ceil(2^64 / d), r % d is the high 64 bits of
-// (M * r mod 2^64) * d, exact for every 32-bit r and d.  The walk kernel keeps
-// M for d <= kModTable in shared memory; longer rows divide.
-constexpr uint32_t kModTable = 255;
-
-__device__ __forceinline__ uint32_t mod_direct(uint32_t r, unsigned long long M, uint32_t d) {
-    const unsigned long long low = M * r;
-    const uint32_t lo = (uint32_t)low, hi = (uint32_t)(low >> 32);
-    return (uint32_t)(((unsigned long long)hi * d + __umulhi(lo, d)) >> 32);
-}
-
-__device__ __forceinline__ uint32_t draw_mod(uint32_t r, uint32_t d, const unsigned long long *mods) {
-    return (mods && d <= kModTable) ? mod_direct(r, mods[d], d) : r % d;
-}
-
 // The uniform move from row d (deg = d.y, past the dead-end test) with draw r.
 template <bool INCR>
 __device__ __forceinline__ int move_uniform(Walker &s, uint2 d, uint32_t r,
                                             const uint2 *__restrict__ slots, uint32_t max_steps,
                                             float thr, bool *moved, uint2 *taken,
-                                            uint32_t *taken_at, const unsigned long long *mods) {
+                                            uint32_t *taken_at) {
     const bool first = (s.step == 1u);
     const uint32_t deg = d.y;
-    uint32_t at = d.x + draw_mod(r, first ? deg : deg - 1u, mods);
+    uint32_t at = d.x + (first ? r % deg : r % (deg - 1u));
     uint2 sl = __ldg(slots + at);
     if (!first) {
         // the row's last slot is loaded beside the drawn one, not after it:
@@ -211,15 +195,14 @@ __device__ __forceinline__ int step_once(Walker &s, const uint2 *__restrict__ de
                                          const uint2 *__restrict__ slots,
                                          const float *__restrict__ wts, uint32_t max_steps,
                                          float thr, uint2 key, bool *moved, uint2 *taken,
-                                         uint32_t *taken_at,
-                                         const unsigned long long *mods = nullptr) {
+                                         uint32_t *taken_at) {
     *moved = false;
     const uint2 d = __ldg(desc + s.cur);
     const uint32_t deg = d.y;
     const bool first = (s.step == 1u);
     if (first ? (deg == 0u) : (deg <= 1u)) return kFail;
     const uint32_t r = draw_next(s, key);
-    if (!WEIGHTED) return move_uniform<INCR>(s, d, r, slots, max_steps, thr, moved, taken, taken_at, mods);
+    if (!WEIGHTED) return move_uniform<INCR>(s, d, r, slots, max_steps, thr, moved, taken, taken_at);
     const uint32_t at = lane_pick_weighted(slots, wts, d.x, deg, s.prev, !first, r);
     if (at == ~0u) return kFail;
     const uint2 sl = __ldg(slots + at);
@@ -423,14 +406,7 @@ template <bool INCR, bool WEIGHTED, int MOVES>
 __global__ void __launch_bounds__(kWalkThreads, WEIGHTED ? 3 : 6) k_walk(WalkArgs a) {
     // per-warp segment sums of the cooperative weighted search
     __shared__ unsigned long long s_seg[WEIGHTED ? (kWalkThreads / 32) * kSegs : 1];
-    // M = ceil(2^64 / d) of the division-free remainder, d <= kModTable
-    __shared__ unsigned long long s_mod[(WEIGHTED || MOVES != 4) ? 1 : kModTable + 1];
     if (a.job.halt && *a.job.halt) return;
-    if constexpr (!WEIGHTED && MOVES == 4) {
-        for (uint32_t d = threadIdx.x; d <= kModTable; d += blockDim.x)
-            s_mod[d] = d ? ~0ull / d + 1ull : 0ull;
-        __syncthreads();
-    }
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
     const uint32_t n = a.job.n_dev ? *a.job.n_dev : a.job.n_host;
@@ -543,10 +519,8 @@ __global__ void __launch_bounds__(kWalkThreads, WEIGHTED ? 3 : 6) k_walk(WalkArg
                 r = (s.step == 1u ? d.y == 0u : d.y <= 1u)
                         ? kFail
                         : move_uniform<INCR>(s, d, rd, a.g.slots, a.max_steps, a.threshold, &moved,
-                                             &taken, &taken_at, s_mod);
+                                             &taken, &taken_at);
             } else if (active) {
-                // (the one- and two-move tuning variants divide: their
-                // register budget has no room for the table's M)
                 r = step_once<INCR, false>(s, a.g.desc, a.g.slots, a.g.wts, a.max_steps,
                                            a.threshold, a.key, &moved, &taken, &taken_at);
             }
