@@ -203,6 +203,7 @@ enum Scalar : int {
     S_RECCAP = 12,    // capacity of the record buffers (follows S_RECCNT)
     S_LONG = 13,      // set by an append that made a row longer than kBigRow
     S_SCAN = 14,      // tile tickets of the single-pass scan (accumulating)
+    S_BLOCKS = 15,    // blocks of an append's sizing pass that finished (the last resets it)
     S_NSCALARS = 16
 };
 enum Count : int {
@@ -379,9 +380,11 @@ dyg_status upload_graph(dyg_graph *G, uint32_t n, const uint64_t *row_ptr, const
                         const float *w);
 dyg_status append_enqueue(dyg_graph *GA, const AppendList &A, dyg_graph *GB, const AppendList *B,
                           unsigned long long *halt, unsigned long long code, cudaStream_t st);
-dyg_status delete_enqueue(dyg_graph *G, const uint32_t *hx, const uint32_t *hy, uint32_t m,
-                          const uint8_t *mask, uint8_t *found, unsigned long long *halt,
-                          cudaStream_t st);
+// Deletes list entries (hx[i], hy[i]) from G in list order (fG[i] = 1 when
+// found), then from H the entries G found on both sides of their edge (fH).
+dyg_status delete_pair_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *hx, const uint32_t *hy,
+                               uint32_t m, uint8_t *fG, uint8_t *fH, unsigned long long *halt,
+                               cudaStream_t st);
 // Copies both graphs' scalars and counts to the host with one synchronize.
 dyg_status read_scalars2(dyg_graph *A, dyg_graph *B, cudaStream_t st);
 // Exclusive scan of in[0, m) into out; with m_dev, of in[0, min(m, *m_dev)).

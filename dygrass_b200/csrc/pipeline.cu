@@ -585,8 +585,7 @@ dyg_status decr_delete_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src,
     k_del_half_edges<<<blocks(n, 256), 256, 0, st>>>(halt, src, dst, n, G->g.n, hx, hy,
                                                       sc + S_ERR);
     count_launch();
-    DYG_TRY(delete_enqueue(G, hx, hy, m, nullptr, fG, halt, st));
-    DYG_TRY(delete_enqueue(H, hx, hy, m, fG, fH, halt, st));
+    DYG_TRY(delete_pair_enqueue(G, H, hx, hy, m, fG, fH, halt, st));
     const DelFilterOp op{fG, fH, status, cond, hx, hy, file_orient ? src : nullptr,
                          file_orient ? dst : nullptr, (unsigned long long)uid0, uids,
                          ptr<uint32_t>(ws.f_src), ptr<uint32_t>(ws.f_dst),

@@ -43,13 +43,14 @@ __device__ __forceinline__ void dev_rank(DevGraph g, const uint32_t *hx, const u
 
 // ------------------------------------------------------------------ append
 
-__device__ __forceinline__ void dev_app_need(DevGraph g, const uint32_t *hx, const uint32_t *m_dev,
-                                             uint32_t m_host, const uint32_t *rank,
-                                             const uint32_t *rowcnt, uint32_t slack, uint32_t *lneed,
-                                             unsigned long long *need_total,
-                                             const unsigned long long *halt) {
-    if (*halt) return;
+// Leaders size their rows; returns the arena slots this thread's moves need.
+__device__ __forceinline__ unsigned long long dev_app_need(DevGraph g, const uint32_t *hx,
+                                                           const uint32_t *m_dev, uint32_t m_host,
+                                                           const uint32_t *rank,
+                                                           const uint32_t *rowcnt, uint32_t slack,
+                                                           uint32_t *lneed) {
     const uint32_t m = dcount(m_dev, m_host);
+    unsigned long long total = 0ull;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
         if (rank[i] != 0u) continue;
         const uint32_t x = hx[i];
@@ -59,29 +60,30 @@ __device__ __forceinline__ void dev_app_need(DevGraph g, const uint32_t *hx, con
         if (nd > g.cap[x]) {
             need = max(2u * nd, nd + slack);
             need = (need + 1u) & ~1u;
-            atomicAdd(need_total, (unsigned long long)need);
+            total += need;
         }
         lneed[i] = need;
     }
+    return total;
 }
 
-// One thread: reserve both graphs' moves or halt.
-__global__ void k_reserve(unsigned long long *top1, uint64_t cap1, const unsigned long long *need1,
-                          unsigned long long *cursor1, unsigned long long *top2, uint64_t cap2,
-                          const unsigned long long *need2, unsigned long long *cursor2,
-                          unsigned long long *halt, unsigned long long code) {
-    if (*halt) return;
-    const bool ok1 = *top1 + *need1 <= cap1;
-    const bool ok2 = !top2 || *top2 + *need2 <= cap2;
+// Reserves the moves of one or both graphs, all or nothing, or halts.
+__device__ __forceinline__ void reserve_moves(const DevGraph &g1, unsigned long long *sc1,
+                                              const DevGraph *g2, unsigned long long *sc2,
+                                              unsigned long long *halt, unsigned long long code) {
+    const unsigned long long need1 = __ldcg(sc1 + S_NEED);
+    const unsigned long long need2 = g2 ? __ldcg(sc2 + S_NEED) : 0ull;
+    const bool ok1 = *g1.top + need1 <= g1.arena_cap;
+    const bool ok2 = !g2 || *g2->top + need2 <= g2->arena_cap;
     if (!(ok1 && ok2)) {
         *halt = code;
         return;
     }
-    *cursor1 = *top1;
-    *top1 += *need1;
-    if (top2) {
-        *cursor2 = *top2;
-        *top2 += *need2;
+    sc1[S_CURSOR] = *g1.top;
+    *g1.top += need1;
+    if (g2) {
+        sc2[S_CURSOR] = *g2->top;
+        *g2->top += need2;
     }
 }
 
@@ -338,12 +340,6 @@ __device__ __forceinline__ void dev_app_finish(DevGraph g, const uint32_t *hx, c
     }
 }
 
-__global__ void k_rank(DevGraph g, const uint32_t *hx, const uint32_t *m_dev, uint32_t m_host,
-                       uint32_t *rank, uint32_t *rowcnt, const unsigned long long *halt,
-                       unsigned long long *ran) {
-    dev_rank(g, hx, m_dev, m_host, rank, rowcnt, halt, ran);
-}
-
 // One append list and its graph.  The append kernels take two and pick one
 // by blockIdx.y, so the appends to H and to G of one batch share each launch.
 struct AppSide {
@@ -367,10 +363,32 @@ __global__ void k_app_rank(AppSides A, const unsigned long long *halt) {
     dev_rank(a.g, a.hx, a.m_dev, a.m_host, a.rank, a.rowcnt, halt, a.sc + S_OPRAN);
 }
 
-__global__ void k_app_need(AppSides A, const unsigned long long *halt) {
+// Row sizes and the graphs' arena needs; the block that finishes last (a
+// ticket taken after its needs were added, no waiting) reserves the moves of
+// both graphs, so no one-thread launch follows.
+__global__ void k_app_need(AppSides A, unsigned long long *halt, unsigned long long code) {
+    __shared__ unsigned long long s_need;
+    __shared__ bool s_last;
+    if (*halt) return;
     const AppSide &a = A.s[blockIdx.y];
-    dev_app_need(a.g, a.hx, a.m_dev, a.m_host, a.rank, a.rowcnt, a.slack, a.lneed, a.sc + S_NEED,
-                 halt);
+    if (threadIdx.x == 0) s_need = 0ull;
+    __syncthreads();
+    const unsigned long long mine =
+        dev_app_need(a.g, a.hx, a.m_dev, a.m_host, a.rank, a.rowcnt, a.slack, a.lneed);
+    if (mine) atomicAdd(&s_need, mine);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (s_need) atomicAdd(a.sc + S_NEED, s_need);
+        __threadfence();   // this block's need is counted before its ticket
+        unsigned long long *done = A.s[0].sc + S_BLOCKS;
+        s_last = atomicAdd(done, 1ull) + 1ull == (unsigned long long)gridDim.x * gridDim.y;
+        if (s_last) {
+            __threadfence();   // every block's need is visible
+            *done = 0ull;
+            reserve_moves(A.s[0].g, A.s[0].sc, gridDim.y > 1 ? &A.s[1].g : nullptr,
+                          A.s[1].sc, halt, code);
+        }
+    }
 }
 
 __global__ void k_app_move(AppSides A, const unsigned long long *halt) {
@@ -394,9 +412,10 @@ __global__ void k_app_finish(AppSides A, const unsigned long long *halt) {
 
 // Leaders take a run of `rowcnt[x]` scratch entries.  One atomic per warp:
 // the warp's requests are prefix-summed with shuffles, lane 31 takes the sum.
-__global__ void k_del_base(DevGraph g, const uint32_t *hx, uint32_t m, const uint32_t *rank,
-                           const uint32_t *rowcnt, uint32_t *rowtmp, unsigned long long *cursor,
-                           const unsigned long long *halt) {
+__device__ __forceinline__ void dev_del_base(const uint32_t *hx, uint32_t m, const uint32_t *rank,
+                                             const uint32_t *rowcnt, uint32_t *rowtmp,
+                                             unsigned long long *cursor,
+                                             const unsigned long long *halt) {
     if (*halt) return;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -422,14 +441,44 @@ __global__ void k_del_base(DevGraph g, const uint32_t *hx, uint32_t m, const uin
     }
 }
 
-__global__ void k_del_scatter(DevGraph g, const uint32_t *hx, uint32_t m, const uint32_t *rank,
-                              const uint32_t *rowtmp, uint32_t *tmp,
-                              const unsigned long long *halt) {
+__device__ __forceinline__ void dev_del_scatter(DevGraph g, const uint32_t *hx, uint32_t m,
+                                                const uint32_t *rank, const uint32_t *rowtmp,
+                                                uint32_t *tmp, const unsigned long long *halt) {
     if (*halt) return;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
         const uint32_t x = hx[i];
         if (x < g.n) tmp[rowtmp[x] + rank[i]] = i;
     }
+}
+
+// The deletion list's graphs (G, then H): their ranks, scratch runs and
+// scatters do not depend on each other, so both share each launch
+// (blockIdx.y picks the graph); only H's removal waits for G's found flags.
+struct DelSide {
+    DevGraph g;
+    uint32_t *rank, *rowcnt, *rowtmp, *dtmp;
+    unsigned long long *cursor;
+};
+struct DelSides {
+    DelSide s[2];
+};
+
+__global__ void k_del_rank(DelSides D, const uint32_t *hx, uint32_t m,
+                           const unsigned long long *halt) {
+    const DelSide &d = D.s[blockIdx.y];
+    dev_rank(d.g, hx, nullptr, m, d.rank, d.rowcnt, halt, nullptr);
+}
+
+__global__ void k_del_base(DelSides D, const uint32_t *hx, uint32_t m,
+                           const unsigned long long *halt) {
+    const DelSide &d = D.s[blockIdx.y];
+    dev_del_base(hx, m, d.rank, d.rowcnt, d.rowtmp, d.cursor, halt);
+}
+
+__global__ void k_del_scatter(DelSides D, const uint32_t *hx, uint32_t m,
+                              const unsigned long long *halt) {
+    const DelSide &d = D.s[blockIdx.y];
+    dev_del_scatter(d.g, hx, m, d.rank, d.rowtmp, d.dtmp, halt);
 }
 
 // Leaders remove their row's entries in list order.  With `mask`, entry
@@ -726,13 +775,7 @@ dyg_status append_enqueue(dyg_graph *GA, const AppendList &A, dyg_graph *GB, con
     const dim3 grid(grid_for(m_max), ns);
     k_app_rank<<<grid, 256, 0, st>>>(S, halt);
     count_launch();
-    k_app_need<<<grid, 256, 0, st>>>(S, halt);
-    count_launch();
-    unsigned long long *s1 = ptr<unsigned long long>(GA->ws.scalars);
-    unsigned long long *s2 = gs[1] ? ptr<unsigned long long>(gs[1]->ws.scalars) : nullptr;
-    k_reserve<<<1, 1, 0, st>>>(GA->g.top, GA->g.arena_cap, s1 + S_NEED, s1 + S_CURSOR,
-                               s2 ? gs[1]->g.top : nullptr, s2 ? gs[1]->g.arena_cap : 0,
-                               s2 ? s2 + S_NEED : nullptr, s2 ? s2 + S_CURSOR : nullptr, halt, code);
+    k_app_need<<<grid, 256, 0, st>>>(S, halt, code);
     count_launch();
     k_app_move<<<grid, 256, 0, st>>>(S, halt);
     count_launch();
@@ -753,39 +796,51 @@ dyg_status append_enqueue(dyg_graph *GA, const AppendList &A, dyg_graph *GB, con
 }
 
 // Deletes the half-edges of a list whose length m is known on the host.
-dyg_status delete_enqueue(dyg_graph *G, const uint32_t *hx, const uint32_t *hy, uint32_t m,
-                          const uint8_t *mask, uint8_t *found, unsigned long long *halt,
-                          cudaStream_t st) {
+dyg_status delete_pair_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *hx, const uint32_t *hy,
+                               uint32_t m, uint8_t *fG, uint8_t *fH, unsigned long long *halt,
+                               cudaStream_t st) {
     if (m == 0) return DYG_OK;
-    DYG_TRY(rowops_ensure(G, m));
-    unsigned long long *sc = ptr<unsigned long long>(G->ws.scalars);
-    // [long-row count,] scratch cursor
-    if (G->long_rows)
-        DYG_CUDA(cudaMemsetAsync(sc + S_NBIG, 0, sizeof(unsigned long long) * 2, st));
-    else
-        DYG_CUDA(cudaMemsetAsync(sc + S_TMPCUR, 0, sizeof(unsigned long long), st));
-    DYG_CUDA(cudaMemsetAsync(found, 0, m, st));
+    dyg_graph *gs[2] = {G, H};
+    DelSides D{};
+    for (int k = 0; k < 2; ++k) {
+        dyg_graph *X = gs[k];
+        DYG_TRY(rowops_ensure(X, m));
+        unsigned long long *sc = ptr<unsigned long long>(X->ws.scalars);
+        // [long-row count,] scratch cursor
+        if (X->long_rows)
+            DYG_CUDA(cudaMemsetAsync(sc + S_NBIG, 0, sizeof(unsigned long long) * 2, st));
+        else
+            DYG_CUDA(cudaMemsetAsync(sc + S_TMPCUR, 0, sizeof(unsigned long long), st));
+        D.s[k] = DelSide{X->g, ptr<uint32_t>(X->ws.rank), ptr<uint32_t>(X->ws.rowcnt),
+                         ptr<uint32_t>(X->ws.rowtmp), ptr<uint32_t>(X->ws.dtmp), sc + S_TMPCUR};
+    }
+    DYG_CUDA(cudaMemsetAsync(fG, 0, m, st));
+    DYG_CUDA(cudaMemsetAsync(fH, 0, m, st));
     const int gr = grid_for(m);
-    k_rank<<<gr, 256, 0, st>>>(G->g, hx, nullptr, m, ptr<uint32_t>(G->ws.rank),
-                               ptr<uint32_t>(G->ws.rowcnt), halt, nullptr);
+    const dim3 grid2(gr, 2);
+    k_del_rank<<<grid2, 256, 0, st>>>(D, hx, m, halt);
     count_launch();
-    k_del_base<<<gr, 256, 0, st>>>(G->g, hx, m, ptr<uint32_t>(G->ws.rank),
-                                   ptr<uint32_t>(G->ws.rowcnt), ptr<uint32_t>(G->ws.rowtmp),
-                                   sc + S_TMPCUR, halt);
+    k_del_base<<<grid2, 256, 0, st>>>(D, hx, m, halt);
     count_launch();
-    k_del_scatter<<<gr, 256, 0, st>>>(G->g, hx, m, ptr<uint32_t>(G->ws.rank),
-                                      ptr<uint32_t>(G->ws.rowtmp), ptr<uint32_t>(G->ws.dtmp), halt);
+    k_del_scatter<<<grid2, 256, 0, st>>>(D, hx, m, halt);
     count_launch();
-    k_del_apply<<<gr, 256, 0, st>>>(G->g, hx, hy, m, ptr<uint32_t>(G->ws.rank),
-                                    ptr<uint32_t>(G->ws.rowcnt), ptr<uint32_t>(G->ws.rowtmp),
-                                    ptr<uint32_t>(G->ws.dtmp), mask, found, ptr<uint4>(G->ws.big),
-                                    sc + S_NBIG, G->long_rows, halt);
-    count_launch();
-    if (G->long_rows) {
-        k_del_apply_big<<<num_sms() * 2, kBigThreads, 0, st>>>(
-            G->g, hx, hy, m, ptr<uint32_t>(G->ws.rowcnt), ptr<uint32_t>(G->ws.rowtmp),
-            ptr<uint32_t>(G->ws.dtmp), mask, found, ptr<uint4>(G->ws.big), sc + S_NBIG, halt);
+    for (int k = 0; k < 2; ++k) {
+        // H's entries only where G found the edge on both sides
+        dyg_graph *X = gs[k];
+        const uint8_t *mask = k ? fG : nullptr;
+        uint8_t *found = k ? fH : fG;
+        unsigned long long *sc = ptr<unsigned long long>(X->ws.scalars);
+        k_del_apply<<<gr, 256, 0, st>>>(X->g, hx, hy, m, ptr<uint32_t>(X->ws.rank),
+                                        ptr<uint32_t>(X->ws.rowcnt), ptr<uint32_t>(X->ws.rowtmp),
+                                        ptr<uint32_t>(X->ws.dtmp), mask, found,
+                                        ptr<uint4>(X->ws.big), sc + S_NBIG, X->long_rows, halt);
         count_launch();
+        if (X->long_rows) {
+            k_del_apply_big<<<num_sms() * 2, kBigThreads, 0, st>>>(
+                X->g, hx, hy, m, ptr<uint32_t>(X->ws.rowcnt), ptr<uint32_t>(X->ws.rowtmp),
+                ptr<uint32_t>(X->ws.dtmp), mask, found, ptr<uint4>(X->ws.big), sc + S_NBIG, halt);
+            count_launch();
+        }
     }
     DYG_CUDA(cudaGetLastError());
     return DYG_OK;

@@ -289,6 +289,64 @@ struct StAcceptOp {
     __device__ void last(uint32_t total) const { counts[C_ACCEPTED] = 2u * total; }
 };
 
+// Files of up to kSortSmall edges are grouped by one block: a bitonic sort
+// of (key, file index) pairs in shared memory.  The pairs are distinct, so
+// the order is the one a stable sort by key gives (equal keys in file order,
+// self-loop keys ~0 last), which is what the radix sort of larger files
+// gives, in one launch instead of six.
+constexpr uint32_t kSortSmall = 8192;
+constexpr int kSortThreads = 1024;
+
+__global__ void __launch_bounds__(kSortThreads)
+k_sort_small(const unsigned long long *key, const uint32_t *val, uint32_t n,
+             unsigned long long *skey, uint32_t *sval) {
+    extern __shared__ unsigned long long s_key[];   // N keys, then N values
+    uint32_t N = 1;
+    while (N < n) N <<= 1;
+    uint32_t *s_val = reinterpret_cast<uint32_t *>(s_key + N);
+    for (uint32_t i = threadIdx.x; i < N; i += blockDim.x) {
+        s_key[i] = i < n ? key[i] : ~0ull;
+        s_val[i] = i < n ? val[i] : ~0u;   // padding sorts after every entry
+    }
+    __syncthreads();
+    for (uint32_t k = 2; k <= N; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = threadIdx.x; i < N; i += blockDim.x) {
+                const uint32_t p = i ^ j;
+                if (p <= i) continue;
+                const unsigned long long ka = s_key[i], kb = s_key[p];
+                const uint32_t va = s_val[i], vb = s_val[p];
+                const bool gt = ka > kb || (ka == kb && va > vb);
+                if (gt == ((i & k) == 0u)) {
+                    s_key[i] = kb;
+                    s_key[p] = ka;
+                    s_val[i] = vb;
+                    s_val[p] = va;
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        skey[i] = s_key[i];
+        sval[i] = s_val[i];
+    }
+}
+
+dyg_status sort_small_enqueue(const unsigned long long *key, const uint32_t *val, uint32_t n,
+                              unsigned long long *skey, uint32_t *sval, cudaStream_t st) {
+    uint32_t N = 1;
+    while (N < n) N <<= 1;
+    const size_t bytes = (size_t)N * (sizeof(unsigned long long) + sizeof(uint32_t));
+    if (bytes > 48u * 1024u)   // the attribute belongs to the current device
+        DYG_CUDA(cudaFuncSetAttribute(k_sort_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)bytes));
+    k_sort_small<<<1, kSortThreads, bytes, st>>>(key, val, n, skey, sval);
+    count_launch();
+    DYG_CUDA(cudaGetLastError());
+    return DYG_OK;
+}
+
 uint32_t key_bits(uint32_t nv) {
     uint32_t b = 1;
     while (b < 32 && (nv - 1u) >> b) ++b;
@@ -318,15 +376,20 @@ dyg_status insert_prep_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src,
                                                               sc + S_NBIG, ptr<uint4>(ws.st_pos));
         count_launch();
     }
-    size_t tmp = 0;
-    DYG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, key, skey, val, sval, (int)n, 0,
-                                             (int)(2 * nb), st));
-    DYG_TRY(ensure(ws.cub_tmp, tmp));
-    tmp = ws.cub_tmp.bytes;
-    // keys ~0 (self-loops) have all bits set: sorting on the low 2*nb bits
-    // still places them after every real key (each real key is < 2^(2nb) - 1)
-    DYG_CUDA(cub::DeviceRadixSort::SortPairs(ws.cub_tmp.p, tmp, key, skey, val, sval, (int)n, 0,
-                                             (int)(2 * nb), st));
+    if (n <= kSortSmall) {
+        DYG_TRY(sort_small_enqueue(key, val, n, skey, sval, st));
+    } else {
+        size_t tmp = 0;
+        DYG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, key, skey, val, sval, (int)n, 0,
+                                                 (int)(2 * nb), st));
+        DYG_TRY(ensure(ws.cub_tmp, tmp));
+        tmp = ws.cub_tmp.bytes;
+        // keys ~0 (self-loops) have all bits set: sorting on the low 2*nb
+        // bits still places them after every real key (each real key is
+        // < 2^(2nb) - 1)
+        DYG_CUDA(cub::DeviceRadixSort::SortPairs(ws.cub_tmp.p, tmp, key, skey, val, sval, (int)n, 0,
+                                                 (int)(2 * nb), st));
+    }
     k_st_merge<<<blocks(n, 256), 256, 0, st>>>(halt, G->g, H->g, skey, sval, n,
                                                 ptr<uint4>(ws.st_pos), w, nflag,
                                                 ptr<float>(ws.st_wapp), status, cond);

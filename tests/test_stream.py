@@ -195,6 +195,24 @@ def test_gpu_insert_file_parity(dyg, oracle, chunk):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("n_file", [8192, 9000])
+def test_gpu_insert_file_sizes(dyg, oracle, n_file):
+    """Files of up to 8,192 edges are grouped by a one-block sort in shared
+    memory, larger ones by a radix sort: both must give the oracle's merges,
+    walks and rows (a file of exactly 8,192 edges fills the one-block sort)."""
+    n_new = n_file - 115   # insert_file adds 115 repeats, merges and self-loops
+    wl = W.grid_2d(150, 150, inserts=n_new, walkers=64)
+    rng = np.random.default_rng(13)
+    G, H, Go, Ho = both(dyg, oracle, wl.n, (wl.g_src, wl.g_dst, wl.g_w),
+                        (wl.h_src, wl.h_dst, wl.h_w))
+    s, d, w = insert_file(wl, rng, n_new)
+    assert len(s) == n_file
+    r = apply_both(dyg, oracle, G, H, Go, Ho, INS, s, d, w, wl.params, uid0=77)
+    assert (r.status == MERGED).sum() >= 100
+    assert (r.status == SELF_LOOP).sum() == 5
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("chunk", [0, 41])
 def test_gpu_delete_file_parity(dyg, oracle, chunk):
     wl = W.mesh_3d(10, inserts=500)
