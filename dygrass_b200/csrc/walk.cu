@@ -412,6 +412,7 @@ __global__ void __launch_bounds__(kWalkThreads, WEIGHTED ? 3 : 6) k_walk(WalkArg
     const uint32_t n = a.job.n_dev ? *a.job.n_dev : a.job.n_host;
     const uint32_t CW = a.chunk;                // walkers per chunk (divides walkers)
     const uint32_t cpe = a.walkers / CW;        // chunks per edge
+    const uint32_t cpe_sh = (cpe & (cpe - 1u)) ? 32u : (uint32_t)(__ffs(cpe) - 1);
     const unsigned long long n_chunks = (unsigned long long)n * cpe;
     unsigned long long *work = a.scalars + S_WORK;
 
@@ -457,7 +458,11 @@ __global__ void __launch_bounds__(kWalkThreads, WEIGHTED ? 3 : 6) k_walk(WalkArg
                     exhausted = true;
                     break;
                 }
-                const uint32_t e = (uint32_t)(c / cpe);
+                // chunk c = edge e, part c mod cpe (cpe is a power of two
+                // whenever the walker count is one)
+                const uint32_t e = (c >> 32) ? (uint32_t)(c / cpe)
+                                             : (cpe_sh < 32u ? (uint32_t)c >> cpe_sh
+                                                             : (uint32_t)c / cpe);
                 if (e != ce) {
                     pe = ce;
                     pe_best = ce_best;
@@ -491,7 +496,8 @@ __global__ void __launch_bounds__(kWalkThreads, WEIGHTED ? 3 : 6) k_walk(WalkArg
                     active = true;
                 }
             }
-            for (uint32_t i = 0; i < take; ++i) free_mask &= free_mask - 1u;
+            // the lanes that took a walker leave the free mask
+            free_mask = __ballot_sync(kFull, ((free_mask >> lane) & 1u) && rank >= take);
             c_next += take;
         }
         if (!__any_sync(kFull, active)) break;
