@@ -289,59 +289,113 @@ struct StAcceptOp {
     __device__ void last(uint32_t total) const { counts[C_ACCEPTED] = 2u * total; }
 };
 
-// Files of up to kSortSmall edges are grouped by one block: a bitonic sort
-// of (key, file index) pairs in shared memory.  The pairs are distinct, so
-// the order is the one a stable sort by key gives (equal keys in file order,
-// self-loop keys ~0 last), which is what the radix sort of larger files
-// gives, in one launch instead of six.
-constexpr uint32_t kSortSmall = 8192;
-constexpr int kSortThreads = 1024;
+// Files of up to kSortSmall edges are grouped by one block: a bitonic sort of
+// words (key << 13 | file index), so equal keys stay in file order -- the
+// order the radix sort of larger files gives -- and self-loop keys (~0),
+// mapped to the largest 2nb-bit key, come last; in one launch instead of six.
+// Each thread holds kSortE consecutive words: partners closer than kSortE
+// are compared in registers, closer than 32 kSortE through warp shuffles,
+// and only the farther ones through shared memory.
+constexpr uint32_t kSortSmall = 8192;   // file indices fit 13 bits
+constexpr uint32_t kSortE = 8;
 
-__global__ void __launch_bounds__(kSortThreads)
-k_sort_small(const unsigned long long *key, const uint32_t *val, uint32_t n,
-             unsigned long long *skey, uint32_t *sval) {
-    extern __shared__ unsigned long long s_key[];   // N keys, then N values
-    uint32_t N = 1;
-    while (N < n) N <<= 1;
-    uint32_t *s_val = reinterpret_cast<uint32_t *>(s_key + N);
-    for (uint32_t i = threadIdx.x; i < N; i += blockDim.x) {
-        s_key[i] = i < n ? key[i] : ~0ull;
-        s_val[i] = i < n ? val[i] : ~0u;   // padding sorts after every entry
-    }
-    __syncthreads();
-    for (uint32_t k = 2; k <= N; k <<= 1) {
-        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-            for (uint32_t i = threadIdx.x; i < N; i += blockDim.x) {
-                const uint32_t p = i ^ j;
-                if (p <= i) continue;
-                const unsigned long long ka = s_key[i], kb = s_key[p];
-                const uint32_t va = s_val[i], vb = s_val[p];
-                const bool gt = ka > kb || (ka == kb && va > vb);
-                if (gt == ((i & k) == 0u)) {
-                    s_key[i] = kb;
-                    s_key[p] = ka;
-                    s_val[i] = vb;
-                    s_val[p] = va;
-                }
+__device__ __forceinline__ unsigned long long sort_keep(unsigned long long mine,
+                                                        unsigned long long other, uint32_t i,
+                                                        uint32_t j, uint32_t k) {
+    // element i keeps the smaller word when it is the lower one of an
+    // ascending pair or the upper one of a descending pair
+    return (((i & j) == 0u) == ((i & k) == 0u)) ? min(mine, other) : max(mine, other);
+}
+
+template <uint32_t J>
+__device__ __forceinline__ void sort_in_thread(unsigned long long (&v)[kSortE], uint32_t t,
+                                               uint32_t k) {
+#pragma unroll
+    for (uint32_t e = 0; e < kSortE; ++e) {
+        constexpr uint32_t kJ = J;
+        const uint32_t p = e ^ kJ;
+        if (p > e) {
+            const bool asc = ((t * kSortE + e) & k) == 0u;
+            const unsigned long long a = v[e], b = v[p];
+            if ((a > b) == asc) {
+                v[e] = b;
+                v[p] = a;
             }
-            __syncthreads();
         }
-    }
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-        skey[i] = s_key[i];
-        sval[i] = s_val[i];
     }
 }
 
-dyg_status sort_small_enqueue(const unsigned long long *key, const uint32_t *val, uint32_t n,
+__global__ void __launch_bounds__(kSortSmall / kSortE)
+k_sort_small(const unsigned long long *key, uint32_t n, uint32_t N, uint32_t kbits,
+             unsigned long long *skey, uint32_t *sval) {
+    extern __shared__ unsigned long long s_w[];   // N words
+    const uint32_t t = threadIdx.x;
+    const unsigned long long kmax = (1ull << kbits) - 1ull;   // above every real key
+    for (uint32_t i = t; i < N; i += blockDim.x) {
+        unsigned long long w = ~0ull;   // padding sorts after every entry
+        if (i < n) {
+            const unsigned long long k = key[i];
+            w = ((k == ~0ull ? kmax : k) << 13) | i;
+        }
+        s_w[i] = w;
+    }
+    __syncthreads();
+    unsigned long long v[kSortE];
+#pragma unroll
+    for (uint32_t e = 0; e < kSortE; ++e) v[e] = s_w[t * kSortE + e];
+    for (uint32_t k = 2; k <= N; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            if (j >= 32u * kSortE) {
+                __syncthreads();   // the last readers of s_w are done
+#pragma unroll
+                for (uint32_t e = 0; e < kSortE; ++e) s_w[t * kSortE + e] = v[e];
+                __syncthreads();
+#pragma unroll
+                for (uint32_t e = 0; e < kSortE; ++e) {
+                    const uint32_t i = t * kSortE + e;
+                    v[e] = sort_keep(v[e], s_w[i ^ j], i, j, k);
+                }
+            } else if (j >= kSortE) {
+                const uint32_t d = j / kSortE;   // partner lane offset
+#pragma unroll
+                for (uint32_t e = 0; e < kSortE; ++e) {
+                    const unsigned long long o = __shfl_xor_sync(0xFFFFFFFFu, v[e], d);
+                    v[e] = sort_keep(v[e], o, t * kSortE + e, j, k);
+                }
+            } else if (j == 4u) {
+                sort_in_thread<4>(v, t, k);
+            } else if (j == 2u) {
+                sort_in_thread<2>(v, t, k);
+            } else {
+                sort_in_thread<1>(v, t, k);
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (uint32_t e = 0; e < kSortE; ++e) s_w[t * kSortE + e] = v[e];
+    __syncthreads();
+    for (uint32_t i = t; i < n; i += blockDim.x) {
+        const unsigned long long w = s_w[i];
+        const unsigned long long k = w >> 13;
+        skey[i] = k == kmax ? ~0ull : k;
+        sval[i] = (uint32_t)(w & 0x1FFFu);
+    }
+}
+
+// The one-block sort applies to files of up to kSortSmall edges whose keys
+// (2 nb bits) and file indices (13 bits) fit one word below the padding.
+bool sort_small_fits(uint32_t n, uint32_t nb) { return n <= kSortSmall && 2u * nb + 13u <= 63u; }
+
+dyg_status sort_small_enqueue(const unsigned long long *key, uint32_t n, uint32_t nb,
                               unsigned long long *skey, uint32_t *sval, cudaStream_t st) {
-    uint32_t N = 1;
+    uint32_t N = 32u * kSortE;
     while (N < n) N <<= 1;
-    const size_t bytes = (size_t)N * (sizeof(unsigned long long) + sizeof(uint32_t));
+    const size_t bytes = (size_t)N * sizeof(unsigned long long);
     if (bytes > 48u * 1024u)   // the attribute belongs to the current device
         DYG_CUDA(cudaFuncSetAttribute(k_sort_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)bytes));
-    k_sort_small<<<1, kSortThreads, bytes, st>>>(key, val, n, skey, sval);
+    k_sort_small<<<1, N / kSortE, bytes, st>>>(key, n, N, 2u * nb, skey, sval);
     count_launch();
     DYG_CUDA(cudaGetLastError());
     return DYG_OK;
@@ -376,8 +430,8 @@ dyg_status insert_prep_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src,
                                                               sc + S_NBIG, ptr<uint4>(ws.st_pos));
         count_launch();
     }
-    if (n <= kSortSmall) {
-        DYG_TRY(sort_small_enqueue(key, val, n, skey, sval, st));
+    if (sort_small_fits(n, nb)) {
+        DYG_TRY(sort_small_enqueue(key, n, nb, skey, sval, st));   // values are file indices
     } else {
         size_t tmp = 0;
         DYG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, key, skey, val, sval, (int)n, 0,
