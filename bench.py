@@ -87,7 +87,8 @@ def parse():
     ap.add_argument("--rgg-graphs", type=int, default=256)
     ap.add_argument("--rgg-n-hi", type=int, default=200_000)
     ap.add_argument("--tune-walkers", action="store_true",
-                    help="let the autotuner lower the walker count at equal kappa")
+                    help="let the autotuner lower the walker count and the walk length at equal "
+                         "kappa (within 5 %% of the workload's own parameters on sample graphs)")
     ap.add_argument("--rmat-scale", type=int, default=20)
     ap.add_argument("--rmat-updates", type=int, default=500_000)
     ap.add_argument("--mesh-k", type=int, default=100)
@@ -713,11 +714,10 @@ def run_many(args, rank, world, local_rank):
     W = make_workload(args, rank, world)
     p = W.params
     best, trials = autotune(W.cases, params=p, chunks=(32, 64), blocks=(0, 4),
-                            walkers=(128, 256) if args.tune_walkers else (), repeats=2,
+                            walkers=(128, 256) if args.tune_walkers else (),
+                            max_steps=(48, 64, 80) if args.tune_walkers else (), repeats=2,
                             device=local_rank, sync=torch.cuda.synchronize)
-    if best["walkers"] != p.walkers:
-        p = dyg.WalkParams.make(threshold=p.threshold, walkers=best["walkers"],
-                                max_steps=p.max_steps, seed=p.seed)
+    p = best["params"]
     M = ManyGraphs(W.cases, device=local_rank)
     plan = M.plan()
     H0, G0 = M.H.clone(), M.G.clone()
@@ -859,7 +859,9 @@ def run_many(args, rank, world, local_rank):
         "dom_kernel": "k_walk<1,0>",
         "dom_bytes_per_launch": dom_bytes(prof, incr_moves, 0.0, args.steps),
         "dom_ms_per_launch": dom_ms(prof),
-        "plain_ms_per_step": plain_ms, "tuned": best, "tune_trials": trials, "W": W,
+        "plain_ms_per_step": plain_ms,
+        "tuned": {k: v for k, v in best.items() if k != "params"},
+        "tune_trials": [{k: v for k, v in t.items() if k != "params"} for t in trials], "W": W,
     }
     for g in (H0, G0):
         g.close()

@@ -211,17 +211,45 @@ __global__ void k_new_caps(DevGraph g, uint32_t slack, uint32_t *caps) {
     caps[v] = (deg == 0u && g.cap[v] == 0u) ? 0u : deg + slack;
 }
 
+// One warp per row: consecutive lanes copy consecutive slots into the new
+// arena, four loads per lane issued before their stores (the new arena never
+// overlaps the old one).  Lane 0 reads the descriptor and hands it to the
+// warp before it rewrites it.
 __global__ void k_move_rows(DevGraph g, uint2 *ns, float *nw, const uint32_t *off,
                             const uint32_t *caps) {
-    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= g.n) return;
-    const uint2 d = g.desc[v];
-    for (uint32_t j = 0; j < d.y; ++j) {
-        ns[off[v] + j] = g.slots[d.x + j];
-        nw[off[v] + j] = g.wts[d.x + j];
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < g.n; v += warps) {
+        uint2 d = make_uint2(0u, 0u);
+        if (lane == 0u) d = g.desc[v];
+        d.x = __shfl_sync(kFull, d.x, 0);
+        d.y = __shfl_sync(kFull, d.y, 0);
+        const uint32_t o = off[v];
+        for (uint32_t j0 = 0; j0 < d.y; j0 += 128u) {
+            uint2 sv[4];
+            float wv[4];
+#pragma unroll
+            for (uint32_t u = 0; u < 4u; ++u) {
+                const uint32_t j = j0 + lane + 32u * u;
+                if (j < d.y) {
+                    sv[u] = g.slots[d.x + j];
+                    wv[u] = g.wts[d.x + j];
+                }
+            }
+#pragma unroll
+            for (uint32_t u = 0; u < 4u; ++u) {
+                const uint32_t j = j0 + lane + 32u * u;
+                if (j < d.y) {
+                    ns[o + j] = sv[u];
+                    nw[o + j] = wv[u];
+                }
+            }
+        }
+        if (lane == 0u) {
+            g.desc[v] = make_uint2(o, d.y);
+            g.cap[v] = caps[v];
+        }
     }
-    g.desc[v] = make_uint2(off[v], d.y);
-    g.cap[v] = caps[v];
 }
 
 dyg_status compact_graph(dyg_graph *G, cudaStream_t st) {
@@ -253,7 +281,8 @@ dyg_status compact_graph(dyg_graph *G, cudaStream_t st) {
         set_error("cudaMalloc during compaction failed");
         return DYG_ENOMEM;
     }
-    k_move_rows<<<gr, th, 0, st>>>(G->g, ns, nw, ptr<uint32_t>(ws.pos), ptr<uint32_t>(ws.flags));
+    k_move_rows<<<num_sms() * 8, th, 0, st>>>(G->g, ns, nw, ptr<uint32_t>(ws.pos),
+                                              ptr<uint32_t>(ws.flags));
     count_launch();
     DYG_CUDA(cudaGetLastError());
     unsigned long long top = used;

@@ -156,13 +156,16 @@ def _timed(fn, sync):
 
 
 def autotune(cases, plan_streams=None, params: WalkParams | None = None,
-             chunks=(32, 64, 128), blocks=(0, 5, 4), walkers=(), kappa_graphs: int = 4,
-             kappa_tol: float = 0.05, repeats: int = 2, device: int = -1, sync=lambda: None):
-    """Times the rounds of the cases' streams for each launch shape (and each
-    walker count in `walkers`, accepted only if the mean kappa of the
-    `kappa_graphs` smallest graphs stays within kappa_tol of params.walkers'
-    value).  Returns (best dict, list of all measurements).  Leaves the best
-    launch shape set (tune_set)."""
+             chunks=(32, 64, 128), blocks=(0, 5, 4), walkers=(), max_steps=(),
+             kappa_graphs: int = 4, kappa_tol: float = 0.05, repeats: int = 2, device: int = -1,
+             sync=lambda: None):
+    """Times the rounds of the cases' streams for each launch shape, then each
+    walker count in `walkers` and each walk length in `max_steps` (below the
+    parameters' own), each accepted only if the mean kappa of the
+    `kappa_graphs` smallest graphs stays within kappa_tol of the value at the
+    parameters' own walker count and walk length.  Returns (best dict, list of
+    all measurements); the best dict's "params" are the walk parameters to
+    use.  Leaves the best launch shape set (tune_set)."""
     params = params or WalkParams.make()
     trials = []
     M = ManyGraphs(cases, device=device)
@@ -189,7 +192,9 @@ def autotune(cases, plan_streams=None, params: WalkParams | None = None,
             trials.append({"walkers": params.walkers, "chunk": chunk, "blocks_per_sm": b,
                            "seconds": measure(params, chunk, b)})
     best = min(trials, key=lambda t: t["seconds"])
-    if walkers:
+    best["params"] = params
+    best["max_steps"] = params.max_steps
+    if walkers or max_steps:
         small = sorted(range(len(cases)), key=lambda i: cases[i].n)[:kappa_graphs]
 
         def mean_kappa(p):
@@ -211,15 +216,22 @@ def autotune(cases, plan_streams=None, params: WalkParams | None = None,
 
         k_ref = mean_kappa(params)
         best["kappa"] = k_ref
-        for wk in walkers:
-            if wk >= params.walkers or wk % 32:
-                continue
-            p = WalkParams.make(threshold=params.threshold, walkers=wk, max_steps=params.max_steps,
-                                heuristic_walkers=params.heuristic_walkers, seed=params.seed)
+        # walker counts at the full walk length, then walk lengths at the
+        # walker count chosen so far
+        options = [(wk, params.max_steps) for wk in walkers
+                   if wk < params.walkers and wk % 32 == 0]
+        options += [(None, ms) for ms in max_steps if 0 < ms < params.max_steps]
+        for wk, ms in options:
+            wk = best["walkers"] if wk is None else wk
+            p = WalkParams.make(threshold=params.threshold, walkers=wk, max_steps=ms,
+                                heuristic_walkers=params.heuristic_walkers,
+                                transition=params.transition, flags=params.flags,
+                                seed=params.seed)
             k = mean_kappa(p)
             chunk = best["chunk"] if wk % best["chunk"] == 0 else 32
-            t = {"walkers": wk, "chunk": chunk, "blocks_per_sm": best["blocks_per_sm"],
-                 "kappa": k, "kappa_ok": abs(k - k_ref) <= kappa_tol * k_ref}
+            t = {"walkers": wk, "max_steps": ms, "chunk": chunk,
+                 "blocks_per_sm": best["blocks_per_sm"], "kappa": k,
+                 "kappa_ok": abs(k - k_ref) <= kappa_tol * k_ref, "params": p}
             t["seconds"] = measure(p, chunk, best["blocks_per_sm"])
             trials.append(t)
             if t["kappa_ok"] and t["seconds"] < best["seconds"]:

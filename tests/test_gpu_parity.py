@@ -317,6 +317,34 @@ def test_compaction_and_snapshots(dyg, oracle):
     assert np.array_equal(r1.accepted, r2.accepted)
 
 
+def test_compaction_long_rows(dyg, oracle):
+    """Compaction moves each row with one warp, 128 slots per pass: a hub row
+    of 9,000 slots (71 passes) and rows of 1 to 3 slots keep their contents
+    and order, and later updates agree with the oracle."""
+    n, gs, gd, gw, hs, hd, hw, es, ed, ew = hub_graph(9000, 21)
+    G = dyg.Graph.from_edges(n, gs, gd, gw, slack_per_row=3, arena_headroom=0.5)
+    Go = oracle.OGraph(n, gs, gd, gw)
+    H = dyg.Graph.from_edges(n, hs, hd, hw)
+    Ho = oracle.OGraph(n, hs, hd, hw)
+    before = G.export()
+    G.compact()
+    after = G.export()
+    for a, b in zip(before, after):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert G.info()["arena_used"] <= sum(len(x) for x in before[1:2]) + 3 * n
+    # deletions of hub edges on the compacted G (walks through the hub)
+    rng = np.random.default_rng(8)
+    k = rng.choice(9000, 30, replace=False)
+    ds, dd = np.zeros(30, np.uint32), (k + 1).astype(np.uint32)
+    pd = dyg.WalkParams.make(walkers=64, max_steps=20)
+    d = dyg.decremental_stream(G, H, ds, dd, pd)
+    st, _, rx, ry, _, _ = oracle.decremental(Go, Ho, ds, dd, pd)
+    assert np.array_equal(d.status, st)
+    assert np.array_equal(d.rec_src, rx) and np.array_equal(d.rec_dst, ry)
+    same_graph(G, Go)
+    same_graph(H, Ho)
+
+
 def hub_graph(n_leaves, seed, huge=0):
     """A hub joined to every leaf, plus a ring through the leaves; weights
     U[0.5, 2] except the hub edges to the first 50 leaves (100; the first

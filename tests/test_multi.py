@@ -78,12 +78,20 @@ def test_autotune(dyg):
     cases, p = W.rgg_many(k=6, n_lo=300, n_hi=3000, walkers=128, seed=5)
     try:
         best, trials = autotune(cases, params=p, chunks=(32, 64), blocks=(0, 4), walkers=(64,),
-                                kappa_graphs=2, repeats=1, sync=torch.cuda.synchronize)
+                                max_steps=(40,), kappa_graphs=2, repeats=1,
+                                sync=torch.cuda.synchronize)
     finally:
         dyg.tune_set(0, 0)
-    assert len(trials) >= 5 and best["seconds"] == min(t["seconds"] for t in trials
+    assert len(trials) >= 6 and best["seconds"] == min(t["seconds"] for t in trials
                                                        if t.get("kappa_ok", True))
     assert any("kappa" in t for t in trials)
+    # the walk-length trial runs at the walker count chosen before it
+    ms = [t for t in trials if t.get("max_steps") == 40]
+    assert len(ms) == 1 and ms[0]["params"].max_steps == 40
+    assert ms[0]["params"].walkers in (64, p.walkers)
+    # the returned parameters are the best trial's
+    assert best["params"].walkers == best["walkers"]
+    assert best["params"].max_steps == best["max_steps"]
 
 
 def test_decremental_ids_match_per_graph(dyg):
