@@ -927,6 +927,7 @@ def run_serve(args, rank, world, local_rank):
     launches0 = dyg.kernel_launches()
     dyg.profile_reset()
     times, steps, moves = [], 0, [0, 0]
+    phases = {k: 0.0 for k in ("admit", "stage", "insert", "delete", "fetch", "split")}
     nrec = 0
     for _ in range(args.steps):
         warm(S)
@@ -946,7 +947,10 @@ def run_serve(args, rank, world, local_rank):
         m1 = S.counters()
         moves[0] += m1[0] - m0[0]
         moves[1] += m1[1] - m0[1]
-        steps = S.stats()["steps"]
+        st = S.stats()   # the replay's own (warm() resets the server)
+        steps = st["steps"]
+        for k in phases:
+            phases[k] += st["ns_" + k] / 1e6 / args.steps
         nrec = sum(len(r.rec_src) for r in done if r.op == 1 and r.rec_src is not None)
     prof = dyg.profile_read()
     launches = dyg.kernel_launches() - launches0
@@ -1015,6 +1019,10 @@ def run_serve(args, rank, world, local_rank):
         "serving": {"server_steps_per_replay": steps, "capacity_req_per_s": capacity,
                     "insertions_per_replay": n_ins, "deletions_per_replay": n_upd - n_ins,
                     "footprint_bytes": fp_total, "budget_bytes": int(fp_total * 1.5),
+                    "host_phase_ms_per_replay": phases,
+                    "phase_note": "host wall time of the server's steps: admission, staging, the "
+                                  "insertion and deletion runs (device work and synchronize "
+                                  "included), result fetch, per-request split",
                     "sweep": sweep, "plain_saturated": plain_sat,
                     "speedup_vs_plain": (n_upd / (ms / 1e3)) / plain_ups if plain_ups else None,
                     "oversubscribed": {"budget_bytes": int(fp_total * 0.5), "replays": over},

@@ -99,7 +99,9 @@ class ServerStats(C.Structure):
     """Mirror of dyg_server_stats (include/dyg_serve.h)."""
     _fields_ = [("graphs", C.c_uint32), ("resident", C.c_uint32), ("waiting", C.c_uint32),
                 ("pending", C.c_uint32), ("resident_bytes", C.c_uint64), ("budget_bytes", C.c_uint64),
-                ("admissions", C.c_uint64), ("evictions", C.c_uint64), ("steps", C.c_uint64)]
+                ("admissions", C.c_uint64), ("evictions", C.c_uint64), ("steps", C.c_uint64),
+                ("ns_admit", C.c_uint64), ("ns_stage", C.c_uint64), ("ns_insert", C.c_uint64),
+                ("ns_delete", C.c_uint64), ("ns_fetch", C.c_uint64), ("ns_split", C.c_uint64)]
 
 
 class ServerGraphInfo(C.Structure):

@@ -37,6 +37,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <iterator>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -147,6 +148,9 @@ struct dyg_server {
     uint32_t pending = 0;
     bool stepping = false, loop_on = false, stop = false;
     uint64_t steps = 0;
+    // host wall time of the steps' phases (ns, cumulative): admission,
+    // staging, insertion run, deletion run, result fetch, result split
+    uint64_t ns_phase[6] = {};
     std::string err;
     std::thread loop;
 
@@ -383,10 +387,16 @@ dyg_status admit_waiting(dyg_server *s, std::vector<std::pair<uint32_t, dyg_stat
 
 // Stages the step's batches, runs both pipelines and splits the results.
 dyg_status stage_and_run(dyg_server *s, const std::vector<Request *> &heads, uint64_t ni,
-                         uint64_t nd) {
+                         uint64_t nd, uint64_t *ns) {
     using namespace dyg;
     const uint64_t nt = ni + nd;
     if (nt == 0) return DYG_OK;
+    uint64_t t = now_ns(s);
+    auto lap = [&](int k) {
+        const uint64_t u = now_ns(s);
+        ns[k] += u - t;
+        t = u;
+    };
     if (ni > 0xFFFFFFFFull || nd > 0xFFFFFFFFull) {
         set_error("a step holds more than 2^32 - 1 updates of one kind");
         return DYG_EINVAL;
@@ -429,17 +439,20 @@ dyg_status stage_and_run(dyg_server *s, const std::vector<Request *> &heads, uin
     DYG_CUDA(cudaMemcpyAsync(d_uid, s->h_uid.p, sizeof(unsigned long long) * nt,
                              cudaMemcpyHostToDevice, st));
     if (ni) DYG_CUDA(cudaMemcpyAsync(d_w, s->h_w.p, sizeof(float) * ni, cudaMemcpyHostToDevice, st));
+    lap(1);
     if (ni) {
         DYG_TRY(incremental_run(s->H, s->G, d_src, d_dst, d_w, (uint32_t)ni, (uint32_t)ni, 0, d_uid,
                                 s->ip, d_out, d_cond, d_acc, st));
         DYG_TRY(device_errors(s->H, st));
     }
+    lap(2);
     uint64_t nrec = 0;
     if (nd) {
         DYG_TRY(decremental_run(s->G, s->H, d_src + ni, d_dst + ni, (uint32_t)nd, (uint32_t)nd, 0,
                                 d_uid + ni, s->dp, d_out + ni, d_cond + ni, &nrec, st));
         DYG_TRY(device_errors(s->G, st));
     }
+    lap(3);
     DYG_TRY(s->h_out.ensure(nt));
     DYG_TRY(s->h_cond.ensure(nt));
     DYG_TRY(s->h_acc.ensure(ni ? ni : 1));
@@ -456,6 +469,7 @@ dyg_status stage_and_run(dyg_server *s, const std::vector<Request *> &heads, uin
         DYG_CUDA(cudaMemcpyAsync(s->h_rk.p, ws.rk2.p, nrec, cudaMemcpyDeviceToHost, st));
     }
     DYG_CUDA(cudaStreamSynchronize(st));
+    lap(4);
     // vertex ranges of the step's deletion requests, ascending
     struct Owner {
         uint32_t lo, hi;
@@ -494,6 +508,7 @@ dyg_status stage_and_run(dyg_server *s, const std::vector<Request *> &heads, uin
         o.r->rk.push_back(s->h_rk.p[j]);
     }
     for (Request *r : heads) r->rec.n_rec = r->rx.size();
+    lap(5);
     return DYG_OK;
 }
 
@@ -523,6 +538,7 @@ dyg_status run_step(dyg_server *s, uint32_t *n_done) {
     std::vector<std::pair<uint32_t, dyg_status>> failed;
     dyg_status arc = DYG_OK;
     std::string amsg;
+    uint64_t ns[6] = {};
     if (s->pool) {
         try {
             arc = admit_waiting(s, &failed);
@@ -531,6 +547,7 @@ dyg_status run_step(dyg_server *s, uint32_t *n_done) {
             arc = DYG_ENOMEM;
         }
         if (arc != DYG_OK || !failed.empty()) amsg = dyg_last_error_string();
+        ns[0] = now_ns(s) - t_start;
     }
     std::vector<Request *> heads, dead;
     uint64_t ni = 0, nd = 0;
@@ -563,7 +580,7 @@ dyg_status run_step(dyg_server *s, uint32_t *n_done) {
     dyg_status rc = arc;
     if (rc == DYG_OK) {
         try {
-            rc = stage_and_run(s, heads, ni, nd);
+            rc = stage_and_run(s, heads, ni, nd, ns);
         } catch (const std::bad_alloc &) {
             dyg::set_error("host allocation failed in a server step");
             rc = DYG_ENOMEM;
@@ -576,6 +593,7 @@ dyg_status run_step(dyg_server *s, uint32_t *n_done) {
         for (Request *r : heads) complete(s, r, rc, t_start, t_done, s->steps);
         for (Request *r : dead) complete(s, r, (dyg_status)r->rec.status, t_start, t_done, s->steps);
         ++s->steps;
+        for (int k = 0; k < 6; ++k) s->ns_phase[k] += ns[k];
         s->stepping = false;
         if (!msg.empty()) s->err = msg;
     }
@@ -1083,6 +1101,7 @@ dyg_status dyg_server_reset(dyg_server *s) {
     s->done.clear();
     std::fill(s->uid_next.begin(), s->uid_next.end(), 0ull);
     s->steps = 0;
+    std::fill(std::begin(s->ns_phase), std::end(s->ns_phase), 0ull);
     return DYG_OK;
 }
 
@@ -1102,6 +1121,12 @@ dyg_status dyg_server_stats_read(dyg_server *s, dyg_server_stats *out) {
     r.evictions = s->evictions;
     r.steps = s->steps;
     r.pending = s->pending;
+    r.ns_admit = s->ns_phase[0];
+    r.ns_stage = s->ns_phase[1];
+    r.ns_insert = s->ns_phase[2];
+    r.ns_delete = s->ns_phase[3];
+    r.ns_fetch = s->ns_phase[4];
+    r.ns_split = s->ns_phase[5];
     *out = r;
     return DYG_OK;
 }

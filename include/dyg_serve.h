@@ -106,6 +106,11 @@ typedef struct dyg_server_stats {
     uint64_t budget_bytes;     /* 0 for a static server                         */
     uint64_t admissions, evictions;
     uint64_t steps;
+    /* host wall time of the steps so far, by phase (ns; reset by
+     * dyg_server_reset): admitting graphs, staging the requests, the
+     * insertion run and the deletion run (each with its device work and
+     * synchronize), fetching the results, splitting them per request     */
+    uint64_t ns_admit, ns_stage, ns_insert, ns_delete, ns_fetch, ns_split;
 } dyg_server_stats;
 dyg_status dyg_server_stats_read(dyg_server *s, dyg_server_stats *out);
 
