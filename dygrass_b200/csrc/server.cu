@@ -494,17 +494,36 @@ dyg_status stage_and_run(dyg_server *s, const std::vector<Request *> &heads, uin
         k += n;
     }
     std::sort(owners.begin(), owners.end(), [](const Owner &a, const Owner &b) { return a.lo < b.lo; });
+    // Recovered edges come in walk-list order, i.e. in runs per request: the
+    // last owner found is tried first.  One pass counts (and checks), so each
+    // request's lists are sized once; the second pass fills them.
+    std::vector<uint32_t> own(nrec), cnt(owners.size(), 0u);
+    size_t last = owners.size();
     for (uint64_t j = 0; j < nrec; ++j) {
         const uint32_t x = s->h_rx.p[j], y = s->h_ry.p[j];
-        auto it = std::upper_bound(owners.begin(), owners.end(), x,
-                                   [](uint32_t v, const Owner &o) { return v < o.lo; });
-        if (it == owners.begin() || x >= (it - 1)->hi || y < (it - 1)->lo || y >= (it - 1)->hi) {
+        if (last == owners.size() || x < owners[last].lo || x >= owners[last].hi) {
+            auto it = std::upper_bound(owners.begin(), owners.end(), x,
+                                       [](uint32_t v, const Owner &o) { return v < o.lo; });
+            last = it == owners.begin() ? owners.size() : (size_t)(it - owners.begin()) - 1;
+        }
+        if (last == owners.size() || x >= owners[last].hi || y < owners[last].lo ||
+            y >= owners[last].hi) {
             set_error("a recovered edge lies outside the graphs deleting in this step");
             return DYG_ESTATE;
         }
-        const Owner &o = *(it - 1);
-        o.r->rx.push_back(x - o.lo);
-        o.r->ry.push_back(y - o.lo);
+        own[j] = (uint32_t)last;
+        ++cnt[last];
+    }
+    for (size_t o = 0; o < owners.size(); ++o) {
+        Request *r = owners[o].r;
+        r->rx.reserve(r->rx.size() + cnt[o]);
+        r->ry.reserve(r->ry.size() + cnt[o]);
+        r->rk.reserve(r->rk.size() + cnt[o]);
+    }
+    for (uint64_t j = 0; j < nrec; ++j) {
+        const Owner &o = owners[own[j]];
+        o.r->rx.push_back(s->h_rx.p[j] - o.lo);
+        o.r->ry.push_back(s->h_ry.p[j] - o.lo);
         o.r->rk.push_back(s->h_rk.p[j]);
     }
     for (Request *r : heads) r->rec.n_rec = r->rx.size();
