@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -338,15 +339,20 @@ dyg_status validate_enqueue(unsigned long long *halt, unsigned long long *err,
 // failed check as the message.
 dyg_status rejected_inputs(dyg_graph *D, cudaStream_t st);
 // uids (device, may be null): per-edge update ids instead of uid_base + e.
+// `during`, if given, runs on the host once the first pass of batches is
+// enqueued and before the call waits for them: host work that overlaps the
+// device work.
 dyg_status incremental_run(dyg_graph *H, dyg_graph *G, const uint32_t *src, const uint32_t *dst,
                            const float *w, uint32_t n, uint32_t B, uint64_t uid_base,
                            const unsigned long long *uids, const dyg_walk_params &p, int32_t *found, float *cond, uint8_t *acc,
-                           cudaStream_t st, bool check_inputs = false);
+                           cudaStream_t st, bool check_inputs = false,
+                           const std::function<void()> *during = nullptr);
 dyg_status decremental_run(dyg_graph *G, dyg_graph *H, const uint32_t *src, const uint32_t *dst,
                            uint32_t n, uint32_t B, uint64_t uid_base,
                            const unsigned long long *uids, const dyg_walk_params &p,
                            int32_t *status, float *cond, uint64_t *n_rec, cudaStream_t st,
-                           bool check_inputs = false);
+                           bool check_inputs = false,
+                           const std::function<void()> *during = nullptr);
 
 dyg_status decr_delete_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src,
                                const uint32_t *dst, uint32_t n, uint64_t uid0,

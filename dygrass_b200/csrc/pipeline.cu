@@ -722,7 +722,8 @@ dyg_status grow_for_halt(dyg_graph *A, dyg_graph *B, cudaStream_t st) {
 dyg_status incremental_run(dyg_graph *H, dyg_graph *G, const uint32_t *src, const uint32_t *dst,
                            const float *w, uint32_t n, uint32_t B, uint64_t uid_base,
                            const unsigned long long *uids, const dyg_walk_params &p, int32_t *found, float *cond, uint8_t *acc,
-                           cudaStream_t st, bool check_inputs) {
+                           cudaStream_t st, bool check_inputs,
+                           const std::function<void()> *during) {
     unsigned long long *sc = ptr<unsigned long long>(H->ws.scalars);
     unsigned long long *halt = sc + S_HALT;
     DYG_TRY(clear_halt(H, st));
@@ -736,6 +737,7 @@ dyg_status incremental_run(dyg_graph *H, dyg_graph *G, const uint32_t *src, cons
                                  found ? found + b0 : nullptr, cond ? cond + b0 : nullptr,
                                  acc ? acc + b0 : nullptr, st));
         }
+        if (during && round == 0) (*during)();
         DYG_TRY(read_scalars2(H, G, st));
         const unsigned long long h = H->ws.host_scalars[S_HALT];
         if (!h) return DYG_OK;
@@ -753,7 +755,7 @@ dyg_status decremental_run(dyg_graph *G, dyg_graph *H, const uint32_t *src, cons
                            uint32_t n, uint32_t B, uint64_t uid_base,
                            const unsigned long long *uids, const dyg_walk_params &p,
                            int32_t *status, float *cond, uint64_t *n_rec, cudaStream_t st,
-                           bool check_inputs) {
+                           bool check_inputs, const std::function<void()> *during) {
     Workspace &ws = G->ws;
     unsigned long long *sc = ptr<unsigned long long>(ws.scalars);
     unsigned long long *halt = sc + S_HALT;
@@ -777,6 +779,7 @@ dyg_status decremental_run(dyg_graph *G, dyg_graph *H, const uint32_t *src, cons
                                  uids ? uids + b0 : nullptr, p, halt, b,
                                  b == b_start ? ph_start : 0, status + b0, cond + b0, st));
         }
+        if (during && round == 0) (*during)();
         DYG_TRY(read_scalars2(G, H, st));
         const unsigned long long h = ws.host_scalars[S_HALT];
         if (!h) {

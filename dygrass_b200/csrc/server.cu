@@ -37,6 +37,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <functional>
 #include <iterator>
 #include <chrono>
 #include <condition_variable>
@@ -66,6 +67,22 @@ struct Request {
     std::vector<uint8_t> out_a;       // accepted (insertion)
     std::vector<uint32_t> rx, ry;     // recovered edges, local ids (deletion)
     std::vector<uint8_t> rk;
+};
+
+// The vertex range [lo, hi) of a deletion request's graph during its step.
+struct Owner {
+    uint32_t lo, hi;
+    Request *r;
+};
+
+// A step whose results still sit in the page-locked result buffers; its
+// requests complete once split_results has handed the results out (during
+// the next step's device work, or at once).
+struct StepResults {
+    bool active = false;
+    std::vector<Request *> heads;
+    std::vector<Owner> owners;   // deletion requests, ascending lo
+    uint64_t ni = 0, nrec = 0, t_start = 0, step = 0;
 };
 
 // Page-locked host staging; grows, contents not kept.
@@ -168,11 +185,14 @@ struct dyg_server {
     dyg::Pinned<int32_t> h_out;
     dyg::Pinned<uint8_t> h_acc, h_rk;
     dyg::Buf d_src, d_dst, d_w, d_uid, d_out, d_cond, d_acc;
+    dyg::StepResults split;   // a step whose results are not handed out yet
 };
 
 namespace {
 
 using dyg::HostRows;
+using dyg::Owner;
+using dyg::StepResults;
 using dyg::PoolGraph;
 using dyg::Request;
 
@@ -385,11 +405,19 @@ dyg_status admit_waiting(dyg_server *s, std::vector<std::pair<uint32_t, dyg_stat
 
 // ------------------------------------------------------------------- steps
 
-// Stages the step's batches, runs both pipelines and splits the results.
+// Stages the step's batches, runs both pipelines and fetches the results
+// into the page-locked result buffers; `out` describes them.  `during`
+// (host work) runs while the first pipeline's kernels execute, and always
+// before the fetch is enqueued.
 dyg_status stage_and_run(dyg_server *s, const std::vector<Request *> &heads, uint64_t ni,
-                         uint64_t nd, uint64_t *ns) {
+                         uint64_t nd, uint64_t *ns, const std::function<void()> &during,
+                         StepResults *out) {
     using namespace dyg;
     const uint64_t nt = ni + nd;
+    out->heads = heads;
+    out->owners.clear();
+    out->ni = ni;
+    out->nrec = 0;
     if (nt == 0) return DYG_OK;
     uint64_t t = now_ns(s);
     auto lap = [&](int k) {
@@ -420,8 +448,11 @@ dyg_status stage_and_run(dyg_server *s, const std::vector<Request *> &heads, uin
             s->h_uid.p[k + i] = r->rec.first_update_id + i;
         }
         if (ins) memcpy(s->h_w.p + k, r->w.data(), sizeof(float) * n);
+        else out->owners.push_back(Owner{o, o + graph_size(s, r->rec.graph), r});
         k += n;
     }
+    std::sort(out->owners.begin(), out->owners.end(),
+              [](const Owner &a, const Owner &b) { return a.lo < b.lo; });
     DYG_TRY(ensure(s->d_src, sizeof(uint32_t) * nt));
     DYG_TRY(ensure(s->d_dst, sizeof(uint32_t) * nt));
     DYG_TRY(ensure(s->d_uid, sizeof(unsigned long long) * nt));
@@ -442,17 +473,19 @@ dyg_status stage_and_run(dyg_server *s, const std::vector<Request *> &heads, uin
     lap(1);
     if (ni) {
         DYG_TRY(incremental_run(s->H, s->G, d_src, d_dst, d_w, (uint32_t)ni, (uint32_t)ni, 0, d_uid,
-                                s->ip, d_out, d_cond, d_acc, st));
+                                s->ip, d_out, d_cond, d_acc, st, false, &during));
         DYG_TRY(device_errors(s->H, st));
     }
     lap(2);
     uint64_t nrec = 0;
     if (nd) {
         DYG_TRY(decremental_run(s->G, s->H, d_src + ni, d_dst + ni, (uint32_t)nd, (uint32_t)nd, 0,
-                                d_uid + ni, s->dp, d_out + ni, d_cond + ni, &nrec, st));
+                                d_uid + ni, s->dp, d_out + ni, d_cond + ni, &nrec, st, false,
+                                &during));
         DYG_TRY(device_errors(s->G, st));
     }
     lap(3);
+    during();   // (a no-op when a pipeline ran it) before the buffers are refilled
     DYG_TRY(s->h_out.ensure(nt));
     DYG_TRY(s->h_cond.ensure(nt));
     DYG_TRY(s->h_acc.ensure(ni ? ni : 1));
@@ -469,31 +502,27 @@ dyg_status stage_and_run(dyg_server *s, const std::vector<Request *> &heads, uin
         DYG_CUDA(cudaMemcpyAsync(s->h_rk.p, ws.rk2.p, nrec, cudaMemcpyDeviceToHost, st));
     }
     DYG_CUDA(cudaStreamSynchronize(st));
+    out->nrec = nrec;
     lap(4);
-    // vertex ranges of the step's deletion requests, ascending
-    struct Owner {
-        uint32_t lo, hi;
-        Request *r;
-    };
-    std::vector<Owner> owners;
-    ki = 0;
-    kd = ni;
-    for (Request *r : heads) {
+    return DYG_OK;
+}
+
+// Hands a step's results out of the result buffers to its requests.
+dyg_status split_results(dyg_server *s, const StepResults &R) {
+    using namespace dyg;
+    uint64_t ki = 0, kd = R.ni;
+    for (Request *r : R.heads) {
         const uint32_t n = r->rec.n;
         if (!n) continue;
         const bool ins = r->rec.op == DYG_STREAM_INSERT;
         uint64_t &k = ins ? ki : kd;
         r->out_i.assign(s->h_out.p + k, s->h_out.p + k + n);
         r->out_c.assign(s->h_cond.p + k, s->h_cond.p + k + n);
-        if (ins) {
-            r->out_a.assign(s->h_acc.p + k, s->h_acc.p + k + n);
-        } else {
-            const uint32_t b = graph_base(s, r->rec.graph);
-            owners.push_back(Owner{b, b + graph_size(s, r->rec.graph), r});
-        }
+        if (ins) r->out_a.assign(s->h_acc.p + k, s->h_acc.p + k + n);
         k += n;
     }
-    std::sort(owners.begin(), owners.end(), [](const Owner &a, const Owner &b) { return a.lo < b.lo; });
+    const std::vector<Owner> &owners = R.owners;
+    const uint64_t nrec = R.nrec;
     // Recovered edges come in walk-list order, i.e. in runs per request: the
     // last owner found is tried first.  One pass counts (and checks), so each
     // request's lists are sized once; the second pass fills them.
@@ -526,8 +555,7 @@ dyg_status stage_and_run(dyg_server *s, const std::vector<Request *> &heads, uin
         o.r->ry.push_back(s->h_ry.p[j] - o.lo);
         o.r->rk.push_back(s->h_rk.p[j]);
     }
-    for (Request *r : heads) r->rec.n_rec = r->rx.size();
-    lap(5);
+    for (Request *r : R.heads) r->rec.n_rec = r->rx.size();
     return DYG_OK;
 }
 
@@ -539,6 +567,30 @@ void complete(dyg_server *s, Request *r, dyg_status rc, uint64_t t_start, uint64
     r->rec.t_done_ns = t_done;
     r->finished = true;
     s->done.push_back(r->rec);
+}
+
+// Completes the step whose results were left in the result buffers (by the
+// thread that holds the step; a no-op when there is none).
+void finish_split(dyg_server *s, uint64_t *ns_split) {
+    if (!s->split.active) return;
+    StepResults R = std::move(s->split);
+    s->split = StepResults{};
+    const uint64_t t0 = now_ns(s);
+    dyg_status rc;
+    try {
+        rc = split_results(s, R);
+    } catch (const std::bad_alloc &) {
+        dyg::set_error("host allocation failed while handing out results");
+        rc = DYG_ENOMEM;
+    }
+    const uint64_t t_done = now_ns(s);
+    if (ns_split) *ns_split += t_done - t0;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (Request *r : R.heads) complete(s, r, rc, R.t_start, t_done, R.step);
+        if (rc != DYG_OK) s->err = dyg_last_error_string();
+    }
+    s->cv_idle.notify_all();
 }
 
 dyg_status run_step(dyg_server *s, uint32_t *n_done) {
@@ -596,25 +648,58 @@ dyg_status run_step(dyg_server *s, uint32_t *n_done) {
         s->pending -= (uint32_t)(heads.size() + dead.size());
     }
     if (n_done) *n_done = (uint32_t)(heads.size() + dead.size());
+    // The previous step's results (if it left them in the result buffers)
+    // are handed out while this step's first pipeline runs on the device.
+    const std::function<void()> during = [s, &ns] { finish_split(s, &ns[5]); };
+    StepResults R;
     dyg_status rc = arc;
     if (rc == DYG_OK) {
         try {
-            rc = stage_and_run(s, heads, ni, nd, ns);
+            rc = stage_and_run(s, heads, ni, nd, ns, during, &R);
         } catch (const std::bad_alloc &) {
             dyg::set_error("host allocation failed in a server step");
             rc = DYG_ENOMEM;
         }
     }
     const std::string msg = rc == DYG_OK ? amsg : std::string(dyg_last_error_string());
+    finish_split(s, &ns[5]);   // when no pipeline ran it
+    uint64_t step;
+    bool defer;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        step = s->steps;
+        // under the loop thread, with requests still queued, this step's
+        // results are handed out during the next step
+        defer = rc == DYG_OK && s->loop_on && !s->stop && s->pending > 0 && !heads.empty();
+    }
+    dyg_status src = DYG_OK;
+    if (defer) {
+        R.active = true;
+        R.t_start = t_start;
+        R.step = step;
+        s->split = std::move(R);
+    } else if (rc == DYG_OK) {
+        const uint64_t t0 = now_ns(s);
+        try {
+            src = split_results(s, R);
+        } catch (const std::bad_alloc &) {
+            dyg::set_error("host allocation failed while handing out results");
+            src = DYG_ENOMEM;
+        }
+        ns[5] += now_ns(s) - t0;
+        if (src != DYG_OK) rc = src;
+    }
+    const std::string emsg = src != DYG_OK ? std::string(dyg_last_error_string()) : msg;
     const uint64_t t_done = now_ns(s);
     {
         std::lock_guard<std::mutex> lk(s->mu);
-        for (Request *r : heads) complete(s, r, rc, t_start, t_done, s->steps);
-        for (Request *r : dead) complete(s, r, (dyg_status)r->rec.status, t_start, t_done, s->steps);
+        if (!defer)
+            for (Request *r : heads) complete(s, r, rc, t_start, t_done, step);
+        for (Request *r : dead) complete(s, r, (dyg_status)r->rec.status, t_start, t_done, step);
         ++s->steps;
         for (int k = 0; k < 6; ++k) s->ns_phase[k] += ns[k];
         s->stepping = false;
-        if (!msg.empty()) s->err = msg;
+        if (!emsg.empty()) s->err = emsg;
     }
     s->cv_idle.notify_all();
     s->cv_work.notify_all();
@@ -632,6 +717,19 @@ void loop_main(dyg_server *s) {
         lk.unlock();
         run_step(s, nullptr);
         lk.lock();
+    }
+    // A step left for the next one to hand out is handed out now.  Another
+    // holder of the step flag can only be a step (requests are queued while
+    // results wait, so no exclusive call starts), and a step hands it out
+    // itself.
+    if (!s->stepping) {
+        s->stepping = true;
+        lk.unlock();
+        finish_split(s, nullptr);
+        lk.lock();
+        s->stepping = false;
+        s->cv_idle.notify_all();
+        s->cv_work.notify_all();
     }
 }
 
