@@ -332,10 +332,16 @@ class Server:
         i = 0
         while i < len(order) and order[i].arrival <= 0.0:   # pending at once
             i += 1
-        self.submit_many(order[:i])
+        # Requests pending at once go in chunks (each one checked and queued
+        # as a whole), the loop starting after the first: steps run on the
+        # device while the client still builds the later chunks' arrays.
+        chunk = 128
+        self.submit_many(order[:min(i, chunk)])
         done = []
         _check(L.dyg_server_start(self._srv), "dyg_server_start")
         try:
+            for k in range(chunk, i, chunk):
+                self.submit_many(order[k:min(i, k + chunk)])
             while i < len(order):
                 t = self.now()
                 j = i
