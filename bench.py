@@ -1507,9 +1507,9 @@ def main():
                      "l2_gbs": (l2_bytes / (res["dom_ms_per_launch"] / 1e3) / 1e9) if l2_bytes else None,
                      "note": "the graphs are largely L2-resident: traffic (ncu DRAM bytes per launch) "
                              "is well below the algorithmic bytes, so frac is an equivalent-bandwidth "
-                             "figure; the walk is bound by instruction issue and L1 gathers "
-                             "(profiles/k_walk_mesh100.md); of each move's two sectors, 16 B "
-                             "(descriptor + slot) are payload"},
+                             "figure (l2_gbs is the L2 rate); the walk is bound by instruction issue "
+                             "and gather latency (ncu counters of the walk kernel under profiles/); "
+                             "of each move's two sectors, 16 B (descriptor + slot) are payload"},
         "clocks": res["clocks"],
         "e2e": res["e2e"],
         "gpu_launches": int(round(res["launches_per_step"] * args.steps)),
