@@ -175,6 +175,7 @@ def lib() -> C.CDLL:
         "dyg_decremental_batch_ids": ([vp, vp, vp, vp, vp, u32, C.POINTER(WalkParams), vp, vp, vp,
                                        vp, vp, u64, C.POINTER(u64), vp], C.c_int),
         "dyg_tune_set": ([u32, u32], None),
+        "dyg_tune_set_prune_interval": ([u32], None),
         "dyg_kappa": ([u32, u64, vp, vp, vp, u64, vp, vp, vp, C.POINTER(KappaOpts),
                        C.POINTER(KappaResult)], C.c_int),
         "dyg_mtx_read_auto": ([C.c_char_p, C.POINTER(MtxInfo), C.POINTER(u64), C.POINTER(vp),
@@ -580,9 +581,12 @@ def decremental_batch_ids(G: Graph, H: Graph, src, dst, update_ids, params: Walk
     return DecrementalResult(st, cd, rx[:k].copy(), ry[:k].copy(), rk[:k].copy())
 
 
-def tune_set(walk_chunk: int = 0, blocks_per_sm: int = 0) -> None:
-    """Walk-kernel launch shape for this process (results do not depend on it)."""
+def tune_set(walk_chunk: int = 0, blocks_per_sm: int = 0, prune_every: int = 0) -> None:
+    """Walk-kernel launch shape for this process and the iterations between a
+    walker's reads of its edge's best result (results do not depend on them;
+    0 = default)."""
     lib().dyg_tune_set(int(walk_chunk), int(blocks_per_sm))
+    lib().dyg_tune_set_prune_interval(int(prune_every))
 
 
 def stream_default_chunk(n_vertices: int) -> int:

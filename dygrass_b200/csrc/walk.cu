@@ -86,6 +86,7 @@ struct WalkArgs {
     WalkJob job;
     uint32_t walkers, max_steps;
     uint32_t prune;
+    uint32_t prune_every;   // iterations between reads of the edge's best (a power of two)
     uint32_t chunk;   // walkers handed to a warp at a time
     float threshold;
     uint2 key;
@@ -556,7 +557,8 @@ __global__ void __launch_bounds__(kWalkThreads, WEIGHTED ? 3 : 6) k_walk(WalkArg
             if (active) {
                 // the edge's best is read again every fourth move
                 constexpr uint32_t kEvery = MOVES >= 4 ? 1u : (MOVES == 2 ? 2u : 4u);
-                if (T % kEvery == kEvery - 1u)
+                const uint32_t pm = kEvery * a.prune_every - 1u;
+                if ((T & pm) == pm)
                     gbest = max(gbest, (uint32_t)(*(volatile unsigned long long *)(a.keys + my_e) >> 32));
                 const uint32_t known = max(gbest, (my_e == ce) ? ce_best
                                                   : (my_e == pe ? pe_best : 0u));
@@ -738,7 +740,13 @@ __global__ void k_fallback(DevGraph g, const unsigned long long *halt, const uin
 // waves on one.  DYG_WALK_CHUNK (a multiple of 32 dividing the walker count)
 // overrides it for tuning sweeps.
 // Launch shape of the walk kernel, process-wide (dyg_tune_set); 0 = default.
-static std::atomic<uint32_t> g_tune_chunk{0}, g_tune_bpsm{0};
+static std::atomic<uint32_t> g_tune_chunk{0}, g_tune_bpsm{0}, g_tune_prune{0};
+
+// Iterations between reads of an edge's best result for pruning (1, 2 or 4).
+static uint32_t prune_every() {
+    const uint32_t t = g_tune_prune.load();
+    return (t == 2u || t == 4u) ? t : 1u;
+}
 
 static uint32_t chunk_for(uint32_t walkers) {
     static int env = -1;
@@ -818,6 +826,7 @@ dyg_status launch_walk(dyg_graph *G, const WalkJob &job, const dyg_walk_params &
     a.walkers = p.walkers;
     a.max_steps = p.max_steps;
     a.prune = (p.flags & DYG_FLAG_EXHAUSTIVE) ? 0u : 1u;
+    a.prune_every = prune_every();
     a.chunk = chunk_for(p.walkers);
     a.threshold = p.threshold;
     a.key = make_uint2((uint32_t)p.seed, (uint32_t)(p.seed >> 32));
@@ -843,6 +852,7 @@ dyg_status launch_walk_scalars(const DevGraph &g, const WalkJob &job, const dyg_
     a.walkers = p.walkers;
     a.max_steps = p.max_steps;
     a.prune = (p.flags & DYG_FLAG_EXHAUSTIVE) ? 0u : 1u;
+    a.prune_every = prune_every();
     a.chunk = chunk_for(p.walkers);
     a.threshold = p.threshold;
     a.key = make_uint2((uint32_t)p.seed, (uint32_t)(p.seed >> 32));
@@ -920,6 +930,10 @@ dyg_status dyg_profile_read(dyg_profile *out) {
 }
 
 }  // extern "C"
+
+extern "C" void dyg_tune_set_prune_interval(uint32_t iterations) {
+    dyg::g_tune_prune.store(iterations);
+}
 
 extern "C" void dyg_tune_set(uint32_t walk_chunk, uint32_t blocks_per_sm) {
     dyg::g_tune_chunk.store(walk_chunk);

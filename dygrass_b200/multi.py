@@ -156,12 +156,13 @@ def _timed(fn, sync):
 
 
 def autotune(cases, plan_streams=None, params: WalkParams | None = None,
-             chunks=(32, 64, 128), blocks=(0, 5, 4), walkers=(), max_steps=(),
+             chunks=(32, 64, 128), blocks=(0, 5, 4), prune_every=(1, 2), walkers=(), max_steps=(),
              kappa_graphs: int = 4, kappa_tol: float = 0.05, repeats: int = 2, device: int = -1,
              sync=lambda: None):
-    """Times the rounds of the cases' streams for each launch shape, then each
-    walker count in `walkers` and each walk length in `max_steps` (below the
-    parameters' own), each accepted only if the mean kappa of the
+    """Times the rounds of the cases' streams for each launch shape and prune
+    interval (tune_set), then each walker count in `walkers` and each walk
+    length in `max_steps` (below the parameters' own), each accepted only if
+    the mean kappa of the
     `kappa_graphs` smallest graphs stays within kappa_tol of the value at the
     parameters' own walker count and walk length.  Returns (best dict, list of
     all measurements); the best dict's "params" are the walk parameters to
@@ -176,8 +177,8 @@ def autotune(cases, plan_streams=None, params: WalkParams | None = None,
     M.run(pl, params)
     sync()
 
-    def measure(p, chunk, bpsm):
-        tune_set(chunk, bpsm)
+    def measure(p, chunk, bpsm, pe=1):
+        tune_set(chunk, bpsm, pe)
         t = []
         for _ in range(repeats):
             M.H.copy_from(H0)
@@ -189,8 +190,9 @@ def autotune(cases, plan_streams=None, params: WalkParams | None = None,
         if params.walkers % chunk:
             continue
         for b in blocks:
-            trials.append({"walkers": params.walkers, "chunk": chunk, "blocks_per_sm": b,
-                           "seconds": measure(params, chunk, b)})
+            for pe in prune_every:
+                trials.append({"walkers": params.walkers, "chunk": chunk, "blocks_per_sm": b,
+                               "prune_every": pe, "seconds": measure(params, chunk, b, pe)})
     best = min(trials, key=lambda t: t["seconds"])
     best["params"] = params
     best["max_steps"] = params.max_steps
@@ -230,14 +232,14 @@ def autotune(cases, plan_streams=None, params: WalkParams | None = None,
             k = mean_kappa(p)
             chunk = best["chunk"] if wk % best["chunk"] == 0 else 32
             t = {"walkers": wk, "max_steps": ms, "chunk": chunk,
-                 "blocks_per_sm": best["blocks_per_sm"], "kappa": k,
-                 "kappa_ok": abs(k - k_ref) <= kappa_tol * k_ref, "params": p}
-            t["seconds"] = measure(p, chunk, best["blocks_per_sm"])
+                 "blocks_per_sm": best["blocks_per_sm"], "prune_every": best["prune_every"],
+                 "kappa": k, "kappa_ok": abs(k - k_ref) <= kappa_tol * k_ref, "params": p}
+            t["seconds"] = measure(p, chunk, best["blocks_per_sm"], best["prune_every"])
             trials.append(t)
             if t["kappa_ok"] and t["seconds"] < best["seconds"]:
                 best = t
     for x in (H0, G0):
         x.close()
     M.close()
-    tune_set(best["chunk"], best["blocks_per_sm"])
+    tune_set(best["chunk"], best["blocks_per_sm"], best["prune_every"])
     return best, trials

@@ -275,6 +275,12 @@ dyg_status dyg_decremental_commit_keys(dyg_graph *G, dyg_graph *H, const dyg_wal
  * one-block-per-edge launch (random_walk_incremental/main.cu:316). */
 void dyg_tune_set(uint32_t walk_chunk, uint32_t blocks_per_sm);
 
+/* Walk iterations (of four moves) between a walker's reads of its edge's best
+ * result, against which it is pruned: 1 (the default; 0 = 1), 2 or 4.  A
+ * bound read less often is only lower, so results do not depend on it; an
+ * autotuner's knob like the two above. */
+void dyg_tune_set_prune_interval(uint32_t iterations);
+
 /* Walk-list chunk of the mixed updater: 5% of |V|, at least 10000
  * (dynamic_update/main.cu:83-84). */
 uint32_t dyg_stream_default_chunk(uint32_t n_vertices);

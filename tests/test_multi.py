@@ -82,8 +82,10 @@ def test_autotune(dyg):
                                 sync=torch.cuda.synchronize)
     finally:
         dyg.tune_set(0, 0)
-    assert len(trials) >= 6 and best["seconds"] == min(t["seconds"] for t in trials
-                                                       if t.get("kappa_ok", True))
+    assert len(trials) >= 10 and best["seconds"] == min(t["seconds"] for t in trials
+                                                        if t.get("kappa_ok", True))
+    # every launch shape with both prune intervals (results do not depend on them)
+    assert {t["prune_every"] for t in trials} == {1, 2}
     assert any("kappa" in t for t in trials)
     # the walk-length trial runs at the walker count chosen before it
     ms = [t for t in trials if t.get("max_steps") == 40]
