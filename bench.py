@@ -31,8 +31,8 @@ union graph and a step is the 10 rounds that carry batch r of every graph
 (dygrass_b200/multi.py), after an autotune of the walk launch shape.  The
 plain per-graph loop on the same updates is timed beside it.
 
-Workload "serve": the serving configuration -- 64 graphs mixed from the
-mesh, R-MAT and random-geometric generators (--serve-mix large: about 10 GB
+Workload "serve": the serving configuration -- 80 graphs mixed from the
+mesh, R-MAT and random-geometric generators (--serve-mix large: about 10.8 GB
 of footprint), update requests of log-uniform size in [1, 4096], 60%
 insertions / 40% deletions.  value = the continuous-batching pool server's
 throughput (the native scheduler of include/dyg_serve.h, driven by
@@ -83,7 +83,9 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=2000)
     ap.add_argument("--serve-mix", choices=["small", "large"], default="large",
                     help="serving graphs: large = meshes 60^3..100^3, R-MAT scales 17..20, "
-                         "random geometric graphs (about 10 GB); small = the quick mix")
+                         "random geometric graphs (about 10.8 GB at 80 graphs); small = the "
+                         "quick mix")
+    ap.add_argument("--serve-graphs", type=int, default=80)
     ap.add_argument("--rgg-graphs", type=int, default=256)
     ap.add_argument("--rgg-n-hi", type=int, default=200_000)
     ap.add_argument("--tune-walkers", action="store_true",
@@ -145,7 +147,8 @@ def make_workload(args, rank, world=1):
     seed = wl.MASTER_SEED + (1000 * rank if args.split_mode == "replicas" else 0)
     if args.workload == "serve":
         from dygrass_b200.serve import Request, footprint_bytes, poisson_requests
-        cases, ip, dp = wl.serving_mix(seed=seed, large=args.serve_mix == "large")
+        cases, ip, dp = wl.serving_mix(k=args.serve_graphs, seed=seed,
+                                        large=args.serve_mix == "large")
         reqs = poisson_requests(cases, 1.0, args.serve_requests, seed + 5)
         job = sum(len(r.src) for r in reqs)
         mine = _my_graphs(args, cases, rank, world)

@@ -481,12 +481,62 @@ __global__ void k_del_scatter(DelSides D, const uint32_t *hx, uint32_t m,
     dev_del_scatter(d.g, hx, m, d.rank, d.rowtmp, d.dtmp, halt);
 }
 
-// Leaders remove their row's entries in list order.  With `mask`, entry
-// i = 2e + side is applied only if edge e was found on both sides of `mask`.
-// A row of up to 32 slots is edited by its leader's lane; a longer one by the
-// whole warp (each search 32 slots at a time); with big_ok, rows longer than
-// kBigRow go to the big list for k_del_apply_big.  Every lane of a warp runs
-// the same iterations.
+// One warp removes row x's cnt entries (its run in tmp at rowtmp[x]) in list
+// order: the run is ordered by list index (each entry placed at its rank,
+// into the second half of the scratch), then each deletion searches the row
+// 32 slots at a time and moves the row's last slot into the hit.  With
+// `mask`, entry i = 2e + side is applied only if edge e was found on both
+// sides of `mask`.  Every lane calls it with the same arguments.
+__device__ __forceinline__ void warp_del_row(const DevGraph &g, const uint32_t *hy, uint32_t m,
+                                             uint32_t x, uint32_t cnt, uint2 d,
+                                             const uint32_t *rowtmp, uint32_t *tmp,
+                                             const uint8_t *mask, uint8_t *found, uint32_t lane) {
+    const uint32_t off = d.x;
+    uint32_t deg = d.y;
+    const uint32_t *run = tmp + rowtmp[x];
+    uint32_t *sorted = tmp + m + rowtmp[x];
+    for (uint32_t a = lane; a < cnt; a += 32u) {   // each entry to its rank
+        const uint32_t v = run[a];
+        uint32_t r = 0;
+        for (uint32_t c = 0; c < cnt; ++c) r += run[c] < v;
+        sorted[r] = v;
+    }
+    __syncwarp();
+    for (uint32_t a = 0; a < cnt; ++a) {
+        const uint32_t k = sorted[a];
+        if (mask && !(mask[k & ~1u] && mask[k | 1u])) continue;
+        const uint32_t y = hy[k];
+        uint32_t pos = ~0u;
+        for (uint32_t j0 = 0; j0 < deg; j0 += 32u) {
+            const uint32_t j = j0 + lane;
+            const unsigned hit = __ballot_sync(kFull, j < deg && g.slots[off + j].x == y);
+            if (hit) {
+                pos = j0 + (uint32_t)(__ffs(hit) - 1);
+                break;
+            }
+        }
+        if (pos != ~0u) {
+            if (lane == 0u) {
+                g.slots[off + pos] = g.slots[off + deg - 1u];
+                g.wts[off + pos] = g.wts[off + deg - 1u];
+                found[k] = 1;
+            }
+            --deg;
+            __syncwarp();   // the moved slot is visible to the next search
+        }
+    }
+    if (lane == 0u) g.desc[x] = make_uint2(off, deg);
+    __syncwarp();
+}
+
+// Leaders remove their row's entries in list order (mask as in
+// warp_del_row).  A row of up to 32 slots is edited by its leader's lane.
+// Without big_ok a longer one is edited by the whole warp; with big_ok (the
+// graph has rows longer than kBigRow) rows longer than kBigRow go to the
+// front of the big list and rows of 33..kBigRow slots to its back (counted in
+// the high half of *nbig), both for k_del_apply_big, so that no warp edits
+// several such rows one after another.  Every lane of a warp runs the same
+// iterations.
 __global__ void k_del_apply(DevGraph g, const uint32_t *hx, const uint32_t *hy, uint32_t m,
                             const uint32_t *rank, uint32_t *rowcnt, const uint32_t *rowtmp,
                             uint32_t *tmp, const uint8_t *mask, uint8_t *found, uint4 *big,
@@ -503,8 +553,12 @@ __global__ void k_del_apply(DevGraph g, const uint32_t *hx, const uint32_t *hy, 
         if (lead) {
             x = hx[i];
             d = g.desc[x];
-            if (big_ok && d.y > kBigRow) {
-                big[atomicAdd(nbig, 1ull)] = make_uint4(i, 0u, 0u, 0u);
+            if (big_ok && d.y > 32u) {
+                if (d.y > kBigRow)   // the count of long rows is the low half
+                    big[(uint32_t)atomicAdd(nbig, 1ull)] = make_uint4(i, 0u, 0u, 0u);
+                else
+                    big[m - 1u - (uint32_t)(atomicAdd(nbig, 1ull << 32) >> 32)] =
+                        make_uint4(i, 0u, 0u, 0u);
                 lead = false;
             } else {
                 cnt = rowcnt[x];
@@ -555,42 +609,8 @@ __global__ void k_del_apply(DevGraph g, const uint32_t *hx, const uint32_t *hy, 
             todo &= todo - 1u;
             const uint32_t sx = __shfl_sync(kFull, x, src);
             const uint32_t sc = __shfl_sync(kFull, cnt, src);
-            const uint32_t off = __shfl_sync(kFull, d.x, src);
-            uint32_t deg = __shfl_sync(kFull, d.y, src);
-            uint32_t *run = tmp + rowtmp[sx];
-            uint32_t *sorted = tmp + m + rowtmp[sx];
-            for (uint32_t a = lane; a < sc; a += 32u) {   // each entry to its rank
-                const uint32_t v = run[a];
-                uint32_t r = 0;
-                for (uint32_t c = 0; c < sc; ++c) r += run[c] < v;
-                sorted[r] = v;
-            }
-            __syncwarp();
-            for (uint32_t a = 0; a < sc; ++a) {
-                const uint32_t k = sorted[a];
-                if (mask && !(mask[k & ~1u] && mask[k | 1u])) continue;
-                const uint32_t y = hy[k];
-                uint32_t pos = ~0u;
-                for (uint32_t j0 = 0; j0 < deg; j0 += 32u) {
-                    const uint32_t j = j0 + lane;
-                    const unsigned hit = __ballot_sync(kFull, j < deg && g.slots[off + j].x == y);
-                    if (hit) {
-                        pos = j0 + (uint32_t)(__ffs(hit) - 1);
-                        break;
-                    }
-                }
-                if (pos != ~0u) {
-                    if (lane == 0u) {
-                        g.slots[off + pos] = g.slots[off + deg - 1u];
-                        g.wts[off + pos] = g.wts[off + deg - 1u];
-                        found[k] = 1;
-                    }
-                    --deg;
-                    __syncwarp();   // the moved slot is visible to the next search
-                }
-            }
-            if (lane == 0u) g.desc[sx] = make_uint2(off, deg);
-            __syncwarp();
+            const uint2 sd = make_uint2(__shfl_sync(kFull, d.x, src), __shfl_sync(kFull, d.y, src));
+            warp_del_row(g, hy, m, sx, sc, sd, rowtmp, tmp, mask, found, lane);
         }
     }
 }
@@ -603,7 +623,8 @@ constexpr uint32_t kTrackMax = 128;   // deletions per long row tracked in share
 // occur once in the row, one pass over the row finds every target's slot and
 // one thread applies the swaps in order, following the single slot each swap
 // moves (the row's last); otherwise every deletion is a block-wide search.
-// Both give the one-thread path's result.
+// Both give the one-thread path's result.  Then the rows of 33..kBigRow
+// slots that k_del_apply left at the back of the list, one warp each.
 __global__ void k_del_apply_big(DevGraph g, const uint32_t *hx, const uint32_t *hy, uint32_t m,
                                 uint32_t *rowcnt, const uint32_t *rowtmp, uint32_t *tmp,
                                 const uint8_t *mask, uint8_t *found, const uint4 *big,
@@ -612,7 +633,8 @@ __global__ void k_del_apply_big(DevGraph g, const uint32_t *hx, const uint32_t *
     __shared__ uint32_t s_y[kTrackMax], s_pos[kTrackMax], s_occ[kTrackMax];
     __shared__ unsigned long long s_key[kTrackMax];   // (column << 8 | a), ascending
     if (*halt) return;
-    const uint32_t nb = (uint32_t)*nbig;
+    const unsigned long long nboth = *nbig;
+    const uint32_t nb = (uint32_t)nboth, nmid = (uint32_t)(nboth >> 32);
     for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
         const uint32_t x = hx[big[b].x];
         const uint32_t cnt = rowcnt[x];
@@ -725,6 +747,14 @@ __global__ void k_del_apply_big(DevGraph g, const uint32_t *hx, const uint32_t *
         }
         __syncthreads();   // s_ok and the shared arrays are reused by the next row
     }
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < nmid; j += nw) {
+        const uint32_t x = hx[big[m - 1u - j].x];
+        const uint32_t cnt = rowcnt[x];
+        warp_del_row(g, hy, m, x, cnt, g.desc[x], rowtmp, tmp, mask, found, lane);
+        if (lane == 0u) rowcnt[x] = 0u;
+    }
 }
 
 int grid_for(uint64_t m) {
@@ -836,7 +866,7 @@ dyg_status delete_pair_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *hx, c
                                         ptr<uint4>(X->ws.big), sc + S_NBIG, X->long_rows, halt);
         count_launch();
         if (X->long_rows) {
-            k_del_apply_big<<<num_sms() * 2, kBigThreads, 0, st>>>(
+            k_del_apply_big<<<num_sms() * 4, kBigThreads, 0, st>>>(
                 X->g, hx, hy, m, ptr<uint32_t>(X->ws.rowcnt), ptr<uint32_t>(X->ws.rowtmp),
                 ptr<uint32_t>(X->ws.dtmp), mask, found, ptr<uint4>(X->ws.big), sc + S_NBIG, halt);
             count_launch();

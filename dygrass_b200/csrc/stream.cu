@@ -74,10 +74,33 @@ __device__ __forceinline__ bool long_rows(const DevGraph &g, uint32_t a, uint32_
     return g.desc[a].y > kBigRow || g.desc[b].y > kBigRow;
 }
 
+// group_edge for an edge with a row longer than kBigRow: the group searches
+// the shorter row when it has at most kBigRow slots, which settles an absent
+// edge; *open is set when a search of a long row remains (the edge is in the
+// short row, whose slot is returned, or both rows are long).
+__device__ __forceinline__ uint2 group_edge_short(const DevGraph &g, uint32_t a, uint32_t b,
+                                                  uint32_t lane, uint32_t gbase, uint32_t gmask,
+                                                  bool *open) {
+    const uint2 da = g.desc[a], db = g.desc[b];
+    const bool a_short = da.y <= db.y;
+    *open = false;
+    if ((a_short ? db.y : da.y) <= kBigRow) return group_edge(g, a, b, lane, gbase, gmask);
+    if ((a_short ? da.y : db.y) > kBigRow) {
+        *open = true;
+        return make_uint2(~0u, ~0u);
+    }
+    const uint32_t ps = group_find(g, a_short ? a : b, a_short ? b : a, lane, gbase, gmask);
+    *open = ps != ~0u;
+    return a_short ? make_uint2(ps, ~0u) : make_uint2(~0u, ps);
+}
+
 // One group of kProbeLanes lanes per edge: slot positions in G and H, the
 // sort key (min << nb | max) and index; self-loops and invalid endpoints get
 // key ~0 (sorted last, never merged or walked).  An edge with a row longer
-// than kBigRow in G or H goes to the big list for k_st_probe_big.
+// than kBigRow in G or H has its short rows searched here
+// (group_edge_short); if a long row remains to be searched it goes to the big
+// list for k_st_probe_big, with bit 0 (G) and bit 1 (H) of .w naming the
+// graphs whose search is open.
 __global__ void k_st_probe(const unsigned long long *halt, DevGraph G, DevGraph H,
                            const uint32_t *src, const uint32_t *dst, uint32_t n, uint32_t nb,
                            unsigned long long *key, uint32_t *val, uint4 *pos, uint32_t *nflag,
@@ -114,7 +137,14 @@ __global__ void k_st_probe(const unsigned long long *halt, DevGraph G, DevGraph 
         nflag[i] = 0;
     }
     if (big_ok && (long_rows(G, a, b) || long_rows(H, a, b))) {
-        if (lane == 0) big[atomicAdd(nbig, 1ull)] = make_uint4(i, a, b, 0u);
+        bool og, oh;
+        const uint2 pg = group_edge_short(G, a, b, lane, gbase, gmask, &og);
+        const uint2 ph = group_edge_short(H, a, b, lane, gbase, gmask, &oh);
+        if (lane == 0) {
+            pos[i] = make_uint4(pg.x, pg.y, ph.x, ph.y);
+            if (og || oh)
+                big[atomicAdd(nbig, 1ull)] = make_uint4(i, a, b, (og ? 1u : 0u) | (oh ? 2u : 0u));
+        }
         return;
     }
     const uint2 pg = group_edge(G, a, b, lane, gbase, gmask);
@@ -122,20 +152,27 @@ __global__ void k_st_probe(const unsigned long long *halt, DevGraph G, DevGraph 
     if (lane == 0) pos[i] = make_uint4(pg.x, pg.y, ph.x, ph.y);
 }
 
-// Slots of edge {a, b} in g by block-wide scans, the shorter row first.
-__device__ uint2 block_edge(const DevGraph &g, uint32_t a, uint32_t b, uint32_t *s_best) {
+// Finishes group_edge_short's search of edge {a, b} in g by block-wide
+// scans: `part` is its result (the short row's slot when only the long row
+// remains).
+__device__ uint2 block_edge(const DevGraph &g, uint32_t a, uint32_t b, uint2 part,
+                            uint32_t *s_best) {
     const uint2 da = g.desc[a], db = g.desc[b];
     const bool a_short = da.y <= db.y;
     const uint2 ds = a_short ? da : db, dl = a_short ? db : da;
     const uint32_t s = a_short ? a : b, l = a_short ? b : a;
-    const uint32_t js = block_find(g.slots, ds.x, ds.y, l, s_best);
-    if (js == ~0u) return make_uint2(~0u, ~0u);
+    uint32_t ps = a_short ? part.x : part.y;
+    if (ds.y > kBigRow) {
+        const uint32_t js = block_find(g.slots, ds.x, ds.y, l, s_best);
+        if (js == ~0u) return make_uint2(~0u, ~0u);
+        ps = ds.x + js;
+    }
     const uint32_t jl = block_find(g.slots, dl.x, dl.y, s, s_best);
-    const uint32_t ps = ds.x + js, pl = jl == ~0u ? ~0u : dl.x + jl;
+    const uint32_t pl = jl == ~0u ? ~0u : dl.x + jl;
     return a_short ? make_uint2(ps, pl) : make_uint2(pl, ps);
 }
 
-// One block per edge on the big list.
+// One block per edge on the big list: the long-row searches k_st_probe left.
 __global__ void k_st_probe_big(const unsigned long long *halt, DevGraph G, DevGraph H,
                                const uint4 *big, const unsigned long long *nbig, uint4 *pos) {
     __shared__ uint32_t s_best;
@@ -143,9 +180,18 @@ __global__ void k_st_probe_big(const unsigned long long *halt, DevGraph G, DevGr
     const uint32_t nbl = (uint32_t)*nbig;
     for (uint32_t q = blockIdx.x; q < nbl; q += gridDim.x) {
         const uint4 e = big[q];
-        const uint2 pg = block_edge(G, e.y, e.z, &s_best);
-        const uint2 ph = block_edge(H, e.y, e.z, &s_best);
-        if (threadIdx.x == 0) pos[e.x] = make_uint4(pg.x, pg.y, ph.x, ph.y);
+        uint4 p = pos[e.x];
+        if (e.w & 1u) {
+            const uint2 pg = block_edge(G, e.y, e.z, make_uint2(p.x, p.y), &s_best);
+            p.x = pg.x;
+            p.y = pg.y;
+        }
+        if (e.w & 2u) {
+            const uint2 ph = block_edge(H, e.y, e.z, make_uint2(p.z, p.w), &s_best);
+            p.z = ph.x;
+            p.w = ph.y;
+        }
+        if (threadIdx.x == 0) pos[e.x] = p;   // each edge is on the list once
     }
 }
 
@@ -426,7 +472,7 @@ dyg_status insert_prep_enqueue(dyg_graph *G, dyg_graph *H, const uint32_t *src,
         ptr<uint4>(ws.big), sc + S_NBIG, big_ok, sc + S_ERR);
     count_launch();
     if (big_ok) {
-        k_st_probe_big<<<num_sms() * 2, kBigThreads, 0, st>>>(halt, G->g, H->g, ptr<uint4>(ws.big),
+        k_st_probe_big<<<num_sms() * 4, kBigThreads, 0, st>>>(halt, G->g, H->g, ptr<uint4>(ws.big),
                                                               sc + S_NBIG, ptr<uint4>(ws.st_pos));
         count_launch();
     }

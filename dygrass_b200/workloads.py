@@ -180,31 +180,46 @@ def rmat_case(scale: int, seed: int, n_ins: int, edge_factor: int = 16) -> Graph
     return GraphCase(n, s, d, w, s[idx], d[idx], w[idx], u.astype(np.uint32), v.astype(np.uint32), iw)
 
 
-def serving_mix(k: int = 64, seed: int = MASTER_SEED, large: bool = False):
+def serving_mix(k: int = 64, seed: int = MASTER_SEED, large: bool = False, threads: int = 0):
     """k resident graphs drawn in turn from the three generators: 3-D meshes
     (k^3, k in [12, 48]), R-MAT (scale 10..16) and random geometric graphs
     (n log-uniform in [1e3, 2e5]); each with an insertion pool of 0.5 n edges
     (at most 20,000).  large: meshes 60^3..100^3 and R-MAT scales 17..20 (about
-    10 GB of footprint for 64 graphs).  Returns (cases, insertion params,
-    deletion params): threshold 100, 512 walkers, max_steps 100."""
+    8.3 GB of footprint for 64 graphs, 10.8 GB for 80).  The sizes are drawn
+    in order from one generator seeded with seed, and each graph from its own
+    seeds, so the graphs are built by `threads` workers (0: one per core; the
+    native generators release the GIL) with the same result as one by one.
+    Returns (cases, insertion params, deletion params): threshold 100, 512
+    walkers, max_steps 100."""
+    import os
+    from concurrent.futures import ThreadPoolExecutor
     rng = np.random.default_rng(seed)
     m_lo, m_hi, sc_lo, sc_hi = (60, 101, 17, 21) if large else (12, 49, 10, 17)
-    cases = []
+    specs = []
     for i in range(k):
         kind = i % 3
         if kind == 0:
-            m = int(rng.integers(m_lo, m_hi))
-            wl = mesh_3d(m, inserts=min(20_000, max(1, m ** 3 // 2)), seed=seed + 31 * i)
-            cases.append(GraphCase(wl.n, wl.g_src, wl.g_dst, wl.g_w, wl.h_src, wl.h_dst, wl.h_w,
-                                   wl.ins_src, wl.ins_dst, wl.ins_w))
+            specs.append((0, int(rng.integers(m_lo, m_hi)), seed + 31 * i))
         elif kind == 1:
-            sc = int(rng.integers(sc_lo, sc_hi))
-            cases.append(rmat_case(sc, seed + 31 * i, n_ins=min(20_000, (1 << sc) // 2)))
+            specs.append((1, int(rng.integers(sc_lo, sc_hi)), seed + 31 * i))
         else:
-            n0 = int(np.exp(rng.uniform(np.log(1e3), np.log(2e5))))
-            n, s, d, w, is_, id_, iw = rgg(n0, 8.0, n0 // 2, seed + 31 * i)
-            idx = sparsifier(n, s, d, w, 0.10, seed + 31 * i + 1)
-            cases.append(GraphCase(n, s, d, w, s[idx], d[idx], w[idx], is_, id_, iw))
+            specs.append((2, int(np.exp(rng.uniform(np.log(1e3), np.log(2e5)))), seed + 31 * i))
+
+    def build(spec):
+        kind, size, sd = spec
+        if kind == 0:
+            wl = mesh_3d(size, inserts=min(20_000, max(1, size ** 3 // 2)), seed=sd)
+            return GraphCase(wl.n, wl.g_src, wl.g_dst, wl.g_w, wl.h_src, wl.h_dst, wl.h_w,
+                             wl.ins_src, wl.ins_dst, wl.ins_w)
+        if kind == 1:
+            return rmat_case(size, sd, n_ins=min(20_000, (1 << size) // 2))
+        n, s, d, w, is_, id_, iw = rgg(size, 8.0, size // 2, sd)
+        idx = sparsifier(n, s, d, w, 0.10, sd + 1)
+        return GraphCase(n, s, d, w, s[idx], d[idx], w[idx], is_, id_, iw)
+
+    workers = max(1, min(threads or os.cpu_count() or 1, len(specs)))
+    with ThreadPoolExecutor(workers) as ex:
+        cases = list(ex.map(build, specs))
     p = WalkParams.make(threshold=100.0, walkers=512, max_steps=100, seed=seed)
     return cases, p, WalkParams.make(walkers=512, max_steps=100, seed=seed)
 
