@@ -201,7 +201,7 @@ void free_graph(dyg_graph *G) {
     DeviceGuard dg(G->device);
     Workspace &ws = G->ws;
     Buf *bufs[] = {&ws.keys, &ws.flags, &ws.pos, &ws.f_src, &ws.f_dst, &ws.f_idx, &ws.f_uid,
-                   &ws.f_w, &ws.found, &ws.hx, &ws.hy, &ws.hw, &ws.path_v, &ws.path_w,
+                   &ws.f_w, &ws.found, &ws.hx, &ws.hy, &ws.hw, &ws.path_v, &ws.path_s,
                    &ws.path_len, &ws.cand_x, &ws.cand_y, &ws.cand_w, &ws.keep, &ws.htab_k,
                    &ws.htab_v, &ws.nop, &ws.cub_tmp, &ws.scan_status, &ws.s_src, &ws.s_dst, &ws.s_w, &ws.s_o1,
                    &ws.s_o2, &ws.s_o3, &ws.rx2, &ws.ry2, &ws.rk2, &ws.rank, &ws.lneed, &ws.dtmp,

@@ -159,7 +159,7 @@ struct Workspace {
     Buf f_w;                                  // f32 per walk-list entry (insertions)
     Buf found;                                // u8 per half-edge
     Buf hx, hy, hw;                           // half-edge lists (u32/f32)
-    Buf path_v, path_w;                       // winner paths: vertices, edge weights
+    Buf path_v, path_s;                       // winner paths: vertices, taken slots
     Buf path_len;                             // i32 per filtered edge
     Buf cand_x, cand_y, cand_w;               // recovery candidates
     Buf keep;                                 // u32 per candidate
@@ -309,7 +309,7 @@ dyg_status launch_walk_scalars(const DevGraph &g, const WalkJob &job, const dyg_
                                unsigned long long *scalars, cudaStream_t st);
 dyg_status launch_winner_paths(dyg_graph *G, const WalkJob &job, const dyg_walk_params &p,
                                const unsigned long long *keys, uint32_t n_max, uint32_t path_stride,
-                               uint32_t *path_v, float *path_w, int32_t *path_len, cudaStream_t st);
+                               uint32_t *path_v, uint32_t *path_s, int32_t *path_len, cudaStream_t st);
 // Writes its candidates at cx/cy/cw + *base_dev.
 dyg_status launch_fallback_walks(dyg_graph *G, const unsigned long long *halt,
                                  const uint32_t *f_src, const uint32_t *f_dst,

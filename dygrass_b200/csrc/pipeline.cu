@@ -219,10 +219,12 @@ struct NoPathOp {
 };
 
 // Path edges of walk-list entry f as recovery candidates at coff[f], one warp
-// per path (consecutive lanes copy consecutive path edges).
-__global__ void k_path_cands(const unsigned long long *halt, const uint32_t *pv, const float *pw,
-                             uint32_t stride, const uint32_t *clen, const uint32_t *coff,
-                             uint32_t n, uint32_t *cx, uint32_t *cy, float *cw) {
+// per path (consecutive lanes copy consecutive path edges); each edge's
+// weight is read from the G slot the replay took (G is unchanged since).
+__global__ void k_path_cands(const unsigned long long *halt, const uint32_t *pv, const uint32_t *ps,
+                             const float *wts, uint32_t stride, const uint32_t *clen,
+                             const uint32_t *coff, uint32_t n, uint32_t *cx, uint32_t *cy,
+                             float *cw) {
     if (HALTED(halt)) return;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
@@ -230,11 +232,11 @@ __global__ void k_path_cands(const unsigned long long *halt, const uint32_t *pv,
         const uint32_t L = clen[f];
         const uint32_t base = coff[f];
         const uint32_t *v = pv + (size_t)f * stride;
-        const float *w = pw + (size_t)f * stride;
+        const uint32_t *sl = ps + (size_t)f * stride;
         for (uint32_t j = lane; j < L; j += 32u) {
             cx[base + j] = v[j];
             cy[base + j] = v[j + 1];
-            cw[base + j] = w[j + 1];
+            cw[base + j] = wts[sl[j + 1]];
         }
     }
 }
@@ -611,7 +613,7 @@ dyg_status decr_walk_enqueue(dyg_graph *G, dyg_graph *H, uint32_t f0, uint32_t n
     const uint32_t hwk = p.heuristic_walkers;
     DYG_TRY(ensure(ws.keys, sizeof(unsigned long long) * n));
     DYG_TRY(ensure(ws.path_v, sizeof(uint32_t) * (size_t)n * stride));
-    DYG_TRY(ensure(ws.path_w, sizeof(float) * (size_t)n * stride));
+    DYG_TRY(ensure(ws.path_s, sizeof(uint32_t) * (size_t)n * stride));
     DYG_TRY(ensure(ws.path_len, sizeof(int32_t) * n));
     DYG_TRY(ensure(ws.nop, sizeof(uint32_t) * (size_t)n * 4));
     // path candidates at [0, C_CANDS), then the fallback candidates
@@ -643,14 +645,14 @@ dyg_status decr_walk_enqueue(dyg_graph *G, dyg_graph *H, uint32_t f0, uint32_t n
             keys = k;
         }
         DYG_TRY(launch_winner_paths(G, job, p, keys, n, stride, ptr<uint32_t>(ws.path_v),
-                                    ptr<float>(ws.path_w), ptr<int32_t>(ws.path_len), st));
+                                    ptr<uint32_t>(ws.path_s), ptr<int32_t>(ws.path_len), st));
         const DecrResultsOp rop{keys, ptr<int32_t>(ws.path_len), fidx, cnt_dev, status, cond,
                                 clen, coff, noflag, counts};
         DYG_TRY(scan_op(ws, rop, n, nullptr, halt, st));
         const NoPathOp nop_op{noflag, ptr<uint32_t>(ws.nop), counts, hwk};
         DYG_TRY(scan_op(ws, nop_op, n, nullptr, halt, st));
         k_path_cands<<<grid_for((uint64_t)n * 32u), 256, 0, st>>>(
-            halt, ptr<uint32_t>(ws.path_v), ptr<float>(ws.path_w), stride, clen, coff, n,
+            halt, ptr<uint32_t>(ws.path_v), ptr<uint32_t>(ws.path_s), G->g.wts, stride, clen, coff, n,
             ptr<uint32_t>(ws.cand_x), ptr<uint32_t>(ws.cand_y), ptr<float>(ws.cand_w));
         count_launch();
         DYG_CUDA(cudaGetLastError());

@@ -584,7 +584,7 @@ __global__ void __launch_bounds__(kWalkThreads, WEIGHTED ? 3 : 6) k_walk(WalkArg
 template <bool WEIGHTED>
 __global__ void k_winner_paths(DevGraph g, WalkJob job, uint32_t max_steps, uint2 key,
                                const unsigned long long *keys, uint32_t stride, uint32_t *pv,
-                               float *pw, int32_t *plen, unsigned long long *scalars) {
+                               uint32_t *ps, int32_t *plen, unsigned long long *scalars) {
     if (job.halt && *job.halt) return;
     const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t n = job.n_dev ? *job.n_dev : job.n_host;
@@ -608,9 +608,8 @@ __global__ void k_winner_paths(DevGraph g, WalkJob job, uint32_t max_steps, uint
     s.R = 0.f;
     s.prev = 0u;
     uint32_t *row_v = pv + (size_t)f * stride;
-    float *row_w = pw + (size_t)f * stride;
+    uint32_t *row_s = ps + (size_t)f * stride;
     row_v[0] = s.cur;
-    row_w[0] = 0.f;
     int r;
     do {
         const uint32_t at = s.step;
@@ -619,9 +618,9 @@ __global__ void k_winner_paths(DevGraph g, WalkJob job, uint32_t max_steps, uint
         uint32_t taken_at;
         r = step_once<false, WEIGHTED>(s, g.desc, g.slots, g.wts, max_steps, 0.f, key, &moved,
                                        &taken, &taken_at);
-        if (moved && at < stride) {
+        if (moved && at < stride) {   // no load: a store waiting on one would stall the chain
             row_v[at] = taken.x;
-            row_w[at] = g.wts[taken_at];
+            row_s[at] = taken_at;
         }
     } while (r == kContinue);
     const int32_t found = (r == kFound) ? (int32_t)s.step : -1;
@@ -636,7 +635,7 @@ __global__ void k_winner_paths(DevGraph g, WalkJob job, uint32_t max_steps, uint
 constexpr int kReplayThreads = 128;
 __global__ void __launch_bounds__(kReplayThreads)
 k_winner_paths_weighted(DevGraph g, WalkJob job, uint32_t max_steps, uint2 key,
-                        const unsigned long long *keys, uint32_t stride, uint32_t *pv, float *pw,
+                        const unsigned long long *keys, uint32_t stride, uint32_t *pv, uint32_t *ps,
                         int32_t *plen, unsigned long long *scalars) {
     __shared__ unsigned long long s_seg[(kReplayThreads / 32) * kSegs];
     if (job.halt && *job.halt) return;
@@ -663,11 +662,8 @@ k_winner_paths_weighted(DevGraph g, WalkJob job, uint32_t max_steps, uint2 key,
     s.R = 0.f;
     s.prev = 0u;
     uint32_t *row_v = pv + (size_t)f * stride;
-    float *row_w = pw + (size_t)f * stride;
-    if (lane == 0u) {
-        row_v[0] = s.cur;
-        row_w[0] = 0.f;
-    }
+    uint32_t *row_s = ps + (size_t)f * stride;
+    if (lane == 0u) row_v[0] = s.cur;
     unsigned long long *seg = s_seg + (threadIdx.x >> 5) * kSegs;
     int r;
     do {
@@ -680,7 +676,7 @@ k_winner_paths_weighted(DevGraph g, WalkJob job, uint32_t max_steps, uint2 key,
         r = __shfl_sync(kFull, r, 0);
         if (lane == 0u && moved && at < stride) {
             row_v[at] = taken.x;
-            row_w[at] = g.wts[taken_at];
+            row_s[at] = taken_at;
         }
     } while (r == kContinue);
     if (lane == 0u) {
@@ -866,7 +862,7 @@ dyg_status launch_walk_scalars(const DevGraph &g, const WalkJob &job, const dyg_
 
 dyg_status launch_winner_paths(dyg_graph *G, const WalkJob &job, const dyg_walk_params &p,
                                const unsigned long long *keys, uint32_t n_max, uint32_t stride,
-                               uint32_t *path_v, float *path_w, int32_t *path_len, cudaStream_t st) {
+                               uint32_t *path_v, uint32_t *path_s, int32_t *path_len, cudaStream_t st) {
     if (n_max == 0) return DYG_OK;
     const uint2 key = make_uint2((uint32_t)p.seed, (uint32_t)(p.seed >> 32));
     const int threads = 128;
@@ -876,10 +872,10 @@ dyg_status launch_winner_paths(dyg_graph *G, const WalkJob &job, const dyg_walk_
     if (p.transition == DYG_TRANSITION_WEIGHTED)
         k_winner_paths_weighted<<<(unsigned)(((uint64_t)n_max * 32 + kReplayThreads - 1) / kReplayThreads),
                                   kReplayThreads, 0, st>>>(G->g, job, p.max_steps, key, keys, stride,
-                                                           path_v, path_w, path_len, sc);
+                                                           path_v, path_s, path_len, sc);
     else
         k_winner_paths<false><<<grid, threads, 0, st>>>(G->g, job, p.max_steps, key, keys, stride,
-                                                        path_v, path_w, path_len, sc);
+                                                        path_v, path_s, path_len, sc);
     count_launch();
     DYG_CUDA(cudaGetLastError());
     return DYG_OK;
