@@ -391,3 +391,71 @@ def test_weighted_long_rows(dyg, oracle, leaves, huge):
     assert np.array_equal(d.rec_src, rx) and np.array_equal(d.rec_dst, ry)
     same_graph(G, Go)
     same_graph(H, Ho)
+
+
+def medium_rows_graph(seed):
+    """A hub joined to 600 leaves (a row longer than 256 slots, which turns
+    the long-row paths on), 40 vertices with 60..199 random neighbours each
+    (rows of 33..256 slots, which such graphs edit one warp per row inside
+    the long-row launch), and a ring through every vertex but the hub.
+    H = the star, the ring and every other edge of the 40 vertices."""
+    rng = np.random.default_rng(seed)
+    n = 1001
+    edges = {(0, v) for v in range(1, 601)}
+    edges |= {(v, v + 1) for v in range(1, n - 1)} | {(1, n - 1)}
+    mids = rng.choice(np.arange(601, n), 40, replace=False)
+    mid_edges = set()
+    for m in mids:
+        for u in rng.choice(np.arange(1, n), int(rng.integers(60, 200)), replace=False):
+            if u != m:
+                mid_edges.add((int(min(m, u)), int(max(m, u))))
+    mid_edges -= edges
+    mid_list = sorted(mid_edges)
+    e = np.array(sorted(edges) + mid_list, np.uint32)
+    gw = rng.uniform(0.5, 2.0, len(e)).astype(np.float32)
+    in_h = np.zeros(len(e), bool)
+    in_h[:len(edges)] = True
+    in_h[len(edges)::2] = True
+    return n, e[:, 0].copy(), e[:, 1].copy(), gw, in_h, np.array(mid_list, np.uint32), rng
+
+
+@pytest.mark.parametrize("seed", [3, 4])
+def test_medium_rows_with_hub(dyg, oracle, seed):
+    """Deletions on graphs with a hub row: rows of 33..256 slots with many
+    deletions each, duplicates, pairs absent from G, hub edges and edges of
+    G only, in one batch and in the reference's batches; statuses,
+    recovered edges and every row of G and H equal the oracle's."""
+    n, gs, gd, gw, in_h, mid, rng = medium_rows_graph(seed)
+    hs, hd, hw = gs[in_h], gd[in_h], gw[in_h]
+    pick = mid[rng.choice(len(mid), 300, replace=False)]
+    dup = pick[rng.choice(300, 20, replace=False)]
+    absent = []
+    have = set(zip(gs.tolist(), gd.tolist()))
+    while len(absent) < 10:
+        a, b = sorted(rng.choice(np.arange(1, n), 2, replace=False).tolist())
+        if (a, b) not in have:
+            absent.append((a, b))
+    hub = np.stack([np.zeros(10, np.uint32), rng.choice(np.arange(1, 601), 10, replace=False)], 1)
+    dl = np.concatenate([pick, dup, np.array(absent, np.uint32), hub.astype(np.uint32)])
+    dl = dl[rng.permutation(len(dl))]
+    flip = rng.random(len(dl)) < 0.5
+    ds = np.where(flip, dl[:, 1], dl[:, 0]).astype(np.uint32)
+    dd = np.where(flip, dl[:, 0], dl[:, 1]).astype(np.uint32)
+    p = dyg.WalkParams.make(walkers=64, max_steps=24, heuristic_walkers=8)
+    for single in (True, False):
+        G, H = dyg.Graph.from_edges(n, gs, gd, gw), dyg.Graph.from_edges(n, hs, hd, hw)
+        Go, Ho = oracle.OGraph(n, gs, gd, gw), oracle.OGraph(n, hs, hd, hw)
+        if single:
+            rd = dyg.decremental_batch(G, H, ds, dd, p, first_update_id=5)
+            st, cd, rx, ry, rk, _ = oracle.decremental(Go, Ho, ds, dd, p, first_uid=5,
+                                                       single_batch=True)
+        else:
+            rd = dyg.decremental_stream(G, H, ds, dd, p)
+            st, cd, rx, ry, rk, _ = oracle.decremental(Go, Ho, ds, dd, p)
+        assert np.array_equal(rd.status, st)
+        assert np.array_equal(rd.conductance.view(np.uint32), cd.view(np.uint32))
+        assert np.array_equal(rd.rec_src, rx) and np.array_equal(rd.rec_dst, ry)
+        assert np.array_equal(rd.rec_kind, rk)
+        same_graph(G, Go)
+        same_graph(H, Ho)
+        assert (st == -3).sum() >= 20   # the duplicates' second copies and the absent pairs
