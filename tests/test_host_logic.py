@@ -187,3 +187,19 @@ def test_bench_split_modes():
     assert bench.resolve_split(ns(workload="rmat"), 8) == "replicas"
     assert bench.resolve_split(ns(workload="mesh", split="replicas"), 8) == "replicas"
     assert bench.resolve_split(ns(workload="rmat", shard=True), 2) == "shard"
+
+
+def test_serving_mix_threads_agree():
+    """The serving mix's graphs are built by a thread pool: each graph comes
+    from its own seeds and the sizes are drawn in order first, so any number
+    of workers gives the same graphs in the same order."""
+    from dygrass_b200 import workloads as wl
+    one, p1, d1 = wl.serving_mix(k=7, seed=11, threads=1)
+    many, p2, d2 = wl.serving_mix(k=7, seed=11, threads=4)
+    assert len(one) == len(many) == 7
+    fields = ("g_src", "g_dst", "g_w", "h_src", "h_dst", "h_w", "ins_src", "ins_dst", "ins_w")
+    for a, b in zip(one, many):
+        assert a.n == b.n
+        for f in fields:
+            assert np.array_equal(getattr(a, f), getattr(b, f)), f
+    assert bytes(p1) == bytes(p2) and bytes(d1) == bytes(d2)
