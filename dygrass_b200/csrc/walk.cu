@@ -137,26 +137,56 @@ __device__ __forceinline__ int finish_move(Walker &s, uint2 sl, uint32_t at, boo
 // Weight-proportional choice in row [lo, lo + deg) by one thread: the first
 // slot, in row order, among those whose column is not `ex` (when has_ex),
 // whose inclusive prefix of fixed-point weights wq(w) exceeds
-// floor(r * total / 2^32).  ~0u when total is 0.
+// floor(r * total / 2^32).  ~0u when total is 0; *picked receives the chosen
+// slot.  The row is read kPickGroup slots at a time with the group's loads
+// issued together (the second pass reads the groups again, from L1 mostly),
+// so a row of up to kPickGroup slots costs two rounds of loads, not 2 deg.
+constexpr uint32_t kPickGroup = 4;
 __device__ __forceinline__ uint32_t lane_pick_weighted(const uint2 *__restrict__ slots,
                                                        const float *__restrict__ wts, uint32_t lo,
                                                        uint32_t deg, uint32_t ex, bool has_ex,
-                                                       uint32_t r) {
+                                                       uint32_t r, uint2 *picked) {
     unsigned long long total = 0ull;
-    for (uint32_t j = 0; j < deg; ++j) {
-        if (has_ex && __ldg(&slots[lo + j].x) == ex) continue;
-        total += wq(__ldg(wts + lo + j));
+    for (uint32_t j0 = 0; j0 < deg; j0 += kPickGroup) {
+        uint2 c[kPickGroup];
+        float w[kPickGroup];
+#pragma unroll
+        for (uint32_t u = 0; u < kPickGroup; ++u) {
+            const bool in = j0 + u < deg;
+            c[u] = in ? __ldg(slots + lo + j0 + u) : make_uint2(0u, 0u);
+            w[u] = in ? __ldg(wts + lo + j0 + u) : 0.f;
+        }
+#pragma unroll
+        for (uint32_t u = 0; u < kPickGroup; ++u)
+            if (j0 + u < deg && !(has_ex && c[u].x == ex)) total += wq(w[u]);
     }
     if (total == 0ull) return ~0u;
     const unsigned long long target = mul_hi32(r, total);
     unsigned long long acc = 0ull;
     uint32_t last = deg;
-    for (uint32_t j = 0; j < deg; ++j) {
-        if (has_ex && __ldg(&slots[lo + j].x) == ex) continue;
-        acc += wq(__ldg(wts + lo + j));
-        last = j;
-        if (acc > target) break;
+    uint2 last_sl = make_uint2(0u, 0u);
+    for (uint32_t j0 = 0; j0 < deg; j0 += kPickGroup) {
+        uint2 c[kPickGroup];
+        float w[kPickGroup];
+#pragma unroll
+        for (uint32_t u = 0; u < kPickGroup; ++u) {
+            const bool in = j0 + u < deg;
+            c[u] = in ? __ldg(slots + lo + j0 + u) : make_uint2(0u, 0u);
+            w[u] = in ? __ldg(wts + lo + j0 + u) : 0.f;
+        }
+#pragma unroll
+        for (uint32_t u = 0; u < kPickGroup; ++u) {
+            if (j0 + u >= deg || (has_ex && c[u].x == ex)) continue;
+            acc += wq(w[u]);
+            last = j0 + u;
+            last_sl = c[u];
+            if (acc > target) {
+                *picked = last_sl;
+                return lo + last;
+            }
+        }
     }
+    *picked = last_sl;
     return lo + last;
 }
 
@@ -204,9 +234,9 @@ __device__ __forceinline__ int step_once(Walker &s, const uint2 *__restrict__ de
     if (first ? (deg == 0u) : (deg <= 1u)) return kFail;
     const uint32_t r = draw_next(s, key);
     if (!WEIGHTED) return move_uniform<INCR>(s, d, r, slots, max_steps, thr, moved, taken, taken_at);
-    const uint32_t at = lane_pick_weighted(slots, wts, d.x, deg, s.prev, !first, r);
+    uint2 sl;
+    const uint32_t at = lane_pick_weighted(slots, wts, d.x, deg, s.prev, !first, r, &sl);
     if (at == ~0u) return kFail;
-    const uint2 sl = __ldg(slots + at);
     return finish_move<INCR>(s, sl, at, first, max_steps, thr, moved, taken, taken_at);
 }
 
@@ -373,7 +403,9 @@ __device__ __forceinline__ int step_weighted_warp(Walker &s, bool active, const 
         }
     }
     uint32_t at = ~0u;
-    if (pick && d.y <= kCoopRow) at = lane_pick_weighted(g.slots, g.wts, d.x, d.y, s.prev, !first, r);
+    uint2 sl = make_uint2(0u, 0u);
+    const bool own_row = pick && d.y <= kCoopRow;   // chosen by this lane, slot in hand
+    if (own_row) at = lane_pick_weighted(g.slots, g.wts, d.x, d.y, s.prev, !first, r, &sl);
     unsigned coop = __ballot_sync(kFull, pick && d.y > kCoopRow);
     while (coop) {
         const uint32_t L = __ffs(coop) - 1u;
@@ -385,7 +417,7 @@ __device__ __forceinline__ int step_weighted_warp(Walker &s, bool active, const 
         if (lane == L) at = j;
     }
     if (!pick || at == ~0u) return kFail;
-    const uint2 sl = __ldg(g.slots + at);
+    if (!own_row) sl = __ldg(g.slots + at);
     return finish_move<INCR>(s, sl, at, first, max_steps, thr, moved, taken, taken_at);
 }
 
