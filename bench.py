@@ -74,7 +74,9 @@ BYTES_PER_MOVE = 64   # two 32-byte sectors: row descriptor + chosen slot
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default 20; 5 for --impl reference, whose step is the "
+                         "whole workload on the host cores)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--refgpu-repeats", type=int, default=10)
@@ -111,7 +113,10 @@ def parse():
                     help="run every walker to its natural end (no pruning)")
     ap.add_argument("--profile-only", action="store_true",
                     help="one short device-resident step (for profilers)")
-    return ap.parse_args()
+    args = ap.parse_args()
+    if args.steps is None:
+        args.steps = 5 if args.impl == "reference" else 20
+    return args
 
 
 def resolve_split(args, world):
