@@ -203,3 +203,18 @@ def test_serving_mix_threads_agree():
         for f in fields:
             assert np.array_equal(getattr(a, f), getattr(b, f)), f
     assert bytes(p1) == bytes(p2) and bytes(d1) == bytes(d2)
+
+
+def test_bench_default_steps(monkeypatch):
+    """20 timed steps by default (several clock samples inside the timed
+    region); 5 for the reference arm, whose step is the whole workload on
+    the host cores; an explicit --steps wins."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    for argv, want in ((["bench.py"], 20), (["bench.py", "--impl", "reference"], 5),
+                       (["bench.py", "--steps", "7"], 7),
+                       (["bench.py", "--impl", "reference", "--steps", "2"], 2)):
+        monkeypatch.setattr(sys, "argv", argv)
+        assert bench.parse().steps == want
